@@ -1,0 +1,232 @@
+"""gyunity_b200: the reference renderer's PathTracing integrator on B200.
+
+Host-side mirror of the reference interfaces this component replaces
+(xiaoyxue/Gyunity, paths inside Gyunity/src), over the C ABI in
+include/gyt.h:
+
+=========================  ==============================================
+this module                reference
+=========================  ==============================================
+``Film``                   visual/Film.h (pixel buffer, SetImage)
+``PinHoleCamera``          camera/PinholeCamera.h (GenerateRay set-up)
+``Scene``                  visual/Scene.h + accelerator/BVHAccel.h
+``GpuPathTracing.Render``  Integrator::Render (integrator/Integrator.h:20)
+                           = TiledIntegrator::Render + PathTracing::Li
+``Renderer.Render``        visual/Renderer.h:22-26
+=========================  ==============================================
+
+Errors raise ``GytError`` (the reference logs and exits, common/Core.h:160-166).
+The CUDA library is required: there is no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import scenes
+from ._capi import GytError, load
+from . import _capi as _c
+from .scenes import Camera, RenderParams, SceneDesc
+
+__all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "Renderer", "GytError", "SceneDesc",
+           "Camera", "RenderParams", "scenes", "default_context"]
+
+
+class Context:
+    """A CUDA device with its stream and path pools (gyt_context)."""
+
+    def __init__(self, device=0, capacity=None):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        rc = self._lib.gyt_context_create(int(device), ctypes.byref(h))
+        if rc != 0:
+            raise GytError(rc, "gyt_context_create(device=%d) failed" % device)
+        self.handle = h
+        self.device = device
+        if capacity is not None:
+            self.check(self._lib.gyt_context_set_capacity(self.handle, int(capacity)))
+
+    def check(self, rc):
+        if rc != 0:
+            raise GytError(rc, self._lib.gyt_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.gyt_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_profile(self, mode):
+        """0 off, 1 per-kernel event timing, 2 timing + traversal counters."""
+        self.check(self._lib.gyt_context_set_profile(self.handle, int(mode)))
+
+    def read_profile(self):
+        p = _c.GytProfile()
+        self.check(self._lib.gyt_profile_read(self.handle, ctypes.byref(p)))
+        names = ["generate", "extend", "shade", "connect"]
+        return {"ms": dict(zip(names, list(p.ms))), "launches": dict(zip(names, list(p.launches))),
+                "closest_rays": p.closest_rays, "shadow_rays": p.shadow_rays, "node_visits": p.node_visits,
+                "tri_tests": p.tri_tests}
+
+    def render_device(self, scene, camera, params, d_film_ptr):
+        """gyt_render_device into a caller-owned device film (res_x*res_y*4 doubles)."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_render_device(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                               ctypes.c_void_p(d_film_ptr), ctypes.byref(st)))
+        return {"paths": st.paths, "path_slots": st.path_slots, "iterations": st.iterations,
+                "launches": st.launches, "ms": st.ms}
+
+    # ---- parity / debug entry points --------------------------------------
+    def sobol(self, dims, indices):
+        """sobol::sample (sampler/Sobol.h:46-61) for (dimension, index) pairs."""
+        d = np.ascontiguousarray(dims, np.uint32)
+        i = np.ascontiguousarray(indices, np.uint64)
+        out = np.empty(d.shape[0], np.float32)
+        self.check(self._lib.gyt_sobol(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
+        return out
+
+    def sobol_enum_index(self, res_x, res_y, s, x, y):
+        """SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for (s, x, y)."""
+        sxy = np.ascontiguousarray(np.stack([np.asarray(s), np.asarray(x), np.asarray(y)], 1), np.uint32)
+        out = np.empty(sxy.shape[0], np.uint64)
+        self.check(self._lib.gyt_sobol_enum_index(self.handle, res_x, res_y, sxy.shape[0], _c.ptr(sxy),
+                                                  _c.ptr(out)))
+        return out
+
+
+_default = None
+
+
+def default_context():
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+class Scene:
+    """Scene + acceleration structure on the device (gyt_scene)."""
+
+    def __init__(self, desc: SceneDesc, ctx: Context = None):
+        self.ctx = ctx or default_context()
+        self.desc = desc
+        s, keep = _c.scene_struct(desc)
+        h = ctypes.c_void_p()
+        self.ctx.check(self.ctx._lib.gyt_scene_create(self.ctx.handle, ctypes.byref(s), ctypes.byref(h)))
+        self.handle = h
+
+    def info(self):
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self.ctx._lib.gyt_scene_info(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"triangles": a.value, "bvh_nodes": b.value, "device_bytes": c.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx._lib.gyt_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def intersect(self, rays, any_hit=False):
+        """BVHAccel::Intersect for rays (n, 7) = origin, direction, tmax.
+        Returns prim ids (-1 miss; 1/0 for any_hit) and t, b1, b2."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 7)
+        n = r.shape[0]
+        prim = np.empty(n, np.int32)
+        t, b1, b2 = (np.empty(n, np.float32) for _ in range(3))
+        self.ctx.check(self.ctx._lib.gyt_intersect(self.ctx.handle, self.handle, n, _c.ptr(r), 1 if any_hit else 0,
+                                                   _c.ptr(prim), _c.ptr(t), _c.ptr(b1), _c.ptr(b2)))
+        return (prim.astype(bool),) if any_hit else (prim, t, b1, b2)
+
+    def trace_paths(self, xys, camera=None, params=None):
+        """PathTracing::Li of explicit samples (n, 3) = x, y, s. Returns
+        radiance (n, 3), Sobol' dimensions used, and roulette-draw masks."""
+        cam = _c.camera_struct(camera or self.desc.camera)
+        prm = _c.params_struct(params or self.desc.params)
+        xys = np.ascontiguousarray(xys, np.uint32).reshape(-1, 3)
+        n = xys.shape[0]
+        L = np.empty((n, 3), np.float32)
+        cur = np.empty(n, np.uint32)
+        rr = np.empty(n, np.uint64)
+        self.ctx.check(self.ctx._lib.gyt_trace_paths(self.ctx.handle, self.handle, ctypes.byref(cam),
+                                                     ctypes.byref(prm), n, _c.ptr(xys), _c.ptr(L), _c.ptr(cur),
+                                                     _c.ptr(rr)))
+        return L, cur, rr
+
+
+class Film:
+    """Film(w, h): the pixel buffer the integrator writes (visual/Film.h)."""
+
+    def __init__(self, res_x, res_y):
+        self.mResX, self.mResY = int(res_x), int(res_y)
+        self.mAspectRatio = float(np.float32(res_x) / np.float32(res_y))
+        self.image = np.zeros((self.mResY, self.mResX, 3), np.float32)
+
+    def SetImage(self, image):
+        """Film::SetImage (visual/Film.h:106-117): colour with weight 1."""
+        self.image = np.asarray(image, np.float32).reshape(self.mResY, self.mResX, 3)
+
+    def GetImage(self):
+        return self.image
+
+
+class PinHoleCamera:
+    """PinHoleCamera(film, position, lookAt, up, fovy, filmDistance)
+    (camera/PinholeCamera.h:16-19)."""
+
+    def __init__(self, film, position, look_at, up, fovy, film_distance):
+        self.film = film
+        self.cam = Camera(tuple(position), tuple(look_at), tuple(up), float(fovy), float(film_distance),
+                          film.mResX, film.mResY)
+
+    def GetFilm(self):
+        return self.film
+
+    def raster_to_world(self):
+        out = np.empty(16, np.float64)
+        c = _c.camera_struct(self.cam)
+        rc = load().gyt_camera_raster_to_world(ctypes.byref(c), _c.ptr(out))
+        if rc:
+            raise GytError(rc, "raster_to_world")
+        return out.reshape(4, 4)
+
+
+class GpuPathTracing:
+    """Drop-in for PathTracing(spp, maxDepth, SobolSampler, SobolEnum)
+    (integrator/PT.h:12). ``rr_depth``: roulette applies at bounce i > rr_depth
+    (the reference hard-codes 5, integrator/PT.cpp:53)."""
+
+    def __init__(self, spp, max_depth, rr_depth=5, ctx: Context = None):
+        self.params = RenderParams(int(spp), int(max_depth), int(rr_depth))
+        self.ctx = ctx
+
+    def Render(self, scene: Scene, camera: PinHoleCamera):
+        ctx = scene.ctx
+        cam = _c.camera_struct(camera.cam)
+        prm = _c.params_struct(self.params)
+        film = camera.GetFilm()
+        rgb = np.empty((film.mResY, film.mResX, 3), np.float32)
+        ctx.check(ctx._lib.gyt_render(ctx.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm), _c.ptr(rgb)))
+        film.SetImage(rgb)
+        return film
+
+
+class Renderer:
+    """Renderer(scene, camera, integrator, film).Render() (visual/Renderer.h:22-26)."""
+
+    def __init__(self, scene, camera, integrator, film=None):
+        self.scene, self.camera, self.integrator = scene, camera, integrator
+        self.film = film or camera.GetFilm()
+
+    def Render(self):
+        return self.integrator.Render(self.scene, self.camera)

@@ -1,0 +1,140 @@
+"""ctypes binding of the native C ABI (include/gyt.h) in libgyunity_b200.so.
+
+There is no fallback: if the library is missing or was built for another
+ABI, loading raises ``GytError`` with the reason.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgyunity_b200.so")
+
+GYT_OK = 0
+STATUS = {0: "GYT_OK", 1: "GYT_ERR_INVALID", 2: "GYT_ERR_CUDA", 3: "GYT_ERR_OUT_OF_MEMORY",
+          4: "GYT_ERR_UNSUPPORTED", 5: "GYT_ERR_WATCHDOG"}
+
+# Every entry point include/gyt.h declares (checked by the CPU tests).
+EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_context_set_capacity",
+           "gyt_context_set_profile", "gyt_profile_read",
+           "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info", "gyt_render", "gyt_render_device",
+           "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world"]
+
+
+class GytError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+class GytSceneDesc(ctypes.Structure):
+    _fields_ = [("n_vertices", ctypes.c_uint32), ("n_triangles", ctypes.c_uint32), ("n_spheres", ctypes.c_uint32),
+                ("n_materials", ctypes.c_uint32), ("n_emission", ctypes.c_uint32),
+                ("vertices", ctypes.c_void_p), ("normals", ctypes.c_void_p), ("indices", ctypes.c_void_p),
+                ("tri_material", ctypes.c_void_p), ("tri_emission", ctypes.c_void_p), ("spheres", ctypes.c_void_p),
+                ("sphere_material", ctypes.c_void_p), ("mat_type", ctypes.c_void_p), ("mat_params", ctypes.c_void_p),
+                ("emission", ctypes.c_void_p), ("env_w", ctypes.c_uint32), ("env_h", ctypes.c_uint32),
+                ("env", ctypes.c_void_p), ("env_scale", ctypes.c_float)]
+
+
+class GytCamera(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_float * 3), ("look_at", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("fovy", ctypes.c_float), ("film_distance", ctypes.c_float), ("res_x", ctypes.c_uint32),
+                ("res_y", ctypes.c_uint32)]
+
+
+class GytRenderParams(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class GytRenderStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_uint64), ("path_slots", ctypes.c_uint64), ("iterations", ctypes.c_uint32),
+                ("launches", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
+class GytProfile(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_float * 4), ("launches", ctypes.c_uint32 * 4), ("closest_rays", ctypes.c_uint64),
+                ("shadow_rays", ctypes.c_uint64), ("node_visits", ctypes.c_uint64), ("tri_tests", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def load():
+    """Load the native library (raises GytError when it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GytError(-1, "native library %s is missing; run gyunity_b200.build.build()" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    P, U32, U64, I32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
+    L.gyt_context_create.argtypes = [I32, ctypes.POINTER(P)]
+    L.gyt_context_destroy.argtypes = [P]
+    L.gyt_context_destroy.restype = None
+    L.gyt_last_error.argtypes = [P]
+    L.gyt_last_error.restype = ctypes.c_char_p
+    L.gyt_context_set_capacity.argtypes = [P, U32]
+    L.gyt_context_set_profile.argtypes = [P, I32]
+    L.gyt_profile_read.argtypes = [P, ctypes.POINTER(GytProfile)]
+    L.gyt_scene_create.argtypes = [P, ctypes.POINTER(GytSceneDesc), ctypes.POINTER(P)]
+    L.gyt_scene_destroy.argtypes = [P]
+    L.gyt_scene_destroy.restype = None
+    L.gyt_scene_info.argtypes = [P, P, P, P]
+    L.gyt_render.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P]
+    L.gyt_render_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P,
+                                    ctypes.POINTER(GytRenderStats)]
+    L.gyt_trace_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P, P, P]
+    L.gyt_intersect.argtypes = [P, P, U64, P, I32, P, P, P, P]
+    L.gyt_sobol.argtypes = [P, U64, P, P, P]
+    L.gyt_sobol_enum_index.argtypes = [P, U32, U32, U64, P, P]
+    L.gyt_camera_raster_to_world.argtypes = [ctypes.POINTER(GytCamera), P]
+    for name in EXPORTS:
+        f = getattr(L, name)
+        if f.restype is ctypes.c_int:  # default
+            f.restype = I32
+    _lib = L
+    return L
+
+
+def ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def camera_struct(cam):
+    c = GytCamera()
+    c.pos[:] = [float(v) for v in cam.pos]
+    c.look_at[:] = [float(v) for v in cam.look_at]
+    c.up[:] = [float(v) for v in cam.up]
+    c.fovy = cam.fovy
+    c.film_distance = cam.film_distance
+    c.res_x = cam.res_x
+    c.res_y = cam.res_y
+    return c
+
+
+def params_struct(p):
+    return GytRenderParams(p.spp, p.max_depth, p.rr_depth, 0)
+
+
+def scene_struct(sd):
+    """Build a GytSceneDesc pointing into contiguous copies of the arrays;
+    returns (struct, keep-alive list)."""
+    def c(a, dt):
+        return None if a is None else np.ascontiguousarray(a, dt)
+    keep = [c(sd.vertices, np.float32), c(sd.normals, np.float32), c(sd.indices, np.uint32),
+            c(sd.tri_material, np.uint32), c(sd.tri_emission, np.int32), c(sd.spheres, np.float32),
+            c(sd.sphere_material, np.uint32), c(sd.mat_type, np.uint32), c(sd.mat_params, np.float32),
+            c(sd.emission, np.float32), c(sd.env, np.float32)]
+    s = GytSceneDesc()
+    s.n_vertices, s.n_triangles = sd.vertices.shape[0], sd.n_triangles
+    s.n_spheres, s.n_materials, s.n_emission = sd.n_spheres, sd.mat_type.shape[0], sd.emission.shape[0]
+    (s.vertices, s.normals, s.indices, s.tri_material, s.tri_emission, s.spheres, s.sphere_material, s.mat_type,
+     s.mat_params, s.emission) = [None if a is None else a.ctypes.data for a in keep[:10]]
+    if sd.env is not None:
+        s.env_h, s.env_w = sd.env.shape[:2]
+        s.env = keep[10].ctypes.data
+    s.env_scale = sd.env_scale
+    return s, keep

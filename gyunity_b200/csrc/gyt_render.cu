@@ -1,0 +1,1208 @@
+// Wavefront path tracer for B200 (sm_100a) behind the C ABI of include/gyt.h.
+//
+// One render = a loop of wavefront iterations over a pool of paths in flight:
+//   k_generate  new camera paths into free pool slots (Sobol' pixel sample,
+//               pinhole ray)                       TiledIntegrator.cpp:40-45
+//   k_extend    closest hit of every continuation ray (binary BVH, watertight
+//               triangles, analytic spheres)       BVHAccel.cpp:401-445
+//   k_shade     surface interaction, emission, light sample + BSDF sample of
+//               the MIS next-event estimate, continuation BSDF sample,
+//               Russian roulette                   PT.cpp:16-65, Integrator.cpp:9-107
+//   k_connect   shadow (any-hit) and MIS (closest-hit) rays, radiance update,
+//               film accumulation of finished paths (FP64 atomics), and
+//               compaction of live paths into the other pool (warp-aggregated
+//               atomics, ballot/popc)              Visibility.cpp:7-10, Film.h:61-87
+// Path state is SoA in HBM; pools are ping-ponged each iteration so live
+// paths stay dense and new paths fill the tail.
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gyt.h"
+#include "../_gen/sobol_tables.h"
+#include "gyt_bvh_host.h"
+#include "gyt_device.cuh"
+
+namespace cg = cooperative_groups;
+using namespace gyt;
+
+// ----------------------------------------------------------- structures ---
+namespace {
+
+struct DevScene {
+  const float4* nodes;        // binary BVH, 4 float4 per node
+  const float4* tris;         // leaf-ordered triangles: (p0, id), (p1, -), (p2, -)
+  const float* V;             // vertices (original order)
+  const float* N;             // per-vertex normals or null
+  const uint32_t* I;          // indices
+  const int2* info;           // per triangle: material, light index (-1 none)
+  const float4* spheres;
+  const uint32_t* sphere_mat;
+  const float* mparams;
+  const uint32_t* mtypes;
+  const float4* lights;       // per light: emission rgb, triangle id as int bits (-1 env)
+  const float* lcdf;          // n_lights + 1
+  const float* lfunc;         // n_lights
+  float lfunc_int;
+  int n_lights, n_tris, n_spheres;
+};
+
+struct PathBuf {
+  float4* o;      // origin
+  float4* d;      // direction
+  float4* tp;     // throughput
+  float4* L;      // radiance so far
+  unsigned long long* sidx;  // Sobol' index of the sample
+  uint32_t* meta; // depth 0-7 | delta 8 | cursor 9-19 | alive 31
+  uint32_t* pix;  // pixel index 0-27 | spill x 30 | spill y 31
+  uint32_t* pid;  // path id within the render (debug outputs)
+  unsigned long long* rr;    // bounces that drew a roulette number
+};
+
+struct Queues {
+  float4* so;  // shadow ray origin, tmax
+  float4* sd;  // shadow ray direction
+  float4* sc;  // shadow contribution, valid flag
+  float4* mo;  // MIS ray origin
+  float4* md;  // MIS ray direction, light index bits
+  float4* mc;  // MIS contribution, valid flag
+  float4* hit; // closest hit of the continuation ray: t, b1, b2, prim bits
+};
+
+struct Params {
+  uint32_t spp, max_depth, rr_depth;
+};
+
+struct DebugOut {
+  float* L;
+  uint32_t* cursor;
+  unsigned long long* rr;
+};
+
+constexpr uint32_t kAlive = 1u << 31;
+constexpr uint32_t kPixMask = 0x0fffffffu;
+constexpr int kStack = 64;
+constexpr int kBlock = 256;
+
+GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive) {
+  return (depth & 255u) | (delta ? 256u : 0u) | ((cursor & 2047u) << 9) | (alive ? kAlive : 0u);
+}
+
+// ------------------------------------------------------------ traversal ---
+// Closest hit (ANY = false) or occlusion (ANY = true) over the BVH and the
+// spheres. Returns the primitive id (triangles first, then spheres), or -1.
+// tmax is updated to the hit distance; spheres report the distance along the
+// re-made object ray of Sphere::Intersect (shape/Sphere.h:35).
+struct TraceCount {
+  uint32_t nodes = 0, tris = 0;
+};
+
+template <bool ANY, bool COUNT = false>
+GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, float& b2, TraceCount* cnt = nullptr) {
+  int prim = -1;
+  if (s.n_tris > 0) {
+    WtRay wr = wt_setup(o, d);
+    const float ooeps = 8.271806125530277e-25f;  // 2^-80
+    float ix = 1.f / (fabsf(d.x) > ooeps ? d.x : copysignf(ooeps, d.x));
+    float iy = 1.f / (fabsf(d.y) > ooeps ? d.y : copysignf(ooeps, d.y));
+    float iz = 1.f / (fabsf(d.z) > ooeps ? d.z : copysignf(ooeps, d.z));
+    float ox = o.x * ix, oy = o.y * iy, oz = o.z * iz;
+    int stack[kStack];
+    int sp = 0;
+    int node = 0;
+    for (;;) {
+      if (node >= 0) {
+        if (COUNT) cnt->nodes++;
+        const float4* n = s.nodes + 4 * node;
+        float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
+        int4 n3 = __ldg((const int4*)(n + 3));
+        float a0 = fmaf(n0.x, ix, -ox), a1 = fmaf(n0.y, ix, -ox);
+        float a2 = fmaf(n0.z, iy, -oy), a3 = fmaf(n0.w, iy, -oy);
+        float a4 = fmaf(n2.x, iz, -oz), a5 = fmaf(n2.y, iz, -oz);
+        float c0 = fmaf(n1.x, ix, -ox), c1 = fmaf(n1.y, ix, -ox);
+        float c2 = fmaf(n1.z, iy, -oy), c3 = fmaf(n1.w, iy, -oy);
+        float c4 = fmaf(n2.z, iz, -oz), c5 = fmaf(n2.w, iz, -oz);
+        float lo0 = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), 0.f));
+        float hi0 = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), tmax));
+        float lo1 = fmaxf(fmaxf(fminf(c0, c1), fminf(c2, c3)), fmaxf(fminf(c4, c5), 0.f));
+        float hi1 = fminf(fminf(fmaxf(c0, c1), fmaxf(c2, c3)), fminf(fmaxf(c4, c5), tmax));
+        bool h0 = lo0 <= hi0, h1 = lo1 <= hi1;
+        if (!h0 && !h1) {
+          if (sp == 0) break;
+          node = stack[--sp];
+          continue;
+        }
+        if (h0 && h1) {
+          int nearc = n3.x, farc = n3.y;
+          if (lo1 < lo0) { nearc = n3.y; farc = n3.x; }
+          stack[sp++] = farc;
+          node = nearc;
+        } else {
+          node = h0 ? n3.x : n3.y;
+        }
+      } else {
+        uint32_t code = ~(uint32_t)node;
+        uint32_t first = code >> 3, count = (code & 7u) + 1u;
+        const float4* t = s.tris + 3 * first;
+        if (COUNT) cnt->tris += count;
+        for (uint32_t k = 0; k < count; ++k, t += 3) {
+          float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
+          float th, u, v;
+          if (wt_intersect(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
+            prim = __float_as_int(t0.w);
+            if (ANY) return prim;
+            tmax = th;
+            b1 = u;
+            b2 = v;
+          }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+      }
+    }
+  }
+  for (int k = 0; k < s.n_spheres; ++k) {
+    float4 sp4 = __ldg(s.spheres + k);
+    Ray r = sphere_object_ray(o, d, tmax, 0.f);
+    float th;
+    if (sphere_root(sp4, r, &th)) {
+      prim = s.n_tris + k;
+      if (ANY) return prim;
+      tmax = th;
+    }
+  }
+  return prim;
+}
+
+GYT_D void load_tri(const DevScene& s, int t, float3* p0, float3* p1, float3* p2, float3* n0, float3* n1, float3* n2,
+                    float3* face) {
+  uint32_t i0 = __ldg(s.I + 3 * t), i1 = __ldg(s.I + 3 * t + 1), i2 = __ldg(s.I + 3 * t + 2);
+  *p0 = mk(__ldg(s.V + 3 * i0), __ldg(s.V + 3 * i0 + 1), __ldg(s.V + 3 * i0 + 2));
+  *p1 = mk(__ldg(s.V + 3 * i1), __ldg(s.V + 3 * i1 + 1), __ldg(s.V + 3 * i1 + 2));
+  *p2 = mk(__ldg(s.V + 3 * i2), __ldg(s.V + 3 * i2 + 1), __ldg(s.V + 3 * i2 + 2));
+  *face = norm(cross(*p1 - *p0, *p2 - *p0));  // Triangle ctor (shape/Triangle.h:52)
+  if (s.N) {
+    *n0 = mk(__ldg(s.N + 3 * i0), __ldg(s.N + 3 * i0 + 1), __ldg(s.N + 3 * i0 + 2));
+    *n1 = mk(__ldg(s.N + 3 * i1), __ldg(s.N + 3 * i1 + 1), __ldg(s.N + 3 * i1 + 2));
+    *n2 = mk(__ldg(s.N + 3 * i2), __ldg(s.N + 3 * i2 + 1), __ldg(s.N + 3 * i2 + 2));
+  } else {
+    *n0 = *n1 = *n2 = *face;
+  }
+}
+
+// Distribution1D::SampleDiscrete over light powers (visual/Sampling.h:86-97,
+// visual/Scene.h:97-109): upper_bound on the CDF.
+GYT_D int sample_light(const DevScene& s, float u, float* pdf) {
+  int lo = 0, hi = s.n_lights + 1;  // first index with cdf > u in [0, n+1)
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(s.lcdf + mid) > u) hi = mid; else lo = mid + 1;
+  }
+  int off = max(0, lo - 1);
+  off = min(off, s.n_lights - 1);
+  *pdf = __ldg(s.lfunc + off) / (s.lfunc_int * (float)s.n_lights);
+  return off;
+}
+
+// Shape::Pdf for a triangle light (shape/Shape.h:34-47): re-intersect the
+// light from the shading point along wi.
+GYT_D float tri_light_pdf(const DevScene& s, int t, const Hit& h, float3 o, float3 wi) {
+  float3 p0, p1, p2, n0, n1, n2, face;
+  load_tri(s, t, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+  WtRay wr = wt_setup(o, wi);
+  float th, b1, b2;
+  if (!wt_intersect(wr, p0, p1, p2, __int_as_float(0x7f800000), &th, &b1, &b2)) return 0.f;
+  Hit lp;
+  tri_hit(p0, p1, p2, n0, n1, n2, face, b1, b2, o, wi, &lp);
+  float3 dd = lp.pos - h.pos;
+  float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+  float pdf = dot(dd, dd) / (fabsf(dot(lp.n, -wi)) * area);
+  if (isinf(pdf)) return 0.f;
+  return pdf;
+}
+
+// -------------------------------------------------------------- kernels ---
+__global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base, uint32_t n_new,
+                                                     unsigned long long first, Cam cam, uint32_t spp,
+                                                     const uint32_t* __restrict__ list, SobolTables tab) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_new) return;
+  unsigned long long p = first + j;
+  uint32_t x, y, s;
+  if (list) {
+    x = __ldg(list + 3 * p);
+    y = __ldg(list + 3 * p + 1);
+    s = __ldg(list + 3 * p + 2);
+  } else {
+    unsigned long long pixel = p / spp;
+    s = (uint32_t)(p - pixel * spp);
+    y = (uint32_t)(pixel / cam.res_x);
+    x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+  }
+  uint64_t idx = enum_index(tab, cam.log2_res, s, x, y);
+  Rng rng{idx, 0};
+  float su = rng.next(tab.matrices), sv = rng.next(tab.matrices);
+  // SobolEnum::SampleX/Y (SobolEnum.h:30-36), kept unfused as the reference
+  float u = __fsub_rn(__fmul_rn(cam.res_pow2, su), (float)x);
+  float v = __fsub_rn(__fmul_rn(cam.res_pow2, sv), (float)y);
+  float3 o, d;
+  camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
+  uint32_t k = base + j;
+  dst.o[k] = make_float4(o.x, o.y, o.z, 0.f);
+  dst.d[k] = make_float4(d.x, d.y, d.z, 0.f);
+  dst.tp[k] = make_float4(1.f, 1.f, 1.f, 0.f);
+  dst.L[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  dst.sidx[k] = idx;
+  dst.meta[k] = meta_pack(0, false, rng.cursor, true);
+  uint32_t pix = (y * cam.res_x + x) | ((u == 0.f && x > 0) ? (1u << 30) : 0u) | ((v == 0.f && y > 0) ? (1u << 31) : 0u);
+  dst.pix[k] = pix;
+  dst.pid[k] = (uint32_t)p;
+  dst.rr[k] = 0ull;
+}
+
+// Per-warp reduction of traversal counters into the profile (counting mode).
+GYT_D void flush_counts(const TraceCount& c, unsigned long long* g) {
+  cg::coalesced_group w = cg::coalesced_threads();
+  unsigned long long nodes = cg::reduce(w, (unsigned long long)c.nodes, cg::plus<unsigned long long>());
+  unsigned long long tris = cg::reduce(w, (unsigned long long)c.tris, cg::plus<unsigned long long>());
+  if (w.thread_rank() == 0) {
+    atomicAdd(g, nodes);
+    atomicAdd(g + 1, tris);
+  }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kBlock) k_extend(PathBuf cur, uint32_t n, DevScene s, float4* __restrict__ hits,
+                                                   unsigned long long* counters) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 o = cur.o[i], d = cur.d[i];
+  float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
+  TraceCount c;
+  int prim = trace<false, COUNT>(s, f3(o), f3(d), tmax, b1, b2, &c);
+  hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
+  if (COUNT) flush_counts(c, counters);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
+                                                  SobolTables tab) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 h4 = q.hit[i];
+  int prim = __float_as_int(h4.w);
+  uint32_t meta = cur.meta[i];
+  uint32_t depth = meta & 255u;
+  bool delta = (meta >> 8) & 1u;
+  Rng rng{cur.sidx[i], (meta >> 9) & 2047u};
+  float3 ro = f3(cur.o[i]), rd = f3(cur.d[i]);
+  float3 tp = f3(cur.tp[i]);
+  float3 L = f3(cur.L[i]);
+  unsigned long long rr = cur.rr[i];
+  bool alive = false;
+  float4 sc = zero4, mc = zero4;
+  if (prim >= 0) {
+    Hit h;
+    uint32_t mat;
+    int light = -1;
+    if (prim < s.n_tris) {
+      float3 p0, p1, p2, n0, n1, n2, face;
+      load_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+      tri_hit(p0, p1, p2, n0, n1, n2, face, h4.y, h4.z, ro, rd, &h);
+      int2 inf = __ldg(s.info + prim);
+      mat = (uint32_t)inf.x;
+      light = inf.y;
+    } else {
+      int k = prim - s.n_tris;
+      Ray r = sphere_object_ray(ro, rd, __int_as_float(0x7f800000), 0.f);
+      sphere_hit(__ldg(s.spheres + k), r, h4.x, &h);
+      mat = __ldg(s.sphere_mat + k);
+    }
+    Bsdf bsdf;
+    bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
+    bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+    if ((depth == 0 || delta) && light >= 0) {
+      float4 le = __ldg(s.lights + light);
+      if (dot(h.n, h.wo) > 0.f) L = L + tp * f3(le);  // AreaLight::Emission (AreaLight.h:40-43)
+    } else {
+      // PT.cpp:38 arguments in GCC's right-to-left order: v.z v.y v.x u.y u.x uLight
+      float vz = rng.next(tab.matrices), vy = rng.next(tab.matrices), vx = rng.next(tab.matrices);
+      float uy = rng.next(tab.matrices), ux = rng.next(tab.matrices);
+      float ul = rng.next(tab.matrices);
+      float lsel = 0.f;
+      int li = s.n_lights > 0 ? sample_light(s, ul, &lsel) : 0;
+      if (lsel > 0.f) {
+        float4 le4 = __ldg(s.lights + li);
+        int ltri = __float_as_int(le4.w);
+        float3 Le = f3(le4);
+        if (ltri >= 0) {
+          // light sample: AreaLight::Sample_Li -> Shape::Sample -> Triangle::Sample
+          float3 p0, p1, p2, n0, n1, n2, face;
+          load_tri(s, ltri, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+          float su0 = sqrtf(ux);
+          float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
+          float3 lpos = p0 * bb0 + p1 * bb1 + p2 * bb2;
+          float3 ln = n0 * bb0 + n1 * bb1 + n2 * bb2;
+          float3 lerr = (vabs(p0 * bb0) + vabs(p1 * bb1) + vabs(p2 * bb2)) * gammaf(6);
+          float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+          float pdf = 1.f / area;
+          float3 w = h.pos - lpos;
+          if (length(w) == 0.f) {
+            pdf = 0.f;
+          } else {
+            w = norm(w);
+            pdf *= dot(h.pos - lpos, h.pos - lpos) / fabsf(dot(ln, -w));
+            if (isinf(pdf)) pdf = 0.f;
+          }
+          float3 wi = norm(lpos - h.pos);
+          float3 Li = dot(ln, -wi) > 0.f ? Le : mk(0.f, 0.f, 0.f);
+          if (pdf > 0.f && !is_zero(Li)) {
+            float spdf = bsdf.pdf(h.wo, wi);
+            float3 f = bsdf.eval(h.wo, wi);
+            float cosT = fabsf(dot(h.n, wi));
+            if (!is_zero(f)) {
+              // Intersection::SpawnTo (Intersection.h:64-72)
+              float3 org = offset_origin(h.pos, h.perr, h.abs_n, lpos - h.pos);
+              float3 tgt = offset_origin(lpos, lerr, face, org - lpos);
+              float3 dd = tgt - org;
+              float dis = length(dd);
+              dd = dd / dis;
+              float3 so = org + dd * kRayEps;
+              q.so[i] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
+              q.sd[i] = make_float4(dd.x, dd.y, dd.z, 0.f);
+              float w1 = power_heuristic(pdf, spdf);
+              float3 c = tp * (Li * f * cosT / pdf) * w1 / lsel;
+              sc = make_float4(c.x, c.y, c.z, 1.f);
+            }
+          }
+          // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
+          float3 wi2;
+          float pdf2;
+          float3 f2 = bsdf.sample(h.wo, &wi2, &pdf2, vx, vy, vz);
+          float cos2 = fabsf(dot(h.n, wi2));
+          if (pdf2 != 0.f && !is_zero(f2)) {
+            float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
+            float lpdf = tri_light_pdf(s, ltri, h, o2, wi2);
+            if (lpdf != 0.f) {
+              float w2 = power_heuristic(pdf2, lpdf);
+              q.mo[i] = make_float4(o2.x, o2.y, o2.z, 0.f);
+              q.md[i] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
+              float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
+              mc = make_float4(c.x, c.y, c.z, 1.f);
+            }
+          }
+        }
+      }
+    }
+    // continuation (PT.cpp:45-62); arguments again in right-to-left order
+    float rz = rng.next(tab.matrices), ry = rng.next(tab.matrices), rx = rng.next(tab.matrices);
+    float3 wi;
+    float pdf;
+    float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
+    if (!(is_zero(f) || pdf == 0.f)) {
+      float3 est = f * fabsf(dot(h.n, wi)) / pdf;
+      delta = bsdf.lobe.delta();
+      float qv = lum(est * tp) / lum(tp);
+      float p = qv < 1.f ? qv : 1.f;  // std::min(1, q): 1 when q is NaN
+      bool survive = true;
+      if (p < 1.f && depth > prm.rr_depth) {
+        rr |= 1ull << depth;
+        if (rng.next(tab.matrices) < p) tp = tp / p;
+        else survive = false;
+      }
+      if (survive) {
+        tp = tp * est;
+        float3 no = offset_origin(h.pos, h.perr, h.abs_n, wi) + wi * kRayEps;
+        cur.o[i] = make_float4(no.x, no.y, no.z, 0.f);
+        cur.d[i] = make_float4(wi.x, wi.y, wi.z, 0.f);
+        cur.tp[i] = make_float4(tp.x, tp.y, tp.z, 0.f);
+        depth += 1;
+        alive = depth < prm.max_depth;
+      }
+    }
+  }
+  cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
+  cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
+  cur.rr[i] = rr;
+  q.sc[i] = sc;
+  q.mc[i] = mc;
+}
+
+GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) {
+  double* p = film + 4ull * ((unsigned long long)y * w + x);
+  atomicAdd(p, (double)L.x);
+  atomicAdd(p + 1, (double)L.y);
+  atomicAdd(p + 2, (double)L.z);
+  atomicAdd(p + 3, 1.0);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, uint32_t n, DevScene s, Queues q,
+                                                    double* __restrict__ film, uint32_t res_x,
+                                                    uint32_t* __restrict__ counter, DebugOut dbg,
+                                                    unsigned long long* counters) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float3 L = f3(cur.L[i]);
+  float4 sc = q.sc[i];
+  TraceCount cnt;
+  bool shadow = sc.w != 0.f, mis = false;
+  if (shadow) {
+    float4 so = q.so[i], sd = q.sd[i];
+    float tmax = so.w, b1, b2;
+    if (trace<true, COUNT>(s, f3(so), f3(sd), tmax, b1, b2, &cnt) < 0) L = L + f3(sc);
+  }
+  float4 mc = q.mc[i];
+  if (mc.w != 0.f) {
+    mis = true;
+    float4 mo = q.mo[i], md = q.md[i];
+    int li = __float_as_int(md.w);
+    float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
+    float3 wi = f3(md);
+    int prim = trace<false, COUNT>(s, f3(mo), wi, tmax, b1, b2, &cnt);
+    if (prim >= 0 && prim < s.n_tris && __ldg(s.info + prim).y == li) {
+      float3 p0, p1, p2, n0, n1, n2, face;
+      load_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+      float b0 = 1.f - b1 - b2;
+      float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
+      if (dot(ns, -wi) > 0.f) L = L + f3(mc) * f3(__ldg(s.lights + li));
+    }
+  }
+  if (COUNT) {
+    flush_counts(cnt, counters);
+    cg::coalesced_group w = cg::coalesced_threads();
+    unsigned long long ns_ = cg::reduce(w, (unsigned long long)(shadow ? 1 : 0), cg::plus<unsigned long long>());
+    unsigned long long nm_ = cg::reduce(w, (unsigned long long)(mis ? 1 : 0), cg::plus<unsigned long long>());
+    if (w.thread_rank() == 0) {
+      atomicAdd(counters + 2, ns_);
+      atomicAdd(counters + 3, nm_);
+    }
+  }
+  uint32_t meta = cur.meta[i];
+  if (meta & kAlive) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    base = g.shfl(base, 0);
+    uint32_t j = base + g.thread_rank();
+    nxt.o[j] = cur.o[i];
+    nxt.d[j] = cur.d[i];
+    nxt.tp[j] = cur.tp[i];
+    nxt.L[j] = make_float4(L.x, L.y, L.z, 0.f);
+    nxt.sidx[j] = cur.sidx[i];
+    nxt.meta[j] = meta;
+    nxt.pix[j] = cur.pix[i];
+    nxt.pid[j] = cur.pid[i];
+    nxt.rr[j] = cur.rr[i];
+  } else {
+    uint32_t pix = cur.pix[i];
+    if (film) {
+      uint32_t p = pix & kPixMask;
+      uint32_t y = p / res_x, x = p - y * res_x;
+      film_add(film, res_x, x, y, L);
+      if (pix & (1u << 30)) film_add(film, res_x, x - 1, y, L);
+      if (pix & (1u << 31)) film_add(film, res_x, x, y - 1, L);
+      if ((pix & (1u << 30)) && (pix & (1u << 31))) film_add(film, res_x, x - 1, y - 1, L);
+    }
+    uint32_t pid = cur.pid[i];
+    if (dbg.L) {
+      dbg.L[3ull * pid] = L.x;
+      dbg.L[3ull * pid + 1] = L.y;
+      dbg.L[3ull * pid + 2] = L.z;
+    }
+    if (dbg.cursor) dbg.cursor[pid] = (meta >> 9) & 2047u;
+    if (dbg.rr) dbg.rr[pid] = cur.rr[i];
+  }
+}
+
+__global__ void k_resolve(const double* __restrict__ film, float* __restrict__ rgb, uint32_t npix) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const double* p = film + 4ull * i;
+  double w = p[3];
+  // Film::WriteToPixelBuffer: colour / weight (visual/Film.h:128-136)
+  rgb[3ull * i] = (float)(p[0] / w);
+  rgb[3ull * i + 1] = (float)(p[1] / w);
+  rgb[3ull * i + 2] = (float)(p[2] / w);
+}
+
+__global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ rays, int any, int32_t* prim,
+                            float* tout, float* b1out, float* b2out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* r = rays + 7 * i;
+  float3 o = mk(r[0], r[1], r[2]), d = mk(r[3], r[4], r[5]);
+  float tmax = r[6], b1 = 0.f, b2 = 0.f;
+  int p = any ? (trace<true>(s, o, d, tmax, b1, b2) >= 0 ? 1 : 0) : trace<false>(s, o, d, tmax, b1, b2);
+  prim[i] = p;
+  if (!any) {
+    tout[i] = p >= 0 ? tmax : 0.f;
+    b1out[i] = p >= 0 && p < s.n_tris ? b1 : 0.f;
+    b2out[i] = p >= 0 && p < s.n_tris ? b2 : 0.f;
+  }
+}
+
+__global__ void k_sobol(const uint32_t* __restrict__ mat, uint64_t n, const uint32_t* dims, const uint64_t* idx,
+                        float* out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = sobol_sample(mat, idx[i], dims[i]);
+}
+
+__global__ void k_enum(SobolTables tab, uint32_t m, uint64_t n, const uint32_t* sxy, uint64_t* out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = enum_index(tab, m, sxy[3 * i], sxy[3 * i + 1], sxy[3 * i + 2]);
+}
+
+inline uint32_t grid_for(uint64_t n) { return (uint32_t)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+// ------------------------------------------------------------- host side ---
+struct gyt_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  uint32_t capacity = 1u << 21;
+  uint32_t pool_cap = 0;
+  PathBuf pool[2] = {};
+  Queues q = {};
+  uint32_t* d_counter = nullptr;
+  uint32_t* h_counter = nullptr;
+  uint32_t* d_sobol = nullptr;
+  uint64_t* d_vdc = nullptr;
+  uint64_t* d_vdc_inv = nullptr;
+  double* d_film = nullptr;
+  size_t film_bytes = 0;
+  float* d_rgb = nullptr;
+  size_t rgb_bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void*> pool_allocs;
+  int profile = 0;
+  cudaEvent_t kev[8] = {};
+  unsigned long long* d_counters = nullptr;  // node visits, tri tests, shadow rays, MIS rays
+  GytProfile prof = {};
+};
+
+struct gyt_scene {
+  gyt_context* ctx = nullptr;
+  DevScene dev = {};
+  std::vector<void*> allocs;
+  uint64_t n_tris = 0, n_nodes = 0, bytes = 0;
+  uint32_t bvh_depth = 0;
+};
+
+namespace {
+
+int32_t fail(gyt_context* ctx, int32_t code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define GYT_CK(ctx, call)                                                                          \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA,     \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                             \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(std::vector<void*>& list, T** p, size_t count) {
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e == cudaSuccess) list.push_back(*p);
+  return e;
+}
+
+SobolTables tables(const gyt_context* c) { return SobolTables{c->d_sobol, c->d_vdc, c->d_vdc_inv}; }
+
+// ProjectiveCamera::Initialize (camera/Camera.cpp:6-59): RasterToWorld in
+// closed form, in double. Raster (x, y, z, 1) -> NDC (2x/W - 1, 1 - 2y/H, z)
+// -> camera through the inverse of Transform::Perspective
+// (math/Transform.cpp:132-150) -> world through the camera basis.
+void raster_to_world(const GytCamera& c, double m[16]) {
+  double pos[3] = {c.pos[0], c.pos[1], c.pos[2]};
+  double cz[3] = {c.look_at[0] - pos[0], c.look_at[1] - pos[1], c.look_at[2] - pos[2]};
+  double l = std::sqrt(cz[0] * cz[0] + cz[1] * cz[1] + cz[2] * cz[2]);
+  for (double& v : cz) v /= l;
+  double up[3] = {c.up[0], c.up[1], c.up[2]};
+  double cx[3] = {-(up[1] * cz[2] - up[2] * cz[1]), -(up[2] * cz[0] - up[0] * cz[2]), -(up[0] * cz[1] - up[1] * cz[0])};
+  l = std::sqrt(cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2]);
+  for (double& v : cx) v /= l;
+  double cy[3] = {-(cz[1] * cx[2] - cz[2] * cx[1]), -(cz[2] * cx[0] - cz[0] * cx[2]), -(cz[0] * cx[1] - cz[1] * cx[0])};
+  double aspect = (double)((float)c.res_x / (float)c.res_y);
+  double dis = c.film_distance, n = dis, f = 100000.0;
+  double t = dis * std::tan(c.fovy * (3.14159265358979 / 180.0) * 0.5);
+  double r = t * aspect;
+  double a = dis / r, b = dis / t, A = (f + n) / (f - n), B = -2.0 * f * n / (f - n);
+  double r2c[4][4] = {{2.0 / (a * c.res_x), 0, 0, -1.0 / a},
+                      {0, -2.0 / (b * c.res_y), 0, 1.0 / b},
+                      {0, 0, 0, 1.0},
+                      {0, 0, 1.0 / B, -A / B}};
+  double c2w[4][4] = {{cx[0], cy[0], cz[0], pos[0]}, {cx[1], cy[1], cz[1], pos[1]}, {cx[2], cy[2], cz[2], pos[2]},
+                      {0, 0, 0, 1}};
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += c2w[i][k] * r2c[k][j];
+      m[4 * i + j] = s;
+    }
+}
+
+int32_t make_cam(gyt_context* ctx, const GytCamera* c, Cam* out) {
+  if (!c || c->res_x == 0 || c->res_y == 0) return fail(ctx, GYT_ERR_INVALID, "camera: empty film");
+  if ((uint64_t)c->res_x * c->res_y > kPixMask) return fail(ctx, GYT_ERR_UNSUPPORTED, "camera: film too large");
+  double m[16];
+  raster_to_world(*c, m);
+  for (int i = 0; i < 16; ++i) out->m[i] = (float)m[i];
+  out->pos = mk(c->pos[0], c->pos[1], c->pos[2]);
+  out->res_x = c->res_x;
+  out->res_y = c->res_y;
+  uint32_t r = std::max(c->res_x, c->res_y), p = 1, lg = 0;
+  while (p < r) { p <<= 1; ++lg; }
+  if (lg > GYT_ENUM_M) return fail(ctx, GYT_ERR_UNSUPPORTED, "camera: resolution beyond the Sobol' enumeration tables");
+  out->log2_res = lg;
+  out->res_pow2 = (float)p;
+  return GYT_OK;
+}
+
+int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
+  if (!p) return fail(ctx, GYT_ERR_INVALID, "params: null");
+  if (p->spp == 0) return fail(ctx, GYT_ERR_INVALID, "params: spp must be > 0");
+  if (p->max_depth == 0 || p->max_depth > 100)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "params: max_depth must be in [1, 100] (Sobol' has 1024 dimensions)");
+  if (p->rr_depth > 255) return fail(ctx, GYT_ERR_INVALID, "params: rr_depth too large");
+  if (p->flags != 0) return fail(ctx, GYT_ERR_INVALID, "params: flags must be 0");
+  return GYT_OK;
+}
+
+int32_t ensure_pool(gyt_context* ctx) {
+  if (ctx->pool_cap == ctx->capacity) return GYT_OK;
+  for (void* p : ctx->pool_allocs) cudaFree(p);
+  ctx->pool_allocs.clear();
+  ctx->pool_cap = 0;
+  size_t n = ctx->capacity;
+  auto& L = ctx->pool_allocs;
+  for (int b = 0; b < 2; ++b) {
+    PathBuf& P = ctx->pool[b];
+    GYT_CK(ctx, dalloc(L, &P.o, n));
+    GYT_CK(ctx, dalloc(L, &P.d, n));
+    GYT_CK(ctx, dalloc(L, &P.tp, n));
+    GYT_CK(ctx, dalloc(L, &P.L, n));
+    GYT_CK(ctx, dalloc(L, &P.sidx, n));
+    GYT_CK(ctx, dalloc(L, &P.meta, n));
+    GYT_CK(ctx, dalloc(L, &P.pix, n));
+    GYT_CK(ctx, dalloc(L, &P.pid, n));
+    GYT_CK(ctx, dalloc(L, &P.rr, n));
+  }
+  Queues& q = ctx->q;
+  GYT_CK(ctx, dalloc(L, &q.so, n));
+  GYT_CK(ctx, dalloc(L, &q.sd, n));
+  GYT_CK(ctx, dalloc(L, &q.sc, n));
+  GYT_CK(ctx, dalloc(L, &q.mo, n));
+  GYT_CK(ctx, dalloc(L, &q.md, n));
+  GYT_CK(ctx, dalloc(L, &q.mc, n));
+  GYT_CK(ctx, dalloc(L, &q.hit, n));
+  ctx->pool_cap = ctx->capacity;
+  return GYT_OK;
+}
+
+// The wavefront loop shared by full renders and explicit path lists.
+int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, const GytRenderParams* p,
+                  unsigned long long total, const uint32_t* d_list, double* d_film, DebugOut dbg,
+                  GytRenderStats* stats) {
+  int32_t st = ensure_pool(ctx);
+  if (st) return st;
+  Params prm{p->spp, p->max_depth, p->rr_depth};
+  SobolTables tab = tables(ctx);
+  cudaStream_t s = ctx->stream;
+  unsigned long long generated = 0;
+  uint32_t active = 0, iters = 0;
+  unsigned long long rays = 0;
+  int cur = 0;
+  const bool prof = ctx->profile > 0, cnt = ctx->profile > 1;
+  uint32_t launches = 0;
+  unsigned long long slots = 0;
+  if (cnt) GYT_CK(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), s));
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
+  while (generated < total || active > 0) {
+    uint32_t n_new = (uint32_t)std::min<unsigned long long>(ctx->capacity - active, total - generated);
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[0], s));
+    if (n_new) {
+      k_generate<<<grid_for(n_new), kBlock, 0, s>>>(ctx->pool[cur], active, n_new, generated, cam, p->spp, d_list, tab);
+      ++launches;
+    }
+    generated += n_new;
+    active += n_new;
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[1], s));
+    if (cnt) k_extend<true><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, ctx->d_counters);
+    else k_extend<false><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, nullptr);
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[2], s));
+    k_shade<<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, prm, ctx->q, tab);
+    GYT_CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(uint32_t), s));
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[3], s));
+    if (cnt)
+      k_connect<true><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], ctx->pool[cur ^ 1], active, scene->dev,
+                                                          ctx->q, d_film, cam.res_x, ctx->d_counter, dbg, ctx->d_counters);
+    else
+      k_connect<false><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], ctx->pool[cur ^ 1], active, scene->dev,
+                                                           ctx->q, d_film, cam.res_x, ctx->d_counter, dbg, nullptr);
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[4], s));
+    launches += 3;
+    GYT_CK(ctx, cudaGetLastError());
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, ctx->d_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaStreamSynchronize(s));
+    if (prof) {
+      for (int k = 0; k < 4; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->kev[k], ctx->kev[k + 1]);
+        ctx->prof.ms[k] += ms;
+      }
+      if (n_new) ctx->prof.launches[0]++;
+      ctx->prof.launches[1]++;
+      ctx->prof.launches[2]++;
+      ctx->prof.launches[3]++;
+      ctx->prof.closest_rays += active;
+    }
+    slots += active;
+    rays += active;
+    active = *ctx->h_counter;
+    cur ^= 1;
+    if (++iters > 100000) return fail(ctx, GYT_ERR_WATCHDOG, "render: wavefront iteration cap reached");
+  }
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
+  GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
+  if (cnt) {
+    unsigned long long c[4];
+    GYT_CK(ctx, cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    ctx->prof.node_visits += c[0];
+    ctx->prof.tri_tests += c[1];
+    ctx->prof.shadow_rays += c[2];
+    ctx->prof.closest_rays += c[3];
+  }
+  if (stats) {
+    stats->paths = total;
+    stats->path_slots = slots;
+    stats->iterations = iters;
+    stats->launches = launches;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->ms = ms;
+  }
+  return GYT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t gyt_context_create(int32_t device, gyt_context** out) {
+  if (!out) return GYT_ERR_INVALID;
+  *out = nullptr;
+  auto* c = new gyt_context();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counter, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_counter, sizeof(uint32_t));
+  const size_t sob = GYT_SOBOL_DIMS * GYT_SOBOL_COLS;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_sobol, (sob + 64) * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(c->d_sobol, 0, (sob + 64) * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_sobol, gyt_sobol_matrices, sob * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc, sizeof(gyt_vdc_sobol));
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_vdc, gyt_vdc_sobol, sizeof(gyt_vdc_sobol), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc_inv, sizeof(gyt_vdc_sobol_inv));
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_vdc_inv, gyt_vdc_sobol_inv, sizeof(gyt_vdc_sobol_inv), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreate(&c->kev[k]);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counters, 4 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    gyt_context_destroy(c);
+    return e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA;
+  }
+  *out = c;
+  return GYT_OK;
+}
+
+void gyt_context_destroy(gyt_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : c->pool_allocs) cudaFree(p);
+  cudaFree(c->d_counter);
+  cudaFreeHost(c->h_counter);
+  cudaFree(c->d_sobol);
+  cudaFree(c->d_vdc);
+  cudaFree(c->d_vdc_inv);
+  cudaFree(c->d_film);
+  cudaFree(c->d_rgb);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  for (int k = 0; k < 8; ++k)
+    if (c->kev[k]) cudaEventDestroy(c->kev[k]);
+  cudaFree(c->d_counters);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* gyt_last_error(const gyt_context* c) { return c ? c->err.c_str() : "null context"; }
+
+int32_t gyt_context_set_capacity(gyt_context* c, uint32_t n) {
+  if (!c) return GYT_ERR_INVALID;
+  if (n < 1024 || n > (1u << 26)) return fail(c, GYT_ERR_INVALID, "capacity must be in [1024, 2^26]");
+  c->capacity = n;
+  return GYT_OK;
+}
+
+int32_t gyt_context_set_profile(gyt_context* c, int32_t mode) {
+  if (!c) return GYT_ERR_INVALID;
+  if (mode < 0 || mode > 2) return fail(c, GYT_ERR_INVALID, "profile mode must be 0, 1 or 2");
+  c->profile = mode;
+  return GYT_OK;
+}
+
+int32_t gyt_profile_read(gyt_context* c, GytProfile* out) {
+  if (!c || !out) return GYT_ERR_INVALID;
+  *out = c->prof;
+  c->prof = GytProfile{};
+  return GYT_OK;
+}
+
+int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** out) {
+  if (!ctx || !d || !out) return fail(ctx, GYT_ERR_INVALID, "scene_create: null argument");
+  *out = nullptr;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, GYT_ERR_CUDA, "scene_create: cudaSetDevice");
+  if (d->n_triangles && (!d->vertices || !d->indices || !d->tri_material || !d->tri_emission))
+    return fail(ctx, GYT_ERR_INVALID, "scene_create: triangle arrays missing");
+  if (d->n_spheres && (!d->spheres || !d->sphere_material))
+    return fail(ctx, GYT_ERR_INVALID, "scene_create: sphere arrays missing");
+  if (d->n_materials == 0 || !d->mat_type || !d->mat_params)
+    return fail(ctx, GYT_ERR_INVALID, "scene_create: no materials");
+  if (d->env && d->env_w && d->env_h)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: environment lights are not supported by this build yet");
+  if ((uint64_t)d->n_triangles >= (1ull << 28)) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many triangles");
+  for (uint32_t m = 0; m < d->n_materials; ++m)
+    if (d->mat_type[m] > 4) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
+  std::vector<int2> info(d->n_triangles);
+  std::vector<float4> lights;
+  std::vector<float> power;
+  for (uint32_t t = 0; t < d->n_triangles; ++t) {
+    for (int k = 0; k < 3; ++k)
+      if (d->indices[3 * t + k] >= d->n_vertices) return fail(ctx, GYT_ERR_INVALID, "scene_create: index out of range");
+    if (d->tri_material[t] >= d->n_materials) return fail(ctx, GYT_ERR_INVALID, "scene_create: material out of range");
+    int e = d->tri_emission[t];
+    info[t].x = (int)d->tri_material[t];
+    info[t].y = -1;
+    if (e >= 0) {
+      if ((uint32_t)e >= d->n_emission || !d->emission) return fail(ctx, GYT_ERR_INVALID, "scene_create: emission out of range");
+      info[t].y = (int)lights.size();
+      const float* em = &d->emission[3 * e];
+      int tid = (int)t;
+      float w;
+      std::memcpy(&w, &tid, 4);
+      lights.push_back(make_float4(em[0], em[1], em[2], w));
+      const float* V = d->vertices;
+      const uint32_t* I = &d->indices[3 * t];
+      float3 p0 = mk(V[3 * I[0]], V[3 * I[0] + 1], V[3 * I[0] + 2]);
+      float3 p1 = mk(V[3 * I[1]], V[3 * I[1] + 1], V[3 * I[1] + 2]);
+      float3 p2 = mk(V[3 * I[2]], V[3 * I[2] + 1], V[3 * I[2] + 2]);
+      float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+      // AreaLight::Power (light/AreaLight.h:45-48)
+      power.push_back(lum(mk(em[0], em[1], em[2]) * area * kPi));
+    }
+  }
+  for (uint32_t k = 0; k < d->n_spheres; ++k)
+    if (d->sphere_material[k] >= d->n_materials) return fail(ctx, GYT_ERR_INVALID, "scene_create: sphere material out of range");
+  // Distribution1D over light power (visual/Sampling.h:18-45), in float
+  int nl = (int)power.size();
+  std::vector<float> cdf(nl + 1, 0.f);
+  float fint = 0.f;
+  if (nl) {
+    for (int i = 1; i < nl + 1; ++i) cdf[i] = cdf[i - 1] + power[i - 1] / nl;
+    fint = cdf[nl];
+    if (fint == 0.f) {
+      for (int i = 1; i < nl + 1; ++i) cdf[i] = (float)i / (float)nl;
+    } else {
+      for (int i = 1; i < nl + 1; ++i) cdf[i] /= fint;
+    }
+  }
+  BvhHost bvh;
+  if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bvh))
+    return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
+  if (bvh.max_depth >= (uint32_t)kStack) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+  std::vector<float4> tris((size_t)bvh.order.size() * 3);
+  for (size_t k = 0; k < bvh.order.size(); ++k) {
+    uint32_t t = bvh.order[k];
+    const uint32_t* I = &d->indices[3 * t];
+    int tid = (int)t;
+    float w;
+    std::memcpy(&w, &tid, 4);
+    for (int c = 0; c < 3; ++c) {
+      const float* v = &d->vertices[3 * I[c]];
+      tris[3 * k + c] = make_float4(v[0], v[1], v[2], c == 0 ? w : 0.f);
+    }
+  }
+  auto* sc = new gyt_scene();
+  sc->ctx = ctx;
+  auto up = [&](auto** dst, const auto* src, size_t count) -> cudaError_t {
+    using T = std::remove_const_t<std::remove_reference_t<decltype(*src)>>;
+    cudaError_t e = dalloc(sc->allocs, (T**)dst, count);
+    if (e == cudaSuccess && count && src) e = cudaMemcpy((void*)*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    sc->bytes += count * sizeof(T);
+    return e;
+  };
+  DevScene& ds = sc->dev;
+  cudaError_t e = cudaSuccess;
+  float4* nodes = nullptr;
+  if (e == cudaSuccess) e = up(&nodes, (const float4*)bvh.nodes.data(), bvh.nodes.size() / 4);
+  ds.nodes = nodes;
+  float4* dtris = nullptr;
+  if (e == cudaSuccess) e = up(&dtris, tris.data(), tris.size());
+  ds.tris = dtris;
+  float* V = nullptr;
+  if (e == cudaSuccess) e = up(&V, d->vertices, (size_t)d->n_vertices * 3);
+  ds.V = V;
+  float* N = nullptr;
+  if (e == cudaSuccess && d->normals) e = up(&N, d->normals, (size_t)d->n_vertices * 3);
+  ds.N = N;
+  uint32_t* I = nullptr;
+  if (e == cudaSuccess) e = up(&I, d->indices, (size_t)d->n_triangles * 3);
+  ds.I = I;
+  int2* inf = nullptr;
+  if (e == cudaSuccess) e = up(&inf, info.data(), info.size());
+  ds.info = inf;
+  std::vector<float4> sph(d->n_spheres);
+  for (uint32_t k = 0; k < d->n_spheres; ++k)
+    sph[k] = make_float4(d->spheres[4 * k], d->spheres[4 * k + 1], d->spheres[4 * k + 2], d->spheres[4 * k + 3]);
+  float4* dsph = nullptr;
+  if (e == cudaSuccess) e = up(&dsph, sph.data(), sph.size());
+  ds.spheres = dsph;
+  uint32_t* smat = nullptr;
+  if (e == cudaSuccess) e = up(&smat, d->sphere_material, d->n_spheres);
+  ds.sphere_mat = smat;
+  float* mp = nullptr;
+  if (e == cudaSuccess) e = up(&mp, d->mat_params, (size_t)d->n_materials * 16);
+  ds.mparams = mp;
+  uint32_t* mt = nullptr;
+  if (e == cudaSuccess) e = up(&mt, d->mat_type, d->n_materials);
+  ds.mtypes = mt;
+  float4* dl = nullptr;
+  if (e == cudaSuccess) e = up(&dl, lights.data(), lights.size());
+  ds.lights = dl;
+  float* dc = nullptr;
+  if (e == cudaSuccess) e = up(&dc, cdf.data(), cdf.size());
+  ds.lcdf = dc;
+  float* df = nullptr;
+  if (e == cudaSuccess) e = up(&df, power.data(), power.size());
+  ds.lfunc = df;
+  ds.lfunc_int = fint;
+  ds.n_lights = nl;
+  ds.n_tris = (int)d->n_triangles;
+  ds.n_spheres = (int)d->n_spheres;
+  sc->n_tris = d->n_triangles;
+  sc->n_nodes = bvh.nodes.size() / 16;
+  sc->bvh_depth = bvh.max_depth;
+  if (e != cudaSuccess) {
+    gyt_scene_destroy(sc);
+    return fail(ctx, e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA,
+                std::string("scene_create: ") + cudaGetErrorString(e));
+  }
+  *out = sc;
+  return GYT_OK;
+}
+
+void gyt_scene_destroy(gyt_scene* s) {
+  if (!s) return;
+  if (s->ctx) cudaSetDevice(s->ctx->device);
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+int32_t gyt_scene_info(const gyt_scene* s, uint64_t* nt, uint64_t* nn, uint64_t* bytes) {
+  if (!s) return GYT_ERR_INVALID;
+  if (nt) *nt = s->n_tris;
+  if (nn) *nn = s->n_nodes;
+  if (bytes) *bytes = s->bytes;
+  return GYT_OK;
+}
+
+int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, double* d_film, GytRenderStats* stats) {
+  if (!ctx || !scene || !d_film) return fail(ctx, GYT_ERR_INVALID, "render_device: null argument");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "render: more than 2^32 paths in one render");
+  return run_paths(ctx, scene, cam, params, total, nullptr, d_film, DebugOut{nullptr, nullptr, nullptr}, stats);
+}
+
+int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
+                   float* rgb_out) {
+  if (!ctx || !scene || !camera || !rgb_out) return fail(ctx, GYT_ERR_INVALID, "render: null argument");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t npix = (size_t)camera->res_x * camera->res_y;
+  size_t fb = npix * 4 * sizeof(double), rb = npix * 3 * sizeof(float);
+  if (fb > ctx->film_bytes) {
+    cudaFree(ctx->d_film);
+    ctx->d_film = nullptr;
+    ctx->film_bytes = 0;
+    GYT_CK(ctx, cudaMalloc((void**)&ctx->d_film, fb));
+    ctx->film_bytes = fb;
+  }
+  if (rb > ctx->rgb_bytes) {
+    cudaFree(ctx->d_rgb);
+    ctx->d_rgb = nullptr;
+    ctx->rgb_bytes = 0;
+    GYT_CK(ctx, cudaMalloc((void**)&ctx->d_rgb, rb));
+    ctx->rgb_bytes = rb;
+  }
+  GYT_CK(ctx, cudaMemsetAsync(ctx->d_film, 0, fb, ctx->stream));
+  int32_t st = gyt_render_device(ctx, scene, camera, params, ctx->d_film, nullptr);
+  if (st) return st;
+  k_resolve<<<grid_for(npix), kBlock, 0, ctx->stream>>>(ctx->d_film, ctx->d_rgb, (uint32_t)npix);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaMemcpyAsync(rgb_out, ctx->d_rgb, rb, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                        const GytRenderParams* params, uint64_t n, const uint32_t* xys, float* L_out,
+                        uint32_t* cursor_out, uint64_t* rr_out) {
+  if (!ctx || !scene || !camera || (n && !xys)) return fail(ctx, GYT_ERR_INVALID, "trace_paths: null argument");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  if (n == 0) return GYT_OK;
+  if (n >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "trace_paths: too many paths");
+  for (uint64_t i = 0; i < n; ++i)
+    if (xys[3 * i] >= camera->res_x || xys[3 * i + 1] >= camera->res_y)
+      return fail(ctx, GYT_ERR_INVALID, "trace_paths: pixel outside the film");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* p : v) cudaFree(p); }
+  } guard{tmp};
+  uint32_t* dl = nullptr;
+  float* dL = nullptr;
+  uint32_t* dc = nullptr;
+  unsigned long long* dr = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dl, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dL, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dc, n));
+  GYT_CK(ctx, dalloc(tmp, &dr, n));
+  GYT_CK(ctx, cudaMemcpy(dl, xys, 3 * n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  st = run_paths(ctx, scene, cam, params, n, dl, nullptr, DebugOut{dL, dc, dr}, nullptr);
+  if (st) return st;
+  if (L_out) GYT_CK(ctx, cudaMemcpy(L_out, dL, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
+  if (cursor_out) GYT_CK(ctx, cudaMemcpy(cursor_out, dc, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (rr_out) GYT_CK(ctx, cudaMemcpy(rr_out, dr, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
+int32_t gyt_intersect(gyt_context* ctx, const gyt_scene* scene, uint64_t n, const float* rays, int32_t any_hit,
+                      int32_t* prim, float* t, float* b1, float* b2) {
+  if (!ctx || !scene || (n && !rays)) return fail(ctx, GYT_ERR_INVALID, "intersect: null argument");
+  if (n == 0) return GYT_OK;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* p : v) cudaFree(p); }
+  } guard{tmp};
+  float* dr = nullptr;
+  int32_t* dp = nullptr;
+  float *dt = nullptr, *d1 = nullptr, *d2 = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dr, 7 * n));
+  GYT_CK(ctx, dalloc(tmp, &dp, n));
+  GYT_CK(ctx, dalloc(tmp, &dt, n));
+  GYT_CK(ctx, dalloc(tmp, &d1, n));
+  GYT_CK(ctx, dalloc(tmp, &d2, n));
+  GYT_CK(ctx, cudaMemcpy(dr, rays, 7 * n * sizeof(float), cudaMemcpyHostToDevice));
+  k_intersect<<<grid_for(n), kBlock, 0, ctx->stream>>>(scene->dev, n, dr, any_hit ? 1 : 0, dp, dt, d1, d2);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (prim) GYT_CK(ctx, cudaMemcpy(prim, dp, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (!any_hit) {
+    if (t) GYT_CK(ctx, cudaMemcpy(t, dt, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (b1) GYT_CK(ctx, cudaMemcpy(b1, d1, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (b2) GYT_CK(ctx, cudaMemcpy(b2, d2, n * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  return GYT_OK;
+}
+
+int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out) {
+  if (!ctx || (n && (!dims || !indices || !out))) return fail(ctx, GYT_ERR_INVALID, "sobol: null argument");
+  if (n == 0) return GYT_OK;
+  for (uint64_t i = 0; i < n; ++i)
+    if (dims[i] >= GYT_SOBOL_DIMS) return fail(ctx, GYT_ERR_INVALID, "sobol: dimension >= 1024");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* p : v) cudaFree(p); }
+  } guard{tmp};
+  uint32_t* dd = nullptr;
+  uint64_t* di = nullptr;
+  float* dout = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dd, n));
+  GYT_CK(ctx, dalloc(tmp, &di, n));
+  GYT_CK(ctx, dalloc(tmp, &dout, n));
+  GYT_CK(ctx, cudaMemcpy(dd, dims, n * 4, cudaMemcpyHostToDevice));
+  GYT_CK(ctx, cudaMemcpy(di, indices, n * 8, cudaMemcpyHostToDevice));
+  k_sobol<<<grid_for(n), kBlock, 0, ctx->stream>>>(ctx->d_sobol, n, dd, di, dout);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  GYT_CK(ctx, cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
+int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n, const uint32_t* sxy,
+                             uint64_t* out) {
+  if (!ctx || (n && (!sxy || !out))) return fail(ctx, GYT_ERR_INVALID, "sobol_enum_index: null argument");
+  uint32_t r = std::max(res_x, res_y), p = 1, m = 0;
+  while (p < r) { p <<= 1; ++m; }
+  if (m > GYT_ENUM_M) return fail(ctx, GYT_ERR_UNSUPPORTED, "sobol_enum_index: resolution too large");
+  if (n == 0) return GYT_OK;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  uint32_t* ds = nullptr;
+  uint64_t* dout = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &ds, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dout, n));
+  GYT_CK(ctx, cudaMemcpy(ds, sxy, 3 * n * 4, cudaMemcpyHostToDevice));
+  k_enum<<<grid_for(n), kBlock, 0, ctx->stream>>>(tables(ctx), m, n, ds, dout);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  GYT_CK(ctx, cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
+int32_t gyt_camera_raster_to_world(const GytCamera* camera, double* out16) {
+  if (!camera || !out16) return GYT_ERR_INVALID;
+  raster_to_world(*camera, out16);
+  return GYT_OK;
+}
+
+}  // extern "C"

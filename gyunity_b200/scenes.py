@@ -1,0 +1,367 @@
+"""Seeded procedural scenes for the path tracing workloads.
+
+A ``SceneDesc`` is the flat, array-only description that crosses the C ABI
+(``GytSceneDesc`` in include/gyt.h). It follows the reference's scene model:
+
+* primitives are triangles (``shape/Triangle.h``) followed by analytic spheres
+  (``shape/Sphere.h``); the primitive id of triangle ``t`` is ``t`` and of
+  sphere ``s`` is ``n_triangles + s`` (the order ``Scene::AddPrimitive`` hands
+  out ids in, ``visual/Scene.h:49-58``);
+* every emitting triangle is its own ``AreaLight`` (``light/AreaLight.h``) and
+  the light list is the emitting triangles in triangle order, then the
+  environment light if there is one (``Scene::AddLight``, ``visual/Scene.h:60``);
+* per-vertex shading normals are interpolated as in
+  ``Triangle::QueryIntersectionInfo`` (``shape/Triangle.cpp:37-38``); without
+  them the face normal ``Cross(p1-p0, p2-p0).Norm()`` is used at every corner.
+
+Material records (type, 16 floats):
+
+====  ======================  ===========================================
+type  reference material      params used
+====  ======================  ===========================================
+0     DiffuseMaterial         [0:3] kd
+1     MirrorMaterial          [0:3] kr
+2     GlassMaterial           [0:3] kr, [3:6] kt, [15] eta1, [8] eta2
+3     GGX conductor           [0:3] R, [6] alpha_x, [7] alpha_y,
+      (RoughnessMaterial)     [9:12] eta, [12:15] k
+4     GGX rough dielectric    [0:3] kr, [3:6] kt, [6] alpha_x, [7] alpha_y,
+      (RoughDielectricMat.)   [8] eta
+====  ======================  ===========================================
+
+Alpha is stored directly; ``roughness_to_alpha`` converts a reference
+roughness value (``visual/Microfacet.h:49-54``) when a caller has one.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+MAT_DIFFUSE, MAT_MIRROR, MAT_GLASS, MAT_CONDUCTOR, MAT_DIELECTRIC = 0, 1, 2, 3, 4
+
+# fovy of the reference's Cornell-box camera (Gyunity_exe/main.cpp:712)
+CORNELL_FOVY = 53.13010235415597
+
+
+@dataclasses.dataclass
+class Camera:
+    pos: tuple = (0.0, 0.0, 3.0)
+    look_at: tuple = (0.0, 0.0, 0.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    fovy: float = CORNELL_FOVY
+    film_distance: float = 1.0
+    res_x: int = 256
+    res_y: int = 256
+
+
+@dataclasses.dataclass
+class RenderParams:
+    spp: int = 16
+    max_depth: int = 8
+    rr_depth: int = 5   # Russian roulette applies when bounce index i > rr_depth (reference: 5)
+
+
+@dataclasses.dataclass
+class SceneDesc:
+    vertices: np.ndarray                 # (nv, 3) float32
+    indices: np.ndarray                  # (nt, 3) uint32
+    tri_material: np.ndarray             # (nt,) uint32
+    tri_emission: np.ndarray             # (nt,) int32, -1 = not a light
+    mat_type: np.ndarray                 # (nm,) uint32
+    mat_params: np.ndarray               # (nm, 16) float32
+    emission: np.ndarray                 # (ne, 3) float32
+    normals: Optional[np.ndarray] = None  # (nv, 3) float32
+    spheres: Optional[np.ndarray] = None  # (ns, 4) float32: cx, cy, cz, r
+    sphere_material: Optional[np.ndarray] = None  # (ns,) uint32
+    env: Optional[np.ndarray] = None     # (h, w, 3) float32, row 0 = top (theta = 0)
+    env_scale: float = 1.0
+    camera: Camera = dataclasses.field(default_factory=Camera)
+    params: RenderParams = dataclasses.field(default_factory=RenderParams)
+    name: str = ""
+
+    @property
+    def n_triangles(self) -> int:
+        return int(self.indices.shape[0])
+
+    @property
+    def n_spheres(self) -> int:
+        return 0 if self.spheres is None else int(self.spheres.shape[0])
+
+    def n_paths(self) -> int:
+        return self.camera.res_x * self.camera.res_y * self.params.spp
+
+
+def roughness_to_alpha(roughness: float) -> float:
+    """``GGXDistribution::RoughnessToAlpha`` (visual/Microfacet.h:49-54) in float32."""
+    r = np.float32(max(roughness, 1e-3))
+    x = np.float32(math.log(r))
+    return float(np.float32(1.62142) + np.float32(0.819955) * x + np.float32(0.1734) * x * x
+                 + np.float32(0.0171201) * x * x * x + np.float32(0.000640711) * x * x * x * x)
+
+
+def _mat(kind, a=(0, 0, 0), b=(0, 0, 0), ax=0.0, ay=0.0, eta=1.5, ceta=(1.5, 1.5, 1.5), k=(1.5, 1.5, 1.5), eta1=1.0):
+    p = np.zeros(16, np.float32)
+    p[0:3] = a
+    p[3:6] = b
+    p[6] = ax
+    p[7] = ay
+    p[8] = eta
+    p[9:12] = ceta
+    p[12:15] = k
+    p[15] = eta1
+    return kind, p
+
+
+class _Builder:
+    def __init__(self):
+        self.v, self.n, self.i, self.tm, self.te = [], [], [], [], []
+        self.mt, self.mp, self.em = [], [], []
+        self.nv = 0
+
+    def material(self, kind, p) -> int:
+        self.mt.append(kind)
+        self.mp.append(p)
+        return len(self.mt) - 1
+
+    def quad(self, p0, p1, p2, p3, normal, mat, emission=None):
+        """Two triangles (p0,p1,p2) and (p2,p3,p0) as the reference fixture
+        (Gyunity_exe/CornellBox.h:437-440) with a constant shading normal."""
+        base = self.nv
+        self.v.append(np.array([p0, p1, p2, p3], np.float32))
+        self.n.append(np.array([normal] * 4, np.float32))
+        self.nv += 4
+        self.i.append(np.array([[base, base + 1, base + 2], [base + 2, base + 3, base]], np.uint32))
+        self.tm += [mat, mat]
+        if emission is None:
+            self.te += [-1, -1]
+        else:
+            e = len(self.em)
+            self.em.append(emission)
+            self.em.append(emission)
+            self.te += [e, e + 1]
+
+    def tris(self, verts, normals, idx, mats):
+        self.v.append(verts.astype(np.float32))
+        self.n.append(normals.astype(np.float32))
+        self.i.append(idx.astype(np.uint32) + np.uint32(self.nv))
+        self.nv += verts.shape[0]
+        self.tm += list(np.asarray(mats, np.uint32))
+        self.te += [-1] * idx.shape[0]
+
+    def build(self, **kw) -> SceneDesc:
+        return SceneDesc(
+            vertices=np.ascontiguousarray(np.concatenate(self.v).astype(np.float32)),
+            normals=np.ascontiguousarray(np.concatenate(self.n).astype(np.float32)),
+            indices=np.ascontiguousarray(np.concatenate(self.i).astype(np.uint32)),
+            tri_material=np.asarray(self.tm, np.uint32),
+            tri_emission=np.asarray(self.te, np.int32),
+            mat_type=np.asarray(self.mt, np.uint32),
+            mat_params=np.ascontiguousarray(np.stack(self.mp).astype(np.float32)),
+            emission=np.asarray(self.em, np.float32).reshape(-1, 3),
+            **kw)
+
+
+def _cornell_walls(b: _Builder, light_radiance=(12.0, 12.0, 12.0), light_half=0.25):
+    """The +-1 Cornell box of CornellBoxMesh (Gyunity_exe/CornellBox.h:402-591):
+    left red, right blue, back/floor/ceiling grey 0.75, and a ceiling light quad
+    at y = 0.965 facing -y. Returns nothing; appends 12 triangles."""
+    grey = b.material(*_mat(MAT_DIFFUSE, (0.75, 0.75, 0.75)))
+    red = b.material(*_mat(MAT_DIFFUSE, (0.75, 0.25, 0.25)))
+    blue = b.material(*_mat(MAT_DIFFUSE, (0.25, 0.25, 0.75)))
+    black = b.material(*_mat(MAT_DIFFUSE, (0.0, 0.0, 0.0)))
+    p = [(-1, -1, 1), (-1, -1, -1), (-1, 1, -1), (-1, 1, 1), (1, -1, 1), (1, -1, -1), (1, 1, -1), (1, 1, 1)]
+    b.quad(p[0], p[1], p[2], p[3], (1, 0, 0), red)
+    # right wall: triangles (p4,p5,p6) and (p4,p6,p7) in the fixture
+    base = b.nv
+    b.v.append(np.array([p[4], p[5], p[6], p[7]], np.float32))
+    b.n.append(np.array([(-1, 0, 0)] * 4, np.float32))
+    b.nv += 4
+    b.i.append(np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]], np.uint32))
+    b.tm += [blue, blue]
+    b.te += [-1, -1]
+    # back (p1,p5,p6),(p1,p6,p2); floor (p0,p4,p5),(p0,p5,p1); ceiling (p3,p7,p6),(p3,p6,p2)
+    for (q0, q1, q2, q3), nrm in (((1, 5, 6, 2), (0, 0, 1)), ((0, 4, 5, 1), (0, 1, 0)), ((3, 7, 6, 2), (0, -1, 0))):
+        base = b.nv
+        b.v.append(np.array([p[q0], p[q1], p[q2], p[q3]], np.float32))
+        b.n.append(np.array([nrm] * 4, np.float32))
+        b.nv += 4
+        b.i.append(np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]], np.uint32))
+        b.tm += [grey, grey]
+        b.te += [-1, -1]
+    h = light_half
+    l0, l1, l2, l3 = (h, 0.965, h), (h, 0.965, -h), (-h, 0.965, -h), (-h, 0.965, h)
+    base = b.nv
+    b.v.append(np.array([l0, l1, l2, l3], np.float32))
+    b.n.append(np.array([(0, -1, 0)] * 4, np.float32))
+    b.nv += 4
+    b.i.append(np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]], np.uint32))
+    b.tm += [black, black]
+    e = len(b.em)
+    b.em += [light_radiance, light_radiance]
+    b.te += [e, e + 1]
+
+
+def cornell_box(res=256, spp=16, max_depth=8, rr_depth=3, spheres=True) -> SceneDesc:
+    """Cornell box, plain path tracing: 10 wall triangles, a 0.5 x 0.5 ceiling
+    light (radiance 12), a mirror and a glass (IOR 1.5) sphere of radius 0.4."""
+    b = _Builder()
+    _cornell_walls(b)
+    kw = {}
+    if spheres:
+        mirror = b.material(*_mat(MAT_MIRROR, (1, 1, 1)))
+        glass = b.material(*_mat(MAT_GLASS, (1, 1, 1), (1, 1, 1), eta=1.5, eta1=1.0))
+        kw["spheres"] = np.array([[-0.5, -0.6, -0.3, 0.4], [0.5, -0.6, 0.3, 0.4]], np.float32)
+        kw["sphere_material"] = np.array([mirror, glass], np.uint32)
+    return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
+                   name="cornell_box_%dx%d_%dspp" % (res, res, spp), **kw)
+
+
+# ---------------------------------------------------------------- meshes ----
+
+def _hash3(ix, iy, iz, seed):
+    """Integer lattice hash -> float in [-1, 1] (xorshift-multiply mix)."""
+    h = (ix.astype(np.uint64) * np.uint64(0x8DA6B343) ^ iy.astype(np.uint64) * np.uint64(0xD8163841)
+         ^ iz.astype(np.uint64) * np.uint64(0xCB1AB31F) ^ np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15))
+    h ^= h >> np.uint64(31)
+    h *= np.uint64(0xBF58476D1CE4E5B9)
+    h ^= h >> np.uint64(29)
+    h *= np.uint64(0x94D049BB133111EB)
+    h ^= h >> np.uint64(32)
+    return (h & np.uint64(0xFFFFFF)).astype(np.float64) / float(0xFFFFFF) * 2.0 - 1.0
+
+
+def value_noise(p: np.ndarray, seed: int, octaves=4, lacunarity=2.0, gain=0.5, freq=2.0) -> np.ndarray:
+    """Fractal value noise: trilinear (smoothstep) interpolation of hashed
+    lattice values, ``octaves`` octaves. Returns values roughly in [-1, 1]."""
+    total = np.zeros(p.shape[0])
+    amp, norm = 1.0, 0.0
+    with np.errstate(over="ignore"):
+        for o in range(octaves):
+            q = p * freq
+            i0 = np.floor(q).astype(np.int64)
+            f = q - i0
+            w = f * f * (3.0 - 2.0 * f)
+            acc = np.zeros(p.shape[0])
+            for dx in (0, 1):
+                for dy in (0, 1):
+                    for dz in (0, 1):
+                        v = _hash3(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed * 131 + o)
+                        wx = w[:, 0] if dx else 1 - w[:, 0]
+                        wy = w[:, 1] if dy else 1 - w[:, 1]
+                        wz = w[:, 2] if dz else 1 - w[:, 2]
+                        acc += v * wx * wy * wz
+            total += amp * acc
+            norm += amp
+            amp *= gain
+            freq *= lacunarity
+    return total / norm
+
+
+def icosphere(level: int):
+    """Unit icosphere subdivided ``level`` times: 20 * 4**level faces."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(level):
+        nv = v.shape[0]
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (nv + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b2 = uniq // (nv + 1), uniq % (nv + 1)
+        mid = v[a] + v[b2]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        v = np.concatenate([v, mid])
+        m = inv.reshape(3, -1).T + nv  # midpoints of edges (01, 12, 20)
+        f = np.concatenate([np.stack([f[:, 0], m[:, 0], m[:, 2]], 1), np.stack([f[:, 1], m[:, 1], m[:, 0]], 1),
+                            np.stack([f[:, 2], m[:, 2], m[:, 1]], 1), m])
+    return v, f
+
+
+def torus_knot(n_u: int, n_v: int, p=2, q=3, R=0.5, r_tube=0.12):
+    """(p,q) torus knot swept with a circular tube: ``2 * n_u * n_v`` faces.
+    Returns unit-free vertices, faces and the per-vertex outward tube normal."""
+    u = np.arange(n_u) / n_u * 2 * np.pi
+    def curve(t):
+        rr = R * (2 + np.cos(q * t)) / 3.0
+        return np.stack([rr * np.cos(p * t), R * np.sin(q * t) / 3.0 * 1.0, rr * np.sin(p * t)], 1)
+    c = curve(u)
+    dc = curve(u + 1e-4) - curve(u - 1e-4)
+    tng = dc / np.linalg.norm(dc, axis=1, keepdims=True)
+    ref = np.array([0.0, 1.0, 0.0])
+    nrm = np.cross(tng, ref)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    bin_ = np.cross(tng, nrm)
+    vv = np.arange(n_v) / n_v * 2 * np.pi
+    dirs = (np.cos(vv)[None, :, None] * nrm[:, None, :] + np.sin(vv)[None, :, None] * bin_[:, None, :])
+    verts = (c[:, None, :] + r_tube * dirs).reshape(-1, 3)
+    iu, iv = np.meshgrid(np.arange(n_u), np.arange(n_v), indexing="ij")
+    a = iu * n_v + iv
+    b2 = ((iu + 1) % n_u) * n_v + iv
+    c2 = ((iu + 1) % n_u) * n_v + (iv + 1) % n_v
+    d = iu * n_v + (iv + 1) % n_v
+    faces = np.concatenate([np.stack([a, b2, c2], -1).reshape(-1, 3), np.stack([a, c2, d], -1).reshape(-1, 3)])
+    return verts, faces, dirs.reshape(-1, 3)
+
+
+def vertex_normals(v: np.ndarray, f: np.ndarray) -> np.ndarray:
+    """Area-weighted smooth normals of a triangle mesh."""
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    n = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(n, f[:, k], fn)
+    return n / np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+
+
+def displaced_icosphere(level: int, radius: float, center, seed: int, amplitude=0.05):
+    v, f = icosphere(level)
+    d = value_noise(v * 1.0, seed)
+    v = v * (radius * (1.0 + amplitude * d))[:, None] + np.asarray(center, np.float64)
+    v32 = v.astype(np.float32)
+    n = vertex_normals(v32.astype(np.float64), f)
+    return v32, n.astype(np.float32), f
+
+
+def procedural_mesh_box(level=8, res=1024, spp=64, max_depth=16, rr_depth=5, seed_mesh=2, seed_alpha=3,
+                        groups=64) -> SceneDesc:
+    """Noise-displaced icosphere (20 * 4**level faces; level 8 = 1,310,720) of
+    radius 0.4 at (0, -0.55, 0) in the Cornell box (no spheres), GGX conductor
+    with eta = k = 1.5 (as Gyunity_exe/CornellBox.h:417-422) and alpha ~
+    U(0.05, 0.5) per contiguous face group."""
+    b = _Builder()
+    _cornell_walls(b)
+    v, n, f = displaced_icosphere(level, 0.4, (0.0, -0.55, 0.0), seed_mesh)
+    rng = np.random.default_rng(seed_alpha)
+    alphas = rng.uniform(0.05, 0.5, groups)
+    mats = [b.material(*_mat(MAT_CONDUCTOR, (1, 1, 1), ax=a, ay=a)) for a in alphas]
+    per = max(1, f.shape[0] // groups)
+    grp = np.minimum(np.arange(f.shape[0]) // per, groups - 1)
+    b.tris(v, n, f, np.asarray(mats, np.uint32)[grp])
+    return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
+                   name="icosphere_L%d_%dx%d_%dspp" % (level, res, res, spp))
+
+
+def mixed_materials_box(level=3, res=64, spp=4, max_depth=8, rr_depth=3, seed=11) -> SceneDesc:
+    """Small test scene touching every material kind: Cornell walls and light,
+    a displaced icosphere split into diffuse / conductor / rough-dielectric
+    thirds, and a mirror and a glass sphere."""
+    b = _Builder()
+    _cornell_walls(b)
+    v, n, f = displaced_icosphere(level, 0.35, (0.0, -0.3, 0.0), seed)
+    diff = b.material(*_mat(MAT_DIFFUSE, (0.6, 0.7, 0.5)))
+    cond = b.material(*_mat(MAT_CONDUCTOR, (0.9, 0.8, 0.7), ax=0.2, ay=0.2))
+    diel = b.material(*_mat(MAT_DIELECTRIC, (1, 1, 1), (1, 1, 1), ax=0.1, ay=0.1, eta=1.5))
+    third = f.shape[0] // 3
+    mats = np.where(np.arange(f.shape[0]) < third, diff, np.where(np.arange(f.shape[0]) < 2 * third, cond, diel))
+    b.tris(v, n, f, mats)
+    mirror = b.material(*_mat(MAT_MIRROR, (1, 1, 1)))
+    glass = b.material(*_mat(MAT_GLASS, (1, 1, 1), (1, 1, 1), eta=1.5, eta1=1.0))
+    return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
+                   spheres=np.array([[-0.55, -0.7, -0.4, 0.25], [0.55, -0.7, 0.4, 0.25]], np.float32),
+                   sphere_material=np.array([mirror, glass], np.uint32), name="mixed_materials_box")

@@ -1,0 +1,180 @@
+/*
+ * gyt.h - C ABI of the B200 path tracer that stands in for the reference
+ * renderer's PathTracing integrator (xiaoyxue/Gyunity).
+ *
+ * Plain C types only: handles, POD descriptors, pointers and sizes, int32
+ * status codes. No C++ or CUDA types cross this boundary, so the reference's
+ * C++ host (or ctypes, or any FFI) can bind it directly.
+ *
+ * Reference interfaces replaced (paths inside Gyunity/src):
+ *   Integrator::Render(const Scene&, const Camera&)   integrator/Integrator.h:20
+ *     -> gyt_render / gyt_render_device
+ *   TiledIntegrator::Render + PathTracing::Li          integrator/TiledIntegrator.cpp:7-60,
+ *                                                       integrator/PT.cpp:10-67
+ *   Scene + BVHAccel construction                      visual/Scene.h:26-77, accelerator/BVHAccel.cpp:154-200
+ *     -> gyt_scene_create / gyt_scene_destroy
+ *   PinHoleCamera / ProjectiveCamera::Initialize        camera/PinholeCamera.h:22-29, camera/Camera.cpp:6-59
+ *     -> GytCamera
+ *   Film::SetImage / Film pixel buffer                  visual/Film.h:106-117
+ *     -> rgb_out of gyt_render (colour / weight per pixel)
+ *
+ * Error behaviour: every call returns GYT_OK or a negative-free status code
+ * and never aborts the process (the reference logs and exits, common/Core.h:160-166);
+ * gyt_last_error() gives the message of the last failing call on a context.
+ *
+ * Threading: one host thread per context at a time. Calls are synchronous
+ * unless stated otherwise.
+ */
+#ifndef GYT_H
+#define GYT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gyt_context gyt_context;
+typedef struct gyt_scene gyt_scene;
+
+enum {
+  GYT_OK = 0,
+  GYT_ERR_INVALID = 1,      /* bad argument or scene description */
+  GYT_ERR_CUDA = 2,         /* CUDA runtime error (message in gyt_last_error) */
+  GYT_ERR_OUT_OF_MEMORY = 3,
+  GYT_ERR_UNSUPPORTED = 4,  /* feature or size outside what this build handles */
+  GYT_ERR_WATCHDOG = 5      /* a bounded device loop hit its iteration cap */
+};
+
+/* Material kinds. Parameters are 16 floats per material:
+ *   0 diffuse          (material/Diffuse.h:27-31)        [0:3] kd
+ *   1 mirror           (material/Mirror.h:26-32)         [0:3] kr
+ *   2 glass            (material/Glass.h:30-34)          [0:3] kr [3:6] kt [15] eta1 [8] eta2
+ *   3 GGX conductor    (material/Roughness.h:36-46)      [0:3] R [6] alpha_x [7] alpha_y [9:12] eta [12:15] k
+ *   4 GGX dielectric   (material/RoughDielectric.h:21-41) [0:3] kr [3:6] kt [6] alpha_x [7] alpha_y [8] eta
+ * Alpha is the GGX alpha (the reference maps roughness to alpha with
+ * GGXDistribution::RoughnessToAlpha, visual/Microfacet.h:49-54, before this). */
+enum { GYT_MAT_DIFFUSE = 0, GYT_MAT_MIRROR = 1, GYT_MAT_GLASS = 2, GYT_MAT_CONDUCTOR = 3, GYT_MAT_DIELECTRIC = 4 };
+
+/* Scene description (all host pointers; copied by gyt_scene_create).
+ * Primitive ids: triangle t has id t, sphere s has id n_triangles + s, the
+ * order Scene::AddPrimitive assigns (visual/Scene.h:39-58). Every triangle
+ * with tri_emission >= 0 is one AreaLight (light/AreaLight.h); the light list
+ * is those triangles in order, then the environment light if env != NULL. */
+typedef struct {
+  uint32_t n_vertices, n_triangles, n_spheres, n_materials, n_emission;
+  const float* vertices;          /* n_vertices * 3 */
+  const float* normals;           /* n_vertices * 3, or NULL for face normals */
+  const uint32_t* indices;        /* n_triangles * 3 */
+  const uint32_t* tri_material;   /* n_triangles */
+  const int32_t* tri_emission;    /* n_triangles, index into emission or -1 */
+  const float* spheres;           /* n_spheres * 4: centre xyz, radius */
+  const uint32_t* sphere_material;/* n_spheres */
+  const uint32_t* mat_type;       /* n_materials */
+  const float* mat_params;        /* n_materials * 16 */
+  const float* emission;          /* n_emission * 3 radiance */
+  uint32_t env_w, env_h;          /* lat-long environment map, 0 if none */
+  const float* env;               /* env_h * env_w * 3, row 0 = top (theta = 0) */
+  float env_scale;
+} GytSceneDesc;
+
+/* PinHoleCamera(film, position, lookAt, up, fovy, filmDistance) on a
+ * res_x x res_y film (Gyunity_exe/main.cpp:708-714). */
+typedef struct {
+  float pos[3], look_at[3], up[3];
+  float fovy, film_distance;
+  uint32_t res_x, res_y;
+} GytCamera;
+
+/* PathTracing(spp, maxDepth, SobolSampler, SobolEnum) (integrator/PT.h:12).
+ * Russian roulette is applied at bounce i when i > rr_depth (the reference
+ * hard-codes 5 at integrator/PT.cpp:53). */
+typedef struct {
+  uint32_t spp, max_depth, rr_depth;
+  uint32_t flags;                 /* reserved, must be 0 */
+} GytRenderParams;
+
+/* Per-render statistics filled by gyt_render_device. */
+typedef struct {
+  uint64_t paths;                 /* camera paths traced */
+  uint64_t path_slots;            /* path-state slots processed (sum of live paths per iteration) */
+  uint32_t iterations;            /* wavefront iterations */
+  uint32_t launches;              /* kernels launched */
+  float ms;                       /* device time of the render (CUDA events on the context stream) */
+} GytRenderStats;
+
+/* Kernel-level profile of the renders since the last gyt_profile_read.
+ * Kernel slots: 0 generate, 1 extend, 2 shade, 3 connect. */
+typedef struct {
+  float ms[4];                    /* summed device time per kernel (CUDA events) */
+  uint32_t launches[4];
+  uint64_t closest_rays;          /* continuation + MIS closest-hit rays traced */
+  uint64_t shadow_rays;           /* any-hit rays traced */
+  uint64_t node_visits;           /* BVH nodes fetched (counting mode only) */
+  uint64_t tri_tests;             /* triangle tests (counting mode only) */
+} GytProfile;
+
+/* Context on one CUDA device; owns a stream and the path-state pools. */
+int32_t gyt_context_create(int32_t device, gyt_context** out);
+void gyt_context_destroy(gyt_context* ctx);
+const char* gyt_last_error(const gyt_context* ctx);
+/* Maximum number of paths in flight (default 2M); call before rendering. */
+int32_t gyt_context_set_capacity(gyt_context* ctx, uint32_t paths_in_flight);
+/* Profiling: 0 off (default), 1 per-kernel event timing, 2 timing plus
+ * traversal counters (slower kernels; counts only, not for timing). */
+int32_t gyt_context_set_profile(gyt_context* ctx, int32_t mode);
+/* Copies the accumulated profile into *out and resets it. */
+int32_t gyt_profile_read(gyt_context* ctx, GytProfile* out);
+
+/* Uploads the scene and builds the acceleration structure on the device.
+ * Replaces Scene::Initialize + new BVHAccel(primitives) (Gyunity_exe/main.cpp:735-738). */
+int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* desc, gyt_scene** out);
+void gyt_scene_destroy(gyt_scene* scene);
+/* Triangle count, BVH node count and device bytes of a scene. */
+int32_t gyt_scene_info(const gyt_scene* scene, uint64_t* n_triangles, uint64_t* n_nodes, uint64_t* device_bytes);
+
+/* Integrator::Render: renders the full image and writes rgb_out (host,
+ * res_x*res_y*3 floats, row-major from the top-left pixel) = colour/weight
+ * per pixel, as Film::WriteToPixelBuffer (visual/Film.h:128-136) computes. */
+int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                   const GytRenderParams* params, float* rgb_out);
+
+/* Same render into a caller-owned DEVICE film of res_x*res_y*4 doubles
+ * (colour sums and filter weights, accumulated, not cleared), on the
+ * context's stream; returns when the render is complete. */
+int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, double* d_film, GytRenderStats* stats);
+
+/* Traces an explicit list of camera paths (xys: n triplets x, y, s; host)
+ * and returns per-path radiance (L_out: n*3 floats), the number of Sobol'
+ * dimensions each path used (cursor_out) and which bounces drew a Russian
+ * roulette number (rr_mask_out, bit i = bounce i). Any output may be NULL.
+ * This is PathTracing::Li for the samples TiledIntegrator::Render would make
+ * (integrator/TiledIntegrator.cpp:40-47). */
+int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                        const GytRenderParams* params, uint64_t n, const uint32_t* xys,
+                        float* L_out, uint32_t* cursor_out, uint64_t* rr_mask_out);
+
+/* Closest-hit (any_hit = 0) or occlusion (any_hit = 1) queries for n rays
+ * (host rays: 7 floats each = origin, direction, tmax; tmin = 0). Outputs
+ * (host, may be NULL): prim (-1 = miss; for any_hit 1/0), t, b1, b2 where b1
+ * and b2 weight vertices 1 and 2 as Triangle::Intersect reports them
+ * (shape/Triangle.cpp:71-103). BVHAccel::Intersect (accelerator/BVHAccel.cpp:401-487). */
+int32_t gyt_intersect(gyt_context* ctx, const gyt_scene* scene, uint64_t n, const float* rays,
+                      int32_t any_hit, int32_t* prim, float* t, float* b1, float* b2);
+
+/* sobol::sample (sampler/Sobol.h:46-61) for n (dimension, index) pairs. */
+int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out);
+
+/* SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for n (s, x, y) triplets. */
+int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
+                             const uint32_t* sxy, uint64_t* out);
+
+/* ProjectiveCamera::RasterToWorld (camera/Camera.cpp:38) as a row-major 4x4. */
+int32_t gyt_camera_raster_to_world(const GytCamera* camera, double* out16);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GYT_H */

@@ -1,0 +1,440 @@
+// Driver for the reference path tracer compiled from its own sources
+// (oracle/ref/build_ref.py). TEST INFRASTRUCTURE ONLY: it produces golden
+// vectors and the CPU baseline timing; nothing in the product links it.
+//
+// Commands (all binary I/O is little-endian, see oracle/scene_io.py):
+//   sobol   <pairs.bin> <out.bin>             (u32 dim, u64 index) -> f32 sobol::sample
+//   enum    <resx> <resy> <trip.bin> <out.bin> (u32 s,x,y) -> u64 SobolEnum::GetIndex
+//   hits    <scene> <rays.bin> <out.bin>       closest-hit through BVHAccel::Intersect
+//   anyhit  <scene> <rays.bin> <out.bin>       occlusion through BVHAccel::Intersect(ray)
+//   paths   <scene> <trip.bin> <out.bin>       PathTracing::Li for (x,y,s) triplets
+//   render  <scene> <out.bin> [rows]           TiledIntegrator::Render, timed
+//   camera  <scene> <out.bin>                  RasterToWorld matrix (row-major f32)
+//   bsdf    <cases.bin> <out.bin>              BxDF Sample/Evaluate/Pdf tables
+// Standard and shim headers first, so the access override below only reaches
+// the reference's own classes (Film's pixel buffer, Scene's counters).
+#include <algorithm>
+#include <atomic>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <list>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <thread>
+#include <vector>
+#include "fmt/fmt.h"
+#include "tbb/parallel_for.h"
+#define private public
+#define protected public
+#include "visual/Scene.h"
+#include "visual/Film.h"
+#include "camera/PinholeCamera.h"
+#include "integrator/PT.h"
+#include "accelerator/BVHAccel.h"
+#include "sampler/Sobol.h"
+#include "sampler/SobolEnum.h"
+#include "material/Diffuse.h"
+#include "material/Mirror.h"
+#include "material/Glass.h"
+#include "material/RoughDielectric.h"
+#include "texture/ConstantTexture.h"
+#include "light/AreaLight.h"
+#include "light/EnvLight.h"
+#include "shape/Sphere.h"
+#include "system/Memory.h"
+#undef private
+#undef protected
+
+#undef STB_IMAGE_WRITE_IMPLEMENTATION
+#include <stb/stb_image_write.h>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+extern int gyref_rr_start_depth;
+
+using namespace Gyunity;
+
+namespace {
+
+std::vector<char> read_file(const char* path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error(std::string("cannot open ") + path);
+  return std::vector<char>((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+}
+
+void write_file(const char* path, const void* data, size_t n) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) throw std::runtime_error(std::string("cannot write ") + path);
+  std::fwrite(data, 1, n, f);
+  std::fclose(f);
+}
+
+struct Reader {
+  const char* p;
+  const char* end;
+  template <typename T> T get() {
+    if (p + sizeof(T) > end) throw std::runtime_error("truncated input");
+    T v;
+    std::memcpy(&v, p, sizeof(T));
+    p += sizeof(T);
+    return v;
+  }
+  template <typename T> std::vector<T> arr(size_t n) {
+    if (p + n * sizeof(T) > end) throw std::runtime_error("truncated array");
+    std::vector<T> v(n);
+    if (n) std::memcpy(v.data(), p, n * sizeof(T));
+    p += n * sizeof(T);
+    return v;
+  }
+};
+
+// GGX conductor with alpha given directly: the reference RoughnessMaterial
+// (material/Roughness.h:36-46) with its RoughnessToAlpha step left out.
+class AlphaConductorMaterial : public Material {
+ public:
+  AlphaConductorMaterial(Vec3 r, real ax, real ay, Vec3 eta, Vec3 k) : r(r), ax(ax), ay(ay), eta(eta), k(k) {}
+  void ComputeScatteringFunction(Intersection* isect, MemoryPool& arena, TransportMode) const override {
+    MicrofacetDistribution* d = MEMORY_POOL_ALLOC(arena, GGXDistribution)(ax, ay, true);
+    isect->mpBSDF = MEMORY_POOL_ALLOC(arena, BSDF)(*isect);
+    Fresnel* fr = MEMORY_POOL_ALLOC(arena, FresnelConductor)(Vec3(1.0, 1.0, 1.0), eta, k);
+    isect->mpBSDF->Add(MEMORY_POOL_ALLOC(arena, MicrofacetReflectionBSDF)(d, fr, r));
+  }
+  Vec3 r; real ax, ay; Vec3 eta, k;
+};
+
+// GGX rough dielectric with alpha given directly: RoughDielectricMaterial
+// (material/RoughDielectric.h:21-41) without RoughnessToAlpha.
+class AlphaDielectricMaterial : public Material {
+ public:
+  AlphaDielectricMaterial(Vec3 kr, Vec3 kt, real ax, real ay, real eta) : kr(kr), kt(kt), ax(ax), ay(ay), eta(eta) {}
+  void ComputeScatteringFunction(Intersection* isect, MemoryPool& arena, TransportMode mode) const override {
+    isect->mpBSDF = MEMORY_POOL_ALLOC(arena, BSDF)(*isect);
+    MicrofacetDistribution* d = MEMORY_POOL_ALLOC(arena, GGXDistribution)(ax, ay, true);
+    isect->mpBSDF->Add(MEMORY_POOL_ALLOC(arena, RoughDielectricBSDF)(d, kr, kt, 1.f, eta, mode));
+  }
+  Vec3 kr, kt; real ax, ay, eta;
+};
+
+std::shared_ptr<Texture<Vec3>> ctex(float r, float g, float b) {
+  return std::make_shared<ConstantTexture<Vec3>>(Vec3(r, g, b));
+}
+
+struct LoadedScene {
+  std::shared_ptr<Scene> scene;
+  std::shared_ptr<Film> film;
+  std::shared_ptr<PinHoleCamera> camera;
+  int spp = 1, maxDepth = 1, rrDepth = 5;
+  int resX = 0, resY = 0;
+};
+
+// Scene file layout: oracle/scene_io.py (write_scene) documents every field.
+LoadedScene load_scene(const char* path) {
+  std::vector<char> buf = read_file(path);
+  Reader r{buf.data(), buf.data() + buf.size()};
+  if (r.get<uint32_t>() != 0x53545947u) throw std::runtime_error("bad scene magic");
+  uint32_t version = r.get<uint32_t>();
+  if (version != 1) throw std::runtime_error("bad scene version");
+  uint32_t nv = r.get<uint32_t>(), nt = r.get<uint32_t>(), ns = r.get<uint32_t>();
+  uint32_t nm = r.get<uint32_t>(), ne = r.get<uint32_t>(), has_normals = r.get<uint32_t>();
+  uint32_t env_w = r.get<uint32_t>(), env_h = r.get<uint32_t>();
+  LoadedScene out;
+  out.resX = (int)r.get<uint32_t>();
+  out.resY = (int)r.get<uint32_t>();
+  out.spp = (int)r.get<uint32_t>();
+  out.maxDepth = (int)r.get<uint32_t>();
+  out.rrDepth = (int)r.get<uint32_t>();
+  std::vector<float> cam = r.arr<float>(11);  // pos3 look3 up3 fovy filmdist
+  float env_scale = r.get<float>();
+  std::vector<float> V = r.arr<float>((size_t)nv * 3);
+  std::vector<float> N = has_normals ? r.arr<float>((size_t)nv * 3) : std::vector<float>();
+  std::vector<uint32_t> I = r.arr<uint32_t>((size_t)nt * 3);
+  std::vector<uint32_t> TM = r.arr<uint32_t>(nt);
+  std::vector<int32_t> TE = r.arr<int32_t>(nt);
+  std::vector<float> SP = r.arr<float>((size_t)ns * 4);
+  std::vector<uint32_t> SM = r.arr<uint32_t>(ns);
+  std::vector<uint32_t> MT = r.arr<uint32_t>(nm);
+  std::vector<float> MP = r.arr<float>((size_t)nm * 16);
+  std::vector<float> EM = r.arr<float>((size_t)ne * 3);
+  std::vector<float> ENV = r.arr<float>((size_t)env_w * env_h * 3);
+
+  std::vector<std::shared_ptr<Material>> mats;
+  for (uint32_t m = 0; m < nm; ++m) {
+    const float* p = &MP[m * 16];
+    switch (MT[m]) {
+      case 0: mats.push_back(std::make_shared<DiffuseMaterial>(ctex(p[0], p[1], p[2]))); break;
+      case 1: mats.push_back(std::make_shared<MirrorMaterial>(ctex(p[0], p[1], p[2]))); break;
+      case 2: mats.push_back(std::make_shared<GlassMaterial>(ctex(p[0], p[1], p[2]), ctex(p[3], p[4], p[5]), p[15], p[8])); break;
+      case 3: mats.push_back(std::make_shared<AlphaConductorMaterial>(Vec3(p[0], p[1], p[2]), p[6], p[7],
+                                                                      Vec3(p[9], p[10], p[11]), Vec3(p[12], p[13], p[14]))); break;
+      case 4: mats.push_back(std::make_shared<AlphaDielectricMaterial>(Vec3(p[0], p[1], p[2]), Vec3(p[3], p[4], p[5]),
+                                                                       p[6], p[7], p[8])); break;
+      default: throw std::runtime_error("unknown material type");
+    }
+  }
+  out.scene = std::make_shared<Scene>();
+  out.scene->mShapeNum = 0;
+  out.scene->mPrimitiveNum = 0;
+  for (uint32_t t = 0; t < nt; ++t) {
+    uint32_t a = I[3 * t], b = I[3 * t + 1], c = I[3 * t + 2];
+    Vec3 p0(V[3 * a], V[3 * a + 1], V[3 * a + 2]);
+    Vec3 p1(V[3 * b], V[3 * b + 1], V[3 * b + 2]);
+    Vec3 p2(V[3 * c], V[3 * c + 1], V[3 * c + 2]);
+    Vec3 n0, n1, n2;
+    if (has_normals) {
+      n0 = Vec3(N[3 * a], N[3 * a + 1], N[3 * a + 2]);
+      n1 = Vec3(N[3 * b], N[3 * b + 1], N[3 * b + 2]);
+      n2 = Vec3(N[3 * c], N[3 * c + 1], N[3 * c + 2]);
+    } else {
+      n0 = n1 = n2 = Cross(p1 - p0, p2 - p0).Norm();
+    }
+    auto shape = std::make_shared<Triangle>(Transform(), Transform(), p0, p1, p2, n0, n1, n2);
+    std::shared_ptr<Light> light;
+    if (TE[t] >= 0) {
+      const float* e = &EM[3 * TE[t]];
+      light = std::make_shared<AreaLight>(shape, Vec3(e[0], e[1], e[2]));
+      out.scene->AddLight(light);
+    }
+    out.scene->AddPrimitive(std::make_shared<Primitive>(shape, mats[TM[t]], light));
+  }
+  for (uint32_t s = 0; s < ns; ++s) {
+    auto shape = std::make_shared<Sphere>(Transform(), Transform(), SP[4 * s + 3],
+                                          Vec3(SP[4 * s], SP[4 * s + 1], SP[4 * s + 2]));
+    out.scene->AddPrimitive(std::make_shared<Primitive>(shape, mats[SM[s]]));
+  }
+  if (env_w * env_h > 0) {
+    // The reference loads environment maps from files only (light/EnvMap.h:291);
+    // the texels in the scene file are already RGBE-exact, so the round trip
+    // through an .hdr file is lossless.
+    // Rows are stored in file order (row 0 = top of the lat-long map).
+    std::string tmp = std::string(path) + ".env.hdr";
+    stbi_write_hdr(tmp.c_str(), (int)env_w, (int)env_h, 3, ENV.data());
+    out.scene->AddLight(std::make_shared<EnvironmentLight>(tmp, 0.f, env_scale));
+  }
+  out.scene->SetAccelerator(std::make_shared<BVHAccel>(out.scene->GetPrimitives()));
+  out.scene->Initialize();
+  out.film = std::make_shared<Film>(out.resX, out.resY, new BoxFilter());
+  out.camera = std::make_shared<PinHoleCamera>(out.film, Vec3(cam[0], cam[1], cam[2]), Vec3(cam[3], cam[4], cam[5]),
+                                               Vec3(cam[6], cam[7], cam[8]), cam[9], cam[10]);
+  gyref_rr_start_depth = out.rrDepth;
+  return out;
+}
+
+struct RayIn { float o[3], d[3], tmax; };
+struct HitOut { int32_t prim; float t, b1, b2; };
+
+Ray make_ray(const RayIn& in) {
+  Ray r;  // default ctor: no RayEps shift, so the origin is exactly the given one
+  r.mOrig = Vec3(in.o[0], in.o[1], in.o[2]);
+  r.mDir = Vec3(in.d[0], in.d[1], in.d[2]);
+  r.m_tMax = in.tmax;
+  r.m_tMin = 0.f;
+  return r;
+}
+
+int cmd_sobol(int argc, char** argv) {
+  std::vector<char> in = read_file(argv[2]);
+  size_t n = in.size() / 12;
+  std::vector<float> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t dim; uint64_t idx;
+    std::memcpy(&dim, &in[12 * i], 4);
+    std::memcpy(&idx, &in[12 * i + 4], 8);
+    out[i] = sobol::sample(idx, dim);
+  }
+  write_file(argv[3], out.data(), out.size() * 4);
+  return 0;
+}
+
+int cmd_enum(int argc, char** argv) {
+  SobolEnum e((uint32)std::atoi(argv[2]), (uint32)std::atoi(argv[3]));
+  std::vector<char> in = read_file(argv[4]);
+  size_t n = in.size() / 12;
+  std::vector<uint64_t> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t v[3];
+    std::memcpy(v, &in[12 * i], 12);
+    out[i] = e.GetIndex(v[0], v[1], v[2]);
+  }
+  write_file(argv[5], out.data(), out.size() * 8);
+  return 0;
+}
+
+int cmd_hits(int argc, char** argv, bool any) {
+  LoadedScene ls = load_scene(argv[2]);
+  std::vector<char> in = read_file(argv[3]);
+  size_t n = in.size() / sizeof(RayIn);
+  std::vector<HitOut> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    RayIn ri;
+    std::memcpy(&ri, &in[i * sizeof(RayIn)], sizeof(RayIn));
+    Ray r = make_ray(ri);
+    HitOut h{-1, 0.f, 0.f, 0.f};
+    if (any) {
+      h.prim = ls.scene->Intersect(r) ? 1 : 0;
+    } else {
+      Intersection isect;
+      if (ls.scene->Intersect(r, &isect)) {
+        h.prim = (int32_t)isect.mPrimId;
+        h.t = r.m_tMax;
+        h.b1 = isect.mB1;
+        h.b2 = isect.mB2;
+      }
+    }
+    out[i] = h;
+  }
+  write_file(argv[4], out.data(), out.size() * sizeof(HitOut));
+  return 0;
+}
+
+std::shared_ptr<PathTracing> make_integrator(const LoadedScene& ls, std::shared_ptr<Sampler>* sampler,
+                                             std::shared_ptr<SamplerEnum>* senum) {
+  *sampler = std::make_shared<SobolSampler>();
+  *senum = std::make_shared<SobolEnum>(ls.resX, ls.resY);
+  return std::make_shared<PathTracing>(ls.spp, ls.maxDepth, *sampler, *senum);
+}
+
+// One sample of TiledIntegrator::Render's inner loop
+// (integrator/TiledIntegrator.cpp:40-47) for pixel (x, y), sample s.
+Vec3 one_path(const LoadedScene& ls, PathTracing& pt, const std::shared_ptr<Sampler>& sampler,
+              const SamplerEnum& senum, uint32_t x, uint32_t y, uint32_t s, MemoryPool& arena, int* cursor) {
+  uint64 instance = senum.GetIndex(s, x, y);
+  RandomStateSequence rand(sampler, instance);
+  real u = senum.SampleX(x, rand());
+  real v = senum.SampleY(y, rand());
+  Ray ray = static_cast<const Camera&>(*ls.camera).GenerateRay(x, y, Vec2(u, v));
+  Vec3 L = pt.Li(ray, *ls.scene, rand, arena);
+  arena.Reset();
+  if (cursor) *cursor = rand.GetCursor();
+  return L;
+}
+
+int cmd_paths(int argc, char** argv) {
+  LoadedScene ls = load_scene(argv[2]);
+  std::shared_ptr<Sampler> sampler;
+  std::shared_ptr<SamplerEnum> senum;
+  auto pt = make_integrator(ls, &sampler, &senum);
+  std::vector<char> in = read_file(argv[3]);
+  size_t n = in.size() / 12;
+  std::vector<float> out(n * 4);
+  MemoryPool arena;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t v[3];
+    std::memcpy(v, &in[12 * i], 12);
+    int cursor = 0;
+    Vec3 L = one_path(ls, *pt, sampler, *senum, v[0], v[1], v[2], arena, &cursor);
+    out[4 * i] = L.x; out[4 * i + 1] = L.y; out[4 * i + 2] = L.z;
+    out[4 * i + 3] = (float)cursor;
+  }
+  write_file(argv[4], out.data(), out.size() * 4);
+  return 0;
+}
+
+// Full TiledIntegrator::Render on all host threads. With [rows] < resY only the
+// first `rows` image rows are rendered (a bounded CPU-baseline sample); the
+// film keeps the reference Render's per-pixel accumulation either way.
+int cmd_render(int argc, char** argv) {
+  LoadedScene ls = load_scene(argv[2]);
+  int rows = argc > 4 ? std::atoi(argv[4]) : ls.resY;
+  if (argc > 5) ls.spp = std::atoi(argv[5]);
+  std::shared_ptr<Sampler> sampler;
+  std::shared_ptr<SamplerEnum> senum;
+  auto pt = make_integrator(ls, &sampler, &senum);
+  int fullY = ls.film->mResY;
+  if (rows < fullY) ls.film->mResY = rows;  // TiledIntegrator::Render tiles [0, mResY)
+  auto t0 = std::chrono::steady_clock::now();
+  pt->Render(*ls.scene, *ls.camera);
+  auto t1 = std::chrono::steady_clock::now();
+  ls.film->mResY = fullY;
+  double sec = std::chrono::duration<double>(t1 - t0).count();
+  size_t npx = (size_t)ls.resX * ls.resY;
+  std::vector<float> img(npx * 4);
+  for (size_t i = 0; i < npx; ++i) {
+    const Pixel& p = ls.film->mPixelBuffer[i];
+    img[4 * i] = p.color.x; img[4 * i + 1] = p.color.y; img[4 * i + 2] = p.color.z; img[4 * i + 3] = p.weight;
+  }
+  write_file(argv[3], img.data(), img.size() * 4);
+  double paths = (double)ls.resX * rows * ls.spp;
+  std::printf("{\"render_s\": %.6f, \"paths\": %.0f, \"mpaths_per_s\": %.6f, \"threads\": %d, \"rows\": %d, \"spp\": %d}\n",
+              sec, paths, paths / sec / 1e6, tbb::detail_shim::thread_count(), rows, ls.spp);
+  return 0;
+}
+
+int cmd_camera(int argc, char** argv) {
+  LoadedScene ls = load_scene(argv[2]);
+  float m[16];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) m[4 * i + j] = ls.camera->RasterToWorld.mat(i, j);
+  write_file(argv[3], m, sizeof(m));
+  return 0;
+}
+
+// BxDF tables in the local shading frame. Case record: u32 type, f32 params[16],
+// f32 wo[3], f32 u[3], f32 wi_eval[3]. Output: f32 sample_f[3], wi[3], pdf,
+// eval_f[3], eval_pdf (11 floats).
+int cmd_bsdf(int argc, char** argv) {
+  std::vector<char> in = read_file(argv[2]);
+  const size_t rec = 4 + 4 * (16 + 9);
+  size_t n = in.size() / rec;
+  std::vector<float> out(n * 11);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t type;
+    float p[25];
+    std::memcpy(&type, &in[i * rec], 4);
+    std::memcpy(p, &in[i * rec + 4], sizeof(p));
+    Vec3 wo(p[16], p[17], p[18]), u(p[19], p[20], p[21]), we(p[22], p[23], p[24]);
+    std::unique_ptr<BxDF> b;
+    switch (type) {
+      case 0: b.reset(new DiffuseBSDF(Vec3(p[0], p[1], p[2]))); break;
+      case 1: b.reset(new SpecularBSDF(Vec3(p[0], p[1], p[2]))); break;
+      case 2: b.reset(new TransmissionBSDF(Vec3(p[3], p[4], p[5]), Vec3(p[0], p[1], p[2]), TransportMode::Radiance, p[15], p[8])); break;
+      case 3: b.reset(new MicrofacetReflectionBSDF(new GGXDistribution(p[6], p[7], true),
+                                                   new FresnelConductor(Vec3(1, 1, 1), Vec3(p[9], p[10], p[11]), Vec3(p[12], p[13], p[14])),
+                                                   Vec3(p[0], p[1], p[2]))); break;
+      case 4: b.reset(new RoughDielectricBSDF(new GGXDistribution(p[6], p[7], true), Vec3(p[0], p[1], p[2]),
+                                              Vec3(p[3], p[4], p[5]), 1.f, p[8], TransportMode::Radiance)); break;
+      default: throw std::runtime_error("bad bsdf type");
+    }
+    Vec3 wi;
+    real pdf = 0;
+    Vec3 f = b->Sample(wo, &wi, &pdf, u);
+    Vec3 fe = b->Evaluate(wo, we);
+    real pe = b->Pdf(wo, we);
+    float* o = &out[i * 11];
+    o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = wi.x; o[4] = wi.y; o[5] = wi.z; o[6] = pdf;
+    o[7] = fe.x; o[8] = fe.y; o[9] = fe.z; o[10] = pe;
+  }
+  write_file(argv[3], out.data(), out.size() * 4);
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) {
+    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|hits|anyhit|paths|render|camera|bsdf> ...\n");
+    return 2;
+  }
+  try {
+    std::string c = argv[1];
+    if (c == "sobol") return cmd_sobol(argc, argv);
+    if (c == "enum") return cmd_enum(argc, argv);
+    if (c == "hits") return cmd_hits(argc, argv, false);
+    if (c == "anyhit") return cmd_hits(argc, argv, true);
+    if (c == "paths") return cmd_paths(argc, argv);
+    if (c == "render") return cmd_render(argc, argv);
+    if (c == "camera") return cmd_camera(argc, argv);
+    if (c == "bsdf") return cmd_bsdf(argc, argv);
+    std::fprintf(stderr, "unknown command %s\n", c.c_str());
+    return 2;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+}

@@ -1,0 +1,137 @@
+"""Binary I/O between the tests and the reference harness (oracle/ref/harness.cpp).
+
+TEST INFRASTRUCTURE ONLY: only tests/, the golden-vector generator and
+bench.py's CPU-baseline leg use this module.
+
+Scene file (little-endian), read by ``load_scene`` in the harness:
+  u32 magic 'GYTS', u32 version=1,
+  u32 nv, nt, ns, nm, ne, has_normals, env_w, env_h,
+  u32 res_x, res_y, spp, max_depth, rr_depth,
+  f32 camera[11] = pos[3], look_at[3], up[3], fovy, film_distance,
+  f32 env_scale,
+  f32 vertices[nv*3], [f32 normals[nv*3] if has_normals], u32 indices[nt*3],
+  u32 tri_material[nt], i32 tri_emission[nt], f32 spheres[ns*4],
+  u32 sphere_material[ns], u32 mat_type[nm], f32 mat_params[nm*16],
+  f32 emission[ne*3], f32 env[env_h*env_w*3] (row 0 = top).
+"""
+import os
+import subprocess
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HARNESS = os.path.join(HERE, "_ref", "gyref_harness")
+
+
+def write_scene(path, sd):
+    ns = sd.n_spheres
+    env = sd.env
+    env_h, env_w = (0, 0) if env is None else env.shape[:2]
+    c = sd.camera
+    p = sd.params
+    with open(path, "wb") as f:
+        f.write(struct.pack("<2I", 0x53545947, 1))
+        f.write(struct.pack("<8I", sd.vertices.shape[0], sd.n_triangles, ns, sd.mat_type.shape[0],
+                            sd.emission.shape[0], 0 if sd.normals is None else 1, env_w, env_h))
+        f.write(struct.pack("<5I", c.res_x, c.res_y, p.spp, p.max_depth, p.rr_depth))
+        f.write(np.array(list(c.pos) + list(c.look_at) + list(c.up) + [c.fovy, c.film_distance], np.float32).tobytes())
+        f.write(struct.pack("<f", sd.env_scale))
+        f.write(np.ascontiguousarray(sd.vertices, np.float32).tobytes())
+        if sd.normals is not None:
+            f.write(np.ascontiguousarray(sd.normals, np.float32).tobytes())
+        f.write(np.ascontiguousarray(sd.indices, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(sd.tri_material, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(sd.tri_emission, np.int32).tobytes())
+        if ns:
+            f.write(np.ascontiguousarray(sd.spheres, np.float32).tobytes())
+            f.write(np.ascontiguousarray(sd.sphere_material, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(sd.mat_type, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(sd.mat_params, np.float32).tobytes())
+        f.write(np.ascontiguousarray(sd.emission, np.float32).tobytes())
+        if env is not None:
+            f.write(np.ascontiguousarray(env, np.float32).tobytes())
+
+
+def have_harness():
+    return os.path.exists(HARNESS)
+
+
+def run(*args, env=None):
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    r = subprocess.run([HARNESS] + [str(a) for a in args], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                       text=True, env=e)
+    if r.returncode != 0:
+        raise RuntimeError("gyref_harness %s failed: %s" % (args[0], r.stderr[-2000:]))
+    return r.stdout
+
+
+RAY_DTYPE = np.dtype([("o", "<f4", 3), ("d", "<f4", 3), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("prim", "<i4"), ("t", "<f4"), ("b1", "<f4"), ("b2", "<f4")])
+
+
+def ref_sobol(tmp, dims, indices):
+    pairs = np.zeros(len(dims), np.dtype([("d", "<u4"), ("i", "<u8")]))
+    pairs["d"] = dims
+    pairs["i"] = indices
+    a, b = os.path.join(tmp, "sobol_in.bin"), os.path.join(tmp, "sobol_out.bin")
+    pairs.tofile(a)
+    run("sobol", a, b)
+    return np.fromfile(b, np.float32)
+
+
+def ref_enum(tmp, res_x, res_y, s, x, y):
+    trip = np.stack([np.asarray(s, np.uint32), np.asarray(x, np.uint32), np.asarray(y, np.uint32)], 1)
+    a, b = os.path.join(tmp, "enum_in.bin"), os.path.join(tmp, "enum_out.bin")
+    trip.astype(np.uint32).tofile(a)
+    run("enum", res_x, res_y, a, b)
+    return np.fromfile(b, np.uint64)
+
+
+def ref_hits(tmp, scene_path, rays, any_hit=False):
+    a, b = os.path.join(tmp, "rays.bin"), os.path.join(tmp, "hits.bin")
+    rays.astype(RAY_DTYPE).tofile(a)
+    run("anyhit" if any_hit else "hits", scene_path, a, b)
+    return np.fromfile(b, HIT_DTYPE)
+
+
+def ref_paths(tmp, scene_path, x, y, s):
+    trip = np.stack([np.asarray(x, np.uint32), np.asarray(y, np.uint32), np.asarray(s, np.uint32)], 1)
+    a, b = os.path.join(tmp, "paths_in.bin"), os.path.join(tmp, "paths_out.bin")
+    trip.astype(np.uint32).tofile(a)
+    run("paths", scene_path, a, b)
+    return np.fromfile(b, np.float32).reshape(-1, 4)
+
+
+def ref_camera(tmp, scene_path):
+    b = os.path.join(tmp, "camera.bin")
+    run("camera", scene_path, b)
+    return np.fromfile(b, np.float32).reshape(4, 4)
+
+
+def ref_render(tmp, scene_path, rows=None, spp=None, threads=None):
+    import json
+    b = os.path.join(tmp, "render.bin")
+    args = ["render", scene_path, b]
+    if rows is not None or spp is not None:
+        args.append(rows if rows is not None else 1 << 30)
+    if spp is not None:
+        args.append(spp)
+    out = run(*args, env={"GYREF_THREADS": str(threads)} if threads else None)
+    info = json.loads(out.strip().splitlines()[-1])
+    img = np.fromfile(b, np.float32).reshape(-1, 4)
+    return img, info
+
+
+def ref_bsdf(tmp, cases):
+    """cases: structured array with fields type (u4), params (16 f4), wo, u, we (3 f4)."""
+    a, b = os.path.join(tmp, "bsdf_in.bin"), os.path.join(tmp, "bsdf_out.bin")
+    cases.tofile(a)
+    run("bsdf", a, b)
+    return np.fromfile(b, np.float32).reshape(-1, 11)
+
+
+BSDF_CASE_DTYPE = np.dtype([("type", "<u4"), ("params", "<f4", 16), ("wo", "<f4", 3), ("u", "<f4", 3),
+                            ("we", "<f4", 3)])

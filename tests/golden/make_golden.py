@@ -1,0 +1,139 @@
+"""Generate the golden vectors in tests/golden/ from the reference itself.
+
+Runs the reference renderer compiled from its own sources by
+oracle/ref/build_ref.py (``oracle/_ref/gyref_harness``) on seeded inputs and
+stores the inputs and the reference outputs as .npz fixtures. The reference
+checkout is only needed to regenerate; the tests read the fixtures.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from gyunity_b200 import scenes  # noqa: E402
+from oracle import scene_io as io  # noqa: E402
+
+
+def random_rays(sd, n, rng):
+    """Rays from inside the box towards random directions, plus camera-like
+    rays through the open front, with finite and infinite tmax."""
+    o = rng.uniform(-0.95, 0.95, (n, 3)).astype(np.float32)
+    half = n // 2
+    o[half:, 2] = 2.9
+    d = rng.normal(size=(n, 3))
+    d[half:, 2] = -np.abs(d[half:, 2]) - 1.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tmax = np.where(rng.uniform(size=n) < 0.2, rng.uniform(0.1, 2.0, n), np.inf).astype(np.float32)
+    rays = np.zeros(n, io.RAY_DTYPE)
+    rays["o"] = o
+    rays["d"] = d.astype(np.float32)
+    rays["tmax"] = tmax
+    return rays
+
+
+def bsdf_cases(rng, n_per=400):
+    cases = []
+    kinds = [
+        (0, dict(a=(0.7, 0.5, 0.3))),
+        (1, dict(a=(0.9, 0.9, 0.9))),
+        (2, dict(a=(1, 1, 1), b=(1, 1, 1), eta=1.5, eta1=1.0)),
+        (3, dict(a=(1, 1, 1), ax=0.05, ay=0.05)), (3, dict(a=(1, 1, 1), ax=0.2, ay=0.2)),
+        (3, dict(a=(0.9, 0.8, 0.7), ax=0.5, ay=0.5)),
+        (4, dict(a=(1, 1, 1), b=(1, 1, 1), ax=0.1, ay=0.1, eta=1.5)),
+        (4, dict(a=(1, 1, 1), b=(1, 1, 1), ax=0.5, ay=0.5, eta=1.5)),
+    ]
+    for kind, kw in kinds:
+        _, p = scenes._mat(kind, **kw)
+        c = np.zeros(n_per, io.BSDF_CASE_DTYPE)
+        c["type"] = kind
+        c["params"] = p
+        wo = rng.normal(size=(n_per, 3))
+        wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+        we = rng.normal(size=(n_per, 3))
+        we /= np.linalg.norm(we, axis=1, keepdims=True)
+        c["wo"] = wo.astype(np.float32)
+        c["u"] = rng.uniform(size=(n_per, 3)).astype(np.float32)
+        c["we"] = we.astype(np.float32)
+        cases.append(c)
+    return np.concatenate(cases)
+
+
+def main():
+    if not io.have_harness():
+        sys.exit("build the reference harness first: python oracle/ref/build_ref.py")
+    rng = np.random.default_rng(20261203)
+    tmp = tempfile.mkdtemp()
+    out = {}
+
+    # Sobol' points: sobol::sample over dimensions and 64-bit indices
+    dims = np.concatenate([rng.integers(0, 1024, 3000), np.arange(16).repeat(8)]).astype(np.uint32)
+    idx = np.concatenate([rng.integers(0, 1 << 40, 3000), rng.integers(0, 1 << 20, 128)]).astype(np.uint64)
+    np.savez_compressed(os.path.join(HERE, "sobol.npz"), dims=dims, indices=idx,
+                        values=io.ref_sobol(tmp, dims, idx))
+
+    # pixel enumeration: SobolEnum::GetIndex at three film sizes
+    enum = {}
+    for rx, ry in ((256, 256), (1024, 1024), (1920, 1080)):
+        s = rng.integers(0, 256, 1500).astype(np.uint32)
+        x = rng.integers(0, rx, 1500).astype(np.uint32)
+        y = rng.integers(0, ry, 1500).astype(np.uint32)
+        key = "%dx%d" % (rx, ry)
+        enum[key + "_sxy"] = np.stack([s, x, y], 1)
+        enum[key + "_index"] = io.ref_enum(tmp, rx, ry, s, x, y)
+    np.savez_compressed(os.path.join(HERE, "enum.npz"), **enum)
+
+    # camera: RasterToWorld of two films
+    cams = {}
+    for rx, ry in ((256, 256), (1920, 1080)):
+        sd = scenes.cornell_box(res=rx, spheres=False)
+        sd.camera.res_x, sd.camera.res_y = rx, ry
+        path = os.path.join(tmp, "cam.gyts")
+        io.write_scene(path, sd)
+        cams["%dx%d" % (rx, ry)] = io.ref_camera(tmp, path)
+    np.savez_compressed(os.path.join(HERE, "camera.npz"), **cams)
+
+    # closest hits on the Cornell box with spheres and on a small mesh scene
+    for name, sd in (("cornell", scenes.cornell_box()), ("mesh", scenes.mixed_materials_box(level=3))):
+        path = os.path.join(tmp, name + ".gyts")
+        io.write_scene(path, sd)
+        rays = random_rays(sd, 3000, rng)
+        h = io.ref_hits(tmp, path, rays)
+        a = io.ref_hits(tmp, path, rays, any_hit=True)
+        np.savez_compressed(os.path.join(HERE, "hits_%s.npz" % name), rays=rays.view(np.float32).reshape(-1, 7),
+                            prim=h["prim"], t=h["t"], b1=h["b1"], b2=h["b2"], any=a["prim"])
+
+    # per-path radiance, PathTracing::Li, for three scenes
+    for name, sd in (("cornell_nospheres", scenes.cornell_box(spheres=False)), ("cornell", scenes.cornell_box()),
+                     ("mixed", scenes.mixed_materials_box(level=3, res=64))):
+        path = os.path.join(tmp, name + ".gyts")
+        io.write_scene(path, sd)
+        n = 3000
+        x = rng.integers(0, sd.camera.res_x, n)
+        y = rng.integers(0, sd.camera.res_y, n)
+        s = rng.integers(0, sd.params.spp, n)
+        r = io.ref_paths(tmp, path, x, y, s)
+        np.savez_compressed(os.path.join(HERE, "paths_%s.npz" % name), xys=np.stack([x, y, s], 1).astype(np.uint32),
+                            L=r[:, :3], cursor=r[:, 3].astype(np.int32))
+
+    # a full low-resolution render through TiledIntegrator::Render
+    sd = scenes.cornell_box(res=64, spp=4)
+    path = os.path.join(tmp, "img.gyts")
+    io.write_scene(path, sd)
+    img, info = io.ref_render(tmp, path)
+    np.savez_compressed(os.path.join(HERE, "image_cornell_64x64_4spp.npz"), film=img)
+
+    # BxDF tables in the local frame
+    cases = bsdf_cases(rng)
+    np.savez_compressed(os.path.join(HERE, "bsdf.npz"), cases=cases.view(np.uint8), out=io.ref_bsdf(tmp, cases))
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

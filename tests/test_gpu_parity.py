@@ -1,0 +1,164 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the
+reference's golden vectors. Needs a B200."""
+import numpy as np
+import pytest
+
+from conftest import golden
+import gyunity_b200 as g
+from gyunity_b200 import scenes
+from oracle.port import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_sobol_bit_exact(ctx):
+    gd = golden("sobol.npz")
+    assert np.array_equal(ctx.sobol(gd["dims"], gd["indices"]), gd["values"])
+
+
+@pytest.mark.parametrize("res", ["256x256", "1024x1024", "1920x1080"])
+def test_enumeration_bit_exact(ctx, res):
+    gd = golden("enum.npz")
+    rx, ry = map(int, res.split("x"))
+    sxy = gd[res + "_sxy"]
+    assert np.array_equal(ctx.sobol_enum_index(rx, ry, sxy[:, 0], sxy[:, 1], sxy[:, 2]), gd[res + "_index"])
+
+
+def test_sobol_edge_cases(ctx):
+    # index 0 (all dims 0), the top of the 64-bit range and the last dimension
+    dims = np.array([0, 1, 1023, 1023, 5, 0], np.uint32)
+    idx = np.array([0, 0, 1, (1 << 52) - 1, (1 << 40) + 12345, (1 << 32) - 1], np.uint64)
+    assert np.array_equal(ctx.sobol(dims, idx), orc.sobol(dims, idx))
+    assert ctx.sobol(np.zeros(0, np.uint32), np.zeros(0, np.uint64)).shape == (0,)
+
+
+def _ties(t_gpu, t_ref):
+    return np.abs(t_gpu - t_ref) <= 1e-6 * np.maximum(np.abs(t_ref), 1e-6)
+
+
+@pytest.mark.parametrize("name", ["cornell", "mesh"])
+def test_closest_hit_ids_match_reference(ctx, name):
+    gd = golden("hits_%s.npz" % name)
+    sd = scenes.cornell_box() if name == "cornell" else scenes.mixed_materials_box(level=3)
+    sc = g.Scene(sd, ctx)
+    prim, t, b1, b2 = sc.intersect(gd["rays"])
+    ref_t = gd["t"].astype(np.float64)
+    same = prim == gd["prim"]
+    tie = (prim >= 0) & (gd["prim"] >= 0) & _ties(t, ref_t)
+    bad = ~(same | tie)
+    assert not bad.any(), (np.nonzero(bad)[0][:10], prim[bad][:10], gd["prim"][bad][:10])
+    hit = same & (prim >= 0)
+    assert np.allclose(t[hit], ref_t[hit], rtol=1e-5, atol=1e-6)
+    tri = hit & (prim < sd.n_triangles)
+    assert np.allclose(b1[tri], gd["b1"][tri], atol=1e-4) and np.allclose(b2[tri], gd["b2"][tri], atol=1e-4)
+    (occ,) = sc.intersect(gd["rays"], any_hit=True)
+    assert np.array_equal(occ, gd["any"].astype(bool))
+
+
+def test_closest_hit_ids_match_oracle_on_large_mesh(ctx):
+    # 1.3M-triangle procedural mesh, seeded ray batch: bit-exact ids except
+    # equal-t ties (reported)
+    sd = scenes.procedural_mesh_box(level=8, res=64, spp=1)
+    sc = g.Scene(sd, ctx)
+    rng = np.random.default_rng(7)
+    n = 20000
+    o = rng.uniform(-0.95, 0.95, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d.astype(np.float32), np.full((n, 1), np.inf, np.float32)], 1)
+    prim, t, _, _ = sc.intersect(rays)
+    oprim, ot, _, _ = orc.OracleScene(sd).closest_hit(rays, precision=32)
+    same = prim == oprim
+    tie = _ties(t, ot)
+    print("near ties:", int((~same & tie).sum()), "of", n)
+    assert np.all(same | tie)
+
+
+def _replay(sd, xys, ctx):
+    sc = g.Scene(sd, ctx)
+    L, cur, rr = sc.trace_paths(xys)
+    o = orc.OracleScene(sd)
+    Lo, co = o.paths(xys[:, 0], xys[:, 1], xys[:, 2], precision=64, force_rr=rr)
+    rel = np.abs(L.astype(np.float64) - Lo).max(1) / np.maximum(np.abs(Lo).max(1), 1e-3)
+    return rel, cur == co, L
+
+
+@pytest.mark.parametrize("name", ["cornell_nospheres", "cornell", "mixed"])
+def test_per_path_radiance_matches_fp64_replay(ctx, name):
+    sd = {"cornell_nospheres": scenes.cornell_box(spheres=False), "cornell": scenes.cornell_box(),
+          "mixed": scenes.mixed_materials_box(level=3, res=64)}[name]
+    xys = golden("paths_%s.npz" % name)["xys"]
+    rel, same_cursor, _ = _replay(sd, xys, ctx)
+    ok = rel < 1e-4  # tolerance: FP32 path vs FP64 replay of the same Sobol' dimensions
+    print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean())
+    assert same_cursor.mean() > 0.995
+    assert ok.mean() > 0.99
+
+
+def test_per_path_radiance_matches_reference(ctx):
+    gd = golden("paths_cornell_nospheres.npz")
+    sc = g.Scene(scenes.cornell_box(spheres=False), ctx)
+    L, cur, _ = sc.trace_paths(gd["xys"])
+    ref = gd["L"].astype(np.float64)
+    rel = np.abs(L - ref).max(1) / np.maximum(np.abs(ref).max(1), 1e-3)
+    assert (cur == gd["cursor"]).mean() > 0.995
+    assert (rel < 1e-4).mean() > 0.99
+
+
+def test_render_matches_reference_image(ctx):
+    gd = golden("image_cornell_64x64_4spp.npz")["film"].reshape(64, 64, 4).astype(np.float64)
+    sd = scenes.cornell_box(res=64, spp=4)
+    sc = g.Scene(sd, ctx)
+    film = g.Film(64, 64)
+    cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    g.GpuPathTracing(4, 8, 3).Render(sc, cam)
+    ref = gd[..., :3] / gd[..., 3:]
+    img = film.image.astype(np.float64)
+    rmse = np.sqrt(np.mean((img - ref) ** 2))
+    print("image RMSE vs reference:", rmse)
+    assert rmse < 0.02 * np.sqrt(np.mean(ref ** 2))
+
+
+def test_render_is_deterministic_up_to_fp64_atomics(ctx):
+    sd = scenes.cornell_box(res=128, spp=8)
+    sc = g.Scene(sd, ctx)
+    film = g.Film(128, 128)
+    cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    a = g.GpuPathTracing(8, 8, 3).Render(sc, cam).image.copy()
+    b = g.GpuPathTracing(8, 8, 3).Render(sc, cam).image.copy()
+    assert np.allclose(a, b, rtol=1e-9, atol=1e-12)
+    assert np.isfinite(a).all() and a.mean() > 0.05
+
+
+def test_small_pool_matches_large_pool(ctx):
+    # path refilling across many wavefront iterations gives the same image
+    sd = scenes.cornell_box(res=64, spp=16)
+    c2 = g.Context(0, capacity=4096)
+    sa, sb = g.Scene(sd, ctx), g.Scene(sd, c2)
+    fa, fb = g.Film(64, 64), g.Film(64, 64)
+    ca = g.PinHoleCamera(fa, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    cb = g.PinHoleCamera(fb, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    g.GpuPathTracing(16, 8, 3).Render(sa, ca)
+    g.GpuPathTracing(16, 8, 3).Render(sb, cb)
+    assert np.allclose(fa.image, fb.image, rtol=1e-6, atol=1e-7)
+    sb.close()
+    c2.close()
+
+
+def test_invalid_scene_is_rejected(ctx):
+    sd = scenes.cornell_box()
+    sd.indices = sd.indices.copy()
+    sd.indices[0, 0] = 10 ** 6
+    with pytest.raises(g.GytError):
+        g.Scene(sd, ctx)
+
+
+def test_edge_sizes(ctx):
+    # one-pixel film, one sample, depth 1; and a single-triangle scene
+    sd = scenes.cornell_box(res=1, spp=1, max_depth=1)
+    sc = g.Scene(sd, ctx)
+    L, cur, rr = sc.trace_paths(np.array([[0, 0, 0]], np.uint32))
+    Lo, co = orc.OracleScene(sd).paths([0], [0], [0], precision=64)
+    assert np.allclose(L, Lo, rtol=1e-4, atol=1e-6) and cur[0] == co[0]
+    empty_L, _, _ = sc.trace_paths(np.zeros((0, 3), np.uint32))
+    assert empty_L.shape == (0, 3)
