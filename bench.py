@@ -182,9 +182,8 @@ def cpu_baseline(sd, spp, rows=None, threads=None):
 
 
 def run_reference(a):
-    d = Dist(a.gpus)
-    if d.rank != 0:
-        d.close()
+    # the reference is a CPU integrator: rank 0 runs it, other ranks exit at once
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     sd = workload(a)
     spp = 1
@@ -203,7 +202,6 @@ def run_reference(a):
                              "sample": info["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    d.close()
 
 
 # ------------------------------------------------------------ our arm ----
@@ -299,10 +297,18 @@ def run_ours(a):
     d.close()
 
 
+# Algorithmic bytes per path slot and per ray (DESIGN.md lists the fields):
+# path state read by a stage = origin 16 + direction 16 + throughput 16 +
+# radiance 16 + Sobol' index 8 + meta 4 = 76 B; written back by shade = 68 B;
+# closest hit 16 B; a queued segment ray (origin+tmax, direction) 32 B and its
+# contribution 16 B.
+STATE_READ, STATE_WRITE, HIT, RAY, CONTRIB = 76, 68, 16, 32, 16
+
+
 def roofline(prof, cnt, stats):
-    """Bandwidth roofline of the dominant kernel. Algorithmic bytes per ray:
-    ray 32 B + hit 16 B + BVH nodes x 64 B + triangle tests x 48 B (counts
-    from the counting pass); plus the path state each kernel streams."""
+    """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
+    of its launches / their CUDA-event time; traversal bytes per ray = ray +
+    BVH nodes x 64 B + triangle tests x 48 B (counts from the counting pass)."""
     peak, src = peaks()
     ms = prof["ms"]
     dom = max(ms, key=ms.get)
@@ -310,29 +316,32 @@ def roofline(prof, cnt, stats):
     nodes, tris = cnt["node_visits"], cnt["tri_tests"]
     rays = max(1, cnt["closest_rays"] + cnt["shadow_rays"])
     slots = stats[-1]["path_slots"]
-    per_ray_nodes, per_ray_tris = nodes / rays, tris / rays
-    state = 64 + 16 + 8 + 4 + 4 + 4 + 8  # path state bytes per slot
+    npr, tpr = nodes / rays, tris / rays
+    trav = npr * 64 + tpr * 48
+    shadow, mis = cnt["shadow_rays"], max(0, cnt["closest_rays"] - slots)
     if dom == "extend":
-        byts = slots * (32 + 16 + per_ray_nodes * 64 + per_ray_tris * 48)
+        byts = slots * (RAY + HIT + trav)
     elif dom == "connect":
-        trav = cnt["shadow_rays"] + max(0, cnt["closest_rays"] - slots)
-        byts = trav * (48 + per_ray_nodes * 64 + per_ray_tris * 48) + slots * (2 * state + 32)
+        # queue flags of every slot, queued rays, path state copy of survivors
+        byts = slots * (2 * CONTRIB + 16) + (shadow + mis) * (RAY + trav) + slots * 2 * STATE_READ
     elif dom == "shade":
-        byts = slots * (state * 2 + 16 + 96 + 64)
+        byts = slots * (STATE_READ + HIT + STATE_WRITE + 2 * CONTRIB) + (shadow + mis) * RAY
     else:
-        byts = slots * state
+        byts = slots * STATE_WRITE
     achieved = byts / (ms[dom] / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(dom)
+            rec = json.load(open(tf)).get("k_" + dom)
+            if rec:
+                traffic = rec["bytes_per_slot"] * slots / launches
         except Exception:
             traffic = None
     return {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic,
             "algorithmic_bytes_per_launch": byts / launches, "launches": launches,
-            "avg_launch_ms": ms[dom] / launches, "nodes_per_ray": per_ray_nodes, "tris_per_ray": per_ray_tris,
+            "avg_launch_ms": ms[dom] / launches, "nodes_per_ray": npr, "tris_per_ray": tpr,
             "share": {k: v / sum(ms.values()) for k, v in ms.items()}}
 
 

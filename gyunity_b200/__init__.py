@@ -148,20 +148,21 @@ class Scene:
                                                    _c.ptr(prim), _c.ptr(t), _c.ptr(b1), _c.ptr(b2)))
         return (prim.astype(bool),) if any_hit else (prim, t, b1, b2)
 
-    def trace_paths(self, xys, camera=None, params=None):
+    def trace_paths(self, xys, camera=None, params=None, decisions=False):
         """PathTracing::Li of explicit samples (n, 3) = x, y, s. Returns
-        radiance (n, 3), Sobol' dimensions used, and roulette-draw masks."""
+        radiance (n, 3), Sobol' dimensions used and roulette-draw masks; with
+        ``decisions`` also the shadow-occlusion and MIS-hit masks."""
         cam = _c.camera_struct(camera or self.desc.camera)
         prm = _c.params_struct(params or self.desc.params)
         xys = np.ascontiguousarray(xys, np.uint32).reshape(-1, 3)
         n = xys.shape[0]
         L = np.empty((n, 3), np.float32)
         cur = np.empty(n, np.uint32)
-        rr = np.empty(n, np.uint64)
+        rr, occ, mis = (np.empty(n, np.uint64) for _ in range(3))
         self.ctx.check(self.ctx._lib.gyt_trace_paths(self.ctx.handle, self.handle, ctypes.byref(cam),
                                                      ctypes.byref(prm), n, _c.ptr(xys), _c.ptr(L), _c.ptr(cur),
-                                                     _c.ptr(rr)))
-        return L, cur, rr
+                                                     _c.ptr(rr), _c.ptr(occ), _c.ptr(mis)))
+        return (L, cur, rr, occ, mis) if decisions else (L, cur, rr)
 
 
 class Film:

@@ -86,7 +86,8 @@ def load():
     L.gyt_render.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P]
     L.gyt_render_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P,
                                     ctypes.POINTER(GytRenderStats)]
-    L.gyt_trace_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P, P, P]
+    L.gyt_trace_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P, P, P,
+                                  P, P]
     L.gyt_intersect.argtypes = [P, P, U64, P, I32, P, P, P, P]
     L.gyt_sobol.argtypes = [P, U64, P, P, P]
     L.gyt_sobol_enum_index.argtypes = [P, U32, U32, U64, P, P]

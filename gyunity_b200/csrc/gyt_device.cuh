@@ -134,7 +134,7 @@ GYT_D void camera_ray(const Cam& c, float px, float py, float3* o, float3* d) {
 // ------------------------------------------------------------ geometry ----
 // Per-ray constants of the watertight test (Woop, Benthin, Wald 2013).
 struct WtRay {
-  float3 o;
+  float3 o, d;
   int kx, ky, kz;
   float Sx, Sy, Sz;
 };
@@ -142,6 +142,7 @@ struct WtRay {
 GYT_D WtRay wt_setup(float3 o, float3 d) {
   WtRay w;
   w.o = o;
+  w.d = d;
   float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
   int kz = 0;
   if (ay > ax && ay >= az) kz = 1;
@@ -157,9 +158,31 @@ GYT_D WtRay wt_setup(float3 o, float3 d) {
   return w;
 }
 
+// The same test in FP64, used only to settle hits whose FP32 distance lands
+// within a few ulps of tmax. Shadow rays end on the light's surface (the Ray
+// constructor's RayEps shift cancels ShadowRayEps, visual/Intersection.h:64-72),
+// so their fate would otherwise be decided by rounding.
+__device__ __noinline__ bool wt_intersect_fp64(const WtRay& r, float3 p0, float3 p1, float3 p2, float tmax) {
+  double dx = comp(r.d, r.kx), dy = comp(r.d, r.ky), dz = comp(r.d, r.kz);
+  double ox = comp(r.o, r.kx), oy = comp(r.o, r.ky), oz = comp(r.o, r.kz);
+  double Sx = dx / dz, Sy = dy / dz, Sz = 1.0 / dz;
+  double Akz = comp(p0, r.kz) - oz, Bkz = comp(p1, r.kz) - oz, Ckz = comp(p2, r.kz) - oz;
+  double Ax = (comp(p0, r.kx) - ox) - Sx * Akz, Ay = (comp(p0, r.ky) - oy) - Sy * Akz;
+  double Bx = (comp(p1, r.kx) - ox) - Sx * Bkz, By = (comp(p1, r.ky) - oy) - Sy * Bkz;
+  double Cx = (comp(p2, r.kx) - ox) - Sx * Ckz, Cy = (comp(p2, r.ky) - oy) - Sy * Ckz;
+  double U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+  if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
+  double det = U + V + W;
+  if (det == 0) return false;
+  double th = (U * (Sz * Akz) + V * (Sz * Bkz) + W * (Sz * Ckz)) / det;
+  return th >= 0.0 && th <= (double)tmax;
+}
+
 // Watertight ray/triangle test. On a hit returns t and the barycentric
 // weights of p1 (b1) and p2 (b2), the convention of Triangle::Intersect
-// (shape/Triangle.cpp:71-103). Accepts 0 <= t <= tmax.
+// (shape/Triangle.cpp:71-103). Accepts 0 <= t <= tmax. With SETTLE (segment
+// rays: shadow rays) a distance within 2e-6 relative of tmax is settled in FP64.
+template <bool SETTLE = false>
 GYT_D bool wt_intersect(const WtRay& r, float3 p0, float3 p1, float3 p2, float tmax, float* t, float* b1,
                         float* b2) {
   float3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
@@ -178,7 +201,15 @@ GYT_D bool wt_intersect(const WtRay& r, float3 p0, float3 p1, float3 p2, float t
   if (det == 0.f) return false;
   float T = U * (r.Sz * Akz) + V * (r.Sz * Bkz) + W * (r.Sz * Ckz);
   float th = T / det;
-  if (!(th >= 0.f && th <= tmax)) return false;
+  if (SETTLE) {
+    if (!(th >= 0.f && th <= tmax * 1.000002f)) return false;
+    if (th >= tmax * 0.999998f) {
+      if (!wt_intersect_fp64(r, p0, p1, p2, tmax)) return false;
+      th = fminf(th, tmax);
+    }
+  } else if (!(th >= 0.f && th <= tmax)) {
+    return false;
+  }
   *t = th;
   *b1 = V / det;
   *b2 = W / det;

@@ -63,7 +63,6 @@ struct PathBuf {
   uint32_t* meta; // depth 0-7 | delta 8 | cursor 9-19 | alive 31
   uint32_t* pix;  // pixel index 0-27 | spill x 30 | spill y 31
   uint32_t* pid;  // path id within the render (debug outputs)
-  unsigned long long* rr;    // bounces that drew a roulette number
 };
 
 struct Queues {
@@ -80,10 +79,16 @@ struct Params {
   uint32_t spp, max_depth, rr_depth;
 };
 
+// Per-path replay record, indexed by path id (explicit path lists only).
+// Bit i of a mask refers to bounce i (< 64): rr = a roulette number was
+// drawn, occ = the shadow ray was occluded, mis = the MIS ray reached the
+// sampled light.
 struct DebugOut {
   float* L;
   uint32_t* cursor;
   unsigned long long* rr;
+  unsigned long long* occ;
+  unsigned long long* mis;
 };
 
 constexpr uint32_t kAlive = 1u << 31;
@@ -155,7 +160,7 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
         for (uint32_t k = 0; k < count; ++k, t += 3) {
           float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
           float th, u, v;
-          if (wt_intersect(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
+          if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
             prim = __float_as_int(t0.w);
             if (ANY) return prim;
             tmax = th;
@@ -264,7 +269,6 @@ __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base,
   uint32_t pix = (y * cam.res_x + x) | ((u == 0.f && x > 0) ? (1u << 30) : 0u) | ((v == 0.f && y > 0) ? (1u << 31) : 0u);
   dst.pix[k] = pix;
   dst.pid[k] = (uint32_t)p;
-  dst.rr[k] = 0ull;
 }
 
 // Per-warp reduction of traversal counters into the profile (counting mode).
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(PathBuf cur, uint32_t n, DevS
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
-                                                  SobolTables tab) {
+                                                  SobolTables tab, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -305,7 +309,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   float3 ro = f3(cur.o[i]), rd = f3(cur.d[i]);
   float3 tp = f3(cur.tp[i]);
   float3 L = f3(cur.L[i]);
-  unsigned long long rr = cur.rr[i];
+  const uint32_t bounce = depth;
   bool alive = false;
   float4 sc = zero4, mc = zero4;
   if (prim >= 0) {
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
               dd = dd / dis;
               float3 so = org + dd * kRayEps;
               q.so[i] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
-              q.sd[i] = make_float4(dd.x, dd.y, dd.z, 0.f);
+              q.sd[i] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(bounce));
               float w1 = power_heuristic(pdf, spdf);
               float3 c = tp * (Li * f * cosT / pdf) * w1 / lsel;
               sc = make_float4(c.x, c.y, c.z, 1.f);
@@ -392,7 +396,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
             float lpdf = tri_light_pdf(s, ltri, h, o2, wi2);
             if (lpdf != 0.f) {
               float w2 = power_heuristic(pdf2, lpdf);
-              q.mo[i] = make_float4(o2.x, o2.y, o2.z, 0.f);
+              q.mo[i] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
               q.md[i] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
               float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
               mc = make_float4(c.x, c.y, c.z, 1.f);
@@ -413,7 +417,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
       float p = qv < 1.f ? qv : 1.f;  // std::min(1, q): 1 when q is NaN
       bool survive = true;
       if (p < 1.f && depth > prm.rr_depth) {
-        rr |= 1ull << depth;
+        if (dbg.rr && depth < 64) dbg.rr[cur.pid[i]] |= 1ull << depth;
         if (rng.next(tab.matrices) < p) tp = tp / p;
         else survive = false;
       }
@@ -430,7 +434,6 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   }
   cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
   cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
-  cur.rr[i] = rr;
   q.sc[i] = sc;
   q.mc[i] = mc;
 }
@@ -457,7 +460,12 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
   if (shadow) {
     float4 so = q.so[i], sd = q.sd[i];
     float tmax = so.w, b1, b2;
-    if (trace<true, COUNT>(s, f3(so), f3(sd), tmax, b1, b2, &cnt) < 0) L = L + f3(sc);
+    if (trace<true, COUNT>(s, f3(so), f3(sd), tmax, b1, b2, &cnt) < 0) {
+      L = L + f3(sc);
+    } else if (dbg.occ) {
+      uint32_t b = __float_as_uint(sd.w);
+      if (b < 64) dbg.occ[cur.pid[i]] |= 1ull << b;
+    }
   }
   float4 mc = q.mc[i];
   if (mc.w != 0.f) {
@@ -473,6 +481,10 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
       float b0 = 1.f - b1 - b2;
       float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
       if (dot(ns, -wi) > 0.f) L = L + f3(mc) * f3(__ldg(s.lights + li));
+      if (dbg.mis) {
+        uint32_t b = __float_as_uint(mo.w);
+        if (b < 64) dbg.mis[cur.pid[i]] |= 1ull << b;
+      }
     }
   }
   if (COUNT) {
@@ -500,7 +512,6 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
     nxt.meta[j] = meta;
     nxt.pix[j] = cur.pix[i];
     nxt.pid[j] = cur.pid[i];
-    nxt.rr[j] = cur.rr[i];
   } else {
     uint32_t pix = cur.pix[i];
     if (film) {
@@ -518,7 +529,6 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
       dbg.L[3ull * pid + 2] = L.z;
     }
     if (dbg.cursor) dbg.cursor[pid] = (meta >> 9) & 2047u;
-    if (dbg.rr) dbg.rr[pid] = cur.rr[i];
   }
 }
 
@@ -702,7 +712,6 @@ int32_t ensure_pool(gyt_context* ctx) {
     GYT_CK(ctx, dalloc(L, &P.meta, n));
     GYT_CK(ctx, dalloc(L, &P.pix, n));
     GYT_CK(ctx, dalloc(L, &P.pid, n));
-    GYT_CK(ctx, dalloc(L, &P.rr, n));
   }
   Queues& q = ctx->q;
   GYT_CK(ctx, dalloc(L, &q.so, n));
@@ -747,7 +756,7 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
     if (cnt) k_extend<true><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, ctx->d_counters);
     else k_extend<false><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, nullptr);
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[2], s));
-    k_shade<<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, prm, ctx->q, tab);
+    k_shade<<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, prm, ctx->q, tab, dbg);
     GYT_CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(uint32_t), s));
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[3], s));
     if (cnt)
@@ -1047,7 +1056,7 @@ int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCam
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
   if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "render: more than 2^32 paths in one render");
-  return run_paths(ctx, scene, cam, params, total, nullptr, d_film, DebugOut{nullptr, nullptr, nullptr}, stats);
+  return run_paths(ctx, scene, cam, params, total, nullptr, d_film, DebugOut{}, stats);
 }
 
 int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
@@ -1082,7 +1091,7 @@ int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
 
 int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
                         const GytRenderParams* params, uint64_t n, const uint32_t* xys, float* L_out,
-                        uint32_t* cursor_out, uint64_t* rr_out) {
+                        uint32_t* cursor_out, uint64_t* rr_out, uint64_t* occ_out, uint64_t* mis_out) {
   if (!ctx || !scene || !camera || (n && !xys)) return fail(ctx, GYT_ERR_INVALID, "trace_paths: null argument");
   int32_t st = check_params(ctx, params);
   if (st) return st;
@@ -1103,17 +1112,20 @@ int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamer
   uint32_t* dl = nullptr;
   float* dL = nullptr;
   uint32_t* dc = nullptr;
-  unsigned long long* dr = nullptr;
+  unsigned long long* dm = nullptr;
   GYT_CK(ctx, dalloc(tmp, &dl, 3 * n));
   GYT_CK(ctx, dalloc(tmp, &dL, 3 * n));
   GYT_CK(ctx, dalloc(tmp, &dc, n));
-  GYT_CK(ctx, dalloc(tmp, &dr, n));
+  GYT_CK(ctx, dalloc(tmp, &dm, 3 * n));
   GYT_CK(ctx, cudaMemcpy(dl, xys, 3 * n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  st = run_paths(ctx, scene, cam, params, n, dl, nullptr, DebugOut{dL, dc, dr}, nullptr);
+  GYT_CK(ctx, cudaMemset(dm, 0, 3 * n * sizeof(unsigned long long)));
+  st = run_paths(ctx, scene, cam, params, n, dl, nullptr, DebugOut{dL, dc, dm, dm + n, dm + 2 * n}, nullptr);
   if (st) return st;
   if (L_out) GYT_CK(ctx, cudaMemcpy(L_out, dL, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
   if (cursor_out) GYT_CK(ctx, cudaMemcpy(cursor_out, dc, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  if (rr_out) GYT_CK(ctx, cudaMemcpy(rr_out, dr, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (rr_out) GYT_CK(ctx, cudaMemcpy(rr_out, dm, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (occ_out) GYT_CK(ctx, cudaMemcpy(occ_out, dm + n, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (mis_out) GYT_CK(ctx, cudaMemcpy(mis_out, dm + 2 * n, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return GYT_OK;
 }
 

@@ -147,13 +147,16 @@ int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCam
 
 /* Traces an explicit list of camera paths (xys: n triplets x, y, s; host)
  * and returns per-path radiance (L_out: n*3 floats), the number of Sobol'
- * dimensions each path used (cursor_out) and which bounces drew a Russian
- * roulette number (rr_mask_out, bit i = bounce i). Any output may be NULL.
- * This is PathTracing::Li for the samples TiledIntegrator::Render would make
- * (integrator/TiledIntegrator.cpp:40-47). */
+ * dimensions each path used (cursor_out) and its discrete decisions for a
+ * replay, bit i = bounce i < 64: a Russian roulette number was drawn
+ * (rr_mask_out), the next-event shadow ray was occluded (occ_mask_out), the
+ * BSDF-sampled MIS ray reached the sampled light (mis_mask_out). Any output
+ * may be NULL. This is PathTracing::Li for the samples
+ * TiledIntegrator::Render would make (integrator/TiledIntegrator.cpp:40-47). */
 int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
                         const GytRenderParams* params, uint64_t n, const uint32_t* xys,
-                        float* L_out, uint32_t* cursor_out, uint64_t* rr_mask_out);
+                        float* L_out, uint32_t* cursor_out, uint64_t* rr_mask_out,
+                        uint64_t* occ_mask_out, uint64_t* mis_mask_out);
 
 /* Closest-hit (any_hit = 0) or occlusion (any_hit = 1) queries for n rays
  * (host rays: 7 floats each = origin, direction, tmax; tmin = 0). Outputs

@@ -69,7 +69,9 @@ def lib():
         L.gyo_any_hit.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
         L.gyo_paths.argtypes = [ctypes.c_void_p, ctypes.POINTER(CameraIn), ctypes.POINTER(ParamsIn), ctypes.c_int64,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
-                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.gyo_set_trace.argtypes = [ctypes.c_int]
         L.gyo_render.argtypes = [ctypes.c_void_p, ctypes.POINTER(CameraIn), ctypes.POINTER(ParamsIn),
                                  ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
         L.gyo_bsdf.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -145,19 +147,24 @@ class OracleScene:
         lib().gyo_any_hit(self.handle, rays.shape[0], _p(rays), _p(out))
         return out.astype(bool)
 
-    def paths(self, x, y, s, precision=64, threads=0, camera=None, params=None, force_rr=None, return_rr=False):
-        """Radiance of paths (x, y, s). ``force_rr`` replays recorded roulette
-        draws (bit i = a roulette number was drawn at bounce i)."""
+    def paths(self, x, y, s, precision=64, threads=0, camera=None, params=None, force_rr=None, return_rr=False,
+              force_occ=None, force_mis=None, return_decisions=False):
+        """Radiance of paths (x, y, s). ``force_rr``/``force_occ``/``force_mis``
+        replay recorded decisions (bit i = bounce i): a roulette number was
+        drawn, the shadow ray was occluded, the MIS ray reached the light."""
         x, y, s = (np.ascontiguousarray(np.asarray(a, np.uint32)) for a in (x, y, s))
         n = x.shape[0]
         L = np.empty((n, 3), np.float64)
         cur = np.empty(n, np.int32)
-        rr = np.empty(n, np.uint64)
-        fr = None if force_rr is None else np.ascontiguousarray(np.asarray(force_rr, np.uint64))
+        rr, occ, mis = (np.empty(n, np.uint64) for _ in range(3))
+        f = [None if a is None else np.ascontiguousarray(np.asarray(a, np.uint64)) for a in (force_rr, force_occ,
+                                                                                           force_mis)]
         c = camera_in(camera or self.sd.camera)
         p = params_in(params or self.sd.params)
         lib().gyo_paths(self.handle, ctypes.byref(c), ctypes.byref(p), n, _p(x), _p(y), _p(s), precision, _p(L),
-                        _p(cur), threads, _p(fr), _p(rr))
+                        _p(cur), threads, _p(f[0]), _p(rr), _p(f[1]), _p(f[2]), _p(occ), _p(mis))
+        if return_decisions:
+            return L, cur, rr, occ, mis
         return (L, cur, rr) if return_rr else (L, cur)
 
     def render(self, rows=None, precision=64, threads=0, camera=None, params=None):

@@ -16,6 +16,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <thread>
@@ -24,6 +25,7 @@
 #include "../../gyunity_b200/_gen/sobol_tables.h"
 
 namespace gyo {
+int g_trace = 0;  // debugging aid: per-bounce trace of gyo_paths on stderr
 
 // ------------------------------------------------------------------ math ---
 template <typename T> struct V3 {
@@ -556,7 +558,13 @@ template <typename T> bool occluded(const Scene<T>& sc, const Ray<T>& r) {
       if (nd.left < 0) {
         for (int k = 0; k < nd.count; ++k) {
           T t, b1, b2;
-          if (tri_intersect(sc.tris[sc.order[nd.start + k]], r, &t, &b1, &b2)) return true;
+          if (tri_intersect(sc.tris[sc.order[nd.start + k]], r, &t, &b1, &b2)) {
+            if (g_trace)
+              std::fprintf(stderr, "      occluder tri %u t %.9g tmax %.9g o (%.9g %.9g %.9g) d (%.9g %.9g %.9g)\n",
+                           sc.order[nd.start + k], (double)t, (double)r.tmax, (double)r.o.x, (double)r.o.y,
+                           (double)r.o.z, (double)r.d.x, (double)r.d.y, (double)r.d.z);
+            return true;
+          }
         }
       } else {
         stack[sp++] = nd.right;
@@ -961,9 +969,19 @@ template <typename T> T tri_light_pdf(const Tri<T>& tr, const Isect<T>& it, cons
   return pdf;
 }
 
+// Discrete decisions of one path for a replay (bit i = bounce i < 64).
+struct Replay {
+  int bounce = 0;
+  const uint64_t* force_occ = nullptr;  // shadow ray occluded
+  const uint64_t* force_mis = nullptr;  // MIS ray reached the sampled light
+  uint64_t occ = 0, mis = 0;            // decisions taken
+  bool forced(const uint64_t* m) const { return m && bounce < 64; }
+  bool bit(const uint64_t* m) const { return ((*m) >> bounce) & 1ull; }
+};
+
 // Integrator::DirectIllumination (integrator/Integrator.cpp:9-107), surfaces only
 template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const Bsdf<T>& bsdf, T uLight,
-                                   T u0, T u1, T v0, T v1, T v2) {
+                                   T u0, T u1, T v0, T v1, T v2, Replay* rp) {
   T lightSel;
   int li = sc.light_power.sample_discrete(uLight, &lightSel);
   if (lightSel == 0) return V3<T>();
@@ -1010,7 +1028,11 @@ template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const
       T cosT = std::abs(dot(is.n, wi));
       if (!f.zero()) {
         Ray<T> sr = spawn_to(is, lpos, lerr, labs);
-        if (occluded(sc, sr)) Li = V3<T>();
+        bool occ = rp->forced(rp->force_occ) ? rp->bit(rp->force_occ) : occluded(sc, sr);
+        if (occ) {
+          Li = V3<T>();
+          if (rp->bounce < 64) rp->occ |= 1ull << rp->bounce;
+        }
         w1 = power_heuristic(pdf, spdf);
         L1 = Li * f * cosT / pdf;
       }
@@ -1030,18 +1052,40 @@ template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const
         Ray<T> r = spawn_ray(is, wi);
         Isect<T> h;
         int prim = closest_hit(sc, r, &h);
-        if (prim >= 0) {
-          if (ltri >= 0 && prim_light(sc, prim) == li) {
+        bool reach = ltri >= 0 ? (prim >= 0 && prim_light(sc, prim) == li) : prim < 0;
+        if (rp->forced(rp->force_mis)) {
+          bool want = rp->bit(rp->force_mis);
+          if (want && !reach && ltri >= 0) {
+            // the replayed path reached the light: take the hit on the light triangle itself
+            Ray<T> rl = spawn_ray(is, wi);
+            T t, b1, b2;
+            if (tri_intersect(sc.tris[ltri], rl, &t, &b1, &b2)) {
+              h = Isect<T>();
+              h.b1 = b1; h.b2 = b2; h.prim = ltri;
+              r = rl;
+              prim = ltri;
+            } else {
+              want = false;
+            }
+          }
+          reach = want;
+        }
+        if (reach && rp->bounce < 64) rp->mis |= 1ull << rp->bounce;
+        if (reach) {
+          if (ltri >= 0) {
             complete_hit(sc, r, &h);
             V3<T> e = dot(h.n, -wi) > 0 ? sc.emission[li] : V3<T>();
             L2 = e * f * cosT / pdf;
+          } else {
+            L2 = sc.env.lookup(wi) * f * cosT / pdf;
           }
-        } else if (ltri < 0) {
-          L2 = sc.env.lookup(wi) * f * cosT / pdf;
         }
       }
     }
   }
+  if (g_trace)
+    std::fprintf(stderr, "    light %d sel %.9g L1 %.9g w1 %.9g L2 %.9g w2 %.9g\n", li, (double)lightSel, (double)L1.x,
+                 (double)w1, (double)L2.x, (double)w2);
   return (L1 * w1 + L2 * w2) / lightSel;
 }
 
@@ -1065,7 +1109,10 @@ template <typename T> Ray<T> camera_ray(const CamT<T>& c, T px, T py) {
 template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, const CameraIn& ci,
                                        const ParamsIn& pr, uint32_t x, uint32_t y, uint32_t s, int* cursor_out,
                                        float* u_out = nullptr, float* v_out = nullptr,
-                                       const uint64_t* force_rr = nullptr, uint64_t* rr_out = nullptr) {
+                                       const uint64_t* force_rr = nullptr, uint64_t* rr_out = nullptr,
+                                       Replay* rp_in = nullptr) {
+  Replay rp_local;
+  Replay* rp = rp_in ? rp_in : &rp_local;
   uint32_t m = log2_pow2_res(ci.res_x, ci.res_y);
   Rand rnd{enum_index(m, s, x, y)};
   float res = (float)(1u << m);
@@ -1095,7 +1142,13 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
       T vz = rnd.next(), vy = rnd.next(), vx = rnd.next();
       T uy = rnd.next(), ux = rnd.next();
       T ul = rnd.next();
-      L = L + tp * direct(sc, is, bsdf, ul, ux, uy, vx, vy, vz);
+      rp->bounce = i;
+      V3<T> di = direct(sc, is, bsdf, ul, ux, uy, vx, vy, vz, rp);
+      if (g_trace)
+        std::fprintf(stderr, "  bounce %d prim %d pos (%.9g %.9g %.9g) DI (%.9g %.9g %.9g) tp %.9g\n", i, prim,
+                     (double)is.pos.x, (double)is.pos.y, (double)is.pos.z, (double)di.x, (double)di.y, (double)di.z,
+                     (double)tp.x);
+      L = L + tp * di;
     }
     T rz = rnd.next(), ry = rnd.next(), rx = rnd.next();  // PT.cpp:47, same order
     V3<T> wi;
@@ -1287,15 +1340,21 @@ template <typename Fn> void parallel_rows(int n, int threads, Fn fn) {
 
 template <typename T> void paths_impl(Handle* h, const CameraIn* c, const ParamsIn* p, int64_t n, const uint32_t* x,
                                       const uint32_t* y, const uint32_t* s, double* L, int32_t* cursor, int threads,
-                                      const uint64_t* force_rr, uint64_t* rr_out) {
+                                      const uint64_t* force_rr, uint64_t* rr_out, const uint64_t* force_occ,
+                                      const uint64_t* force_mis, uint64_t* occ_out, uint64_t* mis_out) {
   Scene<T>* sc = get<T>(h);
   CamT<T> cam = make_cam<T>(*c);
   int chunks = (int)((n + 255) / 256);
   parallel_rows(chunks, threads, [&](int ch) {
     for (int64_t i = (int64_t)ch * 256; i < std::min<int64_t>(n, (int64_t)ch * 256 + 256); ++i) {
       int cur = 0;
+      Replay rp;
+      rp.force_occ = force_occ ? &force_occ[i] : nullptr;
+      rp.force_mis = force_mis ? &force_mis[i] : nullptr;
       V3<T> l = trace_path(*sc, cam, *c, *p, x[i], y[i], s[i], &cur, nullptr, nullptr,
-                           force_rr ? &force_rr[i] : nullptr, rr_out ? &rr_out[i] : nullptr);
+                           force_rr ? &force_rr[i] : nullptr, rr_out ? &rr_out[i] : nullptr, &rp);
+      if (occ_out) occ_out[i] = rp.occ;
+      if (mis_out) mis_out[i] = rp.mis;
       L[3 * i] = (double)l.x; L[3 * i + 1] = (double)l.y; L[3 * i + 2] = (double)l.z;
       if (cursor) cursor[i] = cur;
     }
@@ -1365,6 +1424,8 @@ extern "C" {
 
 const char* gyo_tables_digest() { return GYT_TABLES_DIGEST; }
 
+void gyo_set_trace(int on) { g_trace = on; }
+
 float gyo_sobol(uint32_t dim, uint64_t index) { return sobol_sample(index, dim); }
 
 uint64_t gyo_enum_index(uint32_t res_x, uint32_t res_y, uint32_t s, uint32_t x, uint32_t y) {
@@ -1424,12 +1485,19 @@ int gyo_any_hit(void* p, int64_t n, const float* rays, int32_t* out) {
 
 // force_rr (optional): per-path roulette-draw masks to replay; rr_out
 // (optional) receives the masks this run produced.
+// force_occ / force_mis (optional) replay recorded shadow-occlusion and
+// MIS-hit decisions; occ_out / mis_out receive the decisions taken.
 int gyo_paths(void* p, const CameraIn* c, const ParamsIn* pr, int64_t n, const uint32_t* x, const uint32_t* y,
               const uint32_t* s, int precision, double* L, int32_t* cursor, int threads, const uint64_t* force_rr,
-              uint64_t* rr_out) {
+              uint64_t* rr_out, const uint64_t* force_occ, const uint64_t* force_mis, uint64_t* occ_out,
+              uint64_t* mis_out) {
   auto* h = (Handle*)p;
-  if (precision == 64) paths_impl<double>(h, c, pr, n, x, y, s, L, cursor, threads, force_rr, rr_out);
-  else paths_impl<float>(h, c, pr, n, x, y, s, L, cursor, threads, force_rr, rr_out);
+  if (precision == 64)
+    paths_impl<double>(h, c, pr, n, x, y, s, L, cursor, threads, force_rr, rr_out, force_occ, force_mis, occ_out,
+                       mis_out);
+  else
+    paths_impl<float>(h, c, pr, n, x, y, s, L, cursor, threads, force_rr, rr_out, force_occ, force_mis, occ_out,
+                      mis_out);
   return 0;
 }
 

@@ -342,6 +342,7 @@ int cmd_paths(int argc, char** argv) {
 int cmd_render(int argc, char** argv) {
   LoadedScene ls = load_scene(argv[2]);
   int rows = argc > 4 ? std::atoi(argv[4]) : ls.resY;
+  if (rows <= 0 || rows > ls.resY) rows = ls.resY;
   if (argc > 5) ls.spp = std::atoi(argv[5]);
   std::shared_ptr<Sampler> sampler;
   std::shared_ptr<SamplerEnum> senum;

@@ -116,7 +116,7 @@ def ref_render(tmp, scene_path, rows=None, spp=None, threads=None):
     b = os.path.join(tmp, "render.bin")
     args = ["render", scene_path, b]
     if rows is not None or spp is not None:
-        args.append(rows if rows is not None else 1 << 30)
+        args.append(rows if rows is not None else 0)
     if spp is not None:
         args.append(spp)
     out = run(*args, env={"GYREF_THREADS": str(threads)} if threads else None)

@@ -129,6 +129,13 @@ def main():
     img, info = io.ref_render(tmp, path)
     np.savez_compressed(os.path.join(HERE, "image_cornell_64x64_4spp.npz"), film=img)
 
+    # a higher-spp render for the statistical image comparison
+    sd = scenes.cornell_box(res=128, spp=16)
+    path = os.path.join(tmp, "img2.gyts")
+    io.write_scene(path, sd)
+    img, info = io.ref_render(tmp, path)
+    np.savez_compressed(os.path.join(HERE, "image_cornell_128x128_16spp.npz"), film=img)
+
     # BxDF tables in the local frame
     cases = bsdf_cases(rng)
     np.savez_compressed(os.path.join(HERE, "bsdf.npz"), cases=cases.view(np.uint8), out=io.ref_bsdf(tmp, cases))

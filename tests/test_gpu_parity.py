@@ -75,12 +75,19 @@ def test_closest_hit_ids_match_oracle_on_large_mesh(ctx):
 
 
 def _replay(sd, xys, ctx):
+    """GPU paths and the FP64 oracle's replay of the same paths: same Sobol'
+    dimensions and the GPU's discrete decisions (roulette draws, shadow
+    occlusion, MIS hits). Returns relative error, same-dimension flags and the
+    fraction of decisions the FP64 oracle would have taken differently."""
     sc = g.Scene(sd, ctx)
-    L, cur, rr = sc.trace_paths(xys)
+    L, cur, rr, occ, mis = sc.trace_paths(xys, decisions=True)
     o = orc.OracleScene(sd)
-    Lo, co = o.paths(xys[:, 0], xys[:, 1], xys[:, 2], precision=64, force_rr=rr)
+    x, y, s = xys[:, 0], xys[:, 1], xys[:, 2]
+    Lo, co = o.paths(x, y, s, precision=64, force_rr=rr, force_occ=occ, force_mis=mis)
+    _, _, _, occ_own, mis_own = o.paths(x, y, s, precision=64, force_rr=rr, return_decisions=True)
     rel = np.abs(L.astype(np.float64) - Lo).max(1) / np.maximum(np.abs(Lo).max(1), 1e-3)
-    return rel, cur == co, L
+    flips = float(((occ_own != occ) | (mis_own != mis)).mean())
+    return rel, cur == co, flips
 
 
 @pytest.mark.parametrize("name", ["cornell_nospheres", "cornell", "mixed"])
@@ -88,21 +95,27 @@ def test_per_path_radiance_matches_fp64_replay(ctx, name):
     sd = {"cornell_nospheres": scenes.cornell_box(spheres=False), "cornell": scenes.cornell_box(),
           "mixed": scenes.mixed_materials_box(level=3, res=64)}[name]
     xys = golden("paths_%s.npz" % name)["xys"]
-    rel, same_cursor, _ = _replay(sd, xys, ctx)
-    ok = rel < 1e-4  # tolerance: FP32 path vs FP64 replay of the same Sobol' dimensions
-    print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean())
+    rel, same_cursor, flips = _replay(sd, xys, ctx)
+    ok = rel < 1e-4  # tolerance: FP32 path vs FP64 replay of the same path, relative to max(|L|, 1e-3)
+    print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean(), "decision flips vs FP64:", flips)
     assert same_cursor.mean() > 0.995
     assert ok.mean() > 0.99
+    # shadow rays end on the light surface (the reference's RayEps cancels
+    # ShadowRayEps), so FP32 occlusion by the light itself is a rounding coin
+    # flip; bounded here, replayed above
+    assert flips < 0.05
 
 
 def test_per_path_radiance_matches_reference(ctx):
+    # against the FP32 reference itself: same dimensions for nearly all paths;
+    # radiance agrees except for the light self-occlusion coin flips
     gd = golden("paths_cornell_nospheres.npz")
     sc = g.Scene(scenes.cornell_box(spheres=False), ctx)
     L, cur, _ = sc.trace_paths(gd["xys"])
     ref = gd["L"].astype(np.float64)
     rel = np.abs(L - ref).max(1) / np.maximum(np.abs(ref).max(1), 1e-3)
     assert (cur == gd["cursor"]).mean() > 0.995
-    assert (rel < 1e-4).mean() > 0.99
+    assert (rel < 1e-4).mean() > 0.95
 
 
 def test_render_matches_reference_image(ctx):
@@ -116,6 +129,26 @@ def test_render_matches_reference_image(ctx):
     img = film.image.astype(np.float64)
     rmse = np.sqrt(np.mean((img - ref) ** 2))
     print("image RMSE vs reference:", rmse)
+    assert rmse < 0.02 * np.sqrt(np.mean(ref ** 2))
+
+
+def test_image_statistics_match_reference(ctx):
+    # 128x128 at 16 spp against the reference's own TiledIntegrator::Render:
+    # the same Sobol' points, so the images agree closely; the global mean
+    # checks that rounding-dependent events (light self-occlusion, roulette)
+    # happen at the reference's rate.
+    gd = golden("image_cornell_128x128_16spp.npz")["film"].reshape(128, 128, 4).astype(np.float64)
+    sd = scenes.cornell_box(res=128, spp=16)
+    sc = g.Scene(sd, ctx)
+    film = g.Film(128, 128)
+    cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    g.GpuPathTracing(16, 8, 3).Render(sc, cam)
+    ref = gd[..., :3] / gd[..., 3:]
+    img = film.image.astype(np.float64)
+    rel_mean = abs(img.mean() - ref.mean()) / ref.mean()
+    rmse = np.sqrt(np.mean((img - ref) ** 2))
+    print("mean rel diff %.2e, RMSE %.4f (image RMS %.4f)" % (rel_mean, rmse, np.sqrt(np.mean(ref ** 2))))
+    assert rel_mean < 5e-3
     assert rmse < 0.02 * np.sqrt(np.mean(ref ** 2))
 
 
