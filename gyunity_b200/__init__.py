@@ -82,6 +82,15 @@ class Context:
         return {"paths": st.paths, "path_slots": st.path_slots, "iterations": st.iterations,
                 "launches": st.launches, "ms": st.ms}
 
+    def render_device_noalloc(self, scene, camera, params, d_film_ptr, paths_in_flight=_c.NOALLOC_MAX_PATHS):
+        """gyt_render_device_noalloc: the same render with the paths in flight
+        kept in the library's built-in scratch array, for callers that must
+        not allocate GPU memory during the call. Returns the status code."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        return self._lib.gyt_render_device_noalloc(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                                   ctypes.c_void_p(d_film_ptr), int(paths_in_flight))
+
     # ---- parity / debug entry points --------------------------------------
     def sobol(self, dims, indices):
         """sobol::sample (sampler/Sobol.h:46-61) for (dimension, index) pairs."""

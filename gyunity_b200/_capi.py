@@ -19,7 +19,11 @@ STATUS = {0: "GYT_OK", 1: "GYT_ERR_INVALID", 2: "GYT_ERR_CUDA", 3: "GYT_ERR_OUT_
 EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_context_set_capacity",
            "gyt_context_set_profile", "gyt_profile_read",
            "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info", "gyt_render", "gyt_render_device",
-           "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world"]
+           "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world",
+           "gyt_render_device_noalloc"]
+
+# Path slots of the library's built-in scratch array (GYT_NOALLOC_MAX_PATHS in include/gyt.h).
+NOALLOC_MAX_PATHS = 32768
 
 
 class GytError(RuntimeError):
@@ -86,6 +90,7 @@ def load():
     L.gyt_render.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P]
     L.gyt_render_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P,
                                     ctypes.POINTER(GytRenderStats)]
+    L.gyt_render_device_noalloc.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, U32]
     L.gyt_trace_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P, P, P,
                                   P, P]
     L.gyt_intersect.argtypes = [P, P, U64, P, I32, P, P, P, P]

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1218,3 +1219,134 @@ int32_t gyt_camera_raster_to_world(const GytCamera* camera, double* out16) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ no-alloc variant ---
+// A render entry point for callers that must not allocate device memory while
+// rendering: applications whose GPU memory is owned by another allocator or
+// budget (a host engine's pool, a frame loop with a fixed memory plan) and
+// code that runs where cudaMalloc is not allowed. Its path pools, queues and
+// compaction counter live in the file-scope array below instead of the
+// context's lazily allocated pools.
+//
+// The array is reserved once per device when the library's module is loaded
+// on that device and held until the process exits. All calls on a device
+// share it and it keeps whatever the last call left; only the compaction
+// counter must start at zero and it is cleared every iteration. Two calls
+// whose work overlaps on the GPU (different streams or threads) race on the
+// array.
+namespace {
+
+constexpr size_t kNoAllocSlotBytes = 2 * (4 * sizeof(float4) + 8 + 3 * 4) + 7 * sizeof(float4);
+constexpr size_t kNoAllocAlign = 256;
+constexpr size_t align_up(size_t v) { return (v + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+// per-array rounding adds at most one alignment unit per array (25 arrays)
+constexpr size_t kNoAllocBytes = (size_t)GYT_NOALLOC_MAX_PATHS * kNoAllocSlotBytes + 32 * kNoAllocAlign;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocDevice {
+  unsigned char* base = nullptr;  // device address of g_noalloc_scratch
+  bool ready = false;
+};
+std::mutex g_noalloc_mutex;
+NoAllocDevice g_noalloc_dev[64];
+
+// Device address of the scratch array on the current device. The first call
+// on each device looks it up with cudaGetSymbolAddress (in host code the
+// array's name is only a host-side stand-in, never a device address).
+int32_t noalloc_scratch(gyt_context* ctx, unsigned char** out) {
+  int dev = ctx->device;
+  if (dev < 0 || dev >= 64) return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: device index >= 64");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(ctx, GYT_ERR_CUDA, std::string("render_device_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    d.base = (unsigned char*)p;
+    d.ready = true;
+  }
+  *out = d.base;
+  return GYT_OK;
+}
+
+template <typename T>
+T* carve(unsigned char*& cursor, size_t count) {
+  T* p = (T*)cursor;
+  cursor += align_up(count * sizeof(T));
+  return p;
+}
+
+}  // namespace
+
+extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                             const GytRenderParams* params, double* d_film, uint32_t paths_in_flight) {
+  if (!ctx || !scene || !d_film) return fail(ctx, GYT_ERR_INVALID, "render_device_noalloc: null argument");
+  if (paths_in_flight == 0 || paths_in_flight > GYT_NOALLOC_MAX_PATHS)
+    return fail(ctx, GYT_ERR_UNSUPPORTED,
+                "render_device_noalloc: paths_in_flight must be in [1, " + std::to_string(GYT_NOALLOC_MAX_PATHS) +
+                    "] (the size of the library's built-in scratch array)");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: more than 2^32 paths");
+  unsigned char* base = nullptr;
+  st = noalloc_scratch(ctx, &base);
+  if (st) return st;
+  const size_t n = paths_in_flight;
+  unsigned char* c = base;
+  PathBuf pool[2];
+  for (int b = 0; b < 2; ++b) {
+    pool[b].o = carve<float4>(c, n);
+    pool[b].d = carve<float4>(c, n);
+    pool[b].tp = carve<float4>(c, n);
+    pool[b].L = carve<float4>(c, n);
+    pool[b].sidx = carve<unsigned long long>(c, n);
+    pool[b].meta = carve<uint32_t>(c, n);
+    pool[b].pix = carve<uint32_t>(c, n);
+    pool[b].pid = carve<uint32_t>(c, n);
+  }
+  Queues q;
+  q.so = carve<float4>(c, n);
+  q.sd = carve<float4>(c, n);
+  q.sc = carve<float4>(c, n);
+  q.mo = carve<float4>(c, n);
+  q.md = carve<float4>(c, n);
+  q.mc = carve<float4>(c, n);
+  q.hit = carve<float4>(c, n);
+  uint32_t* counter = carve<uint32_t>(c, 1);
+  if ((size_t)(c - base) > kNoAllocBytes)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: scratch layout exceeds the array");
+
+  Params prm{params->spp, params->max_depth, params->rr_depth};
+  SobolTables tab = tables(ctx);
+  cudaStream_t s = ctx->stream;
+  unsigned long long generated = 0;
+  uint32_t active = 0, iters = 0, live = 0;
+  int cur = 0;
+  while (generated < total || active > 0) {
+    uint32_t n_new = (uint32_t)std::min<unsigned long long>(paths_in_flight - active, total - generated);
+    if (n_new)
+      k_generate<<<grid_for(n_new), kBlock, 0, s>>>(pool[cur], active, n_new, generated, cam, params->spp, nullptr, tab);
+    generated += n_new;
+    active += n_new;
+    k_extend<false><<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, scene->dev, q.hit, nullptr);
+    k_shade<<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, scene->dev, prm, q, tab, DebugOut{});
+    GYT_CK(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
+    k_connect<false><<<grid_for(active), kBlock, 0, s>>>(pool[cur], pool[cur ^ 1], active, scene->dev, q, d_film,
+                                                         cam.res_x, counter, DebugOut{}, nullptr);
+    GYT_CK(ctx, cudaGetLastError());
+    // pageable destination: the copy completes before cudaMemcpyAsync returns
+    GYT_CK(ctx, cudaMemcpyAsync(&live, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaStreamSynchronize(s));
+    active = live;
+    cur ^= 1;
+    if (++iters > 10000000) return fail(ctx, GYT_ERR_WATCHDOG, "render_device_noalloc: iteration cap reached");
+  }
+  return GYT_OK;
+}

@@ -173,6 +173,25 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
 
+/* Render without allocating: the same render as gyt_render_device, for
+ * callers that must not allocate GPU memory during the call (an engine that
+ * owns all device memory through its own allocator or a fixed budget, or code
+ * running where cudaMalloc is not allowed). The paths in flight, their queues
+ * and the compaction counter live in a scratch array built into the library
+ * (GYT_NOALLOC_MAX_PATHS path slots, about 9 MB, reserved on every device that
+ * loads the library until the process exits) instead of the context's pools,
+ * which are allocated on first use. paths_in_flight (1..GYT_NOALLOC_MAX_PATHS)
+ * sets how many paths share it; larger values are rejected with
+ * GYT_ERR_UNSUPPORTED. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls on a device share the array: calls whose GPU work
+ * overlaps (other streams or threads) race on it. The scene, the Sobol' tables
+ * of the context and the caller's device film (accumulated, not cleared) are
+ * the inputs and output. No counterpart in the reference. */
+#define GYT_NOALLOC_MAX_PATHS 32768u
+int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                  const GytRenderParams* params, double* d_film, uint32_t paths_in_flight);
+
 /* ProjectiveCamera::RasterToWorld (camera/Camera.cpp:38) as a row-major 4x4. */
 int32_t gyt_camera_raster_to_world(const GytCamera* camera, double* out16);
 
