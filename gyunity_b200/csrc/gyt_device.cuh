@@ -66,7 +66,40 @@ struct SobolTables {
   const uint32_t* matrices;   // 1024 * 52 (+ padding) generator columns
   const uint64_t* vdc;        // m levels * 52
   const uint64_t* vdc_inv;    // m levels * 52
+  const uint32_t* bits;       // transposed: column b of every dimension, kSobolRow per b
 };
+
+// Transposed generator table: row b holds column b of dimensions 0..1039 (the
+// last 16 are padding), so consecutive dimensions of one column are adjacent.
+// Column b >= 52 of dimension d is column b - 52 of dimension d + 1, which is
+// what sobol::sample reads for indices of 52 bits or more.
+constexpr int kSobolRow = 1040;
+
+// Ten consecutive dimensions [c, c + 10) of one Sobol' point at once: one pass
+// over the set bits of the index, four 128-bit loads per bit. Same values as
+// ten sobol_sample calls (RandomStateSequence's >= 1 -> 0 rule applied).
+GYT_D void sobol10(const uint32_t* __restrict__ bits, uint64_t index, uint32_t c, float out[10]) {
+  const uint32_t base = c & ~3u, sh = c & 3u;
+  uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0, a2 = a0, a3 = a0;
+  while (index) {
+    int b = __ffsll((long long)index) - 1;
+    const uint4* row = (const uint4*)(bits + (size_t)b * kSobolRow + base);
+    uint4 v0 = __ldg(row), v1 = __ldg(row + 1), v2 = __ldg(row + 2), v3 = __ldg(row + 3);
+    a0.x ^= v0.x; a0.y ^= v0.y; a0.z ^= v0.z; a0.w ^= v0.w;
+    a1.x ^= v1.x; a1.y ^= v1.y; a1.z ^= v1.z; a1.w ^= v1.w;
+    a2.x ^= v2.x; a2.y ^= v2.y; a2.z ^= v2.z; a2.w ^= v2.w;
+    a3.x ^= v3.x; a3.y ^= v3.y; a3.z ^= v3.z; a3.w ^= v3.w;
+    index &= index - 1;
+  }
+  const uint32_t acc[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                            a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    uint32_t r = sh == 0 ? acc[k] : (sh == 1 ? acc[k + 1] : (sh == 2 ? acc[k + 2] : acc[k + 3]));
+    float f = __fmul_rn(__uint2float_rn(r), 2.3283064365386963e-10f);
+    out[k] = f >= 1.f ? 0.f : f;
+  }
+}
 
 // sobol::sample (sampler/Sobol.h:46-61): XOR of the columns selected by the
 // set bits of the index, then float(result) * 2^-32 (both steps exact here).

@@ -39,21 +39,22 @@ namespace {
 
 struct DevScene {
   const float4* nodes;        // binary BVH, 4 float4 per node
-  const float4* tris;         // leaf-ordered triangles: (p0, id), (p1, -), (p2, -)
-  const float* V;             // vertices (original order)
-  const float* N;             // per-vertex normals or null
-  const uint32_t* I;          // indices
-  const int2* info;           // per triangle: material, light index (-1 none)
+  const float4* tris;         // leaf order: (p0, original id), (p1, -), (p2, -)
+  const float4* tnrm;         // leaf order: (n0, material), (n1, light index or -1), (n2, -)
   const float4* spheres;
   const uint32_t* sphere_mat;
   const float* mparams;
   const uint32_t* mtypes;
-  const float4* lights;       // per light: emission rgb, triangle id as int bits (-1 env)
+  const float4* ltab;         // kLightRec float4 per light (see light record below)
   const float* lcdf;          // n_lights + 1
   const float* lfunc;         // n_lights
   float lfunc_int;
   int n_lights, n_tris, n_spheres;
 };
+
+// Light record (kLightRec float4): (p0, Le.r) (p1, Le.g) (p2, Le.b)
+// (n0, area) (n1, leaf index) (n2, original id) (face normal, -).
+constexpr int kLightRec = 7;
 
 struct PathBuf {
   float4* o;      // origin
@@ -103,7 +104,8 @@ GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive
 
 // ------------------------------------------------------------ traversal ---
 // Closest hit (ANY = false) or occlusion (ANY = true) over the BVH and the
-// spheres. Returns the primitive id (triangles first, then spheres), or -1.
+// spheres. Returns the triangle's leaf position (< n_tris; the original id is
+// in tris[3k].w), n_tris + sphere index, or -1.
 // tmax is updated to the hit distance; spheres report the distance along the
 // re-made object ray of Sphere::Intersect (shape/Sphere.h:35).
 struct TraceCount {
@@ -162,7 +164,7 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
           float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
           float th, u, v;
           if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
-            prim = __float_as_int(t0.w);
+            prim = (int)(first + k);
             if (ANY) return prim;
             tmax = th;
             b1 = u;
@@ -187,20 +189,37 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
   return prim;
 }
 
-GYT_D void load_tri(const DevScene& s, int t, float3* p0, float3* p1, float3* p2, float3* n0, float3* n1, float3* n2,
-                    float3* face) {
-  uint32_t i0 = __ldg(s.I + 3 * t), i1 = __ldg(s.I + 3 * t + 1), i2 = __ldg(s.I + 3 * t + 2);
-  *p0 = mk(__ldg(s.V + 3 * i0), __ldg(s.V + 3 * i0 + 1), __ldg(s.V + 3 * i0 + 2));
-  *p1 = mk(__ldg(s.V + 3 * i1), __ldg(s.V + 3 * i1 + 1), __ldg(s.V + 3 * i1 + 2));
-  *p2 = mk(__ldg(s.V + 3 * i2), __ldg(s.V + 3 * i2 + 1), __ldg(s.V + 3 * i2 + 2));
-  *face = norm(cross(*p1 - *p0, *p2 - *p0));  // Triangle ctor (shape/Triangle.h:52)
-  if (s.N) {
-    *n0 = mk(__ldg(s.N + 3 * i0), __ldg(s.N + 3 * i0 + 1), __ldg(s.N + 3 * i0 + 2));
-    *n1 = mk(__ldg(s.N + 3 * i1), __ldg(s.N + 3 * i1 + 1), __ldg(s.N + 3 * i1 + 2));
-    *n2 = mk(__ldg(s.N + 3 * i2), __ldg(s.N + 3 * i2 + 1), __ldg(s.N + 3 * i2 + 2));
-  } else {
-    *n0 = *n1 = *n2 = *face;
-  }
+// Hit triangle k in leaf order: positions, shading normals, face normal
+// (Triangle ctor, shape/Triangle.h:52), material and light index.
+GYT_D void load_leaf_tri(const DevScene& s, int k, float3* p0, float3* p1, float3* p2, float3* n0, float3* n1,
+                         float3* n2, float3* face, int* mat, int* light) {
+  const float4* t = s.tris + 3 * k;
+  const float4* n = s.tnrm + 3 * k;
+  float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+  float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+  *p0 = f3(a); *p1 = f3(b); *p2 = f3(c);
+  *n0 = f3(na); *n1 = f3(nb); *n2 = f3(nc);
+  *face = norm(cross(*p1 - *p0, *p2 - *p0));
+  *mat = __float_as_int(na.w);
+  *light = __float_as_int(nb.w);
+}
+
+struct LightTri {
+  float3 p0, p1, p2, n0, n1, n2, face, Le;
+  float area;
+};
+
+GYT_D LightTri load_light(const DevScene& s, int li) {
+  const float4* r = s.ltab + kLightRec * li;
+  float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3), e = __ldg(r + 4), f = __ldg(r + 5),
+         g = __ldg(r + 6);
+  LightTri l;
+  l.p0 = f3(a); l.p1 = f3(b); l.p2 = f3(c);
+  l.Le = mk(a.w, b.w, c.w);
+  l.n0 = f3(d); l.n1 = f3(e); l.n2 = f3(f);
+  l.area = d.w;
+  l.face = f3(g);
+  return l;
 }
 
 // Distribution1D::SampleDiscrete over light powers (visual/Sampling.h:86-97,
@@ -219,17 +238,14 @@ GYT_D int sample_light(const DevScene& s, float u, float* pdf) {
 
 // Shape::Pdf for a triangle light (shape/Shape.h:34-47): re-intersect the
 // light from the shading point along wi.
-GYT_D float tri_light_pdf(const DevScene& s, int t, const Hit& h, float3 o, float3 wi) {
-  float3 p0, p1, p2, n0, n1, n2, face;
-  load_tri(s, t, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+GYT_D float tri_light_pdf(const LightTri& l, const Hit& h, float3 o, float3 wi) {
   WtRay wr = wt_setup(o, wi);
   float th, b1, b2;
-  if (!wt_intersect(wr, p0, p1, p2, __int_as_float(0x7f800000), &th, &b1, &b2)) return 0.f;
+  if (!wt_intersect(wr, l.p0, l.p1, l.p2, __int_as_float(0x7f800000), &th, &b1, &b2)) return 0.f;
   Hit lp;
-  tri_hit(p0, p1, p2, n0, n1, n2, face, b1, b2, o, wi, &lp);
+  tri_hit(l.p0, l.p1, l.p2, l.n0, l.n1, l.n2, l.face, b1, b2, o, wi, &lp);
   float3 dd = lp.pos - h.pos;
-  float area = 0.5f * length(cross(p1 - p0, p2 - p0));
-  float pdf = dot(dd, dd) / (fabsf(dot(lp.n, -wi)) * area);
+  float pdf = dot(dd, dd) / (fabsf(dot(lp.n, -wi)) * l.area);
   if (isinf(pdf)) return 0.f;
   return pdf;
 }
@@ -319,11 +335,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
     int light = -1;
     if (prim < s.n_tris) {
       float3 p0, p1, p2, n0, n1, n2, face;
-      load_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+      int m;
+      load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, &light);
       tri_hit(p0, p1, p2, n0, n1, n2, face, h4.y, h4.z, ro, rd, &h);
-      int2 inf = __ldg(s.info + prim);
-      mat = (uint32_t)inf.x;
-      light = inf.y;
+      mat = (uint32_t)m;
     } else {
       int k = prim - s.n_tris;
       Ray r = sphere_object_ray(ro, rd, __int_as_float(0x7f800000), 0.f);
@@ -333,31 +348,34 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
     Bsdf bsdf;
     bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
     bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
-    if ((depth == 0 || delta) && light >= 0) {
-      float4 le = __ldg(s.lights + light);
-      if (dot(h.n, h.wo) > 0.f) L = L + tp * f3(le);  // AreaLight::Emission (AreaLight.h:40-43)
+    // the ten dimensions this bounce can use: six for direct lighting (PT.cpp:38
+    // arguments in GCC's right-to-left order: v.z v.y v.x u.y u.x uLight), three
+    // for the BSDF sample (PT.cpp:47, again z y x) and one for roulette
+    float u10[10];
+    sobol10(tab.bits, rng.index, rng.cursor, u10);
+    const bool emit = (depth == 0 || delta) && light >= 0;
+    if (emit) {
+      LightTri l = load_light(s, light);
+      if (dot(h.n, h.wo) > 0.f) L = L + tp * l.Le;  // AreaLight::Emission (AreaLight.h:40-43)
     } else {
-      // PT.cpp:38 arguments in GCC's right-to-left order: v.z v.y v.x u.y u.x uLight
-      float vz = rng.next(tab.matrices), vy = rng.next(tab.matrices), vx = rng.next(tab.matrices);
-      float uy = rng.next(tab.matrices), ux = rng.next(tab.matrices);
-      float ul = rng.next(tab.matrices);
+      float vz = u10[0], vy = u10[1], vx = u10[2];
+      float uy = u10[3], ux = u10[4];
+      float ul = u10[5];
+      rng.cursor += 6;
       float lsel = 0.f;
       int li = s.n_lights > 0 ? sample_light(s, ul, &lsel) : 0;
       if (lsel > 0.f) {
-        float4 le4 = __ldg(s.lights + li);
-        int ltri = __float_as_int(le4.w);
-        float3 Le = f3(le4);
-        if (ltri >= 0) {
+        LightTri l = load_light(s, li);
+        float3 Le = l.Le;
+        {
           // light sample: AreaLight::Sample_Li -> Shape::Sample -> Triangle::Sample
-          float3 p0, p1, p2, n0, n1, n2, face;
-          load_tri(s, ltri, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+          const float3 p0 = l.p0, p1 = l.p1, p2 = l.p2, n0 = l.n0, n1 = l.n1, n2 = l.n2, face = l.face;
           float su0 = sqrtf(ux);
           float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
           float3 lpos = p0 * bb0 + p1 * bb1 + p2 * bb2;
           float3 ln = n0 * bb0 + n1 * bb1 + n2 * bb2;
           float3 lerr = (vabs(p0 * bb0) + vabs(p1 * bb1) + vabs(p2 * bb2)) * gammaf(6);
-          float area = 0.5f * length(cross(p1 - p0, p2 - p0));
-          float pdf = 1.f / area;
+          float pdf = 1.f / l.area;
           float3 w = h.pos - lpos;
           if (length(w) == 0.f) {
             pdf = 0.f;
@@ -394,7 +412,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
           float cos2 = fabsf(dot(h.n, wi2));
           if (pdf2 != 0.f && !is_zero(f2)) {
             float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
-            float lpdf = tri_light_pdf(s, ltri, h, o2, wi2);
+            float lpdf = tri_light_pdf(l, h, o2, wi2);
             if (lpdf != 0.f) {
               float w2 = power_heuristic(pdf2, lpdf);
               q.mo[i] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
@@ -407,7 +425,9 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
       }
     }
     // continuation (PT.cpp:45-62); arguments again in right-to-left order
-    float rz = rng.next(tab.matrices), ry = rng.next(tab.matrices), rx = rng.next(tab.matrices);
+    float rz = emit ? u10[0] : u10[6], ry = emit ? u10[1] : u10[7], rx = emit ? u10[2] : u10[8];
+    const float urr = emit ? u10[3] : u10[9];
+    rng.cursor += 3;
     float3 wi;
     float pdf;
     float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
@@ -419,7 +439,8 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
       bool survive = true;
       if (p < 1.f && depth > prm.rr_depth) {
         if (dbg.rr && depth < 64) dbg.rr[cur.pid[i]] |= 1ull << depth;
-        if (rng.next(tab.matrices) < p) tp = tp / p;
+        rng.cursor += 1;
+        if (urr < p) tp = tp / p;
         else survive = false;
       }
       if (survive) {
@@ -476,12 +497,15 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
     float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
     float3 wi = f3(md);
     int prim = trace<false, COUNT>(s, f3(mo), wi, tmax, b1, b2, &cnt);
-    if (prim >= 0 && prim < s.n_tris && __ldg(s.info + prim).y == li) {
-      float3 p0, p1, p2, n0, n1, n2, face;
-      load_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face);
+    if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
+      float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
+      float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
       float b0 = 1.f - b1 - b2;
       float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
-      if (dot(ns, -wi) > 0.f) L = L + f3(mc) * f3(__ldg(s.lights + li));
+      if (dot(ns, -wi) > 0.f) {
+        const float4* r = s.ltab + kLightRec * li;
+        L = L + f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
+      }
       if (dbg.mis) {
         uint32_t b = __float_as_uint(mo.w);
         if (b < 64) dbg.mis[cur.pid[i]] |= 1ull << b;
@@ -552,6 +576,7 @@ __global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ ra
   float3 o = mk(r[0], r[1], r[2]), d = mk(r[3], r[4], r[5]);
   float tmax = r[6], b1 = 0.f, b2 = 0.f;
   int p = any ? (trace<true>(s, o, d, tmax, b1, b2) >= 0 ? 1 : 0) : trace<false>(s, o, d, tmax, b1, b2);
+  if (!any && p >= 0 && p < s.n_tris) p = __float_as_int(__ldg(s.tris + 3 * p).w);
   prim[i] = p;
   if (!any) {
     tout[i] = p >= 0 ? tmax : 0.f;
@@ -589,6 +614,7 @@ struct gyt_context {
   uint32_t* d_counter = nullptr;
   uint32_t* h_counter = nullptr;
   uint32_t* d_sobol = nullptr;
+  uint32_t* d_sobol_bits = nullptr;
   uint64_t* d_vdc = nullptr;
   uint64_t* d_vdc_inv = nullptr;
   double* d_film = nullptr;
@@ -634,7 +660,7 @@ cudaError_t dalloc(std::vector<void*>& list, T** p, size_t count) {
   return e;
 }
 
-SobolTables tables(const gyt_context* c) { return SobolTables{c->d_sobol, c->d_vdc, c->d_vdc_inv}; }
+SobolTables tables(const gyt_context* c) { return SobolTables{c->d_sobol, c->d_vdc, c->d_vdc_inv, c->d_sobol_bits}; }
 
 // ProjectiveCamera::Initialize (camera/Camera.cpp:6-59): RasterToWorld in
 // closed form, in double. Raster (x, y, z, 1) -> NDC (2x/W - 1, 1 - 2y/H, z)
@@ -828,6 +854,17 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_sobol, (sob + 64) * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(c->d_sobol, 0, (sob + 64) * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemcpy(c->d_sobol, gyt_sobol_matrices, sob * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    // transposed copy: row b = column b of every dimension (see sobol10)
+    std::vector<uint32_t> tr((size_t)64 * kSobolRow, 0u);
+    for (int b = 0; b < 64; ++b)
+      for (int dm = 0; dm < kSobolRow; ++dm) {
+        size_t flat = (size_t)dm * 52 + b;
+        tr[(size_t)b * kSobolRow + dm] = flat < sob ? gyt_sobol_matrices[flat] : 0u;
+      }
+    e = cudaMalloc((void**)&c->d_sobol_bits, tr.size() * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_sobol_bits, tr.data(), tr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc, sizeof(gyt_vdc_sobol));
   if (e == cudaSuccess) e = cudaMemcpy(c->d_vdc, gyt_vdc_sobol, sizeof(gyt_vdc_sobol), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc_inv, sizeof(gyt_vdc_sobol_inv));
@@ -852,6 +889,7 @@ void gyt_context_destroy(gyt_context* c) {
   cudaFree(c->d_counter);
   cudaFreeHost(c->h_counter);
   cudaFree(c->d_sobol);
+  cudaFree(c->d_sobol_bits);
   cudaFree(c->d_vdc);
   cudaFree(c->d_vdc_inv);
   cudaFree(c->d_film);
@@ -904,8 +942,10 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   for (uint32_t m = 0; m < d->n_materials; ++m)
     if (d->mat_type[m] > 4) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
   std::vector<int2> info(d->n_triangles);
-  std::vector<float4> lights;
+  std::vector<int> light_tris;
   std::vector<float> power;
+  const float* V = d->vertices;
+  auto vtx = [&](uint32_t i) { return mk(V[3 * i], V[3 * i + 1], V[3 * i + 2]); };
   for (uint32_t t = 0; t < d->n_triangles; ++t) {
     for (int k = 0; k < 3; ++k)
       if (d->indices[3 * t + k] >= d->n_vertices) return fail(ctx, GYT_ERR_INVALID, "scene_create: index out of range");
@@ -915,18 +955,11 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     info[t].y = -1;
     if (e >= 0) {
       if ((uint32_t)e >= d->n_emission || !d->emission) return fail(ctx, GYT_ERR_INVALID, "scene_create: emission out of range");
-      info[t].y = (int)lights.size();
+      info[t].y = (int)light_tris.size();
+      light_tris.push_back((int)t);
       const float* em = &d->emission[3 * e];
-      int tid = (int)t;
-      float w;
-      std::memcpy(&w, &tid, 4);
-      lights.push_back(make_float4(em[0], em[1], em[2], w));
-      const float* V = d->vertices;
       const uint32_t* I = &d->indices[3 * t];
-      float3 p0 = mk(V[3 * I[0]], V[3 * I[0] + 1], V[3 * I[0] + 2]);
-      float3 p1 = mk(V[3 * I[1]], V[3 * I[1] + 1], V[3 * I[1] + 2]);
-      float3 p2 = mk(V[3 * I[2]], V[3 * I[2] + 1], V[3 * I[2] + 2]);
-      float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+      float area = 0.5f * length(cross(vtx(I[1]) - vtx(I[0]), vtx(I[2]) - vtx(I[0])));
       // AreaLight::Power (light/AreaLight.h:45-48)
       power.push_back(lum(mk(em[0], em[1], em[2]) * area * kPi));
     }
@@ -950,17 +983,41 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bvh))
     return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
   if (bvh.max_depth >= (uint32_t)kStack) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
-  std::vector<float4> tris((size_t)bvh.order.size() * 3);
+  // leaf-order triangle positions and shading data
+  auto bits = [](int v) { float f; std::memcpy(&f, &v, 4); return f; };
+  std::vector<float4> tris((size_t)bvh.order.size() * 3), tnrm((size_t)bvh.order.size() * 3);
+  std::vector<int> leaf_of(d->n_triangles, -1);
   for (size_t k = 0; k < bvh.order.size(); ++k) {
     uint32_t t = bvh.order[k];
+    leaf_of[t] = (int)k;
     const uint32_t* I = &d->indices[3 * t];
-    int tid = (int)t;
-    float w;
-    std::memcpy(&w, &tid, 4);
+    float3 p[3] = {vtx(I[0]), vtx(I[1]), vtx(I[2])};
+    float3 face = norm(cross(p[1] - p[0], p[2] - p[0]));
     for (int c = 0; c < 3; ++c) {
-      const float* v = &d->vertices[3 * I[c]];
-      tris[3 * k + c] = make_float4(v[0], v[1], v[2], c == 0 ? w : 0.f);
+      tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : 0.f);
+      float3 n = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
+      float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : 0.f);
+      tnrm[3 * k + c] = make_float4(n.x, n.y, n.z, w);
     }
+  }
+  // light records: (p0, Le.r) (p1, Le.g) (p2, Le.b) (n0, area) (n1, leaf) (n2, id) (face, -)
+  std::vector<float4> ltab((size_t)nl * kLightRec);
+  for (int li = 0; li < nl; ++li) {
+    int t = light_tris[li];
+    int k = leaf_of[t];
+    const float* em = &d->emission[3 * d->tri_emission[t]];
+    float3 p0 = f3(tris[3 * k]), p1 = f3(tris[3 * k + 1]), p2 = f3(tris[3 * k + 2]);
+    float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+    float3 face = norm(cross(p1 - p0, p2 - p0));
+    float4* r = &ltab[(size_t)li * kLightRec];
+    r[0] = make_float4(p0.x, p0.y, p0.z, em[0]);
+    r[1] = make_float4(p1.x, p1.y, p1.z, em[1]);
+    r[2] = make_float4(p2.x, p2.y, p2.z, em[2]);
+    float3 n0 = f3(tnrm[3 * k]), n1 = f3(tnrm[3 * k + 1]), n2 = f3(tnrm[3 * k + 2]);
+    r[3] = make_float4(n0.x, n0.y, n0.z, area);
+    r[4] = make_float4(n1.x, n1.y, n1.z, bits(k));
+    r[5] = make_float4(n2.x, n2.y, n2.z, bits(t));
+    r[6] = make_float4(face.x, face.y, face.z, 0.f);
   }
   auto* sc = new gyt_scene();
   sc->ctx = ctx;
@@ -979,18 +1036,9 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   float4* dtris = nullptr;
   if (e == cudaSuccess) e = up(&dtris, tris.data(), tris.size());
   ds.tris = dtris;
-  float* V = nullptr;
-  if (e == cudaSuccess) e = up(&V, d->vertices, (size_t)d->n_vertices * 3);
-  ds.V = V;
-  float* N = nullptr;
-  if (e == cudaSuccess && d->normals) e = up(&N, d->normals, (size_t)d->n_vertices * 3);
-  ds.N = N;
-  uint32_t* I = nullptr;
-  if (e == cudaSuccess) e = up(&I, d->indices, (size_t)d->n_triangles * 3);
-  ds.I = I;
-  int2* inf = nullptr;
-  if (e == cudaSuccess) e = up(&inf, info.data(), info.size());
-  ds.info = inf;
+  float4* dn = nullptr;
+  if (e == cudaSuccess) e = up(&dn, tnrm.data(), tnrm.size());
+  ds.tnrm = dn;
   std::vector<float4> sph(d->n_spheres);
   for (uint32_t k = 0; k < d->n_spheres; ++k)
     sph[k] = make_float4(d->spheres[4 * k], d->spheres[4 * k + 1], d->spheres[4 * k + 2], d->spheres[4 * k + 3]);
@@ -1007,8 +1055,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   if (e == cudaSuccess) e = up(&mt, d->mat_type, d->n_materials);
   ds.mtypes = mt;
   float4* dl = nullptr;
-  if (e == cudaSuccess) e = up(&dl, lights.data(), lights.size());
-  ds.lights = dl;
+  if (e == cudaSuccess) e = up(&dl, ltab.data(), ltab.size());
+  ds.ltab = dl;
   float* dc = nullptr;
   if (e == cudaSuccess) e = up(&dc, cdf.data(), cdf.size());
   ds.lcdf = dc;
