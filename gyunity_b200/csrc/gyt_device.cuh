@@ -655,4 +655,107 @@ struct Bsdf {
 
 GYT_D float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }  // Integrator.h:11-15
 
+// ----------------------------------------------------- environment light ---
+// EnvironmentMap (light/EnvMap.h) over a lat-long RGB image with the
+// Distribution2D of ConvertImageToPdf (EnvMap.h:75-90, visual/Sampling.h:101-150).
+struct EnvDev {
+  const float4* tex;   // w*h texels in file order (row 0 = theta 0)
+  const float* ccdf;   // h rows of w+1 conditional CDF entries
+  const float* cfunc;  // h rows of w function values
+  const float* cint;   // h row integrals
+  const float* mcdf;   // h+1 marginal CDF
+  const float* mfunc;  // h marginal function values (the row integrals)
+  float mint;          // marginal integral
+  int w, h;
+  float scale, radius; // radiance scale; bounding-sphere radius (EnvLight.cpp:6-9)
+};
+
+// ImageTexture::Texel with CLAMP (texture/ImageTexture.h:48-54); the texture
+// holds the file rows bottom-up (image/ImageIO.cpp:100-114).
+GYT_D float3 env_texel(const EnvDev& e, int x, int y) {
+  x = min(max(x, 0), e.w - 1);
+  y = min(max(y, 0), e.h - 1);
+  return f3(__ldg(e.tex + (size_t)(e.h - 1 - y) * e.w + x));
+}
+
+// ImageTexture::Triangle, bilinear (ImageTexture.h:58-69)
+GYT_D float3 env_bilinear(const EnvDev& e, float u, float v) {
+  float s = __fsub_rn(__fmul_rn((float)e.w, u), 0.5f), t = __fsub_rn(__fmul_rn((float)e.h, v), 0.5f);
+  int s0 = (int)floorf(s), t0 = (int)floorf(t);
+  float ds = s - s0, dt = t - t0;
+  float3 a = env_texel(e, s0, t0) * (1.f - ds) + env_texel(e, s0 + 1, t0) * ds;
+  float3 b = env_texel(e, s0, t0 + 1) * (1.f - ds) + env_texel(e, s0 + 1, t0 + 1) * ds;
+  return a * (1.f - dt) + b * dt;
+}
+
+GYT_D float3 env_radiance(const EnvDev& e, float u, float v) {  // LookupRadiance (EnvMap.h:63-65)
+  return env_bilinear(e, u, 1.f - v) * e.scale;
+}
+
+GYT_D void env_dir_to_uv(float3 d, float* u, float* v) {  // DirToLatLong (EnvMap.h:102-116)
+  float phi = (d.x != 0.f || d.z != 0.f) ? atan2f(d.z, d.x) : 0.f;
+  float theta = acosf(d.y);
+  phi = phi < 0.f ? phi + 2.f * kPi : phi;
+  *u = phi * kInvPi * 0.5f;
+  *v = fminf(fmaxf(theta * kInvPi, 0.f), 1.f);
+}
+
+GYT_D float env_sin_theta(const EnvDev& e, float v) {  // SinTheta (EnvMap.h:119-127)
+  if (v < 1.f) return sinf(kPi * (float)(int)(v * (float)e.h + 0.5f) / (float)e.h);
+  return sinf(kPi * ((float)(e.h - 1) + 0.5f) / (float)e.h);
+}
+
+GYT_D float3 env_lookup(const EnvDev& e, float3 d) {  // Lookup (EnvMap.h:30-51)
+  float u, v;
+  env_dir_to_uv(norm(d), &u, &v);
+  return env_radiance(e, u, v);
+}
+
+GYT_D float env_pdf_dir(const EnvDev& e, float3 d) {  // PdfDir (EnvMap.h:53-61)
+  float u, v;
+  env_dir_to_uv(norm(d), &u, &v);
+  float st = env_sin_theta(e, v);
+  if (st == 0.f) return 0.f;
+  int iu = min(max((int)(u * e.w), 0), e.w - 1), iv = min(max((int)(v * e.h), 0), e.h - 1);
+  float ci = __ldg(e.cint + iv);
+  if (ci * e.mint == 0.f) return 0.f;
+  float p = (__ldg(e.cfunc + (size_t)iv * e.w + iu) * __ldg(e.mfunc + iv)) / (ci * e.mint);
+  return p / (2.f * kPi * kPi * st);
+}
+
+// Distribution1D::SampleContinuous (visual/Sampling.h:53-84)
+GYT_D float dist_sample(const float* cdf, const float* func, int n, float fint, float u, float* pdf, int* off) {
+  int lo = 0, hi = n + 1;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(cdf + mid) > u) hi = mid; else lo = mid + 1;
+  }
+  int o = min(max(lo - 1, 0), n - 1);
+  if (__ldg(cdf + o) == __ldg(cdf + o + 1)) {
+    do { o--; } while (o > 0 && __ldg(cdf + o) == __ldg(cdf + o + 1));
+    o = max(o, 0);
+  }
+  *off = o;
+  float c0 = __ldg(cdf + o), c1 = __ldg(cdf + o + 1);
+  float du = (u - c0) / (c1 - c0);
+  *pdf = __ldg(func + o) / fint;
+  return ((float)o + du) / (float)n;
+}
+
+// EnvironmentMap::Sample (EnvMap.h:16-28)
+GYT_D float3 env_sample(const EnvDev& e, float u0, float u1, float3* dir, float* pdfW) {
+  float p0, p1;
+  int row, col;
+  float v = dist_sample(e.mcdf, e.mfunc, e.h, e.mint, u1, &p1, &row);
+  float u = dist_sample(e.ccdf + (size_t)row * (e.w + 1), e.cfunc + (size_t)row * e.w, e.w, __ldg(e.cint + row), u0,
+                        &p0, &col);
+  float pdf = p0 * p1;
+  float st = env_sin_theta(e, v);
+  *pdfW = st == 0.f ? 0.f : pdf / (2.f * kPi * kPi * st);
+  float phi = u * 2.f * kPi, theta = v * kPi;  // LatLongToDir (EnvMap.h:92-100)
+  float sth = sinf(theta);
+  *dir = mk(sth * cosf(phi), cosf(theta), sth * sinf(phi));
+  return env_radiance(e, u, v);
+}
+
 }  // namespace gyt

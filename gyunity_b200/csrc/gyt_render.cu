@@ -19,6 +19,7 @@
 #include <cooperative_groups/reduce.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -50,6 +51,9 @@ struct DevScene {
   const float* lfunc;         // n_lights
   float lfunc_int;
   int n_lights, n_tris, n_spheres;
+  int n_area;        // area lights come first; light n_area is the environment
+  int has_env;
+  EnvDev env;
 };
 
 // Light record (kLightRec float4): (p0, Le.r) (p1, Le.g) (p2, Le.b)
@@ -329,7 +333,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   const uint32_t bounce = depth;
   bool alive = false;
   float4 sc = zero4, mc = zero4;
-  if (prim >= 0) {
+  if (prim < 0) {
+    // PT.cpp:18-21: environment emission on the camera ray or after a delta bounce
+    if ((depth == 0 || delta) && s.has_env) L = L + tp * env_lookup(s.env, rd);
+  } else {
     Hit h;
     uint32_t mat;
     int light = -1;
@@ -365,17 +372,20 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
       float lsel = 0.f;
       int li = s.n_lights > 0 ? sample_light(s, ul, &lsel) : 0;
       if (lsel > 0.f) {
-        LightTri l = load_light(s, li);
-        float3 Le = l.Le;
-        {
+        const bool env_light = li >= s.n_area;
+        LightTri l;
+        float3 wi, Li, lpos, lerr, labs;
+        float pdf;
+        if (!env_light) {
           // light sample: AreaLight::Sample_Li -> Shape::Sample -> Triangle::Sample
-          const float3 p0 = l.p0, p1 = l.p1, p2 = l.p2, n0 = l.n0, n1 = l.n1, n2 = l.n2, face = l.face;
+          l = load_light(s, li);
           float su0 = sqrtf(ux);
           float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
-          float3 lpos = p0 * bb0 + p1 * bb1 + p2 * bb2;
-          float3 ln = n0 * bb0 + n1 * bb1 + n2 * bb2;
-          float3 lerr = (vabs(p0 * bb0) + vabs(p1 * bb1) + vabs(p2 * bb2)) * gammaf(6);
-          float pdf = 1.f / l.area;
+          lpos = l.p0 * bb0 + l.p1 * bb1 + l.p2 * bb2;
+          float3 ln = l.n0 * bb0 + l.n1 * bb1 + l.n2 * bb2;
+          lerr = (vabs(l.p0 * bb0) + vabs(l.p1 * bb1) + vabs(l.p2 * bb2)) * gammaf(6);
+          labs = l.face;
+          pdf = 1.f / l.area;
           float3 w = h.pos - lpos;
           if (length(w) == 0.f) {
             pdf = 0.f;
@@ -384,42 +394,50 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
             pdf *= dot(h.pos - lpos, h.pos - lpos) / fabsf(dot(ln, -w));
             if (isinf(pdf)) pdf = 0.f;
           }
-          float3 wi = norm(lpos - h.pos);
-          float3 Li = dot(ln, -wi) > 0.f ? Le : mk(0.f, 0.f, 0.f);
-          if (pdf > 0.f && !is_zero(Li)) {
-            float spdf = bsdf.pdf(h.wo, wi);
-            float3 f = bsdf.eval(h.wo, wi);
-            float cosT = fabsf(dot(h.n, wi));
-            if (!is_zero(f)) {
-              // Intersection::SpawnTo (Intersection.h:64-72)
-              float3 org = offset_origin(h.pos, h.perr, h.abs_n, lpos - h.pos);
-              float3 tgt = offset_origin(lpos, lerr, face, org - lpos);
-              float3 dd = tgt - org;
-              float dis = length(dd);
-              dd = dd / dis;
-              float3 so = org + dd * kRayEps;
-              q.so[i] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
-              q.sd[i] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(bounce));
-              float w1 = power_heuristic(pdf, spdf);
-              float3 c = tp * (Li * f * cosT / pdf) * w1 / lsel;
-              sc = make_float4(c.x, c.y, c.z, 1.f);
-            }
+          wi = norm(lpos - h.pos);
+          Li = dot(ln, -wi) > 0.f ? l.Le : mk(0.f, 0.f, 0.f);
+        } else {
+          // EnvironmentLight::Sample_Li (light/EnvLight.cpp:41-51): a point 2R away
+          float3 sd;
+          Li = env_sample(s.env, ux, uy, &sd, &pdf);
+          wi = norm(sd);
+          lpos = h.pos + wi * (2.f * s.env.radius);
+          lerr = mk(0.f, 0.f, 0.f);
+          labs = wi;
+        }
+        if (pdf > 0.f && !is_zero(Li)) {
+          float spdf = bsdf.pdf(h.wo, wi);
+          float3 f = bsdf.eval(h.wo, wi);
+          float cosT = fabsf(dot(h.n, wi));
+          if (!is_zero(f)) {
+            // Intersection::SpawnTo (Intersection.h:64-72)
+            float3 org = offset_origin(h.pos, h.perr, h.abs_n, lpos - h.pos);
+            float3 tgt = offset_origin(lpos, lerr, labs, org - lpos);
+            float3 dd = tgt - org;
+            float dis = length(dd);
+            dd = dd / dis;
+            float3 so = org + dd * kRayEps;
+            q.so[i] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
+            q.sd[i] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(bounce));
+            float w1 = power_heuristic(pdf, spdf);
+            float3 c = tp * (Li * f * cosT / pdf) * w1 / lsel;
+            sc = make_float4(c.x, c.y, c.z, 1.f);
           }
-          // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
-          float3 wi2;
-          float pdf2;
-          float3 f2 = bsdf.sample(h.wo, &wi2, &pdf2, vx, vy, vz);
-          float cos2 = fabsf(dot(h.n, wi2));
-          if (pdf2 != 0.f && !is_zero(f2)) {
-            float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
-            float lpdf = tri_light_pdf(l, h, o2, wi2);
-            if (lpdf != 0.f) {
-              float w2 = power_heuristic(pdf2, lpdf);
-              q.mo[i] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
-              q.md[i] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
-              float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
-              mc = make_float4(c.x, c.y, c.z, 1.f);
-            }
+        }
+        // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
+        float3 wi2;
+        float pdf2;
+        float3 f2 = bsdf.sample(h.wo, &wi2, &pdf2, vx, vy, vz);
+        float cos2 = fabsf(dot(h.n, wi2));
+        if (pdf2 != 0.f && !is_zero(f2)) {
+          float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
+          float lpdf = env_light ? env_pdf_dir(s.env, wi2) : tri_light_pdf(l, h, o2, wi2);
+          if (lpdf != 0.f) {
+            float w2 = power_heuristic(pdf2, lpdf);
+            q.mo[i] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
+            q.md[i] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
+            float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
+            mc = make_float4(c.x, c.y, c.z, 1.f);
           }
         }
       }
@@ -497,6 +515,11 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
     float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
     float3 wi = f3(md);
     int prim = trace<false, COUNT>(s, f3(mo), wi, tmax, b1, b2, &cnt);
+    bool reach = false;
+    if (prim < 0 && li >= s.n_area) {
+      L = L + f3(mc) * env_lookup(s.env, wi);  // Integrator.cpp:97-99
+      reach = true;
+    }
     if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
       float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
       float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
@@ -506,10 +529,11 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
         const float4* r = s.ltab + kLightRec * li;
         L = L + f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
       }
-      if (dbg.mis) {
-        uint32_t b = __float_as_uint(mo.w);
-        if (b < 64) dbg.mis[cur.pid[i]] |= 1ull << b;
-      }
+      reach = true;
+    }
+    if (reach && dbg.mis) {
+      uint32_t b = __float_as_uint(mo.w);
+      if (b < 64) dbg.mis[cur.pid[i]] |= 1ull << b;
     }
   }
   if (COUNT) {
@@ -936,8 +960,9 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     return fail(ctx, GYT_ERR_INVALID, "scene_create: sphere arrays missing");
   if (d->n_materials == 0 || !d->mat_type || !d->mat_params)
     return fail(ctx, GYT_ERR_INVALID, "scene_create: no materials");
-  if (d->env && d->env_w && d->env_h)
-    return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: environment lights are not supported by this build yet");
+  const bool has_env = d->env && d->env_w && d->env_h;
+  if (has_env && ((uint64_t)d->env_w * d->env_h > (1ull << 28) || d->env_w < 1 || d->env_h < 1))
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: environment map too large");
   if ((uint64_t)d->n_triangles >= (1ull << 28)) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many triangles");
   for (uint32_t m = 0; m < d->n_materials; ++m)
     if (d->mat_type[m] > 4) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
@@ -966,6 +991,73 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   }
   for (uint32_t k = 0; k < d->n_spheres; ++k)
     if (d->sphere_material[k] >= d->n_materials) return fail(ctx, GYT_ERR_INVALID, "scene_create: sphere material out of range");
+  const int n_area = (int)power.size();
+  // environment light (light/EnvLight.cpp, light/EnvMap.h): texels, the
+  // Distribution2D of ConvertImageToPdf (EnvMap.h:75-90) and the light's power,
+  // all in float as the reference computes them
+  std::vector<float4> env_tex;
+  std::vector<float> env_ccdf, env_cfunc, env_cint, env_mcdf, env_mfunc;
+  float env_mint = 0.f, env_radius = 0.f;
+  if (has_env) {
+    const int w = (int)d->env_w, hgt = (int)d->env_h;
+    env_tex.resize((size_t)w * hgt);
+    for (size_t k = 0; k < env_tex.size(); ++k)
+      env_tex[k] = make_float4(d->env[3 * k], d->env[3 * k + 1], d->env[3 * k + 2], 0.f);
+    auto dist1d = [](const float* f, int n, float* cdf, float* fint) {
+      cdf[0] = 0.f;
+      for (int i = 1; i < n + 1; ++i) cdf[i] = cdf[i - 1] + f[i - 1] / n;
+      *fint = cdf[n];
+      if (*fint == 0.f) {
+        for (int i = 1; i < n + 1; ++i) cdf[i] = (float)i / (float)n;
+      } else {
+        for (int i = 1; i < n + 1; ++i) cdf[i] /= *fint;
+      }
+    };
+    env_cfunc.resize((size_t)w * hgt);
+    env_ccdf.resize((size_t)(w + 1) * hgt);
+    env_cint.resize(hgt);
+    for (int r = 0; r < hgt; ++r) {
+      float v = (float)(r + 0.5f) / (float)hgt;
+      float st = std::sin(kPi * v);
+      for (int c = 0; c < w; ++c) {
+        const float* px = &d->env[((size_t)r * w + c) * 3];
+        env_cfunc[(size_t)r * w + c] = st * lum(mk(px[0], px[1], px[2]));
+      }
+      dist1d(&env_cfunc[(size_t)r * w], w, &env_ccdf[(size_t)r * (w + 1)], &env_cint[r]);
+    }
+    env_mfunc = env_cint;
+    env_mcdf.resize(hgt + 1);
+    dist1d(env_mfunc.data(), hgt, env_mcdf.data(), &env_mint);
+    // AABB::GetBoundingSphere of the accelerator's bounds (math/AABB.h:69-72)
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t t = 0; t < d->n_triangles; ++t)
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) {
+          float vv = d->vertices[3 * d->indices[3 * t + k] + a];
+          lo[a] = std::min(lo[a], vv);
+          hi[a] = std::max(hi[a], vv);
+        }
+    for (uint32_t k = 0; k < d->n_spheres; ++k)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], d->spheres[4 * k + a] - d->spheres[4 * k + 3]);
+        hi[a] = std::max(hi[a], d->spheres[4 * k + a] + d->spheres[4 * k + 3]);
+      }
+    env_radius = length(mk(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2])) * 0.5f;
+    // EnvironmentLight::Power (EnvLight.cpp:59-62): Y(LookupRadiance(0.5, 0.5) * PI * R * R)
+    auto texel = [&](int x, int y) {
+      x = std::min(std::max(x, 0), w - 1);
+      y = std::min(std::max(y, 0), hgt - 1);
+      const float* px = &d->env[((size_t)(hgt - 1 - y) * w + x) * 3];
+      return mk(px[0], px[1], px[2]);
+    };
+    float su = (float)w * 0.5f - 0.5f, sv = (float)hgt * (1.f - 0.5f) - 0.5f;
+    int s0 = (int)std::floor(su), t0 = (int)std::floor(sv);
+    float ds = su - s0, dt = sv - t0;
+    float3 a = texel(s0, t0) * (1.f - ds) + texel(s0 + 1, t0) * ds;
+    float3 b2 = texel(s0, t0 + 1) * (1.f - ds) + texel(s0 + 1, t0 + 1) * ds;
+    float3 mid = (a * (1.f - dt) + b2 * dt) * d->env_scale;
+    power.push_back(lum(mid * kPi * env_radius * env_radius));
+  }
   // Distribution1D over light power (visual/Sampling.h:18-45), in float
   int nl = (int)power.size();
   std::vector<float> cdf(nl + 1, 0.f);
@@ -1001,8 +1093,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     }
   }
   // light records: (p0, Le.r) (p1, Le.g) (p2, Le.b) (n0, area) (n1, leaf) (n2, id) (face, -)
-  std::vector<float4> ltab((size_t)nl * kLightRec);
-  for (int li = 0; li < nl; ++li) {
+  std::vector<float4> ltab((size_t)n_area * kLightRec);
+  for (int li = 0; li < n_area; ++li) {
     int t = light_tris[li];
     int k = leaf_of[t];
     const float* em = &d->emission[3 * d->tri_emission[t]];
@@ -1065,6 +1157,25 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   ds.lfunc = df;
   ds.lfunc_int = fint;
   ds.n_lights = nl;
+  ds.n_area = n_area;
+  ds.has_env = has_env ? 1 : 0;
+  if (has_env) {
+    EnvDev& ev = ds.env;
+    float4* et = nullptr;
+    float *cc = nullptr, *cf = nullptr, *ci = nullptr, *mc = nullptr, *mf = nullptr;
+    if (e == cudaSuccess) e = up(&et, env_tex.data(), env_tex.size());
+    if (e == cudaSuccess) e = up(&cc, env_ccdf.data(), env_ccdf.size());
+    if (e == cudaSuccess) e = up(&cf, env_cfunc.data(), env_cfunc.size());
+    if (e == cudaSuccess) e = up(&ci, env_cint.data(), env_cint.size());
+    if (e == cudaSuccess) e = up(&mc, env_mcdf.data(), env_mcdf.size());
+    if (e == cudaSuccess) e = up(&mf, env_mfunc.data(), env_mfunc.size());
+    ev.tex = et; ev.ccdf = cc; ev.cfunc = cf; ev.cint = ci; ev.mcdf = mc; ev.mfunc = mf;
+    ev.mint = env_mint;
+    ev.w = (int)d->env_w;
+    ev.h = (int)d->env_h;
+    ev.scale = d->env_scale;
+    ev.radius = env_radius;
+  }
   ds.n_tris = (int)d->n_triangles;
   ds.n_spheres = (int)d->n_spheres;
   sc->n_tris = d->n_triangles;

@@ -365,3 +365,78 @@ def mixed_materials_box(level=3, res=64, spp=4, max_depth=8, rr_depth=3, seed=11
     return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
                    spheres=np.array([[-0.55, -0.7, -0.4, 0.25], [0.55, -0.7, 0.4, 0.25]], np.float32),
                    sphere_material=np.array([mirror, glass], np.uint32), name="mixed_materials_box")
+
+
+# ----------------------------------------------------------- environment ---
+
+def rgbe_quantize(img: np.ndarray) -> np.ndarray:
+    """Round an RGB float image to the values an RGBE (.hdr) file stores:
+    shared exponent from frexp of the largest component, 8-bit mantissas by
+    truncation, decoded as mantissa * 2^(exponent - 8) (Ward's RGBE format).
+    The result survives a write/read round trip unchanged, so an environment
+    map given to the reference through a file and to the GPU directly holds
+    identical texels."""
+    img = np.ascontiguousarray(img, np.float32)
+    m = img.max(axis=2)
+    mant, ex = np.frexp(m.astype(np.float64))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        normalize = (mant.astype(np.float32) * np.float32(256.0)) / m
+        b = np.trunc(img * normalize[..., None]).astype(np.int64) % 256
+    out = (b.astype(np.float64) * np.ldexp(1.0, (ex - 8))[..., None]).astype(np.float32)
+    out[m < np.float32(1e-32)] = 0.0
+    return out
+
+
+def sky_envmap(width=2048, height=1024, seed=5, sun_elevation_deg=45.0, sun_azimuth_deg=30.0,
+               sun_diameter_deg=0.5, sun_radiance=None):
+    """Synthetic lat-long sky: zenith (0.3, 0.5, 1.0) to horizon 0.8 gradient
+    above the horizon, ground 0.1 below, plus a sun disk whose radiance is one
+    draw from lognormal(mu=8, sigma=1). Row 0 is the zenith (theta = 0) and
+    directions follow EnvironmentMap::LatLongToDir (light/EnvMap.h:92-100):
+    (sin(theta) cos(phi), cos(theta), sin(theta) sin(phi))."""
+    rng = np.random.default_rng(seed)
+    if sun_radiance is None:
+        sun_radiance = float(rng.lognormal(8.0, 1.0))
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = v[:, None] * np.pi
+    phi = u[None, :] * 2 * np.pi
+    d = np.stack([np.sin(theta) * np.cos(phi), np.cos(theta) * np.ones_like(phi), np.sin(theta) * np.sin(phi)], -1)
+    y = d[..., 1:2]
+    zen = np.array([0.3, 0.5, 1.0])
+    hor = np.array([0.8, 0.8, 0.8])
+    t = np.clip(y, 0, 1)
+    img = np.where(y > 0, hor * (1 - t) + zen * t, 0.1)
+    el, az = np.radians(sun_elevation_deg), np.radians(sun_azimuth_deg)
+    sdir = np.array([np.cos(el) * np.cos(az), np.sin(el), np.cos(el) * np.sin(az)])
+    cosang = (d * sdir).sum(-1)
+    disk = cosang >= np.cos(np.radians(sun_diameter_deg / 2))
+    img[disk] = sun_radiance
+    return rgbe_quantize(img.astype(np.float32))
+
+
+def env_torus_knot(n_u=2000, n_v=1000, res_x=1920, res_y=1080, spp=256, max_depth=32, rr_depth=5, seed=4,
+                   env_w=2048, env_h=1024, sun_diameter_deg=0.5, alpha=0.1) -> SceneDesc:
+    """Environment-lit rough glass: a (2,3) torus knot tube swept with
+    n_u x n_v quads (2 n_u n_v triangles; 2000 x 1000 = 4M), displaced by 5% of
+    the tube radius with 4-octave value noise, GGX rough dielectric
+    (alpha 0.1, IOR 1.5), lit only by the synthetic sky map."""
+    b = _Builder()
+    v, f, nrm = torus_knot(n_u, n_v)
+    r_tube = 0.12
+    disp = value_noise(v * 2.0, seed)
+    v = v + nrm * (0.05 * r_tube * disp)[:, None]
+    v32 = v.astype(np.float32)
+    n = vertex_normals(v32.astype(np.float64), f)
+    glass = b.material(*_mat(MAT_DIELECTRIC, (1, 1, 1), (1, 1, 1), ax=alpha, ay=alpha, eta=1.5))
+    b.tris(v32, n.astype(np.float32), f, np.full(f.shape[0], glass, np.uint32))
+    env = sky_envmap(env_w, env_h, seed=5, sun_diameter_deg=sun_diameter_deg)
+    return b.build(camera=Camera(res_x=res_x, res_y=res_y), params=RenderParams(spp, max_depth, rr_depth),
+                   env=env, env_scale=1.0, name="env_torus_knot_%dtris" % f.shape[0])
+
+
+def env_knot_small() -> SceneDesc:
+    """Small environment-lit rough-glass scene for tests: 3,840 triangles,
+    128 x 64 sky map with a 12-degree sun, 96 x 54 film, 4 spp, depth 8."""
+    return env_torus_knot(n_u=120, n_v=16, res_x=96, res_y=54, spp=4, max_depth=8, env_w=128, env_h=64,
+                          sun_diameter_deg=12)

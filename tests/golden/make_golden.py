@@ -111,7 +111,7 @@ def main():
 
     # per-path radiance, PathTracing::Li, for three scenes
     for name, sd in (("cornell_nospheres", scenes.cornell_box(spheres=False)), ("cornell", scenes.cornell_box()),
-                     ("mixed", scenes.mixed_materials_box(level=3, res=64))):
+                     ("mixed", scenes.mixed_materials_box(level=3, res=64)), ("env", scenes.env_knot_small())):
         path = os.path.join(tmp, name + ".gyts")
         io.write_scene(path, sd)
         n = 3000
@@ -135,6 +135,13 @@ def main():
     io.write_scene(path, sd)
     img, info = io.ref_render(tmp, path)
     np.savez_compressed(os.path.join(HERE, "image_cornell_128x128_16spp.npz"), film=img)
+
+    # the environment-lit scene through TiledIntegrator::Render
+    sd = scenes.env_knot_small()
+    path = os.path.join(tmp, "img3.gyts")
+    io.write_scene(path, sd)
+    img, info = io.ref_render(tmp, path)
+    np.savez_compressed(os.path.join(HERE, "image_env_knot_96x54_4spp.npz"), film=img)
 
     # BxDF tables in the local frame
     cases = bsdf_cases(rng)

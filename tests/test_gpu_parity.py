@@ -90,10 +90,10 @@ def _replay(sd, xys, ctx):
     return rel, cur == co, flips
 
 
-@pytest.mark.parametrize("name", ["cornell_nospheres", "cornell", "mixed"])
+@pytest.mark.parametrize("name", ["cornell_nospheres", "cornell", "mixed", "env"])
 def test_per_path_radiance_matches_fp64_replay(ctx, name):
     sd = {"cornell_nospheres": scenes.cornell_box(spheres=False), "cornell": scenes.cornell_box(),
-          "mixed": scenes.mixed_materials_box(level=3, res=64)}[name]
+          "mixed": scenes.mixed_materials_box(level=3, res=64), "env": scenes.env_knot_small()}[name]
     xys = golden("paths_%s.npz" % name)["xys"]
     rel, same_cursor, flips = _replay(sd, xys, ctx)
     ok = rel < 1e-4  # tolerance: FP32 path vs FP64 replay of the same path, relative to max(|L|, 1e-3)
@@ -150,6 +150,22 @@ def test_image_statistics_match_reference(ctx):
     print("mean rel diff %.2e, RMSE %.4f (image RMS %.4f)" % (rel_mean, rmse, np.sqrt(np.mean(ref ** 2))))
     assert rel_mean < 5e-3
     assert rmse < 0.02 * np.sqrt(np.mean(ref ** 2))
+
+
+def test_env_image_matches_reference(ctx):
+    gd = golden("image_env_knot_96x54_4spp.npz")["film"].reshape(54, 96, 4).astype(np.float64)
+    sd = scenes.env_knot_small()
+    sc = g.Scene(sd, ctx)
+    film = g.Film(96, 54)
+    cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    g.GpuPathTracing(4, 8).Render(sc, cam)
+    ref = gd[..., :3] / gd[..., 3:]
+    img = film.image.astype(np.float64)
+    rel_mean = abs(img.mean() - ref.mean()) / ref.mean()
+    rmse = np.sqrt(np.mean((img - ref) ** 2))
+    print("env: mean rel diff %.2e, RMSE %.4f (image RMS %.4f)" % (rel_mean, rmse, np.sqrt(np.mean(ref ** 2))))
+    assert rel_mean < 5e-3
+    assert rmse < 0.05 * np.sqrt(np.mean(ref ** 2))
 
 
 def test_render_is_deterministic_up_to_fp64_atomics(ctx):

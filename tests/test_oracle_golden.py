@@ -87,6 +87,26 @@ def test_paths_match_reference_without_delta_lobes():
     assert (rel < 1e-4).mean() > 0.995
 
 
+def test_paths_match_reference_with_environment_light():
+    rel, same_cursor = _path_agreement("env", scenes.env_knot_small(), 64)
+    assert same_cursor.mean() > 0.995
+    assert (rel < 1e-4).mean() > 0.99
+
+
+def test_environment_map_is_rgbe_exact():
+    # a second quantisation changes nothing: the texels survive the .hdr round trip
+    env = scenes.env_knot_small().env
+    assert np.array_equal(scenes.rgbe_quantize(env), env)
+
+
+def test_env_image_matches_reference_render():
+    g = golden("image_env_knot_96x54_4spp.npz")["film"].reshape(54, 96, 4).astype(np.float64)
+    film = orc.OracleScene(scenes.env_knot_small()).render(precision=64)
+    assert np.array_equal(film[..., 3], g[..., 3])
+    img, ref = film[..., :3] / film[..., 3:], g[..., :3] / g[..., 3:]
+    assert abs(img.mean() - ref.mean()) < 1e-3 * ref.mean()
+
+
 @pytest.mark.parametrize("name", ["cornell", "mixed"])
 def test_paths_match_reference_with_delta_lobes(name):
     # after a mirror/glass bounce the roulette probability is 1 in exact
