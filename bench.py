@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--depth", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bvh-width", type=int, default=None, choices=[2, 8])
     return ap.parse_args()
 
 
@@ -211,7 +212,7 @@ def run_ours(a):
     torch.cuda.set_device(d.local)
     import gyunity_b200 as g
     sd = workload(a)
-    ctx = g.Context(d.local)
+    ctx = g.Context(d.local, bvh_width=a.bvh_width)
     t0 = time.perf_counter()
     scene = g.Scene(sd, ctx)
     scene_s = time.perf_counter() - t0
@@ -269,7 +270,7 @@ def run_ours(a):
         ctx.render_device(scene, cam, prm, film.data_ptr())
         cnt = ctx.read_profile()
         ctx.set_profile(0)
-        out = roofline(prof, cnt, stats)
+        out = roofline(prof, cnt, stats, node_bytes=80 if a.bvh_width == 8 else 64)
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -301,31 +302,33 @@ def run_ours(a):
 # path state read by a stage = origin 16 + direction 16 + throughput 16 +
 # radiance 16 + Sobol' index 8 + meta 4 = 76 B; written back by shade = 68 B;
 # closest hit 16 B; a queued segment ray (origin+tmax, direction) 32 B and its
-# contribution 16 B.
+# contribution 16 B; a BVH node 64 B (binary) or 80 B (8-wide); a triangle 48 B.
 STATE_READ, STATE_WRITE, HIT, RAY, CONTRIB = 76, 68, 16, 32, 16
 
 
-def roofline(prof, cnt, stats):
+def roofline(prof, cnt, stats, node_bytes=64):
     """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
-    of its launches / their CUDA-event time; traversal bytes per ray = ray +
-    BVH nodes x 64 B + triangle tests x 48 B (counts from the counting pass)."""
+    of its launches / their CUDA-event time; traversal bytes per ray = BVH
+    nodes x node size + triangle tests x 48 B (counts from the counting pass)."""
     peak, src = peaks()
     ms = prof["ms"]
     dom = max(ms, key=ms.get)
     launches = max(1, prof["launches"][dom])
-    nodes, tris = cnt["node_visits"], cnt["tri_tests"]
-    rays = max(1, cnt["closest_rays"] + cnt["shadow_rays"])
     slots = stats[-1]["path_slots"]
-    npr, tpr = nodes / rays, tris / rays
-    trav = npr * 64 + tpr * 48
-    shadow, mis = cnt["shadow_rays"], max(0, cnt["closest_rays"] - slots)
+    rays = cnt["rays"]
+
+    def trav(k):
+        r = max(1, rays[k])
+        return cnt["node_visits"][k] / r * node_bytes + cnt["tri_tests"][k] / r * 48
+
     if dom == "extend":
-        byts = slots * (RAY + HIT + trav)
-    elif dom == "connect":
-        # queue flags of every slot, queued rays, path state copy of survivors
-        byts = slots * (2 * CONTRIB + 16) + (shadow + mis) * (RAY + trav) + slots * 2 * STATE_READ
+        byts = rays["extend"] * (RAY + HIT + trav("extend"))
+    elif dom in ("shadow", "mis"):
+        byts = rays[dom] * (RAY + CONTRIB + 16 + trav(dom))
     elif dom == "shade":
-        byts = slots * (STATE_READ + HIT + STATE_WRITE + 2 * CONTRIB) + (shadow + mis) * RAY
+        byts = slots * (STATE_READ + HIT + STATE_WRITE) + (rays["shadow"] + rays["mis"]) * (RAY + CONTRIB)
+    elif dom == "finish":
+        byts = slots * (STATE_READ + 4) + slots * (STATE_READ + 8)
     else:
         byts = slots * STATE_WRITE
     achieved = byts / (ms[dom] / 1e3) / 1e9
@@ -338,10 +341,12 @@ def roofline(prof, cnt, stats):
                 traffic = rec["bytes_per_slot"] * slots / launches
         except Exception:
             traffic = None
+    per_ray = {k: {"nodes": cnt["node_visits"][k] / max(1, rays[k]), "tris": cnt["tri_tests"][k] / max(1, rays[k]),
+                   "rays": rays[k]} for k in rays}
     return {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic,
             "algorithmic_bytes_per_launch": byts / launches, "launches": launches,
-            "avg_launch_ms": ms[dom] / launches, "nodes_per_ray": npr, "tris_per_ray": tpr,
+            "avg_launch_ms": ms[dom] / launches, "traversal": per_ray,
             "share": {k: v / sum(ms.values()) for k, v in ms.items()}}
 
 

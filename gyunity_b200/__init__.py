@@ -34,7 +34,7 @@ __all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "Rende
 class Context:
     """A CUDA device with its stream and path pools (gyt_context)."""
 
-    def __init__(self, device=0, capacity=None):
+    def __init__(self, device=0, capacity=None, bvh_width=None):
         self._lib = load()
         h = ctypes.c_void_p()
         rc = self._lib.gyt_context_create(int(device), ctypes.byref(h))
@@ -44,6 +44,8 @@ class Context:
         self.device = device
         if capacity is not None:
             self.check(self._lib.gyt_context_set_capacity(self.handle, int(capacity)))
+        if bvh_width is not None:
+            self.check(self._lib.gyt_context_set_bvh_width(self.handle, int(bvh_width)))
 
     def check(self, rc):
         if rc != 0:
@@ -67,10 +69,10 @@ class Context:
     def read_profile(self):
         p = _c.GytProfile()
         self.check(self._lib.gyt_profile_read(self.handle, ctypes.byref(p)))
-        names = ["generate", "extend", "shade", "connect"]
-        return {"ms": dict(zip(names, list(p.ms))), "launches": dict(zip(names, list(p.launches))),
-                "closest_rays": p.closest_rays, "shadow_rays": p.shadow_rays, "node_visits": p.node_visits,
-                "tri_tests": p.tri_tests}
+        k, t = _c.KERNELS, _c.TRAVERSALS
+        return {"ms": dict(zip(k, list(p.ms))), "launches": dict(zip(k, list(p.launches))),
+                "rays": dict(zip(t, list(p.rays))), "node_visits": dict(zip(t, list(p.node_visits))),
+                "tri_tests": dict(zip(t, list(p.tri_tests)))}
 
     def render_device(self, scene, camera, params, d_film_ptr):
         """gyt_render_device into a caller-owned device film (res_x*res_y*4 doubles)."""

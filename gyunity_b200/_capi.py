@@ -17,7 +17,7 @@ STATUS = {0: "GYT_OK", 1: "GYT_ERR_INVALID", 2: "GYT_ERR_CUDA", 3: "GYT_ERR_OUT_
 
 # Every entry point include/gyt.h declares (checked by the CPU tests).
 EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_context_set_capacity",
-           "gyt_context_set_profile", "gyt_profile_read",
+           "gyt_context_set_profile", "gyt_profile_read", "gyt_context_set_bvh_width",
            "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info", "gyt_render", "gyt_render_device",
            "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world",
            "gyt_render_device_noalloc"]
@@ -59,8 +59,12 @@ class GytRenderStats(ctypes.Structure):
 
 
 class GytProfile(ctypes.Structure):
-    _fields_ = [("ms", ctypes.c_float * 4), ("launches", ctypes.c_uint32 * 4), ("closest_rays", ctypes.c_uint64),
-                ("shadow_rays", ctypes.c_uint64), ("node_visits", ctypes.c_uint64), ("tri_tests", ctypes.c_uint64)]
+    _fields_ = [("ms", ctypes.c_float * 6), ("launches", ctypes.c_uint32 * 6), ("rays", ctypes.c_uint64 * 3),
+                ("node_visits", ctypes.c_uint64 * 3), ("tri_tests", ctypes.c_uint64 * 3)]
+
+
+KERNELS = ["generate", "extend", "shade", "shadow", "mis", "finish"]
+TRAVERSALS = ["extend", "shadow", "mis"]
 
 
 _lib = None
@@ -83,6 +87,7 @@ def load():
     L.gyt_context_set_capacity.argtypes = [P, U32]
     L.gyt_context_set_profile.argtypes = [P, I32]
     L.gyt_profile_read.argtypes = [P, ctypes.POINTER(GytProfile)]
+    L.gyt_context_set_bvh_width.argtypes = [P, I32]
     L.gyt_scene_create.argtypes = [P, ctypes.POINTER(GytSceneDesc), ctypes.POINTER(P)]
     L.gyt_scene_destroy.argtypes = [P]
     L.gyt_scene_destroy.restype = None

@@ -26,7 +26,6 @@ struct Box {
 };
 
 constexpr int kBins = 16;
-constexpr int kMaxLeaf = 8;
 
 // Widen a box by a few ulps of its largest coordinate magnitude so that
 // rounding in the slab test cannot cull a boundary hit.
@@ -39,7 +38,8 @@ void pad(Box& b) {
 
 }  // namespace
 
-bool build_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt, BvhHost* out) {
+bool build_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt, BvhHost* out, int max_leaf) {
+  const int kMaxLeaf = std::min(8, std::max(1, max_leaf));
   out->nodes.clear();
   out->order.clear();
   out->max_depth = 0;
@@ -117,7 +117,7 @@ bool build_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt,
       for (uint32_t k = start; k < start + count; ++k) b.grow(pb[idx[k]]);
       set_child(parent, slot, b, leaf_code(first, count));
     };
-    if (j.parent >= 0 && j.count <= (uint32_t)kMaxLeaf && j.count <= 2) {
+    if (j.parent >= 0 && j.count <= (uint32_t)kMaxLeaf && j.count <= 2u) {
       make_leaf(j.start, j.count, j.parent, j.slot);
       continue;
     }
@@ -185,6 +185,144 @@ bool build_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt,
     stack.push_back({j.start, mid - j.start, node, 0, j.depth + 1});
   }
   return true;
+}
+
+namespace {
+
+struct Elem {
+  Box box;
+  int node;           // binary inner node, or -1 for a leaf
+  uint32_t first, count;
+};
+
+Elem child_elem(const std::vector<float>& nodes, int node, int slot) {
+  const float* n = &nodes[(size_t)node * 16];
+  Elem e;
+  if (slot == 0) {
+    e.box.lo[0] = n[0]; e.box.hi[0] = n[1]; e.box.lo[1] = n[2]; e.box.hi[1] = n[3];
+    e.box.lo[2] = n[8]; e.box.hi[2] = n[9];
+  } else {
+    e.box.lo[0] = n[4]; e.box.hi[0] = n[5]; e.box.lo[1] = n[6]; e.box.hi[1] = n[7];
+    e.box.lo[2] = n[10]; e.box.hi[2] = n[11];
+  }
+  int c;
+  std::memcpy(&c, &n[12 + slot], 4);
+  if (c >= 0) {
+    e.node = c;
+    e.first = e.count = 0;
+  } else {
+    uint32_t code = ~(uint32_t)c;
+    e.node = -1;
+    e.first = code >> 3;
+    e.count = (code & 7u) + 1u;
+  }
+  return e;
+}
+
+}  // namespace
+
+bool build_wide_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt, WideBvhHost* out) {
+  out->nodes.clear();
+  out->order.clear();
+  out->max_depth = 0;
+  if (nt == 0) return true;
+  BvhHost bin;
+  if (!build_bvh_host(V, nv, I, nt, &bin, 3)) return false;
+  // the binary root's own box is not stored: build it from its two children
+  struct Pending { std::vector<Elem> children; uint32_t depth; };
+  std::vector<std::vector<Elem>> todo;  // children of each wide node, in node order
+  std::vector<uint32_t> depth;
+  auto expand = [&](std::vector<Elem> ch) {
+    while (ch.size() < 8) {
+      int best = -1;
+      float area = -1.f;
+      for (size_t k = 0; k < ch.size(); ++k)
+        if (ch[k].node >= 0 && ch[k].box.area() > area) { area = ch[k].box.area(); best = (int)k; }
+      if (best < 0) break;
+      int b = ch[best].node;
+      Elem a = child_elem(bin.nodes, b, 0), c = child_elem(bin.nodes, b, 1);
+      ch[best] = a;
+      if (c.node >= 0 || c.count > 0) ch.push_back(c);
+    }
+    return ch;
+  };
+  std::vector<Elem> root = {child_elem(bin.nodes, 0, 0), child_elem(bin.nodes, 0, 1)};
+  if (root[1].node < 0 && root[1].count > 0 && !(root[1].box.lo[0] <= root[1].box.hi[0])) root.pop_back();
+  todo.push_back(expand(root));
+  depth.push_back(1);
+  for (size_t w = 0; w < todo.size(); ++w) {
+    std::vector<Elem> ch = todo[w];
+    // inner children first get consecutive node indices
+    uint32_t child_base = (uint32_t)todo.size();
+    uint32_t tri_base = (uint32_t)out->order.size();
+    // widen every child box by a margin of the node's size so that FP32
+    // rounding in the slab test can never cull a boundary hit
+    Box raw;
+    for (const Elem& e : ch) raw.grow(e.box);
+    float mext = 0.f, mabs = 0.f;
+    for (int a = 0; a < 3; ++a) {
+      mext = std::max(mext, raw.hi[a] - raw.lo[a]);
+      mabs = std::max(mabs, std::max(std::fabs(raw.lo[a]), std::fabs(raw.hi[a])));
+    }
+    const float margin = 1e-5f * mext + 1e-6f * mabs + 1e-30f;
+    for (Elem& e : ch)
+      for (int a = 0; a < 3; ++a) { e.box.lo[a] -= margin; e.box.hi[a] += margin; }
+    Box nb;
+    for (const Elem& e : ch) nb.grow(e.box);
+    double p[3], sc[3];
+    int ex[3];
+    for (int a = 0; a < 3; ++a) {
+      p[a] = nb.lo[a];
+      double ext = (double)nb.hi[a] - (double)nb.lo[a];
+      int e = ext > 0 ? (int)std::ceil(std::log2(ext / 255.0)) : -100;
+      if (e < -100) e = -100;
+      // one ulp of headroom so the outward rounding below always fits in 255
+      while (std::ldexp(255.0, e) < ext * (1.0 + 1e-6)) ++e;
+      ex[a] = e;
+      sc[a] = std::ldexp(1.0, e);
+    }
+    uint32_t words[20] = {};
+    float pf[3] = {nb.lo[0], nb.lo[1], nb.lo[2]};
+    std::memcpy(&words[0], &pf[0], 4);
+    std::memcpy(&words[1], &pf[1], 4);
+    std::memcpy(&words[2], &pf[2], 4);
+    uint32_t imask = 0;
+    uint8_t meta[8] = {}, qlo[3][8] = {}, qhi[3][8] = {};
+    uint32_t inner_rank = 0;
+    for (size_t k = 0; k < ch.size(); ++k) {
+      const Elem& e = ch[k];
+      for (int a = 0; a < 3; ++a) {
+        double lo = std::floor(((double)e.box.lo[a] - p[a]) / sc[a] * (1.0 - 1e-6) - 1e-6);
+        double hi = std::ceil(((double)e.box.hi[a] - p[a]) / sc[a] * (1.0 + 1e-6) + 1e-6);
+        qlo[a][k] = (uint8_t)std::min(255.0, std::max(0.0, lo));
+        qhi[a][k] = (uint8_t)std::min(255.0, std::max(0.0, hi));
+      }
+      if (e.node >= 0) {
+        imask |= 1u << k;
+        std::vector<Elem> sub = {child_elem(bin.nodes, e.node, 0), child_elem(bin.nodes, e.node, 1)};
+        todo.push_back(expand(sub));
+        depth.push_back(depth[w] + 1);
+        ++inner_rank;
+      } else {
+        uint32_t off = (uint32_t)out->order.size() - tri_base;
+        if (e.count > 3 || off > 31) return false;
+        for (uint32_t t = 0; t < e.count; ++t) out->order.push_back(bin.order[e.first + t]);
+        meta[k] = (uint8_t)((e.count << 5) | off);
+      }
+    }
+    out->max_depth = std::max(out->max_depth, depth[w]);
+    words[3] = (uint32_t)(uint8_t)(int8_t)ex[0] | ((uint32_t)(uint8_t)(int8_t)ex[1] << 8) |
+               ((uint32_t)(uint8_t)(int8_t)ex[2] << 16) | (imask << 24);
+    words[4] = child_base;
+    words[5] = tri_base;
+    std::memcpy(&words[6], meta, 8);
+    for (int a = 0; a < 3; ++a) {
+      std::memcpy(&words[8 + 4 * a], qlo[a], 8);
+      std::memcpy(&words[10 + 4 * a], qhi[a], 8);
+    }
+    out->nodes.insert(out->nodes.end(), words, words + 20);
+  }
+  return out->order.size() == nt;
 }
 
 }  // namespace gyt

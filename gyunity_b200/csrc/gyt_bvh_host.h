@@ -26,7 +26,30 @@ struct BvhHost {
   uint32_t max_depth = 0;
 };
 
-// vertices: nv*3, indices: nt*3. Returns false on invalid input.
-bool build_bvh_host(const float* vertices, uint32_t nv, const uint32_t* indices, uint32_t nt, BvhHost* out);
+// vertices: nv*3, indices: nt*3. Returns false on invalid input. max_leaf
+// bounds the triangles per leaf (at most 8).
+bool build_bvh_host(const float* vertices, uint32_t nv, const uint32_t* indices, uint32_t nt, BvhHost* out,
+                    int max_leaf = 8);
+
+// 8-wide BVH with quantized child boxes, collapsed from the binary tree.
+//
+// Node = 5 x uint4 = 80 bytes:
+//   [0] origin p (3 x f32), exponents ex, ey, ez (int8 each, scale 2^e) and
+//       the inner-child mask in byte 3 of .w
+//   [1] child_base (first inner child node), tri_base (first triangle of the
+//       node's leaves), meta[0..7] (one byte per child slot)
+//   [2] qlo.x[0..7], qhi.x[0..7]   [3] the same for y   [4] the same for z
+// Child slot i: inner if bit i of the mask is set, node index child_base +
+// popcount(mask & ((1 << i) - 1)); a leaf if meta[i] != 0: (count << 5) |
+// offset, 1..3 triangles starting at tri_base + offset; empty otherwise.
+// Child box = p + q * 2^e per axis (q in 0..255), rounded outwards.
+struct WideBvhHost {
+  std::vector<uint32_t> nodes;    // 20 words per node
+  std::vector<uint32_t> order;    // leaf order -> triangle id
+  uint32_t max_depth = 0;         // wide levels
+};
+
+bool build_wide_bvh_host(const float* vertices, uint32_t nv, const uint32_t* indices, uint32_t nt,
+                         WideBvhHost* out);
 
 }  // namespace gyt

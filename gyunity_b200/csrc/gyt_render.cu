@@ -6,12 +6,19 @@
 //   k_extend    closest hit of every continuation ray (binary BVH, watertight
 //               triangles, analytic spheres)       BVHAccel.cpp:401-445
 //   k_shade     surface interaction, emission, light sample + BSDF sample of
-//               the MIS next-event estimate, continuation BSDF sample,
-//               Russian roulette                   PT.cpp:16-65, Integrator.cpp:9-107
-//   k_connect   shadow (any-hit) and MIS (closest-hit) rays, radiance update,
-//               film accumulation of finished paths (FP64 atomics), and
+//               the MIS next-event estimate (queued as shadow / MIS rays),
+//               continuation BSDF sample, Russian roulette
+//                                                  PT.cpp:16-65, Integrator.cpp:9-107
+//   k_shadow    next-event shadow rays (any hit) from a compact queue
+//                                                  Visibility.cpp:7-10
+//   k_mis       BSDF-sampled MIS rays (closest hit) from a compact queue
+//                                                  Integrator.cpp:86-101
+//   k_finish    film accumulation of finished paths (FP64 atomics) and
 //               compaction of live paths into the other pool (warp-aggregated
-//               atomics, ballot/popc)              Visibility.cpp:7-10, Film.h:61-87
+//               atomics)                           Film.h:61-87
+// The three traversal kernels are persistent: lanes whose ray is done fetch
+// the next queue entry before each traversal step (dynamic ray fetching), so
+// warps stay full while rays of very different lengths are in flight.
 // Path state is SoA in HBM; pools are ping-ponged each iteration so live
 // paths stay dense and new paths fill the tail.
 #include <cuda_runtime.h>
@@ -39,7 +46,8 @@ using namespace gyt;
 namespace {
 
 struct DevScene {
-  const float4* nodes;        // binary BVH, 4 float4 per node
+  const uint4* wnodes;        // 8-wide BVH, 5 uint4 per node (gyt_bvh_host.h), or null
+  const float4* nodes;        // binary BVH, 4 float4 per node (gyt_bvh_host.h), or null
   const float4* tris;         // leaf order: (p0, original id), (p1, -), (p2, -)
   const float4* tnrm;         // leaf order: (n0, material), (n1, light index or -1), (n2, -)
   const float4* spheres;
@@ -71,14 +79,17 @@ struct PathBuf {
   uint32_t* pid;  // path id within the render (debug outputs)
 };
 
+// Compact ray queues filled by k_shade (positions from warp-aggregated
+// atomics on counts[0] and counts[1]) and the closest hit of every path slot.
 struct Queues {
-  float4* so;  // shadow ray origin, tmax
-  float4* sd;  // shadow ray direction
-  float4* sc;  // shadow contribution, valid flag
-  float4* mo;  // MIS ray origin
-  float4* md;  // MIS ray direction, light index bits
-  float4* mc;  // MIS contribution, valid flag
-  float4* hit; // closest hit of the continuation ray: t, b1, b2, prim bits
+  float4* so;  // shadow ray: origin, tmax
+  float4* sd;  // shadow ray: direction, path slot bits
+  float4* sc;  // shadow ray: contribution, bounce bits
+  float4* mo;  // MIS ray: origin, bounce bits
+  float4* md;  // MIS ray: direction, light index bits
+  float4* mc;  // MIS ray: contribution, path slot bits
+  float4* hit; // per path slot: t, b1, b2, prim bits
+  uint32_t* counts;  // [0] shadow rays, [1] MIS rays, [2..4] fetch counters, [5] compaction
 };
 
 struct Params {
@@ -99,7 +110,8 @@ struct DebugOut {
 
 constexpr uint32_t kAlive = 1u << 31;
 constexpr uint32_t kPixMask = 0x0fffffffu;
-constexpr int kStack = 64;
+constexpr int kWStack = 48;  // node groups: one per level of the wide BVH
+constexpr int kBStack = 64;  // binary BVH: one entry per level
 constexpr int kBlock = 256;
 
 GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive) {
@@ -107,90 +119,302 @@ GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive
 }
 
 // ------------------------------------------------------------ traversal ---
-// Closest hit (ANY = false) or occlusion (ANY = true) over the BVH and the
-// spheres. Returns the triangle's leaf position (< n_tris; the original id is
-// in tris[3k].w), n_tris + sphere index, or -1.
-// tmax is updated to the hit distance; spheres report the distance along the
-// re-made object ray of Sphere::Intersect (shape/Sphere.h:35).
 struct TraceCount {
   uint32_t nodes = 0, tris = 0;
 };
 
-template <bool ANY, bool COUNT = false>
-GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, float& b2, TraceCount* cnt = nullptr) {
-  int prim = -1;
-  if (s.n_tris > 0) {
-    WtRay wr = wt_setup(o, d);
-    const float ooeps = 8.271806125530277e-25f;  // 2^-80
-    float ix = 1.f / (fabsf(d.x) > ooeps ? d.x : copysignf(ooeps, d.x));
-    float iy = 1.f / (fabsf(d.y) > ooeps ? d.y : copysignf(ooeps, d.y));
-    float iz = 1.f / (fabsf(d.z) > ooeps ? d.z : copysignf(ooeps, d.z));
-    float ox = o.x * ix, oy = o.y * iy, oz = o.z * iz;
-    int stack[kStack];
-    int sp = 0;
-    int node = 0;
-    for (;;) {
-      if (node >= 0) {
-        if (COUNT) cnt->nodes++;
-        const float4* n = s.nodes + 4 * node;
-        float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
-        int4 n3 = __ldg((const int4*)(n + 3));
-        float a0 = fmaf(n0.x, ix, -ox), a1 = fmaf(n0.y, ix, -ox);
-        float a2 = fmaf(n0.z, iy, -oy), a3 = fmaf(n0.w, iy, -oy);
-        float a4 = fmaf(n2.x, iz, -oz), a5 = fmaf(n2.y, iz, -oz);
-        float c0 = fmaf(n1.x, ix, -ox), c1 = fmaf(n1.y, ix, -ox);
-        float c2 = fmaf(n1.z, iy, -oy), c3 = fmaf(n1.w, iy, -oy);
-        float c4 = fmaf(n2.z, iz, -oz), c5 = fmaf(n2.w, iz, -oz);
-        float lo0 = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), 0.f));
-        float hi0 = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), tmax));
-        float lo1 = fmaxf(fmaxf(fminf(c0, c1), fminf(c2, c3)), fmaxf(fminf(c4, c5), 0.f));
-        float hi1 = fminf(fminf(fmaxf(c0, c1), fmaxf(c2, c3)), fminf(fmaxf(c4, c5), tmax));
-        bool h0 = lo0 <= hi0, h1 = lo1 <= hi1;
-        if (!h0 && !h1) {
-          if (sp == 0) break;
-          node = stack[--sp];
-          continue;
-        }
-        if (h0 && h1) {
-          int nearc = n3.x, farc = n3.y;
-          if (lo1 < lo0) { nearc = n3.y; farc = n3.x; }
-          stack[sp++] = farc;
-          node = nearc;
-        } else {
-          node = h0 ? n3.x : n3.y;
-        }
-      } else {
-        uint32_t code = ~(uint32_t)node;
-        uint32_t first = code >> 3, count = (code & 7u) + 1u;
-        const float4* t = s.tris + 3 * first;
-        if (COUNT) cnt->tris += count;
-        for (uint32_t k = 0; k < count; ++k, t += 3) {
-          float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
-          float th, u, v;
-          if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
-            prim = (int)(first + k);
-            if (ANY) return prim;
-            tmax = th;
-            b1 = u;
-            b2 = v;
-          }
-        }
-        if (sp == 0) break;
-        node = stack[--sp];
-      }
+// Per-ray constants shared by both traversals.
+struct RayConst {
+  WtRay wr;
+  float ix, iy, iz;  // reciprocal direction (tiny components clamped to 2^-80)
+};
+
+GYT_D RayConst ray_const(float3 o, float3 d) {
+  RayConst c;
+  c.wr = wt_setup(o, d);
+  const float ooeps = 8.271806125530277e-25f;  // 2^-80
+  c.ix = 1.f / (fabsf(d.x) > ooeps ? d.x : copysignf(ooeps, d.x));
+  c.iy = 1.f / (fabsf(d.y) > ooeps ? d.y : copysignf(ooeps, d.y));
+  c.iz = 1.f / (fabsf(d.z) > ooeps ? d.z : copysignf(ooeps, d.z));
+  return c;
+}
+
+// Triangles [first, first + count) in leaf order against the ray. ANY stops
+// at the first hit (returns true).
+template <bool ANY, bool COUNT>
+GYT_D bool test_tris(const DevScene& s, const WtRay& wr, uint32_t first, uint32_t count, float& tmax, float& b1,
+                     float& b2, int& prim, TraceCount* cnt) {
+  if (COUNT) cnt->tris += count;
+  for (uint32_t k = 0; k < count; ++k) {
+    const float4* t = s.tris + 3 * (size_t)(first + k);
+    float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
+    float th, u, v;
+    if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
+      prim = (int)(first + k);
+      if (ANY) return true;
+      tmax = th;
+      b1 = u;
+      b2 = v;
     }
   }
+  return false;
+}
+
+// Binary BVH (two child boxes per 64-byte node, gyt_bvh_host.h), one step =
+// one inner node or one leaf. The stack holds one far child per level.
+struct BinaryTraversal {
+  int node, sp;
+  int stack[kBStack];
+
+  GYT_D void init() { node = 0; sp = 0; }
+
+  // Returns true when the traversal is finished (or, for ANY, on a hit).
+  template <bool ANY, bool COUNT>
+  GYT_D bool step(const DevScene& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
+                  TraceCount* cnt) {
+    if (node >= 0) {
+      if (COUNT) cnt->nodes++;
+      const float4* n = s.nodes + 4 * (size_t)node;
+      float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
+      int4 n3 = __ldg((const int4*)(n + 3));
+      const float ox = o.x * rc.ix, oy = o.y * rc.iy, oz = o.z * rc.iz;
+      float a0 = fmaf(n0.x, rc.ix, -ox), a1 = fmaf(n0.y, rc.ix, -ox);
+      float a2 = fmaf(n0.z, rc.iy, -oy), a3 = fmaf(n0.w, rc.iy, -oy);
+      float a4 = fmaf(n2.x, rc.iz, -oz), a5 = fmaf(n2.y, rc.iz, -oz);
+      float c0 = fmaf(n1.x, rc.ix, -ox), c1 = fmaf(n1.y, rc.ix, -ox);
+      float c2 = fmaf(n1.z, rc.iy, -oy), c3 = fmaf(n1.w, rc.iy, -oy);
+      float c4 = fmaf(n2.z, rc.iz, -oz), c5 = fmaf(n2.w, rc.iz, -oz);
+      float lo0 = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), 0.f));
+      float hi0 = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), tmax));
+      float lo1 = fmaxf(fmaxf(fminf(c0, c1), fminf(c2, c3)), fmaxf(fminf(c4, c5), 0.f));
+      float hi1 = fminf(fminf(fmaxf(c0, c1), fmaxf(c2, c3)), fminf(fmaxf(c4, c5), tmax));
+      bool h0 = lo0 <= hi0, h1 = lo1 <= hi1;
+      if (!h0 && !h1) {
+        if (sp == 0) return true;
+        node = stack[--sp];
+        return false;
+      }
+      if (h0 && h1) {
+        int nearc = n3.x, farc = n3.y;
+        if (lo1 < lo0) { nearc = n3.y; farc = n3.x; }
+        stack[sp++] = farc;
+        node = nearc;
+      } else {
+        node = h0 ? n3.x : n3.y;
+      }
+      return false;
+    }
+    uint32_t code = ~(uint32_t)node;
+    if (test_tris<ANY, COUNT>(s, rc.wr, code >> 3, (code & 7u) + 1u, tmax, b1, b2, prim, cnt)) return true;
+    if (sp == 0) return true;
+    node = stack[--sp];
+    return false;
+  }
+};
+
+// Byte k of w as a float: PRMT builds the bit pattern 2^23 + byte, the
+// subtraction removes 2^23 (both exact).
+GYT_D float qbyte(uint32_t w, int k) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440 + k)) - 8388608.f; }
+
+// 8-wide BVH with quantized child boxes (gyt_bvh_host.h); one step = one node
+// (its leaf children nearer than the first hit inner child are tested in
+// the same step) or one pending child of a group. Stack entries are child
+// groups, at most one per level: x = node whose children are pending, y =
+// inner mask (bits 0-7) | children left (bits 8-10) | their slots near to far
+// (3 bits each from bit 11), z = a lower bound of their entry distances.
+struct WideTraversal {
+  uint32_t node;
+  int sp;
+  bool have_node;
+  uint3 stack[kWStack];
+
+  GYT_D void init() { node = 0; sp = 0; have_node = true; }
+
+  template <bool ANY, bool COUNT>
+  GYT_D bool step(const DevScene& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
+                  TraceCount* cnt) {
+    if (!have_node) {
+      // next pending child of the nearest group that can still be hit
+      while (sp > 0) {
+        uint3 e = stack[sp - 1];
+        if (__uint_as_float(e.z) > tmax) { --sp; continue; }
+        const uint32_t m = (e.y >> 8) & 7u, slot = (e.y >> 11) & 7u;
+        if (m == 1) --sp;
+        else stack[sp - 1].y = (e.y & 0xffu) | ((m - 1) << 8) | ((e.y >> 14) << 11);
+        const uint32_t emask = e.y & 0xffu;
+        const uint4 pw = __ldg(s.wnodes + 5 * (size_t)e.x + 1);
+        if ((emask >> slot) & 1u) {
+          node = pw.x + __popc(emask & ((1u << slot) - 1u));
+          have_node = true;
+          return false;
+        }
+        const uint32_t meta = ((slot < 4 ? pw.z : pw.w) >> (8 * (slot & 3u))) & 0xffu;
+        if (test_tris<ANY, COUNT>(s, rc.wr, pw.y + (meta & 31u), meta >> 5, tmax, b1, b2, prim, cnt)) return true;
+        return false;
+      }
+      return true;
+    }
+    if (COUNT) cnt->nodes++;
+    const uint4* n = s.wnodes + 5 * (size_t)node;
+    uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
+    const float sx = __int_as_float(((int)(int8_t)(w0.w & 0xffu) + 127) << 23);
+    const float sy = __int_as_float(((int)(int8_t)((w0.w >> 8) & 0xffu) + 127) << 23);
+    const float sz = __int_as_float(((int)(int8_t)((w0.w >> 16) & 0xffu) + 127) << 23);
+    const uint32_t imask = w0.w >> 24;
+    const float ax = sx * rc.ix, ay = sy * rc.iy, az = sz * rc.iz;
+    const float bx = (__uint_as_float(w0.x) - o.x) * rc.ix, by = (__uint_as_float(w0.y) - o.y) * rc.iy,
+                bz = (__uint_as_float(w0.z) - o.z) * rc.iz;
+    uint32_t key[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int k = i & 3;
+      const float t0x = fmaf(qbyte(i < 4 ? w2.x : w2.y, k), ax, bx), t1x = fmaf(qbyte(i < 4 ? w2.z : w2.w, k), ax, bx);
+      const float t0y = fmaf(qbyte(i < 4 ? w3.x : w3.y, k), ay, by), t1y = fmaf(qbyte(i < 4 ? w3.z : w3.w, k), ay, by);
+      const float t0z = fmaf(qbyte(i < 4 ? w4.x : w4.y, k), az, bz), t1z = fmaf(qbyte(i < 4 ? w4.z : w4.w, k), az, bz);
+      const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.f));
+      const float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tmax));
+      const uint32_t meta = ((i < 4 ? w1.z : w1.w) >> (8 * k)) & 0xffu;
+      const bool live = ((imask >> i) & 1u) || meta;
+      key[i] = (tn <= tf && live) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)i) : 0xffffffffu;
+    }
+#define GYT_CX(a, b) { uint32_t lo_ = min(key[a], key[b]), hi_ = max(key[a], key[b]); key[a] = lo_; key[b] = hi_; }
+    GYT_CX(0, 1) GYT_CX(2, 3) GYT_CX(4, 5) GYT_CX(6, 7)
+    GYT_CX(0, 2) GYT_CX(1, 3) GYT_CX(4, 6) GYT_CX(5, 7)
+    GYT_CX(1, 2) GYT_CX(5, 6) GYT_CX(0, 4) GYT_CX(3, 7)
+    GYT_CX(1, 5) GYT_CX(2, 6)
+    GYT_CX(1, 4) GYT_CX(3, 6)
+    GYT_CX(2, 4) GYT_CX(3, 5)
+    GYT_CX(3, 4)
+#undef GYT_CX
+    have_node = false;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (!have_node && key[k] != 0xffffffffu && __uint_as_float(key[k] & ~7u) <= tmax) {
+        const uint32_t slot = key[k] & 7u;
+        if ((imask >> slot) & 1u) {
+          uint32_t list = 0, m = 0;
+#pragma unroll
+          for (int j = k + 1; j < 8; ++j)
+            if (key[j] != 0xffffffffu) { list |= (key[j] & 7u) << (11 + 3 * m); ++m; }
+          if (m) stack[sp++] = make_uint3(node, imask | (m << 8) | list, key[k] & ~7u);
+          node = w1.x + __popc(imask & ((1u << slot) - 1u));
+          have_node = true;
+        } else {
+          const uint32_t meta = ((slot < 4 ? w1.z : w1.w) >> (8 * (slot & 3u))) & 0xffu;
+          if (test_tris<ANY, COUNT>(s, rc.wr, w1.y + (meta & 31u), meta >> 5, tmax, b1, b2, prim, cnt)) return true;
+        }
+      }
+    }
+    return !have_node && sp == 0;
+  }
+};
+
+template <int W>
+struct TraversalOf { using type = BinaryTraversal; };
+template <>
+struct TraversalOf<8> { using type = WideTraversal; };
+
+// The analytic spheres after the BVH (linear; the configurations hold few).
+template <bool ANY>
+GYT_D void trace_spheres(const DevScene& s, float3 o, float3 d, float& tmax, int& prim) {
   for (int k = 0; k < s.n_spheres; ++k) {
+    if (ANY && prim >= 0) return;
     float4 sp4 = __ldg(s.spheres + k);
     Ray r = sphere_object_ray(o, d, tmax, 0.f);
     float th;
     if (sphere_root(sp4, r, &th)) {
       prim = s.n_tris + k;
-      if (ANY) return prim;
       tmax = th;
     }
   }
+}
+
+// Closest hit (ANY = false) or occlusion (ANY = true) of one ray over the BVH
+// (binary or 8-wide) and the spheres. Returns the triangle's leaf position
+// (< n_tris; the original id is in tris[3k].w), n_tris + sphere index, or -1.
+// tmax is updated to the hit distance; spheres report the distance along the
+// re-made object ray of Sphere::Intersect (shape/Sphere.h:35).
+template <int W, bool ANY, bool COUNT = false>
+GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, float& b2, TraceCount* cnt = nullptr) {
+  int prim = -1;
+  if (s.n_tris > 0) {
+    RayConst rc = ray_const(o, d);
+    typename TraversalOf<W>::type tv;
+    tv.init();
+    while (!tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, cnt)) {
+    }
+  }
+  trace_spheres<ANY>(s, o, d, tmax, prim);
   return prim;
+}
+
+// Persistent traversal with dynamic ray fetching: every lane of a warp keeps
+// a ray; lanes whose ray is finished take new ray indices (one atomicAdd per
+// warp) before the next traversal step, so warps stay full until the queue
+// runs dry. load(i, o, d, tmax) fetches ray i; done(i, prim, tmax, b1, b2)
+// consumes its result.
+template <int W, bool ANY, bool COUNT, class Load, class Done>
+GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load load, Done done,
+                            unsigned long long* counters) {
+  const uint32_t lane = threadIdx.x & 31u;
+  int ri = -1;  // -1 idle, -2 queue exhausted
+  float3 o = mk(0.f, 0.f, 0.f), d = o;
+  float tmax = 0.f, b1 = 0.f, b2 = 0.f;
+  int prim = -1;
+  RayConst rc;
+  typename TraversalOf<W>::type tv;
+  TraceCount cnt;
+  for (;;) {
+    const uint32_t idle = __ballot_sync(0xffffffffu, ri == -1);
+    if (idle) {
+      const int leader = __ffs(idle) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(next, (uint32_t)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (ri == -1) {
+        const uint32_t r = base + __popc(idle & ((1u << lane) - 1u));
+        if (r < n) {
+          ri = (int)r;
+          load(r, o, d, tmax);
+          b1 = b2 = 0.f;
+          prim = -1;
+          rc = ray_const(o, d);
+          tv.init();
+          if (s.n_tris == 0) {
+            trace_spheres<ANY>(s, o, d, tmax, prim);
+            done((uint32_t)ri, prim, tmax, b1, b2);
+            ri = -1;
+          }
+        } else {
+          ri = -2;
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, ri == -2)) break;
+    if (ri >= 0) {
+      // a few steps per fetch check keep the ballot cost small
+#pragma unroll 1
+      for (int k = 0; k < 4; ++k) {
+        if (tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, &cnt)) {
+          trace_spheres<ANY>(s, o, d, tmax, prim);
+          done((uint32_t)ri, prim, tmax, b1, b2);
+          ri = -1;
+          break;
+        }
+      }
+    }
+  }
+  if (COUNT) {
+    unsigned long long nodes = cnt.nodes, tris = cnt.tris;
+    for (int off = 16; off > 0; off >>= 1) {
+      nodes += __shfl_down_sync(0xffffffffu, nodes, off);
+      tris += __shfl_down_sync(0xffffffffu, tris, off);
+    }
+    if (lane == 0) {
+      atomicAdd(counters, nodes);
+      atomicAdd(counters + 1, tris);
+    }
+  }
 }
 
 // Hit triangle k in leaf order: positions, shading normals, face normal
@@ -303,17 +527,28 @@ GYT_D void flush_counts(const TraceCount& c, unsigned long long* g) {
   }
 }
 
-template <bool COUNT>
+template <int W, bool COUNT>
 __global__ void __launch_bounds__(kBlock) k_extend(PathBuf cur, uint32_t n, DevScene s, float4* __restrict__ hits,
-                                                   unsigned long long* counters) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 o = cur.o[i], d = cur.d[i];
-  float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
-  TraceCount c;
-  int prim = trace<false, COUNT>(s, f3(o), f3(d), tmax, b1, b2, &c);
-  hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
-  if (COUNT) flush_counts(c, counters);
+                                                   uint32_t* __restrict__ fetch, unsigned long long* counters) {
+  persistent_trace<W, false, COUNT>(
+      s, fetch, n,
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        o = f3(cur.o[i]);
+        d = f3(cur.d[i]);
+        tmax = __int_as_float(0x7f800000);
+      },
+      [&](uint32_t i, int prim, float tmax, float b1, float b2) {
+        hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
+      },
+      counters);
+}
+
+// Append to a compact queue: one atomicAdd per warp.
+GYT_D uint32_t queue_slot(uint32_t* count) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(count, g.size());
+  return g.shfl(base, 0) + g.thread_rank();
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
@@ -332,7 +567,6 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   float3 L = f3(cur.L[i]);
   const uint32_t bounce = depth;
   bool alive = false;
-  float4 sc = zero4, mc = zero4;
   if (prim < 0) {
     // PT.cpp:18-21: environment emission on the camera ray or after a delta bounce
     if ((depth == 0 || delta) && s.has_env) L = L + tp * env_lookup(s.env, rd);
@@ -417,11 +651,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
             float dis = length(dd);
             dd = dd / dis;
             float3 so = org + dd * kRayEps;
-            q.so[i] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
-            q.sd[i] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(bounce));
             float w1 = power_heuristic(pdf, spdf);
             float3 c = tp * (Li * f * cosT / pdf) * w1 / lsel;
-            sc = make_float4(c.x, c.y, c.z, 1.f);
+            const uint32_t j = queue_slot(q.counts);
+            q.so[j] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
+            q.sd[j] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(i));
+            q.sc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(bounce));
           }
         }
         // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
@@ -434,10 +669,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
           float lpdf = env_light ? env_pdf_dir(s.env, wi2) : tri_light_pdf(l, h, o2, wi2);
           if (lpdf != 0.f) {
             float w2 = power_heuristic(pdf2, lpdf);
-            q.mo[i] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
-            q.md[i] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
             float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
-            mc = make_float4(c.x, c.y, c.z, 1.f);
+            const uint32_t j = queue_slot(q.counts + 1);
+            q.mo[j] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
+            q.md[j] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
+            q.mc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(i));
           }
         }
       }
@@ -474,8 +710,79 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   }
   cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
   cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
-  q.sc[i] = sc;
-  q.mc[i] = mc;
+}
+
+// Next-event shadow rays (any hit): an unoccluded ray adds its contribution
+// to its path's radiance (VisibilityTester::Unoccluded, Visibility.cpp:7-10).
+template <int W, bool COUNT>
+__global__ void __launch_bounds__(kBlock) k_shadow(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
+                                                   unsigned long long* counters) {
+  const uint32_t n = *(volatile uint32_t*)q.counts;
+  persistent_trace<W, true, COUNT>(
+      s, q.counts + 3, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        float4 a = q.so[j], b = q.sd[j];
+        o = f3(a);
+        d = f3(b);
+        tmax = a.w;
+      },
+      [&](uint32_t j, int prim, float, float, float) {
+        const uint32_t slot = __float_as_uint(q.sd[j].w);
+        if (prim < 0) {
+          float4 c = q.sc[j], l = cur.L[slot];
+          cur.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.f);
+        } else if (dbg.occ) {
+          const uint32_t b = __float_as_uint(q.sc[j].w);
+          if (b < 64) dbg.occ[cur.pid[slot]] |= 1ull << b;
+        }
+      },
+      counters);
+}
+
+// BSDF-sampled MIS rays (closest hit): the sampled light's emission where the
+// ray reaches it (Integrator.cpp:86-101).
+template <int W, bool COUNT>
+__global__ void __launch_bounds__(kBlock) k_mis(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
+                                                unsigned long long* counters) {
+  const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
+  persistent_trace<W, false, COUNT>(
+      s, q.counts + 4, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        o = f3(q.mo[j]);
+        d = f3(q.md[j]);
+        tmax = __int_as_float(0x7f800000);
+      },
+      [&](uint32_t j, int prim, float, float b1, float b2) {
+        const float4 md = q.md[j], mc = q.mc[j];
+        const int li = __float_as_int(md.w);
+        const uint32_t slot = __float_as_uint(mc.w);
+        const float3 wi = f3(md);
+        bool reach = false;
+        float3 add = mk(0.f, 0.f, 0.f);
+        if (prim < 0 && li >= s.n_area) {
+          add = f3(mc) * env_lookup(s.env, wi);  // Integrator.cpp:97-99
+          reach = true;
+        } else if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
+          float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
+          float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
+          float b0 = 1.f - b1 - b2;
+          float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
+          if (dot(ns, -wi) > 0.f) {
+            const float4* r = s.ltab + kLightRec * li;
+            add = f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
+          }
+          reach = true;
+        }
+        if (reach) {
+          float4 l = cur.L[slot];
+          cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
+          if (dbg.mis) {
+            const uint32_t b = __float_as_uint(q.mo[j].w);
+            if (b < 64) dbg.mis[cur.pid[slot]] |= 1ull << b;
+          }
+        }
+      },
+      counters);
 }
 
 GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) {
@@ -486,67 +793,14 @@ GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) 
   atomicAdd(p + 3, 1.0);
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, uint32_t n, DevScene s, Queues q,
-                                                    double* __restrict__ film, uint32_t res_x,
-                                                    uint32_t* __restrict__ counter, DebugOut dbg,
-                                                    unsigned long long* counters) {
+// Finished paths go to the film (FP64 atomics, Film::AddSample with the box
+// filter, visual/Film.h:61-87); live paths are compacted into the next pool.
+__global__ void __launch_bounds__(kBlock) k_finish(PathBuf cur, PathBuf nxt, uint32_t n, double* __restrict__ film,
+                                                   uint32_t res_x, uint32_t* __restrict__ counter, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float3 L = f3(cur.L[i]);
-  float4 sc = q.sc[i];
-  TraceCount cnt;
-  bool shadow = sc.w != 0.f, mis = false;
-  if (shadow) {
-    float4 so = q.so[i], sd = q.sd[i];
-    float tmax = so.w, b1, b2;
-    if (trace<true, COUNT>(s, f3(so), f3(sd), tmax, b1, b2, &cnt) < 0) {
-      L = L + f3(sc);
-    } else if (dbg.occ) {
-      uint32_t b = __float_as_uint(sd.w);
-      if (b < 64) dbg.occ[cur.pid[i]] |= 1ull << b;
-    }
-  }
-  float4 mc = q.mc[i];
-  if (mc.w != 0.f) {
-    mis = true;
-    float4 mo = q.mo[i], md = q.md[i];
-    int li = __float_as_int(md.w);
-    float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
-    float3 wi = f3(md);
-    int prim = trace<false, COUNT>(s, f3(mo), wi, tmax, b1, b2, &cnt);
-    bool reach = false;
-    if (prim < 0 && li >= s.n_area) {
-      L = L + f3(mc) * env_lookup(s.env, wi);  // Integrator.cpp:97-99
-      reach = true;
-    }
-    if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
-      float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
-      float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
-      float b0 = 1.f - b1 - b2;
-      float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
-      if (dot(ns, -wi) > 0.f) {
-        const float4* r = s.ltab + kLightRec * li;
-        L = L + f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
-      }
-      reach = true;
-    }
-    if (reach && dbg.mis) {
-      uint32_t b = __float_as_uint(mo.w);
-      if (b < 64) dbg.mis[cur.pid[i]] |= 1ull << b;
-    }
-  }
-  if (COUNT) {
-    flush_counts(cnt, counters);
-    cg::coalesced_group w = cg::coalesced_threads();
-    unsigned long long ns_ = cg::reduce(w, (unsigned long long)(shadow ? 1 : 0), cg::plus<unsigned long long>());
-    unsigned long long nm_ = cg::reduce(w, (unsigned long long)(mis ? 1 : 0), cg::plus<unsigned long long>());
-    if (w.thread_rank() == 0) {
-      atomicAdd(counters + 2, ns_);
-      atomicAdd(counters + 3, nm_);
-    }
-  }
   uint32_t meta = cur.meta[i];
+  float4 L4 = cur.L[i];
   if (meta & kAlive) {
     cg::coalesced_group g = cg::coalesced_threads();
     uint32_t base = 0;
@@ -556,12 +810,13 @@ __global__ void __launch_bounds__(kBlock) k_connect(PathBuf cur, PathBuf nxt, ui
     nxt.o[j] = cur.o[i];
     nxt.d[j] = cur.d[i];
     nxt.tp[j] = cur.tp[i];
-    nxt.L[j] = make_float4(L.x, L.y, L.z, 0.f);
+    nxt.L[j] = L4;
     nxt.sidx[j] = cur.sidx[i];
     nxt.meta[j] = meta;
     nxt.pix[j] = cur.pix[i];
     nxt.pid[j] = cur.pid[i];
   } else {
+    const float3 L = f3(L4);
     uint32_t pix = cur.pix[i];
     if (film) {
       uint32_t p = pix & kPixMask;
@@ -592,6 +847,7 @@ __global__ void k_resolve(const double* __restrict__ film, float* __restrict__ r
   rgb[3ull * i + 2] = (float)(p[2] / w);
 }
 
+template <int W>
 __global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ rays, int any, int32_t* prim,
                             float* tout, float* b1out, float* b2out) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -599,7 +855,7 @@ __global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ ra
   const float* r = rays + 7 * i;
   float3 o = mk(r[0], r[1], r[2]), d = mk(r[3], r[4], r[5]);
   float tmax = r[6], b1 = 0.f, b2 = 0.f;
-  int p = any ? (trace<true>(s, o, d, tmax, b1, b2) >= 0 ? 1 : 0) : trace<false>(s, o, d, tmax, b1, b2);
+  int p = any ? (trace<W, true>(s, o, d, tmax, b1, b2) >= 0 ? 1 : 0) : trace<W, false>(s, o, d, tmax, b1, b2);
   if (!any && p >= 0 && p < s.n_tris) p = __float_as_int(__ldg(s.tris + 3 * p).w);
   prim[i] = p;
   if (!any) {
@@ -624,11 +880,25 @@ __global__ void k_enum(SobolTables tab, uint32_t m, uint64_t n, const uint32_t* 
 
 inline uint32_t grid_for(uint64_t n) { return (uint32_t)((n + kBlock - 1) / kBlock); }
 
+// Persistent traversal kernels and their grid sizes (blocks per SM at full
+// occupancy times the SM count), computed once per context.
+enum { kPExtend = 0, kPShadow = 1, kPMis = 2 };
+constexpr int kPersistentKinds = 3 * 2 * 2;  // kernel x width (2, 8) x counting
+inline int pindex(int kind, int w, bool count) { return (kind * 2 + (w == 8 ? 1 : 0)) * 2 + (count ? 1 : 0); }
+
+template <int W, bool C>
+const void* persistent_fn(int kind) {
+  if (kind == kPExtend) return (const void*)k_extend<W, C>;
+  if (kind == kPShadow) return (const void*)k_shadow<W, C>;
+  return (const void*)k_mis<W, C>;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host side ---
 struct gyt_context {
   int device = 0;
+  int pgrid[kPersistentKinds] = {};
   cudaStream_t stream = nullptr;
   std::string err;
   uint32_t capacity = 1u << 21;
@@ -648,8 +918,9 @@ struct gyt_context {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<void*> pool_allocs;
   int profile = 0;
+  int bvh_width = 2;
   cudaEvent_t kev[8] = {};
-  unsigned long long* d_counters = nullptr;  // node visits, tri tests, shadow rays, MIS rays
+  unsigned long long* d_counters = nullptr;  // node visits and triangle tests per traversal kernel
   GytProfile prof = {};
 };
 
@@ -772,6 +1043,7 @@ int32_t ensure_pool(gyt_context* ctx) {
   GYT_CK(ctx, dalloc(L, &q.md, n));
   GYT_CK(ctx, dalloc(L, &q.mc, n));
   GYT_CK(ctx, dalloc(L, &q.hit, n));
+  GYT_CK(ctx, dalloc(L, &q.counts, 8));
   ctx->pool_cap = ctx->capacity;
   return GYT_OK;
 }
@@ -792,10 +1064,16 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
   const bool prof = ctx->profile > 0, cnt = ctx->profile > 1;
   uint32_t launches = 0;
   unsigned long long slots = 0;
-  if (cnt) GYT_CK(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), s));
+  const int W = scene->dev.wnodes ? 8 : 2;
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, cnt)], g_sh = ctx->pgrid[pindex(kPShadow, W, cnt)],
+            g_mis = ctx->pgrid[pindex(kPMis, W, cnt)];
+  Queues q = ctx->q;
+  if (cnt) GYT_CK(ctx, cudaMemsetAsync(ctx->d_counters, 0, 6 * sizeof(unsigned long long), s));
+  uint32_t hcounts[8];
   GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
   while (generated < total || active > 0) {
     uint32_t n_new = (uint32_t)std::min<unsigned long long>(ctx->capacity - active, total - generated);
+    GYT_CK(ctx, cudaMemsetAsync(q.counts, 0, 8 * sizeof(uint32_t), s));
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[0], s));
     if (n_new) {
       k_generate<<<grid_for(n_new), kBlock, 0, s>>>(ctx->pool[cur], active, n_new, generated, cam, p->spp, d_list, tab);
@@ -803,51 +1081,69 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
     }
     generated += n_new;
     active += n_new;
+    const PathBuf P = ctx->pool[cur], N = ctx->pool[cur ^ 1];
+    const DevScene& D = scene->dev;
+    unsigned long long* C = ctx->d_counters;
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[1], s));
-    if (cnt) k_extend<true><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, ctx->d_counters);
-    else k_extend<false><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, ctx->q.hit, nullptr);
+    if (W == 8) {
+      if (cnt) k_extend<8, true><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, C);
+      else k_extend<8, false><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+    } else {
+      if (cnt) k_extend<2, true><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, C);
+      else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+    }
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[2], s));
-    k_shade<<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], active, scene->dev, prm, ctx->q, tab, dbg);
-    GYT_CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(uint32_t), s));
+    k_shade<<<grid_for(active), kBlock, 0, s>>>(P, active, D, prm, q, tab, dbg);
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[3], s));
-    if (cnt)
-      k_connect<true><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], ctx->pool[cur ^ 1], active, scene->dev,
-                                                          ctx->q, d_film, cam.res_x, ctx->d_counter, dbg, ctx->d_counters);
-    else
-      k_connect<false><<<grid_for(active), kBlock, 0, s>>>(ctx->pool[cur], ctx->pool[cur ^ 1], active, scene->dev,
-                                                           ctx->q, d_film, cam.res_x, ctx->d_counter, dbg, nullptr);
+    if (W == 8) {
+      if (cnt) k_shadow<8, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
+      else k_shadow<8, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+    } else {
+      if (cnt) k_shadow<2, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
+      else k_shadow<2, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+    }
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[4], s));
-    launches += 3;
+    if (W == 8) {
+      if (cnt) k_mis<8, true><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, C + 4);
+      else k_mis<8, false><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+    } else {
+      if (cnt) k_mis<2, true><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, C + 4);
+      else k_mis<2, false><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+    }
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[5], s));
+    k_finish<<<grid_for(active), kBlock, 0, s>>>(P, N, active, d_film, cam.res_x, q.counts + 5, dbg);
+    if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[6], s));
+    launches += 5;
     GYT_CK(ctx, cudaGetLastError());
-    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, ctx->d_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, q.counts, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GYT_CK(ctx, cudaStreamSynchronize(s));
+    std::memcpy(hcounts, ctx->h_counter, sizeof(hcounts));
     if (prof) {
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < 6; ++k) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->kev[k], ctx->kev[k + 1]);
         ctx->prof.ms[k] += ms;
+        if (k != 0 || n_new) ctx->prof.launches[k]++;
       }
-      if (n_new) ctx->prof.launches[0]++;
-      ctx->prof.launches[1]++;
-      ctx->prof.launches[2]++;
-      ctx->prof.launches[3]++;
-      ctx->prof.closest_rays += active;
+      ctx->prof.rays[0] += active;
+      ctx->prof.rays[1] += hcounts[0];
+      ctx->prof.rays[2] += hcounts[1];
     }
     slots += active;
     rays += active;
-    active = *ctx->h_counter;
+    active = hcounts[5];
     cur ^= 1;
     if (++iters > 100000) return fail(ctx, GYT_ERR_WATCHDOG, "render: wavefront iteration cap reached");
   }
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
   if (cnt) {
-    unsigned long long c[4];
+    unsigned long long c[6];
     GYT_CK(ctx, cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
-    ctx->prof.node_visits += c[0];
-    ctx->prof.tri_tests += c[1];
-    ctx->prof.shadow_rays += c[2];
-    ctx->prof.closest_rays += c[3];
+    for (int k = 0; k < 3; ++k) {
+      ctx->prof.node_visits[k] += c[2 * k];
+      ctx->prof.tri_tests[k] += c[2 * k + 1];
+    }
   }
   if (stats) {
     stats->paths = total;
@@ -873,7 +1169,7 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counter, sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_counter, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_counter, 8 * sizeof(uint32_t));
   const size_t sob = GYT_SOBOL_DIMS * GYT_SOBOL_COLS;
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_sobol, (sob + 64) * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(c->d_sobol, 0, (sob + 64) * sizeof(uint32_t));
@@ -896,7 +1192,23 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreate(&c->kev[k]);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counters, 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counters, 6 * sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind)
+      for (int w : {2, 8})
+        for (int cntm = 0; cntm < 2 && e == cudaSuccess; ++cntm) {
+          const void* fn = w == 8 ? (cntm ? persistent_fn<8, true>(kind) : persistent_fn<8, false>(kind))
+                                  : (cntm ? persistent_fn<2, true>(kind) : persistent_fn<2, false>(kind));
+          int nb = 0;
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kBlock, 0);
+          // MIS rays are rare (only BSDF samples that would reach the sampled
+          // light): one block per SM keeps the launch cheap
+          if (kind == kPMis) nb = 1;
+          c->pgrid[pindex(kind, w, cntm != 0)] = std::max(1, nb) * std::max(1, sms);
+        }
+  }
   if (e != cudaSuccess) {
     gyt_context_destroy(c);
     return e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA;
@@ -940,6 +1252,13 @@ int32_t gyt_context_set_profile(gyt_context* c, int32_t mode) {
   if (!c) return GYT_ERR_INVALID;
   if (mode < 0 || mode > 2) return fail(c, GYT_ERR_INVALID, "profile mode must be 0, 1 or 2");
   c->profile = mode;
+  return GYT_OK;
+}
+
+int32_t gyt_context_set_bvh_width(gyt_context* c, int32_t width) {
+  if (!c) return GYT_ERR_INVALID;
+  if (width != 2 && width != 8) return fail(c, GYT_ERR_INVALID, "bvh width must be 2 or 8");
+  c->bvh_width = width;
   return GYT_OK;
 }
 
@@ -1071,10 +1390,25 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       for (int i = 1; i < nl + 1; ++i) cdf[i] /= fint;
     }
   }
-  BvhHost bvh;
-  if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bvh))
-    return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
-  if (bvh.max_depth >= (uint32_t)kStack) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+  // acceleration structure: binary (two child boxes per 64-byte node) or
+  // 8-wide with quantized child boxes (80-byte nodes), per context setting
+  WideBvhHost wide;
+  BvhHost bin;
+  const bool use_wide = ctx->bvh_width == 8;
+  if (use_wide) {
+    if (!build_wide_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &wide))
+      return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
+    if (wide.max_depth >= (uint32_t)kWStack)
+      return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+  } else {
+    if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bin))
+      return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
+    if (bin.max_depth >= (uint32_t)kBStack)
+      return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+  }
+  struct {
+    const std::vector<uint32_t>& order;
+  } bvh{use_wide ? wide.order : bin.order};
   // leaf-order triangle positions and shading data
   auto bits = [](int v) { float f; std::memcpy(&f, &v, 4); return f; };
   std::vector<float4> tris((size_t)bvh.order.size() * 3), tnrm((size_t)bvh.order.size() * 3);
@@ -1122,9 +1456,17 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   };
   DevScene& ds = sc->dev;
   cudaError_t e = cudaSuccess;
-  float4* nodes = nullptr;
-  if (e == cudaSuccess) e = up(&nodes, (const float4*)bvh.nodes.data(), bvh.nodes.size() / 4);
-  ds.nodes = nodes;
+  if (use_wide) {
+    uint4* nodes = nullptr;
+    if (e == cudaSuccess) e = up(&nodes, (const uint4*)wide.nodes.data(), wide.nodes.size() / 4);
+    ds.wnodes = nodes;
+    ds.nodes = nullptr;
+  } else {
+    float4* nodes = nullptr;
+    if (e == cudaSuccess) e = up(&nodes, (const float4*)bin.nodes.data(), bin.nodes.size() / 4);
+    ds.nodes = nodes;
+    ds.wnodes = nullptr;
+  }
   float4* dtris = nullptr;
   if (e == cudaSuccess) e = up(&dtris, tris.data(), tris.size());
   ds.tris = dtris;
@@ -1179,8 +1521,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   ds.n_tris = (int)d->n_triangles;
   ds.n_spheres = (int)d->n_spheres;
   sc->n_tris = d->n_triangles;
-  sc->n_nodes = bvh.nodes.size() / 16;
-  sc->bvh_depth = bvh.max_depth;
+  sc->n_nodes = use_wide ? wide.nodes.size() / 20 : bin.nodes.size() / 16;
+  sc->bvh_depth = use_wide ? wide.max_depth : bin.max_depth;
   if (e != cudaSuccess) {
     gyt_scene_destroy(sc);
     return fail(ctx, e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA,
@@ -1308,7 +1650,10 @@ int32_t gyt_intersect(gyt_context* ctx, const gyt_scene* scene, uint64_t n, cons
   GYT_CK(ctx, dalloc(tmp, &d1, n));
   GYT_CK(ctx, dalloc(tmp, &d2, n));
   GYT_CK(ctx, cudaMemcpy(dr, rays, 7 * n * sizeof(float), cudaMemcpyHostToDevice));
-  k_intersect<<<grid_for(n), kBlock, 0, ctx->stream>>>(scene->dev, n, dr, any_hit ? 1 : 0, dp, dt, d1, d2);
+  if (scene->dev.wnodes)
+    k_intersect<8><<<grid_for(n), kBlock, 0, ctx->stream>>>(scene->dev, n, dr, any_hit ? 1 : 0, dp, dt, d1, d2);
+  else
+    k_intersect<2><<<grid_for(n), kBlock, 0, ctx->stream>>>(scene->dev, n, dr, any_hit ? 1 : 0, dp, dt, d1, d2);
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
   if (prim) GYT_CK(ctx, cudaMemcpy(prim, dp, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
@@ -1478,30 +1823,39 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   q.md = carve<float4>(c, n);
   q.mc = carve<float4>(c, n);
   q.hit = carve<float4>(c, n);
-  uint32_t* counter = carve<uint32_t>(c, 1);
+  q.counts = carve<uint32_t>(c, 8);
   if ((size_t)(c - base) > kNoAllocBytes)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: scratch layout exceeds the array");
 
   Params prm{params->spp, params->max_depth, params->rr_depth};
   SobolTables tab = tables(ctx);
   cudaStream_t s = ctx->stream;
+  const int W = scene->dev.wnodes ? 8 : 2;
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)],
+            g_mis = ctx->pgrid[pindex(kPMis, W, false)];
+  const DevScene& D = scene->dev;
   unsigned long long generated = 0;
   uint32_t active = 0, iters = 0, live = 0;
   int cur = 0;
   while (generated < total || active > 0) {
     uint32_t n_new = (uint32_t)std::min<unsigned long long>(paths_in_flight - active, total - generated);
+    GYT_CK(ctx, cudaMemsetAsync(q.counts, 0, 8 * sizeof(uint32_t), s));
     if (n_new)
       k_generate<<<grid_for(n_new), kBlock, 0, s>>>(pool[cur], active, n_new, generated, cam, params->spp, nullptr, tab);
     generated += n_new;
     active += n_new;
-    k_extend<false><<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, scene->dev, q.hit, nullptr);
-    k_shade<<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, scene->dev, prm, q, tab, DebugOut{});
-    GYT_CK(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s));
-    k_connect<false><<<grid_for(active), kBlock, 0, s>>>(pool[cur], pool[cur ^ 1], active, scene->dev, q, d_film,
-                                                         cam.res_x, counter, DebugOut{}, nullptr);
+    if (W == 8) k_extend<8, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
+    else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
+    k_shade<<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, D, prm, q, tab, DebugOut{});
+    if (W == 8) k_shadow<8, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    else k_shadow<2, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    if (W == 8) k_mis<8, false><<<g_mis, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    else k_mis<2, false><<<g_mis, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    k_finish<<<grid_for(active), kBlock, 0, s>>>(pool[cur], pool[cur ^ 1], active, d_film, cam.res_x, q.counts + 5,
+                                                DebugOut{});
     GYT_CK(ctx, cudaGetLastError());
     // pageable destination: the copy completes before cudaMemcpyAsync returns
-    GYT_CK(ctx, cudaMemcpyAsync(&live, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaMemcpyAsync(&live, q.counts + 5, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GYT_CK(ctx, cudaStreamSynchronize(s));
     active = live;
     cur ^= 1;

@@ -104,14 +104,15 @@ typedef struct {
 } GytRenderStats;
 
 /* Kernel-level profile of the renders since the last gyt_profile_read.
- * Kernel slots: 0 generate, 1 extend, 2 shade, 3 connect. */
+ * Kernel slots: 0 generate, 1 extend (continuation rays), 2 shade,
+ * 3 shadow (next-event shadow rays), 4 mis (BSDF-sampled MIS rays),
+ * 5 finish (film and compaction). Traversal slots: 0 extend, 1 shadow, 2 mis. */
 typedef struct {
-  float ms[4];                    /* summed device time per kernel (CUDA events) */
-  uint32_t launches[4];
-  uint64_t closest_rays;          /* continuation + MIS closest-hit rays traced */
-  uint64_t shadow_rays;           /* any-hit rays traced */
-  uint64_t node_visits;           /* BVH nodes fetched (counting mode only) */
-  uint64_t tri_tests;             /* triangle tests (counting mode only) */
+  float ms[6];                    /* summed device time per kernel (CUDA events) */
+  uint32_t launches[6];
+  uint64_t rays[3];               /* rays traced per traversal kernel */
+  uint64_t node_visits[3];        /* BVH nodes fetched (counting mode only) */
+  uint64_t tri_tests[3];          /* triangle tests (counting mode only) */
 } GytProfile;
 
 /* Context on one CUDA device; owns a stream and the path-state pools. */
@@ -123,6 +124,10 @@ int32_t gyt_context_set_capacity(gyt_context* ctx, uint32_t paths_in_flight);
 /* Profiling: 0 off (default), 1 per-kernel event timing, 2 timing plus
  * traversal counters (slower kernels; counts only, not for timing). */
 int32_t gyt_context_set_profile(gyt_context* ctx, int32_t mode);
+/* Branching factor of the BVH built by later gyt_scene_create calls: 2
+ * (binary, two child boxes per 64-byte node; the default) or 8 (quantized
+ * child boxes, 80-byte nodes). Both replace BVHAccel (accelerator/BVHAccel.cpp). */
+int32_t gyt_context_set_bvh_width(gyt_context* ctx, int32_t width);
 /* Copies the accumulated profile into *out and resets it. */
 int32_t gyt_profile_read(gyt_context* ctx, GytProfile* out);
 
