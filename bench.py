@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--depth", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bvh-width", type=int, default=None, choices=[2, 8])
+    ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
     return ap.parse_args()
 
 
@@ -212,7 +213,7 @@ def run_ours(a):
     torch.cuda.set_device(d.local)
     import gyunity_b200 as g
     sd = workload(a)
-    ctx = g.Context(d.local, bvh_width=a.bvh_width)
+    ctx = g.Context(d.local, bvh_width=a.bvh_width, bvh_builder=a.bvh_builder)
     t0 = time.perf_counter()
     scene = g.Scene(sd, ctx)
     scene_s = time.perf_counter() - t0
@@ -258,6 +259,14 @@ def run_ours(a):
     cold_s = time.perf_counter() - t
     s2.close()
 
+    # scene creation with the other binary-BVH builder, for comparison
+    other = "host" if a.bvh_builder == "device" else "device"
+    ctx_o = g.Context(d.local, bvh_width=a.bvh_width, bvh_builder=other)
+    t = time.perf_counter()
+    g.Scene(sd, ctx_o).close()
+    other_s = time.perf_counter() - t
+    ctx_o.close()
+
     out = None
     if d.rank == 0:
         # kernel-level profile of one render (event timing) and traversal counts
@@ -276,10 +285,12 @@ def run_ours(a):
                 "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh, no dataset)",
                 "config": config(a, sd, {"parallelism": "independent frames per GPU" if d.world > 1 else "1 GPU",
-                                         "paths_in_flight": 1 << 21}),
+                                         "paths_in_flight": 1 << 21,
+                                         "bvh": "8-wide, host-built" if a.bvh_width == 8
+                                         else "binary, %s-built" % a.bvh_builder}),
                 "wall_ms_per_step": wall * 1e3 / a.steps,
                 "iterations_per_step": stats[-1]["iterations"],
-                "scene_upload_and_bvh_s": scene_s,
+                "scene_upload_and_bvh_s": {a.bvh_builder: scene_s, other: other_s},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 + 16,
                         "d2h_bytes_per_step": W * H * 3 * 4,
                         "note": "public Render call with the scene resident, image copied to host each step"},
@@ -298,7 +309,7 @@ def run_ours(a):
     d.close()
 
 
-# Algorithmic bytes per path slot and per ray (DESIGN.md lists the fields):
+# Algorithmic bytes per path slot and per ray:
 # path state read by a stage = origin 16 + direction 16 + throughput 16 +
 # radiance 16 + Sobol' index 8 + meta 4 = 76 B; written back by shade = 68 B;
 # closest hit 16 B; a queued segment ray (origin+tmax, direction) 32 B and its

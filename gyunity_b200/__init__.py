@@ -34,7 +34,7 @@ __all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "Rende
 class Context:
     """A CUDA device with its stream and path pools (gyt_context)."""
 
-    def __init__(self, device=0, capacity=None, bvh_width=None):
+    def __init__(self, device=0, capacity=None, bvh_width=None, bvh_builder=None):
         self._lib = load()
         h = ctypes.c_void_p()
         rc = self._lib.gyt_context_create(int(device), ctypes.byref(h))
@@ -46,6 +46,9 @@ class Context:
             self.check(self._lib.gyt_context_set_capacity(self.handle, int(capacity)))
         if bvh_width is not None:
             self.check(self._lib.gyt_context_set_bvh_width(self.handle, int(bvh_width)))
+        if bvh_builder is not None:
+            code = {"host": _c.BVH_BUILD_HOST, "device": _c.BVH_BUILD_DEVICE}.get(bvh_builder, bvh_builder)
+            self.check(self._lib.gyt_context_set_bvh_builder(self.handle, int(code)))
 
     def check(self, rc):
         if rc != 0:
@@ -93,6 +96,53 @@ class Context:
         return self._lib.gyt_render_device_noalloc(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
                                                    ctypes.c_void_p(d_film_ptr), int(paths_in_flight))
 
+    # ---- batched renders ---------------------------------------------------
+    def set_batch_config(self, paths_in_flight=0, stride_blocks_per_sm=0, trace_blocks_per_sm=0, use_graph=True):
+        c = _c.GytBatchConfig(int(paths_in_flight), int(stride_blocks_per_sm), int(trace_blocks_per_sm),
+                              1 if use_graph else 0, 0)
+        self.check(self._lib.gyt_context_set_batch_config(self.handle, ctypes.byref(c)))
+
+    def batch_config(self):
+        c = _c.GytBatchConfig()
+        self.check(self._lib.gyt_context_get_batch_config(self.handle, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in _c.GytBatchConfig._fields_}
+
+    @staticmethod
+    def _batch_arrays(scenes, cameras, params):
+        n = len(scenes)
+        sc = (ctypes.c_void_p * n)(*[s.handle.value for s in scenes])
+        cams = (_c.GytCamera * n)(*[_c.camera_struct(c) for c in cameras])
+        prms = (_c.GytRenderParams * n)(*[_c.params_struct(p) for p in params])
+        return n, sc, cams, prms
+
+    def render_batch_device(self, scenes, cameras, params, d_film_ptrs):
+        """gyt_render_batch_device: instance i = scenes[i] through cameras[i]
+        with params[i], accumulated into the device film at d_film_ptrs[i]."""
+        n, sc, cams, prms = self._batch_arrays(scenes, cameras, params)
+        films = (ctypes.c_void_p * n)(*[int(p) for p in d_film_ptrs])
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_render_batch_device(self.handle, n, sc, cams, prms, films, ctypes.byref(st)))
+        return {"paths": st.paths, "iterations": st.iterations, "launches": st.launches, "ms": st.ms}
+
+    def render_batch(self, scenes, cameras, params):
+        """gyt_render_batch: one host image (h, w, 3) per instance."""
+        n, sc, cams, prms = self._batch_arrays(scenes, cameras, params)
+        imgs = [np.empty((c.res_y, c.res_x, 3), np.float32) for c in cameras]
+        outs = (ctypes.c_void_p * n)(*[im.ctypes.data for im in imgs])
+        self.check(self._lib.gyt_render_batch(self.handle, n, sc, cams, prms, outs))
+        return imgs
+
+    def batch_autotune(self, scenes, cameras, params, scenes_alt=None, sample_spp=1):
+        """gyt_batch_autotune: sets and returns the fastest batch
+        configuration and its throughput (Mpaths/s) on a sample of the batch."""
+        n, sc, cams, prms = self._batch_arrays(scenes, cameras, params)
+        alt = None if scenes_alt is None else (ctypes.c_void_p * n)(*[s.handle.value for s in scenes_alt])
+        best = _c.GytBatchConfig()
+        mp = ctypes.c_float()
+        self.check(self._lib.gyt_batch_autotune(self.handle, n, sc, alt, cams, prms, int(sample_spp),
+                                                ctypes.byref(best), ctypes.byref(mp)))
+        return {f: getattr(best, f) for f, _ in _c.GytBatchConfig._fields_}, mp.value
+
     # ---- parity / debug entry points --------------------------------------
     def sobol(self, dims, indices):
         """sobol::sample (sampler/Sobol.h:46-61) for (dimension, index) pairs."""
@@ -136,6 +186,18 @@ class Scene:
         a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
         self.ctx.check(self.ctx._lib.gyt_scene_info(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return {"triangles": a.value, "bvh_nodes": b.value, "device_bytes": c.value}
+
+    def read_bvh(self):
+        """The binary BVH on the host: node slots (n, 16) float32 in the
+        traversal layout and the scene triangle id of each leaf-order position."""
+        n = ctypes.c_uint64()
+        lib = self.ctx._lib
+        self.ctx.check(lib.gyt_scene_read_bvh(self.handle, None, 0, None, 0, ctypes.byref(n)))
+        nodes = np.zeros((n.value, 16), np.float32)
+        ids = np.zeros(self.info()["triangles"], np.uint32)
+        self.ctx.check(lib.gyt_scene_read_bvh(self.handle, _c.ptr(nodes), nodes.size, _c.ptr(ids), ids.size,
+                                              ctypes.byref(n)))
+        return nodes, ids
 
     def close(self):
         if getattr(self, "handle", None):

@@ -18,9 +18,15 @@ STATUS = {0: "GYT_OK", 1: "GYT_ERR_INVALID", 2: "GYT_ERR_CUDA", 3: "GYT_ERR_OUT_
 # Every entry point include/gyt.h declares (checked by the CPU tests).
 EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_context_set_capacity",
            "gyt_context_set_profile", "gyt_profile_read", "gyt_context_set_bvh_width",
-           "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info", "gyt_render", "gyt_render_device",
+           "gyt_context_set_bvh_builder", "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info",
+           "gyt_scene_read_bvh", "gyt_render", "gyt_render_device",
            "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world",
-           "gyt_render_device_noalloc"]
+           "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
+           "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune"]
+
+# BVH builders (GYT_BVH_BUILD_* in include/gyt.h)
+BVH_BUILD_HOST = 0
+BVH_BUILD_DEVICE = 1
 
 # Path slots of the library's built-in scratch array (GYT_NOALLOC_MAX_PATHS in include/gyt.h).
 NOALLOC_MAX_PATHS = 32768
@@ -63,6 +69,12 @@ class GytProfile(ctypes.Structure):
                 ("node_visits", ctypes.c_uint64 * 3), ("tri_tests", ctypes.c_uint64 * 3)]
 
 
+class GytBatchConfig(ctypes.Structure):
+    _fields_ = [("paths_in_flight", ctypes.c_uint32), ("stride_blocks_per_sm", ctypes.c_uint32),
+                ("trace_blocks_per_sm", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
+                ("bvh_width", ctypes.c_uint32)]
+
+
 KERNELS = ["generate", "extend", "shade", "shadow", "mis", "finish"]
 TRAVERSALS = ["extend", "shadow", "mis"]
 
@@ -88,6 +100,8 @@ def load():
     L.gyt_context_set_profile.argtypes = [P, I32]
     L.gyt_profile_read.argtypes = [P, ctypes.POINTER(GytProfile)]
     L.gyt_context_set_bvh_width.argtypes = [P, I32]
+    L.gyt_context_set_bvh_builder.argtypes = [P, I32]
+    L.gyt_scene_read_bvh.argtypes = [P, P, U64, P, U64, ctypes.POINTER(U64)]
     L.gyt_scene_create.argtypes = [P, ctypes.POINTER(GytSceneDesc), ctypes.POINTER(P)]
     L.gyt_scene_destroy.argtypes = [P]
     L.gyt_scene_destroy.restype = None
@@ -102,6 +116,12 @@ def load():
     L.gyt_sobol.argtypes = [P, U64, P, P, P]
     L.gyt_sobol_enum_index.argtypes = [P, U32, U32, U64, P, P]
     L.gyt_camera_raster_to_world.argtypes = [ctypes.POINTER(GytCamera), P]
+    L.gyt_context_set_batch_config.argtypes = [P, ctypes.POINTER(GytBatchConfig)]
+    L.gyt_context_get_batch_config.argtypes = [P, ctypes.POINTER(GytBatchConfig)]
+    L.gyt_render_batch_device.argtypes = [P, U32, P, P, P, P, ctypes.POINTER(GytRenderStats)]
+    L.gyt_render_batch.argtypes = [P, U32, P, P, P, P]
+    L.gyt_batch_autotune.argtypes = [P, U32, P, P, P, P, U32, ctypes.POINTER(GytBatchConfig),
+                                     ctypes.POINTER(ctypes.c_float)]
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is ctypes.c_int:  # default

@@ -1,6 +1,6 @@
 """Build recipe of the native library ``gyunity_b200/libgyunity_b200.so``.
 
-nvcc compiles the CUDA translation unit for sm_100a only and links the CUDA
+nvcc compiles the CUDA translation units for sm_100a only and links the CUDA
 runtime statically, so the library loads through a plain ``dlopen`` (ctypes
 or a C/C++ host) without any Python or torch dependency.
 """
@@ -11,8 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgyunity_b200.so")
-SOURCES = ["gyt_render.cu", "gyt_bvh_host.cpp"]
-HEADERS = ["gyt_device.cuh", "gyt_bvh_host.h"]
+SOURCES = ["gyt_render.cu", "gyt_bvh_gpu.cu", "gyt_bvh_host.cpp"]
+HEADERS = ["gyt_device.cuh", "gyt_bvh_host.h", "gyt_bvh_gpu.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]

@@ -111,6 +111,8 @@ bool build_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt,
       cb.grow(&cen[3 * t]);
     }
     auto make_leaf = [&](uint32_t start, uint32_t count, int parent, int slot) {
+      // triangles of a leaf in ascending id order (the device builder's order too)
+      std::sort(idx.begin() + start, idx.begin() + start + count);
       uint32_t first = (uint32_t)out->order.size();
       for (uint32_t k = start; k < start + count; ++k) out->order.push_back(idx[k]);
       Box b;

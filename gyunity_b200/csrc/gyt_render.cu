@@ -23,7 +23,6 @@
 // paths stay dense and new paths fill the tail.
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
-#include <cooperative_groups/reduce.h>
 
 #include <algorithm>
 #include <cfloat>
@@ -36,6 +35,7 @@
 
 #include "../../include/gyt.h"
 #include "../_gen/sobol_tables.h"
+#include "gyt_bvh_gpu.h"
 #include "gyt_bvh_host.h"
 #include "gyt_device.cuh"
 
@@ -77,6 +77,7 @@ struct PathBuf {
   uint32_t* meta; // depth 0-7 | delta 8 | cursor 9-19 | alive 31
   uint32_t* pix;  // pixel index 0-27 | spill x 30 | spill y 31
   uint32_t* pid;  // path id within the render (debug outputs)
+  uint32_t* inst; // instance of the path (batched renders)
 };
 
 // Compact ray queues filled by k_shade (positions from warp-aggregated
@@ -129,6 +130,16 @@ struct RayConst {
   float ix, iy, iz;  // reciprocal direction (tiny components clamped to 2^-80)
 };
 
+// The geometry one ray is traced against: the scene's, or in a batch the
+// ray's own instance's (the traversal reads only these fields).
+struct TraceGeo {
+  const uint4* wnodes;
+  const float4* nodes;
+  const float4* tris;
+  const float4* spheres;
+  int n_tris, n_spheres;
+};
+
 GYT_D RayConst ray_const(float3 o, float3 d) {
   RayConst c;
   c.wr = wt_setup(o, d);
@@ -141,8 +152,8 @@ GYT_D RayConst ray_const(float3 o, float3 d) {
 
 // Triangles [first, first + count) in leaf order against the ray. ANY stops
 // at the first hit (returns true).
-template <bool ANY, bool COUNT>
-GYT_D bool test_tris(const DevScene& s, const WtRay& wr, uint32_t first, uint32_t count, float& tmax, float& b1,
+template <bool ANY, bool COUNT, class S>
+GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count, float& tmax, float& b1,
                      float& b2, int& prim, TraceCount* cnt) {
   if (COUNT) cnt->tris += count;
   for (uint32_t k = 0; k < count; ++k) {
@@ -169,8 +180,8 @@ struct BinaryTraversal {
   GYT_D void init() { node = 0; sp = 0; }
 
   // Returns true when the traversal is finished (or, for ANY, on a hit).
-  template <bool ANY, bool COUNT>
-  GYT_D bool step(const DevScene& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
+  template <bool ANY, bool COUNT, class S>
+  GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
     if (node >= 0) {
       if (COUNT) cnt->nodes++;
@@ -230,8 +241,8 @@ struct WideTraversal {
 
   GYT_D void init() { node = 0; sp = 0; have_node = true; }
 
-  template <bool ANY, bool COUNT>
-  GYT_D bool step(const DevScene& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
+  template <bool ANY, bool COUNT, class S>
+  GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
     if (!have_node) {
       // next pending child of the nearest group that can still be hit
@@ -315,8 +326,8 @@ template <>
 struct TraversalOf<8> { using type = WideTraversal; };
 
 // The analytic spheres after the BVH (linear; the configurations hold few).
-template <bool ANY>
-GYT_D void trace_spheres(const DevScene& s, float3 o, float3 d, float& tmax, int& prim) {
+template <bool ANY, class S>
+GYT_D void trace_spheres(const S& s, float3 o, float3 d, float& tmax, int& prim) {
   for (int k = 0; k < s.n_spheres; ++k) {
     if (ANY && prim >= 0) return;
     float4 sp4 = __ldg(s.spheres + k);
@@ -353,7 +364,10 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
 // warp) before the next traversal step, so warps stay full until the queue
 // runs dry. load(i, o, d, tmax) fetches ray i; done(i, prim, tmax, b1, b2)
 // consumes its result.
-template <int W, bool ANY, bool COUNT, class Load, class Done>
+//
+// BATCH: every ray carries its own geometry (load fills the lane's TraceGeo);
+// otherwise all rays use the scene s.
+template <int W, bool ANY, bool COUNT, bool BATCH = false, class Load, class Done>
 GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load load, Done done,
                             unsigned long long* counters) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -364,6 +378,7 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
   RayConst rc;
   typename TraversalOf<W>::type tv;
   TraceCount cnt;
+  TraceGeo lg{};  // the lane's geometry (BATCH)
   for (;;) {
     const uint32_t idle = __ballot_sync(0xffffffffu, ri == -1);
     if (idle) {
@@ -375,13 +390,14 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
         const uint32_t r = base + __popc(idle & ((1u << lane) - 1u));
         if (r < n) {
           ri = (int)r;
-          load(r, o, d, tmax);
+          load(r, o, d, tmax, lg);
           b1 = b2 = 0.f;
           prim = -1;
           rc = ray_const(o, d);
           tv.init();
-          if (s.n_tris == 0) {
-            trace_spheres<ANY>(s, o, d, tmax, prim);
+          if ((BATCH ? lg.n_tris : s.n_tris) == 0) {
+            if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
+            else trace_spheres<ANY>(s, o, d, tmax, prim);
             done((uint32_t)ri, prim, tmax, b1, b2);
             ri = -1;
           }
@@ -395,8 +411,11 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
       // a few steps per fetch check keep the ballot cost small
 #pragma unroll 1
       for (int k = 0; k < 4; ++k) {
-        if (tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, &cnt)) {
-          trace_spheres<ANY>(s, o, d, tmax, prim);
+        const bool fin = BATCH ? tv.template step<ANY, COUNT>(lg, rc, o, tmax, b1, b2, prim, &cnt)
+                               : tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, &cnt);
+        if (fin) {
+          if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
+          else trace_spheres<ANY>(s, o, d, tmax, prim);
           done((uint32_t)ri, prim, tmax, b1, b2);
           ri = -1;
           break;
@@ -479,6 +498,27 @@ GYT_D float tri_light_pdf(const LightTri& l, const Hit& h, float3 o, float3 wi) 
 }
 
 // -------------------------------------------------------------- kernels ---
+// Camera path of sample s in pixel (x, y) into slot k (TiledIntegrator::Render
+// body, integrator/TiledIntegrator.cpp:37-48).
+GYT_D void gen_path(PathBuf& dst, uint32_t k, uint32_t x, uint32_t y, uint32_t s, const Cam& cam, SobolTables tab) {
+  uint64_t idx = enum_index(tab, cam.log2_res, s, x, y);
+  Rng rng{idx, 0};
+  float su = rng.next(tab.matrices), sv = rng.next(tab.matrices);
+  // SobolEnum::SampleX/Y (SobolEnum.h:30-36), kept unfused as the reference
+  float u = __fsub_rn(__fmul_rn(cam.res_pow2, su), (float)x);
+  float v = __fsub_rn(__fmul_rn(cam.res_pow2, sv), (float)y);
+  float3 o, d;
+  camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
+  dst.o[k] = make_float4(o.x, o.y, o.z, 0.f);
+  dst.d[k] = make_float4(d.x, d.y, d.z, 0.f);
+  dst.tp[k] = make_float4(1.f, 1.f, 1.f, 0.f);
+  dst.L[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  dst.sidx[k] = idx;
+  dst.meta[k] = meta_pack(0, false, rng.cursor, true);
+  uint32_t pix = (y * cam.res_x + x) | ((u == 0.f && x > 0) ? (1u << 30) : 0u) | ((v == 0.f && y > 0) ? (1u << 31) : 0u);
+  dst.pix[k] = pix;
+}
+
 __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base, uint32_t n_new,
                                                      unsigned long long first, Cam cam, uint32_t spp,
                                                      const uint32_t* __restrict__ list, SobolTables tab) {
@@ -496,35 +536,8 @@ __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base,
     y = (uint32_t)(pixel / cam.res_x);
     x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
   }
-  uint64_t idx = enum_index(tab, cam.log2_res, s, x, y);
-  Rng rng{idx, 0};
-  float su = rng.next(tab.matrices), sv = rng.next(tab.matrices);
-  // SobolEnum::SampleX/Y (SobolEnum.h:30-36), kept unfused as the reference
-  float u = __fsub_rn(__fmul_rn(cam.res_pow2, su), (float)x);
-  float v = __fsub_rn(__fmul_rn(cam.res_pow2, sv), (float)y);
-  float3 o, d;
-  camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
-  uint32_t k = base + j;
-  dst.o[k] = make_float4(o.x, o.y, o.z, 0.f);
-  dst.d[k] = make_float4(d.x, d.y, d.z, 0.f);
-  dst.tp[k] = make_float4(1.f, 1.f, 1.f, 0.f);
-  dst.L[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-  dst.sidx[k] = idx;
-  dst.meta[k] = meta_pack(0, false, rng.cursor, true);
-  uint32_t pix = (y * cam.res_x + x) | ((u == 0.f && x > 0) ? (1u << 30) : 0u) | ((v == 0.f && y > 0) ? (1u << 31) : 0u);
-  dst.pix[k] = pix;
-  dst.pid[k] = (uint32_t)p;
-}
-
-// Per-warp reduction of traversal counters into the profile (counting mode).
-GYT_D void flush_counts(const TraceCount& c, unsigned long long* g) {
-  cg::coalesced_group w = cg::coalesced_threads();
-  unsigned long long nodes = cg::reduce(w, (unsigned long long)c.nodes, cg::plus<unsigned long long>());
-  unsigned long long tris = cg::reduce(w, (unsigned long long)c.tris, cg::plus<unsigned long long>());
-  if (w.thread_rank() == 0) {
-    atomicAdd(g, nodes);
-    atomicAdd(g + 1, tris);
-  }
+  gen_path(dst, base + j, x, y, s, cam, tab);
+  dst.pid[base + j] = (uint32_t)p;
 }
 
 template <int W, bool COUNT>
@@ -532,7 +545,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(PathBuf cur, uint32_t n, DevS
                                                    uint32_t* __restrict__ fetch, unsigned long long* counters) {
   persistent_trace<W, false, COUNT>(
       s, fetch, n,
-      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+      [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo&) {
         o = f3(cur.o[i]);
         d = f3(cur.d[i]);
         tmax = __int_as_float(0x7f800000);
@@ -551,11 +564,11 @@ GYT_D uint32_t queue_slot(uint32_t* count) {
   return g.shfl(base, 0) + g.thread_rank();
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
-                                                  SobolTables tab, DebugOut dbg) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+// One bounce of path slot i (PathTracing::Li loop body, integrator/PT.cpp:14-63,
+// with Integrator::DirectIllumination, integrator/Integrator.cpp:9-107): emission,
+// light and BSDF samples queued as shadow and MIS rays, the continuation ray.
+GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
+                      SobolTables tab, const DebugOut& dbg) {
   float4 h4 = q.hit[i];
   int prim = __float_as_int(h4.w);
   uint32_t meta = cur.meta[i];
@@ -712,6 +725,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
   cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
 }
 
+__global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
+                                                  SobolTables tab, DebugOut dbg) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  shade_path(cur, i, s, prm, q, tab, dbg);
+}
+
 // Next-event shadow rays (any hit): an unoccluded ray adds its contribution
 // to its path's radiance (VisibilityTester::Unoccluded, Visibility.cpp:7-10).
 template <int W, bool COUNT>
@@ -720,7 +740,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(PathBuf cur, DevScene s, Queu
   const uint32_t n = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, COUNT>(
       s, q.counts + 3, n,
-      [&](uint32_t j, float3& o, float3& d, float& tmax) {
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
         float4 a = q.so[j], b = q.sd[j];
         o = f3(a);
         d = f3(b);
@@ -739,6 +759,39 @@ __global__ void __launch_bounds__(kBlock) k_shadow(PathBuf cur, DevScene s, Queu
       counters);
 }
 
+// MIS-ray result of one queue entry (shared by both MIS kernels).
+GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint32_t j, int prim, float b1, float b2,
+                    const DebugOut& dbg) {
+  const float4 md = q.md[j], mc = q.mc[j];
+  const int li = __float_as_int(md.w);
+  const uint32_t slot = __float_as_uint(mc.w);
+  const float3 wi = f3(md);
+  bool reach = false;
+  float3 add = mk(0.f, 0.f, 0.f);
+  if (prim < 0 && li >= s.n_area) {
+    add = f3(mc) * env_lookup(s.env, wi);  // Integrator.cpp:97-99
+    reach = true;
+  } else if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
+    float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
+    float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
+    float b0 = 1.f - b1 - b2;
+    float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
+    if (dot(ns, -wi) > 0.f) {
+      const float4* r = s.ltab + kLightRec * li;
+      add = f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
+    }
+    reach = true;
+  }
+  if (reach) {
+    float4 l = cur.L[slot];
+    cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
+    if (dbg.mis) {
+      const uint32_t b = __float_as_uint(q.mo[j].w);
+      if (b < 64) dbg.mis[cur.pid[slot]] |= 1ull << b;
+    }
+  }
+}
+
 // BSDF-sampled MIS rays (closest hit): the sampled light's emission where the
 // ray reaches it (Integrator.cpp:86-101).
 template <int W, bool COUNT>
@@ -747,41 +800,12 @@ __global__ void __launch_bounds__(kBlock) k_mis(PathBuf cur, DevScene s, Queues 
   const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
   persistent_trace<W, false, COUNT>(
       s, q.counts + 4, n,
-      [&](uint32_t j, float3& o, float3& d, float& tmax) {
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
         o = f3(q.mo[j]);
         d = f3(q.md[j]);
         tmax = __int_as_float(0x7f800000);
       },
-      [&](uint32_t j, int prim, float, float b1, float b2) {
-        const float4 md = q.md[j], mc = q.mc[j];
-        const int li = __float_as_int(md.w);
-        const uint32_t slot = __float_as_uint(mc.w);
-        const float3 wi = f3(md);
-        bool reach = false;
-        float3 add = mk(0.f, 0.f, 0.f);
-        if (prim < 0 && li >= s.n_area) {
-          add = f3(mc) * env_lookup(s.env, wi);  // Integrator.cpp:97-99
-          reach = true;
-        } else if (prim >= 0 && prim < s.n_tris && __float_as_int(__ldg(s.tnrm + 3 * prim + 1).w) == li) {
-          float3 n0 = f3(__ldg(s.tnrm + 3 * prim)), n1 = f3(__ldg(s.tnrm + 3 * prim + 1));
-          float3 n2 = f3(__ldg(s.tnrm + 3 * prim + 2));
-          float b0 = 1.f - b1 - b2;
-          float3 ns = norm(n0 * b0 + n1 * b1 + n2 * b2);
-          if (dot(ns, -wi) > 0.f) {
-            const float4* r = s.ltab + kLightRec * li;
-            add = f3(mc) * mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
-          }
-          reach = true;
-        }
-        if (reach) {
-          float4 l = cur.L[slot];
-          cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
-          if (dbg.mis) {
-            const uint32_t b = __float_as_uint(q.mo[j].w);
-            if (b < 64) dbg.mis[cur.pid[slot]] |= 1ull << b;
-          }
-        }
-      },
+      [&](uint32_t j, int prim, float, float b1, float b2) { mis_done(cur, q, s, j, prim, b1, b2, dbg); },
       counters);
 }
 
@@ -834,6 +858,194 @@ __global__ void __launch_bounds__(kBlock) k_finish(PathBuf cur, PathBuf nxt, uin
     }
     if (dbg.cursor) dbg.cursor[pid] = (meta >> 9) & 2047u;
   }
+}
+
+// ------------------------------------------------------ batched renders ---
+// Many scenes, cameras and sample counts in one wavefront: the path pool is
+// refilled from the concatenation of all instances' paths (instance-major),
+// every path slot carries its instance, and each kernel reads the scene,
+// camera, parameters and film of the instance it works on.
+struct Inst {
+  DevScene s;
+  Cam cam;
+  Params prm;
+  double* film;
+  unsigned long long first;  // first global path index of the instance
+};
+
+// Device-side loop state of a batched render (one half-iteration moves the
+// pool from one buffer to the other).
+struct IterState {
+  unsigned long long generated, total;
+  uint32_t active;    // live paths at the start of a half-iteration
+  uint32_t n_new;     // paths generated in it
+  uint32_t n;         // active + n_new
+  uint32_t iter;      // half-iterations run
+  uint32_t max_iter;  // watchdog
+  uint32_t watchdog;  // set when max_iter stopped the loop
+  uint32_t n_inst, capacity;
+};
+
+__global__ void k_batch_begin(IterState* __restrict__ st, uint32_t* __restrict__ counts) {
+  if (threadIdx.x == 0) {
+    const unsigned long long rem = st->total - st->generated;
+    const uint32_t room = st->capacity - st->active;
+    const uint32_t n_new = (uint32_t)(rem < room ? rem : room);
+    st->n_new = n_new;
+    st->n = st->active + n_new;
+  }
+  if (threadIdx.x < 8) counts[threadIdx.x] = 0;
+}
+
+__global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const IterState* __restrict__ st,
+                                                           const Inst* __restrict__ insts, SobolTables tab) {
+  const uint32_t n_new = st->n_new, base = st->active, ni = st->n_inst;
+  const unsigned long long first = st->generated;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_new; j += gridDim.x * blockDim.x) {
+    const unsigned long long g = first + j;
+    // last instance whose first path is <= g
+    uint32_t lo = 0, hi = ni;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (insts[mid].first <= g) lo = mid; else hi = mid;
+    }
+    const Inst& I = insts[lo];
+    const unsigned long long p = g - I.first;
+    const unsigned long long pixel = p / I.prm.spp;
+    const uint32_t s = (uint32_t)(p - pixel * I.prm.spp);
+    const uint32_t y = (uint32_t)(pixel / I.cam.res_x);
+    const uint32_t x = (uint32_t)(pixel - (unsigned long long)y * I.cam.res_x);
+    const Cam cam = I.cam;
+    gen_path(dst, base + j, x, y, s, cam, tab);
+    dst.pid[base + j] = (uint32_t)p;
+    dst.inst[base + j] = lo;
+  }
+}
+
+GYT_D TraceGeo geo_of(const DevScene& s) {
+  return TraceGeo{s.wnodes, s.nodes, s.tris, s.spheres, s.n_tris, s.n_spheres};
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const IterState* __restrict__ st,
+                                                         const Inst* __restrict__ insts, float4* __restrict__ hits,
+                                                         uint32_t* __restrict__ fetch) {
+  const uint32_t n = st->n;
+  persistent_trace<W, false, false, true>(
+      insts[0].s, fetch, n,
+      [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo& g) {
+        o = f3(cur.o[i]);
+        d = f3(cur.d[i]);
+        tmax = __int_as_float(0x7f800000);
+        g = geo_of(insts[cur.inst[i]].s);
+      },
+      [&](uint32_t i, int prim, float tmax, float b1, float b2) {
+        hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
+      },
+      nullptr);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st,
+                                                        const Inst* __restrict__ insts, Queues q, SobolTables tab) {
+  const uint32_t n = st->n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Inst& I = insts[cur.inst[i]];
+    shade_path(cur, i, I.s, I.prm, q, tab, DebugOut{});
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_shadow_batch(PathBuf cur, const Inst* __restrict__ insts, Queues q) {
+  const uint32_t n = *(volatile uint32_t*)q.counts;
+  persistent_trace<W, true, false, true>(
+      insts[0].s, q.counts + 3, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
+        const float4 a = q.so[j], b = q.sd[j];
+        o = f3(a);
+        d = f3(b);
+        tmax = a.w;
+        g = geo_of(insts[cur.inst[__float_as_uint(b.w)]].s);
+      },
+      [&](uint32_t j, int prim, float, float, float) {
+        if (prim < 0) {
+          const uint32_t slot = __float_as_uint(q.sd[j].w);
+          const float4 c = q.sc[j], l = cur.L[slot];
+          cur.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.f);
+        }
+      },
+      nullptr);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_mis_batch(PathBuf cur, const Inst* __restrict__ insts, Queues q) {
+  const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
+  persistent_trace<W, false, false, true>(
+      insts[0].s, q.counts + 4, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
+        o = f3(q.mo[j]);
+        d = f3(q.md[j]);
+        tmax = __int_as_float(0x7f800000);
+        g = geo_of(insts[cur.inst[__float_as_uint(q.mc[j].w)]].s);
+      },
+      [&](uint32_t j, int prim, float, float b1, float b2) {
+        const uint32_t slot = __float_as_uint(q.mc[j].w);
+        mis_done(cur, q, insts[cur.inst[slot]].s, j, prim, b1, b2, DebugOut{});
+      },
+      nullptr);
+}
+
+// Finished paths to their instance's film, live paths compacted.
+__global__ void __launch_bounds__(kBlock) k_finish_batch(PathBuf cur, PathBuf nxt, const IterState* __restrict__ st,
+                                                         const Inst* __restrict__ insts,
+                                                         uint32_t* __restrict__ counter) {
+  const uint32_t n = st->n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t meta = cur.meta[i];
+    const float4 L4 = cur.L[i];
+    if (meta & kAlive) {
+      cg::coalesced_group g = cg::coalesced_threads();
+      uint32_t base = 0;
+      if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+      const uint32_t j = g.shfl(base, 0) + g.thread_rank();
+      nxt.o[j] = cur.o[i];
+      nxt.d[j] = cur.d[i];
+      nxt.tp[j] = cur.tp[i];
+      nxt.L[j] = L4;
+      nxt.sidx[j] = cur.sidx[i];
+      nxt.meta[j] = meta;
+      nxt.pix[j] = cur.pix[i];
+      nxt.pid[j] = cur.pid[i];
+      nxt.inst[j] = cur.inst[i];
+    } else {
+      const Inst& I = insts[cur.inst[i]];
+      const float3 L = f3(L4);
+      const uint32_t pix = cur.pix[i], res_x = I.cam.res_x;
+      double* film = I.film;
+      const uint32_t p = pix & kPixMask;
+      const uint32_t y = p / res_x, x = p - y * res_x;
+      film_add(film, res_x, x, y, L);
+      if (pix & (1u << 30)) film_add(film, res_x, x - 1, y, L);
+      if (pix & (1u << 31)) film_add(film, res_x, x, y - 1, L);
+      if ((pix & (1u << 30)) && (pix & (1u << 31))) film_add(film, res_x, x - 1, y - 1, L);
+    }
+  }
+}
+
+// Closes a half-iteration: live count, refill progress, and the loop
+// condition of the enclosing graph (while more paths remain, bounded by the
+// watchdog).
+__global__ void k_batch_end(IterState* __restrict__ st, const uint32_t* __restrict__ counts,
+                            cudaGraphConditionalHandle cond, int in_graph) {
+  if (threadIdx.x != 0) return;
+  st->generated += st->n_new;
+  st->active = counts[5];
+  st->iter += 1;
+  bool more = st->generated < st->total || st->active > 0;
+  if (more && st->iter >= st->max_iter) {
+    st->watchdog = 1;
+    more = false;
+  }
+  if (in_graph) cudaGraphSetConditional(cond, more ? 1u : 0u);
 }
 
 __global__ void k_resolve(const double* __restrict__ film, float* __restrict__ rgb, uint32_t npix) {
@@ -895,6 +1107,49 @@ const void* persistent_fn(int kind) {
 
 }  // namespace
 
+// Leaf-order triangle data of a device-built BVH, the same records the host
+// path writes: tris[3k + c] = (p_c, triangle id bits for c = 0) and
+// tnrm[3k + c] = (vertex normal, or the face normal without normals; material
+// bits for c = 0, light bits for c = 1). The face normal is computed with the
+// host's IEEE operations in the host's order (no contraction), so both paths
+// store identical floats. leaf_of[t] = k.
+__global__ void k_leaf_data(uint32_t nt, const uint32_t* __restrict__ order, const float* __restrict__ V,
+                            const uint32_t* __restrict__ I, const float* __restrict__ N,
+                            const int2* __restrict__ info, float4* __restrict__ tris, float4* __restrict__ tnrm,
+                            int* __restrict__ leaf_of) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  const uint32_t t = order[k];
+  leaf_of[t] = (int)k;
+  uint32_t vi[3];
+  float3 p[3];
+  for (int c = 0; c < 3; ++c) {
+    vi[c] = I[3 * (size_t)t + c];
+    p[c] = mk(V[3 * (size_t)vi[c]], V[3 * (size_t)vi[c] + 1], V[3 * (size_t)vi[c] + 2]);
+  }
+  const float3 a = mk(__fsub_rn(p[1].x, p[0].x), __fsub_rn(p[1].y, p[0].y), __fsub_rn(p[1].z, p[0].z));
+  const float3 b = mk(__fsub_rn(p[2].x, p[0].x), __fsub_rn(p[2].y, p[0].y), __fsub_rn(p[2].z, p[0].z));
+  const float3 cr = mk(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+                       __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+                       __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+  const float len =
+      __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(cr.x, cr.x), __fmul_rn(cr.y, cr.y)), __fmul_rn(cr.z, cr.z)));
+  const float3 face = mk(__fdiv_rn(cr.x, len), __fdiv_rn(cr.y, len), __fdiv_rn(cr.z, len));
+  const int2 in = info[t];
+  for (int c = 0; c < 3; ++c) {
+    tris[3 * (size_t)k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? __int_as_float((int)t) : 0.f);
+    const float3 n = N ? mk(N[3 * (size_t)vi[c]], N[3 * (size_t)vi[c] + 1], N[3 * (size_t)vi[c] + 2]) : face;
+    const float w = c == 0 ? __int_as_float(in.x) : (c == 1 ? __int_as_float(in.y) : 0.f);
+    tnrm[3 * (size_t)k + c] = make_float4(n.x, n.y, n.z, w);
+  }
+}
+
+__global__ void k_gather_int(uint32_t n, const int* __restrict__ index, const int* __restrict__ src,
+                             int* __restrict__ dst) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[index[i]];
+}
+
 // ------------------------------------------------------------- host side ---
 struct gyt_context {
   int device = 0;
@@ -916,19 +1171,34 @@ struct gyt_context {
   float* d_rgb = nullptr;
   size_t rgb_bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_in = nullptr;  // orders a render after the caller's legacy-stream work
   std::vector<void*> pool_allocs;
   int profile = 0;
   int bvh_width = 2;
+  int bvh_builder = GYT_BVH_BUILD_DEVICE;
   cudaEvent_t kev[8] = {};
   unsigned long long* d_counters = nullptr;  // node visits and triangle tests per traversal kernel
   GytProfile prof = {};
+  int sms = 0;
+  // batched renders: instance table, device loop state, configuration and
+  // the captured graph (rebuilt when its kernels' arguments change)
+  Inst* d_insts = nullptr;
+  uint32_t insts_cap = 0;
+  IterState* d_iter = nullptr;
+  IterState* h_iter = nullptr;  // pinned
+  GytBatchConfig bcfg = {0, 0, 0, 1, 0};
+  int btrace[2][2] = {};  // occupancy limit (blocks per SM) of the batched extend/shadow, width 2/8
+  cudaGraph_t bgraph = nullptr;
+  cudaGraphExec_t bexec = nullptr;
+  uint64_t bkey[6] = {};
 };
 
 struct gyt_scene {
-  gyt_context* ctx = nullptr;
+  gyt_context* ctx = nullptr;  // the creating context (may be destroyed before the scene)
+  int device = 0;
   DevScene dev = {};
   std::vector<void*> allocs;
-  uint64_t n_tris = 0, n_nodes = 0, bytes = 0;
+  uint64_t n_tris = 0, n_nodes = 0, n_slots = 0, bytes = 0;
   uint32_t bvh_depth = 0;
 };
 
@@ -952,6 +1222,15 @@ cudaError_t dalloc(std::vector<void*>& list, T** p, size_t count) {
   if (count == 0) count = 1;
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
   if (e == cudaSuccess) list.push_back(*p);
+  return e;
+}
+
+// The context's stream does not synchronise with the legacy default stream,
+// where callers (and torch) typically clear a film: the render waits for the
+// work already queued there.
+cudaError_t after_legacy_stream(gyt_context* ctx) {
+  cudaError_t e = cudaEventRecord(ctx->ev_in, cudaStreamLegacy);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_in, 0);
   return e;
 }
 
@@ -1034,6 +1313,7 @@ int32_t ensure_pool(gyt_context* ctx) {
     GYT_CK(ctx, dalloc(L, &P.meta, n));
     GYT_CK(ctx, dalloc(L, &P.pix, n));
     GYT_CK(ctx, dalloc(L, &P.pid, n));
+    GYT_CK(ctx, dalloc(L, &P.inst, n));
   }
   Queues& q = ctx->q;
   GYT_CK(ctx, dalloc(L, &q.so, n));
@@ -1070,6 +1350,7 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
   Queues q = ctx->q;
   if (cnt) GYT_CK(ctx, cudaMemsetAsync(ctx->d_counters, 0, 6 * sizeof(unsigned long long), s));
   uint32_t hcounts[8];
+  GYT_CK(ctx, after_legacy_stream(ctx));
   GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
   while (generated < total || active > 0) {
     uint32_t n_new = (uint32_t)std::min<unsigned long long>(ctx->capacity - active, total - generated);
@@ -1172,8 +1453,8 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_counter, 8 * sizeof(uint32_t));
   const size_t sob = GYT_SOBOL_DIMS * GYT_SOBOL_COLS;
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_sobol, (sob + 64) * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemset(c->d_sobol, 0, (sob + 64) * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemcpy(c->d_sobol, gyt_sobol_matrices, sob * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_sobol, 0, (sob + 64) * sizeof(uint32_t), c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_sobol, gyt_sobol_matrices, sob * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) {
     // transposed copy: row b = column b of every dimension (see sobol10)
     std::vector<uint32_t> tr((size_t)64 * kSobolRow, 0u);
@@ -1183,19 +1464,34 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
         tr[(size_t)b * kSobolRow + dm] = flat < sob ? gyt_sobol_matrices[flat] : 0u;
       }
     e = cudaMalloc((void**)&c->d_sobol_bits, tr.size() * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemcpy(c->d_sobol_bits, tr.data(), tr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_sobol_bits, tr.data(), tr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
   }
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc, sizeof(gyt_vdc_sobol));
-  if (e == cudaSuccess) e = cudaMemcpy(c->d_vdc, gyt_vdc_sobol, sizeof(gyt_vdc_sobol), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_vdc, gyt_vdc_sobol, sizeof(gyt_vdc_sobol), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc_inv, sizeof(gyt_vdc_sobol_inv));
-  if (e == cudaSuccess) e = cudaMemcpy(c->d_vdc_inv, gyt_vdc_sobol_inv, sizeof(gyt_vdc_sobol_inv), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_vdc_inv, gyt_vdc_sobol_inv, sizeof(gyt_vdc_sobol_inv), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming);
   for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreate(&c->kev[k]);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_counters, 6 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // tables resident before the first launch
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_iter, sizeof(IterState));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_iter, sizeof(IterState));
+  if (e == cudaSuccess) {
+    const void* fns[2][2] = {{(const void*)k_extend_batch<2>, (const void*)k_shadow_batch<2>},
+                             {(const void*)k_extend_batch<8>, (const void*)k_shadow_batch<8>}};
+    for (int w = 0; w < 2 && e == cudaSuccess; ++w)
+      for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fns[w][k], kBlock, 0);
+        c->btrace[w][k] = std::max(1, nb);
+      }
+  }
   if (e == cudaSuccess) {
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    c->sms = sms;
     for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind)
       for (int w : {2, 8})
         for (int cntm = 0; cntm < 2 && e == cudaSuccess; ++cntm) {
@@ -1230,8 +1526,14 @@ void gyt_context_destroy(gyt_context* c) {
   cudaFree(c->d_vdc_inv);
   cudaFree(c->d_film);
   cudaFree(c->d_rgb);
+  if (c->bexec) cudaGraphExecDestroy(c->bexec);
+  if (c->bgraph) cudaGraphDestroy(c->bgraph);
+  if (c->d_insts) cudaFree(c->d_insts);
+  if (c->d_iter) cudaFree(c->d_iter);
+  if (c->h_iter) cudaFreeHost(c->h_iter);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_in) cudaEventDestroy(c->ev_in);
   for (int k = 0; k < 8; ++k)
     if (c->kev[k]) cudaEventDestroy(c->kev[k]);
   cudaFree(c->d_counters);
@@ -1259,6 +1561,14 @@ int32_t gyt_context_set_bvh_width(gyt_context* c, int32_t width) {
   if (!c) return GYT_ERR_INVALID;
   if (width != 2 && width != 8) return fail(c, GYT_ERR_INVALID, "bvh width must be 2 or 8");
   c->bvh_width = width;
+  return GYT_OK;
+}
+
+int32_t gyt_context_set_bvh_builder(gyt_context* c, int32_t builder) {
+  if (!c) return GYT_ERR_INVALID;
+  if (builder != GYT_BVH_BUILD_HOST && builder != GYT_BVH_BUILD_DEVICE)
+    return fail(c, GYT_ERR_INVALID, "bvh builder must be GYT_BVH_BUILD_HOST or GYT_BVH_BUILD_DEVICE");
+  c->bvh_builder = builder;
   return GYT_OK;
 }
 
@@ -1390,89 +1700,161 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       for (int i = 1; i < nl + 1; ++i) cdf[i] /= fint;
     }
   }
-  // acceleration structure: binary (two child boxes per 64-byte node) or
-  // 8-wide with quantized child boxes (80-byte nodes), per context setting
-  WideBvhHost wide;
-  BvhHost bin;
+  // acceleration structure: binary (two child boxes per 64-byte node, built
+  // on the device or the host) or 8-wide with quantized child boxes (80-byte
+  // nodes, host), per context setting
   const bool use_wide = ctx->bvh_width == 8;
-  if (use_wide) {
-    if (!build_wide_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &wide))
-      return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
-    if (wide.max_depth >= (uint32_t)kWStack)
-      return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
-  } else {
-    if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bin))
-      return fail(ctx, GYT_ERR_INVALID, "scene_create: BVH build failed");
-    if (bin.max_depth >= (uint32_t)kBStack)
-      return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
-  }
-  struct {
-    const std::vector<uint32_t>& order;
-  } bvh{use_wide ? wide.order : bin.order};
-  // leaf-order triangle positions and shading data
+  const bool use_dev = !use_wide && ctx->bvh_builder == GYT_BVH_BUILD_DEVICE && d->n_triangles > 0;
+  auto* sc = new gyt_scene();
+  sc->ctx = ctx;
+  sc->device = ctx->device;
+  auto bail = [&](int32_t code, const std::string& msg) {
+    gyt_scene_destroy(sc);
+    return fail(ctx, code, msg);
+  };
+  auto up = [&](auto** dst, const auto* src, size_t count) -> cudaError_t {
+    using T = std::remove_const_t<std::remove_reference_t<decltype(*src)>>;
+    cudaError_t e = dalloc(sc->allocs, (T**)dst, count);
+    if (e == cudaSuccess && count && src) e = cudaMemcpyAsync((void*)*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    sc->bytes += count * sizeof(T);
+    return e;
+  };
+  auto cuda_code = [](cudaError_t e) { return e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA; };
+  DevScene& ds = sc->dev;
+  cudaError_t e = cudaSuccess;
+  std::vector<int> light_leaf(n_area, -1);  // leaf-order position of each area light's triangle
   auto bits = [](int v) { float f; std::memcpy(&f, &v, 4); return f; };
-  std::vector<float4> tris((size_t)bvh.order.size() * 3), tnrm((size_t)bvh.order.size() * 3);
-  std::vector<int> leaf_of(d->n_triangles, -1);
-  for (size_t k = 0; k < bvh.order.size(); ++k) {
-    uint32_t t = bvh.order[k];
-    leaf_of[t] = (int)k;
-    const uint32_t* I = &d->indices[3 * t];
-    float3 p[3] = {vtx(I[0]), vtx(I[1]), vtx(I[2])};
-    float3 face = norm(cross(p[1] - p[0], p[2] - p[0]));
-    for (int c = 0; c < 3; ++c) {
-      tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : 0.f);
-      float3 n = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
-      float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : 0.f);
-      tnrm[3 * k + c] = make_float4(n.x, n.y, n.z, w);
+  if (use_dev) {
+    const uint32_t nt = d->n_triangles;
+    std::vector<void*> tmp;
+    struct Free {
+      std::vector<void*>& v;
+      ~Free() {
+        for (void* q : v) cudaFree(q);
+      }
+    } tmp_free{tmp};
+    auto tup = [&](auto** dst, const auto* src, size_t count) -> cudaError_t {
+      using T = std::remove_const_t<std::remove_reference_t<decltype(*src)>>;
+      cudaError_t e2 = dalloc(tmp, (T**)dst, count);
+      if (e2 == cudaSuccess && count && src)
+        e2 = cudaMemcpyAsync((void*)*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+      return e2;
+    };
+    float *dV = nullptr, *dN = nullptr;
+    uint32_t* dI = nullptr;
+    int2* dInfo = nullptr;
+    int *dLeafOf = nullptr, *dLights = nullptr, *dLightLeaf = nullptr;
+    e = tup(&dV, d->vertices, (size_t)d->n_vertices * 3);
+    if (e == cudaSuccess) e = tup(&dI, d->indices, (size_t)nt * 3);
+    if (e == cudaSuccess && d->normals) e = tup(&dN, d->normals, (size_t)d->n_vertices * 3);
+    if (e == cudaSuccess) e = tup(&dInfo, info.data(), info.size());
+    if (e == cudaSuccess) e = tup(&dLeafOf, (const int*)nullptr, nt);
+    if (e == cudaSuccess && n_area) e = tup(&dLights, light_tris.data(), light_tris.size());
+    if (e == cudaSuccess && n_area) e = tup(&dLightLeaf, (const int*)nullptr, light_tris.size());
+    if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
+    GpuBvh g;
+    std::string berr;
+    const int rc = build_bvh_gpu(ctx->stream, dV, dI, nt, &g, &berr);
+    if (rc) return bail(rc, "scene_create: " + berr);
+    sc->allocs.push_back(g.nodes);  // the scene owns the nodes
+    tmp.push_back(g.order);
+    sc->bytes += (uint64_t)g.n_slots * 64;
+    if (g.max_depth >= (uint32_t)kBStack) return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+    float4 *dtris = nullptr, *dn = nullptr;
+    e = dalloc(sc->allocs, &dtris, (size_t)nt * 3);
+    if (e == cudaSuccess) e = dalloc(sc->allocs, &dn, (size_t)nt * 3);
+    if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
+    sc->bytes += (uint64_t)nt * 3 * 2 * sizeof(float4);
+    k_leaf_data<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(nt, g.order, dV, dI, dN, dInfo, dtris, dn, dLeafOf);
+    if (n_area)
+      k_gather_int<<<(n_area + 255) / 256, 256, 0, ctx->stream>>>((uint32_t)n_area, dLights, dLeafOf, dLightLeaf);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && n_area)
+      e = cudaMemcpyAsync(light_leaf.data(), dLightLeaf, n_area * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
+    ds.nodes = g.nodes;
+    ds.wnodes = nullptr;
+    ds.tris = dtris;
+    ds.tnrm = dn;
+    sc->n_nodes = g.n_inner;
+    sc->n_slots = g.n_slots;
+    sc->bvh_depth = g.max_depth;
+  } else {
+    WideBvhHost wide;
+    BvhHost bin;
+    if (use_wide) {
+      if (!build_wide_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &wide))
+        return bail(GYT_ERR_INVALID, "scene_create: BVH build failed");
+      if (wide.max_depth >= (uint32_t)kWStack)
+        return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+    } else {
+      if (!build_bvh_host(d->vertices, d->n_vertices, d->indices, d->n_triangles, &bin))
+        return bail(GYT_ERR_INVALID, "scene_create: BVH build failed");
+      if (bin.max_depth >= (uint32_t)kBStack)
+        return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
     }
+    const std::vector<uint32_t>& order = use_wide ? wide.order : bin.order;
+    // leaf-order triangle positions and shading data
+    std::vector<float4> tris((size_t)order.size() * 3), tnrm((size_t)order.size() * 3);
+    std::vector<int> leaf_of(d->n_triangles, -1);
+    for (size_t k = 0; k < order.size(); ++k) {
+      uint32_t t = order[k];
+      leaf_of[t] = (int)k;
+      const uint32_t* I = &d->indices[3 * t];
+      float3 p[3] = {vtx(I[0]), vtx(I[1]), vtx(I[2])};
+      float3 face = norm(cross(p[1] - p[0], p[2] - p[0]));
+      for (int c = 0; c < 3; ++c) {
+        tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : 0.f);
+        float3 n = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
+        float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : 0.f);
+        tnrm[3 * k + c] = make_float4(n.x, n.y, n.z, w);
+      }
+    }
+    for (int li = 0; li < n_area; ++li) light_leaf[li] = leaf_of[light_tris[li]];
+    if (use_wide) {
+      uint4* nodes = nullptr;
+      e = up(&nodes, (const uint4*)wide.nodes.data(), wide.nodes.size() / 4);
+      ds.wnodes = nodes;
+      ds.nodes = nullptr;
+    } else {
+      float4* nodes = nullptr;
+      e = up(&nodes, (const float4*)bin.nodes.data(), bin.nodes.size() / 4);
+      ds.nodes = nodes;
+      ds.wnodes = nullptr;
+    }
+    float4* dtris = nullptr;
+    if (e == cudaSuccess) e = up(&dtris, tris.data(), tris.size());
+    ds.tris = dtris;
+    float4* dn = nullptr;
+    if (e == cudaSuccess) e = up(&dn, tnrm.data(), tnrm.size());
+    ds.tnrm = dn;
+    sc->n_nodes = use_wide ? wide.nodes.size() / 20 : bin.nodes.size() / 16;
+    sc->n_slots = use_wide ? 0 : bin.nodes.size() / 16;
+    sc->bvh_depth = use_wide ? wide.max_depth : bin.max_depth;
   }
   // light records: (p0, Le.r) (p1, Le.g) (p2, Le.b) (n0, area) (n1, leaf) (n2, id) (face, -)
   std::vector<float4> ltab((size_t)n_area * kLightRec);
   for (int li = 0; li < n_area; ++li) {
-    int t = light_tris[li];
-    int k = leaf_of[t];
+    const int t = light_tris[li];
+    const int k = light_leaf[li];
+    const uint32_t* I = &d->indices[3 * t];
     const float* em = &d->emission[3 * d->tri_emission[t]];
-    float3 p0 = f3(tris[3 * k]), p1 = f3(tris[3 * k + 1]), p2 = f3(tris[3 * k + 2]);
+    float3 p0 = vtx(I[0]), p1 = vtx(I[1]), p2 = vtx(I[2]);
     float area = 0.5f * length(cross(p1 - p0, p2 - p0));
     float3 face = norm(cross(p1 - p0, p2 - p0));
+    float3 nc[3];
+    for (int c = 0; c < 3; ++c)
+      nc[c] = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
     float4* r = &ltab[(size_t)li * kLightRec];
     r[0] = make_float4(p0.x, p0.y, p0.z, em[0]);
     r[1] = make_float4(p1.x, p1.y, p1.z, em[1]);
     r[2] = make_float4(p2.x, p2.y, p2.z, em[2]);
-    float3 n0 = f3(tnrm[3 * k]), n1 = f3(tnrm[3 * k + 1]), n2 = f3(tnrm[3 * k + 2]);
-    r[3] = make_float4(n0.x, n0.y, n0.z, area);
-    r[4] = make_float4(n1.x, n1.y, n1.z, bits(k));
-    r[5] = make_float4(n2.x, n2.y, n2.z, bits(t));
+    r[3] = make_float4(nc[0].x, nc[0].y, nc[0].z, area);
+    r[4] = make_float4(nc[1].x, nc[1].y, nc[1].z, bits(k));
+    r[5] = make_float4(nc[2].x, nc[2].y, nc[2].z, bits(t));
     r[6] = make_float4(face.x, face.y, face.z, 0.f);
   }
-  auto* sc = new gyt_scene();
-  sc->ctx = ctx;
-  auto up = [&](auto** dst, const auto* src, size_t count) -> cudaError_t {
-    using T = std::remove_const_t<std::remove_reference_t<decltype(*src)>>;
-    cudaError_t e = dalloc(sc->allocs, (T**)dst, count);
-    if (e == cudaSuccess && count && src) e = cudaMemcpy((void*)*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
-    sc->bytes += count * sizeof(T);
-    return e;
-  };
-  DevScene& ds = sc->dev;
-  cudaError_t e = cudaSuccess;
-  if (use_wide) {
-    uint4* nodes = nullptr;
-    if (e == cudaSuccess) e = up(&nodes, (const uint4*)wide.nodes.data(), wide.nodes.size() / 4);
-    ds.wnodes = nodes;
-    ds.nodes = nullptr;
-  } else {
-    float4* nodes = nullptr;
-    if (e == cudaSuccess) e = up(&nodes, (const float4*)bin.nodes.data(), bin.nodes.size() / 4);
-    ds.nodes = nodes;
-    ds.wnodes = nullptr;
-  }
-  float4* dtris = nullptr;
-  if (e == cudaSuccess) e = up(&dtris, tris.data(), tris.size());
-  ds.tris = dtris;
-  float4* dn = nullptr;
-  if (e == cudaSuccess) e = up(&dn, tnrm.data(), tnrm.size());
-  ds.tnrm = dn;
   std::vector<float4> sph(d->n_spheres);
   for (uint32_t k = 0; k < d->n_spheres; ++k)
     sph[k] = make_float4(d->spheres[4 * k], d->spheres[4 * k + 1], d->spheres[4 * k + 2], d->spheres[4 * k + 3]);
@@ -1521,8 +1903,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   ds.n_tris = (int)d->n_triangles;
   ds.n_spheres = (int)d->n_spheres;
   sc->n_tris = d->n_triangles;
-  sc->n_nodes = use_wide ? wide.nodes.size() / 20 : bin.nodes.size() / 16;
-  sc->bvh_depth = use_wide ? wide.max_depth : bin.max_depth;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // uploads are ordered on the context stream
   if (e != cudaSuccess) {
     gyt_scene_destroy(sc);
     return fail(ctx, e == cudaErrorMemoryAllocation ? GYT_ERR_OUT_OF_MEMORY : GYT_ERR_CUDA,
@@ -1534,7 +1915,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
 
 void gyt_scene_destroy(gyt_scene* s) {
   if (!s) return;
-  if (s->ctx) cudaSetDevice(s->ctx->device);
+  cudaSetDevice(s->device);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
 }
@@ -1544,6 +1925,25 @@ int32_t gyt_scene_info(const gyt_scene* s, uint64_t* nt, uint64_t* nn, uint64_t*
   if (nt) *nt = s->n_tris;
   if (nn) *nn = s->n_nodes;
   if (bytes) *bytes = s->bytes;
+  return GYT_OK;
+}
+
+int32_t gyt_scene_read_bvh(const gyt_scene* s, float* nodes, uint64_t node_capacity, uint32_t* tri_ids,
+                           uint64_t tri_capacity, uint64_t* n_slots) {
+  if (!s || !n_slots) return GYT_ERR_INVALID;
+  gyt_context* ctx = s->ctx;
+  if (!s->dev.nodes && s->n_tris) return fail(ctx, GYT_ERR_UNSUPPORTED, "read_bvh: not a binary BVH");
+  *n_slots = s->n_slots;
+  if (!nodes) return GYT_OK;
+  if (node_capacity < s->n_slots * 16 || (tri_ids && tri_capacity < s->n_tris))
+    return fail(ctx, GYT_ERR_INVALID, "read_bvh: output arrays too small");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  if (s->n_slots) GYT_CK(ctx, cudaMemcpy(nodes, s->dev.nodes, s->n_slots * 64, cudaMemcpyDeviceToHost));
+  if (tri_ids && s->n_tris) {
+    std::vector<float4> t0((size_t)s->n_tris * 3);
+    GYT_CK(ctx, cudaMemcpy(t0.data(), s->dev.tris, t0.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint64_t k = 0; k < s->n_tris; ++k) std::memcpy(&tri_ids[k], &t0[3 * k].w, 4);
+  }
   return GYT_OK;
 }
 
@@ -1619,8 +2019,8 @@ int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamer
   GYT_CK(ctx, dalloc(tmp, &dL, 3 * n));
   GYT_CK(ctx, dalloc(tmp, &dc, n));
   GYT_CK(ctx, dalloc(tmp, &dm, 3 * n));
-  GYT_CK(ctx, cudaMemcpy(dl, xys, 3 * n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  GYT_CK(ctx, cudaMemset(dm, 0, 3 * n * sizeof(unsigned long long)));
+  GYT_CK(ctx, cudaMemcpyAsync(dl, xys, 3 * n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemsetAsync(dm, 0, 3 * n * sizeof(unsigned long long), ctx->stream));
   st = run_paths(ctx, scene, cam, params, n, dl, nullptr, DebugOut{dL, dc, dm, dm + n, dm + 2 * n}, nullptr);
   if (st) return st;
   if (L_out) GYT_CK(ctx, cudaMemcpy(L_out, dL, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
@@ -1649,7 +2049,7 @@ int32_t gyt_intersect(gyt_context* ctx, const gyt_scene* scene, uint64_t n, cons
   GYT_CK(ctx, dalloc(tmp, &dt, n));
   GYT_CK(ctx, dalloc(tmp, &d1, n));
   GYT_CK(ctx, dalloc(tmp, &d2, n));
-  GYT_CK(ctx, cudaMemcpy(dr, rays, 7 * n * sizeof(float), cudaMemcpyHostToDevice));
+  GYT_CK(ctx, cudaMemcpyAsync(dr, rays, 7 * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   if (scene->dev.wnodes)
     k_intersect<8><<<grid_for(n), kBlock, 0, ctx->stream>>>(scene->dev, n, dr, any_hit ? 1 : 0, dp, dt, d1, d2);
   else
@@ -1682,8 +2082,8 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
   GYT_CK(ctx, dalloc(tmp, &dd, n));
   GYT_CK(ctx, dalloc(tmp, &di, n));
   GYT_CK(ctx, dalloc(tmp, &dout, n));
-  GYT_CK(ctx, cudaMemcpy(dd, dims, n * 4, cudaMemcpyHostToDevice));
-  GYT_CK(ctx, cudaMemcpy(di, indices, n * 8, cudaMemcpyHostToDevice));
+  GYT_CK(ctx, cudaMemcpyAsync(dd, dims, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(di, indices, n * 8, cudaMemcpyHostToDevice, ctx->stream));
   k_sobol<<<grid_for(n), kBlock, 0, ctx->stream>>>(ctx->d_sobol, n, dd, di, dout);
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1708,7 +2108,7 @@ int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, u
   uint64_t* dout = nullptr;
   GYT_CK(ctx, dalloc(tmp, &ds, 3 * n));
   GYT_CK(ctx, dalloc(tmp, &dout, n));
-  GYT_CK(ctx, cudaMemcpy(ds, sxy, 3 * n * 4, cudaMemcpyHostToDevice));
+  GYT_CK(ctx, cudaMemcpyAsync(ds, sxy, 3 * n * 4, cudaMemcpyHostToDevice, ctx->stream));
   k_enum<<<grid_for(n), kBlock, 0, ctx->stream>>>(tables(ctx), m, n, ds, dout);
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1738,6 +2138,370 @@ int32_t gyt_camera_raster_to_world(const GytCamera* camera, double* out16) {
 // counter must start at zero and it is cleared every iteration. Two calls
 // whose work overlaps on the GPU (different streams or threads) race on the
 // array.
+// ------------------------------------------------------ batched renders ---
+namespace {
+
+struct BatchPlan {
+  int W = 2;
+  uint32_t stride_grid = 0, ext_grid = 0, sh_grid = 0, mis_grid = 0;
+};
+
+BatchPlan batch_plan(const gyt_context* ctx, int W) {
+  BatchPlan b;
+  b.W = W;
+  const GytBatchConfig& c = ctx->bcfg;
+  const int wi = W == 8 ? 1 : 0;
+  const uint32_t sms = (uint32_t)std::max(1, ctx->sms);
+  b.stride_grid = sms * (c.stride_blocks_per_sm ? c.stride_blocks_per_sm : 8u);
+  const uint32_t te = c.trace_blocks_per_sm ? std::min<uint32_t>(c.trace_blocks_per_sm, ctx->btrace[wi][0])
+                                            : (uint32_t)ctx->btrace[wi][0];
+  const uint32_t ts = c.trace_blocks_per_sm ? std::min<uint32_t>(c.trace_blocks_per_sm, ctx->btrace[wi][1])
+                                            : (uint32_t)ctx->btrace[wi][1];
+  b.ext_grid = sms * std::max(1u, te);
+  b.sh_grid = sms * std::max(1u, ts);
+  b.mis_grid = sms;  // MIS rays are rare: one block per SM
+  return b;
+}
+
+// One half-iteration of the batched wavefront: pool P (current) to N (next).
+cudaError_t enqueue_half(gyt_context* ctx, const BatchPlan& b, const PathBuf& P, const PathBuf& N,
+                         cudaGraphConditionalHandle cond, int in_graph) {
+  cudaStream_t s = ctx->stream;
+  const Queues q = ctx->q;
+  const SobolTables tab = tables(ctx);
+  IterState* st = ctx->d_iter;
+  const Inst* I = ctx->d_insts;
+  k_batch_begin<<<1, 32, 0, s>>>(st, q.counts);
+  k_generate_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, I, tab);
+  if (b.W == 8) k_extend_batch<8><<<b.ext_grid, kBlock, 0, s>>>(P, st, I, q.hit, q.counts + 2);
+  else k_extend_batch<2><<<b.ext_grid, kBlock, 0, s>>>(P, st, I, q.hit, q.counts + 2);
+  k_shade_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, I, q, tab);
+  if (b.W == 8) k_shadow_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, I, q);
+  else k_shadow_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, I, q);
+  if (b.W == 8) k_mis_batch<8><<<b.mis_grid, kBlock, 0, s>>>(P, I, q);
+  else k_mis_batch<2><<<b.mis_grid, kBlock, 0, s>>>(P, I, q);
+  k_finish_batch<<<b.stride_grid, kBlock, 0, s>>>(P, N, st, I, q.counts + 5);
+  k_batch_end<<<1, 32, 0, s>>>(st, q.counts, cond, in_graph);
+  return cudaGetLastError();
+}
+constexpr uint32_t kKernelsPerHalf = 8;
+
+// The batched render as one graph: a while-loop node whose body is two
+// half-iterations (pool 0 -> 1 -> 0); k_batch_end sets the loop condition.
+int32_t ensure_batch_graph(gyt_context* ctx, const BatchPlan& b) {
+  const uint64_t key[6] = {(uint64_t)b.W, (uint64_t)b.stride_grid, ((uint64_t)b.ext_grid << 32) | b.sh_grid,
+                           (uint64_t)(uintptr_t)ctx->d_insts, (uint64_t)(uintptr_t)ctx->pool[0].o,
+                           (uint64_t)ctx->pool_cap};
+  if (ctx->bexec && std::memcmp(key, ctx->bkey, sizeof(key)) == 0) return GYT_OK;
+  if (ctx->bexec) cudaGraphExecDestroy(ctx->bexec);
+  if (ctx->bgraph) cudaGraphDestroy(ctx->bgraph);
+  ctx->bexec = nullptr;
+  ctx->bgraph = nullptr;
+  cudaGraph_t g = nullptr;
+  GYT_CK(ctx, cudaGraphCreate(&g, 0));
+  ctx->bgraph = g;
+  cudaGraphConditionalHandle cond;
+  GYT_CK(ctx, cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  GYT_CK(ctx, cudaGraphAddNode(&node, g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  GYT_CK(ctx, cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = enqueue_half(ctx, b, ctx->pool[0], ctx->pool[1], cond, 1);
+  if (e == cudaSuccess) e = enqueue_half(ctx, b, ctx->pool[1], ctx->pool[0], cond, 1);
+  cudaGraph_t captured = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &captured);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, GYT_ERR_CUDA, std::string("batch graph capture: ") +
+                                       cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  cudaGraphExec_t ex = nullptr;
+  GYT_CK(ctx, cudaGraphInstantiate(&ex, g, 0));
+  ctx->bexec = ex;
+  std::memcpy(ctx->bkey, key, sizeof(key));
+  return GYT_OK;
+}
+
+struct BatchInput {
+  std::vector<Inst> insts;
+  unsigned long long total = 0;
+  uint32_t max_depth = 0;
+  int W = 2;
+};
+
+int32_t batch_input(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes, const GytCamera* cameras,
+                    const GytRenderParams* params, double* const* films, BatchInput* in) {
+  if (n && (!scenes || !cameras || !params || !films)) return fail(ctx, GYT_ERR_INVALID, "batch: null array");
+  in->insts.resize(n);
+  in->total = 0;
+  in->max_depth = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const gyt_scene* sc = scenes[i];
+    if (!sc || !films[i]) return fail(ctx, GYT_ERR_INVALID, "batch: null scene or film at " + std::to_string(i));
+    if (sc->device != ctx->device)
+      return fail(ctx, GYT_ERR_INVALID, "batch: scene " + std::to_string(i) + " lives on another device");
+    const int W = sc->dev.wnodes ? 8 : 2;
+    if (i == 0) in->W = W;
+    else if (W != in->W) return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: scenes of different BVH widths");
+    int32_t st = check_params(ctx, &params[i]);
+    if (st) return st;
+    Inst& I = in->insts[i];
+    st = make_cam(ctx, &cameras[i], &I.cam);
+    if (st) return st;
+    const unsigned long long np = (unsigned long long)cameras[i].res_x * cameras[i].res_y * params[i].spp;
+    if (np >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: more than 2^32 paths in one instance");
+    I.s = sc->dev;
+    I.prm = Params{params[i].spp, params[i].max_depth, params[i].rr_depth};
+    I.film = films[i];
+    I.first = in->total;
+    in->total += np;
+    in->max_depth = std::max(in->max_depth, params[i].max_depth);
+  }
+  return GYT_OK;
+}
+
+// Runs a prepared batch: instance table and loop state to the device, then
+// the graph (or the host loop), timed with events on the context stream.
+int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats) {
+  const uint32_t n = (uint32_t)in.insts.size();
+  if (stats) *stats = GytRenderStats{};
+  if (n == 0 || in.total == 0) return GYT_OK;
+  if (ctx->bcfg.paths_in_flight && ctx->bcfg.paths_in_flight != ctx->capacity) {
+    if (ctx->bcfg.paths_in_flight < 1024) return fail(ctx, GYT_ERR_INVALID, "batch: paths_in_flight below 1024");
+    ctx->capacity = ctx->bcfg.paths_in_flight;
+  }
+  int32_t st = ensure_pool(ctx);
+  if (st) return st;
+  if (n > ctx->insts_cap) {
+    if (ctx->d_insts) cudaFree(ctx->d_insts);
+    ctx->d_insts = nullptr;
+    ctx->insts_cap = 0;
+    const uint32_t cap = std::max<uint32_t>(n, 64);
+    GYT_CK(ctx, cudaMalloc((void**)&ctx->d_insts, cap * sizeof(Inst)));
+    ctx->insts_cap = cap;
+  }
+  cudaStream_t s = ctx->stream;
+  GYT_CK(ctx, after_legacy_stream(ctx));
+  GYT_CK(ctx, cudaMemcpyAsync(ctx->d_insts, in.insts.data(), n * sizeof(Inst), cudaMemcpyHostToDevice, s));
+  IterState is = {};
+  is.total = in.total;
+  is.n_inst = n;
+  is.capacity = ctx->capacity;
+  // a path holds a slot for at most max_depth half-iterations and a full
+  // pool retires at least one slot per half-iteration: generous bound
+  const unsigned long long bound =
+      2ull * (in.total / ctx->capacity + 2) * ((unsigned long long)in.max_depth + 2) + 64;
+  is.max_iter = (uint32_t)std::min<unsigned long long>(bound, 1u << 30);
+  *ctx->h_iter = is;
+  GYT_CK(ctx, cudaMemcpyAsync(ctx->d_iter, ctx->h_iter, sizeof(IterState), cudaMemcpyHostToDevice, s));
+  const BatchPlan b = batch_plan(ctx, in.W);
+  if (ctx->bcfg.use_graph) {
+    st = ensure_batch_graph(ctx, b);
+    if (st) return st;
+  }
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
+  if (ctx->bcfg.use_graph) {
+    GYT_CK(ctx, cudaGraphLaunch(ctx->bexec, s));
+  } else {
+    for (;;) {
+      GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[0], ctx->pool[1], 0, 0));
+      GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[1], ctx->pool[0], 0, 0));
+      GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+      GYT_CK(ctx, cudaStreamSynchronize(s));
+      const IterState& h = *ctx->h_iter;
+      if (h.watchdog || !(h.generated < h.total || h.active > 0)) break;
+      if (h.iter >= h.max_iter) break;
+    }
+  }
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
+  GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+  GYT_CK(ctx, cudaStreamSynchronize(s));
+  const IterState h = *ctx->h_iter;
+  if (h.watchdog || h.generated < h.total || h.active > 0)
+    return fail(ctx, GYT_ERR_WATCHDOG, "batch: the device loop hit its iteration bound");
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->paths = in.total;
+    stats->path_slots = 0;
+    stats->iterations = h.iter;
+    stats->launches = h.iter * kKernelsPerHalf;
+    stats->ms = ms;
+  }
+  return GYT_OK;
+}
+
+}  // namespace
+
+int32_t gyt_context_set_batch_config(gyt_context* ctx, const GytBatchConfig* c) {
+  if (!ctx) return GYT_ERR_INVALID;
+  if (!c) {
+    ctx->bcfg = GytBatchConfig{0, 0, 0, 1, 0};
+    return GYT_OK;
+  }
+  if (c->paths_in_flight && c->paths_in_flight < 1024)
+    return fail(ctx, GYT_ERR_INVALID, "batch config: paths_in_flight must be 0 or >= 1024");
+  if (c->stride_blocks_per_sm > 64 || c->trace_blocks_per_sm > 64)
+    return fail(ctx, GYT_ERR_INVALID, "batch config: blocks per SM above 64");
+  ctx->bcfg = *c;
+  ctx->bcfg.use_graph = c->use_graph ? 1 : 0;
+  return GYT_OK;
+}
+
+int32_t gyt_context_get_batch_config(const gyt_context* ctx, GytBatchConfig* out) {
+  if (!ctx || !out) return GYT_ERR_INVALID;
+  *out = ctx->bcfg;
+  return GYT_OK;
+}
+
+int32_t gyt_render_batch_device(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes,
+                                const GytCamera* cameras, const GytRenderParams* params, double* const* d_films,
+                                GytRenderStats* stats) {
+  if (!ctx) return GYT_ERR_INVALID;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  BatchInput in;
+  int32_t st = batch_input(ctx, n, scenes, cameras, params, d_films, &in);
+  if (st) return st;
+  return run_batch(ctx, in, stats);
+}
+
+int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes, const GytCamera* cameras,
+                         const GytRenderParams* params, float* const* rgb_out) {
+  if (!ctx) return GYT_ERR_INVALID;
+  if (n && (!cameras || !rgb_out)) return fail(ctx, GYT_ERR_INVALID, "batch: null array");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<size_t> off(n + 1, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!rgb_out[i]) return fail(ctx, GYT_ERR_INVALID, "batch: null image at " + std::to_string(i));
+    off[i + 1] = off[i] + (size_t)cameras[i].res_x * cameras[i].res_y;
+  }
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() {
+      for (void* p : v) cudaFree(p);
+    }
+  } guard{tmp};
+  double* films = nullptr;
+  float* rgb = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &films, off[n] * 4));
+  GYT_CK(ctx, dalloc(tmp, &rgb, off[n] * 3));
+  GYT_CK(ctx, cudaMemsetAsync(films, 0, off[n] * 4 * sizeof(double), ctx->stream));
+  std::vector<double*> fp(n);
+  for (uint32_t i = 0; i < n; ++i) fp[i] = films + 4 * off[i];
+  int32_t st = gyt_render_batch_device(ctx, n, scenes, cameras, params, fp.data(), nullptr);
+  if (st) return st;
+  for (uint32_t i = 0; i < n; ++i) {
+    const size_t npix = off[i + 1] - off[i];
+    if (!npix) continue;
+    k_resolve<<<grid_for(npix), kBlock, 0, ctx->stream>>>(fp[i], rgb + 3 * off[i], (uint32_t)npix);
+    GYT_CK(ctx, cudaGetLastError());
+    GYT_CK(ctx, cudaMemcpyAsync(rgb_out[i], rgb + 3 * off[i], npix * 3 * sizeof(float), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  }
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes,
+                           const gyt_scene* const* scenes_alt, const GytCamera* cameras,
+                           const GytRenderParams* params, uint32_t sample_spp, GytBatchConfig* best,
+                           float* best_mpaths) {
+  if (!ctx || !best) return GYT_ERR_INVALID;
+  if (n == 0) return fail(ctx, GYT_ERR_INVALID, "autotune: empty batch");
+  if (!params || !cameras) return fail(ctx, GYT_ERR_INVALID, "autotune: null array");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  const uint32_t sspp = sample_spp ? sample_spp : 1u;
+  std::vector<GytRenderParams> prm(params, params + n);
+  size_t npix = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    prm[i].spp = std::max(1u, std::min(prm[i].spp, sspp));
+    npix += (size_t)cameras[i].res_x * cameras[i].res_y;
+  }
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() {
+      for (void* p : v) cudaFree(p);
+    }
+  } guard{tmp};
+  double* films = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &films, npix * 4));
+  std::vector<double*> fp(n);
+  for (uint32_t i = 0, o = 0; i < n; ++i) {
+    fp[i] = films + 4ull * o;
+    o += cameras[i].res_x * cameras[i].res_y;
+  }
+  const GytBatchConfig saved = ctx->bcfg;
+  const uint32_t saved_cap = ctx->capacity;
+  // one timed render (after an untimed one) per candidate
+  auto trial = [&](const GytBatchConfig& c, const gyt_scene* const* sc, float* mp) -> int32_t {
+    ctx->bcfg = c;
+    BatchInput in;
+    int32_t st = batch_input(ctx, n, sc, cameras, prm.data(), fp.data(), &in);
+    if (st) return st;
+    GytRenderStats rs;
+    for (int k = 0; k < 2; ++k) {
+      st = run_batch(ctx, in, &rs);
+      if (st) return st;
+    }
+    *mp = rs.ms > 0.f ? (float)(rs.paths / (rs.ms * 1e3)) : 0.f;
+    return GYT_OK;
+  };
+  GytBatchConfig cur = {saved_cap, 8, 0, 1, (uint32_t)(scenes[0] && scenes[0]->dev.wnodes ? 8 : 2)};
+  const gyt_scene* const* cur_scenes = scenes;
+  float cur_mp = 0.f;
+  int32_t st = trial(cur, cur_scenes, &cur_mp);
+  if (st) { ctx->bcfg = saved; return st; }
+  // coordinate search: BVH width, pool size, grid-stride blocks, traversal blocks
+  if (scenes_alt) {
+    float mp = 0.f;
+    st = trial(cur, scenes_alt, &mp);
+    if (st) { ctx->bcfg = saved; return st; }
+    if (mp > cur_mp) {
+      cur_mp = mp;
+      cur_scenes = scenes_alt;
+      cur.bvh_width = scenes_alt[0] && scenes_alt[0]->dev.wnodes ? 8 : 2;
+    }
+  }
+  for (uint32_t cap : {1u << 20, 1u << 21, 1u << 22}) {
+    if (cap == cur.paths_in_flight) continue;
+    GytBatchConfig c = cur;
+    c.paths_in_flight = cap;
+    float mp = 0.f;
+    st = trial(c, cur_scenes, &mp);
+    if (st == GYT_ERR_OUT_OF_MEMORY) { cudaGetLastError(); continue; }
+    if (st) { ctx->bcfg = saved; return st; }
+    if (mp > cur_mp) { cur_mp = mp; cur = c; }
+  }
+  for (uint32_t sb : {4u, 16u}) {
+    GytBatchConfig c = cur;
+    c.stride_blocks_per_sm = sb;
+    float mp = 0.f;
+    st = trial(c, cur_scenes, &mp);
+    if (st) { ctx->bcfg = saved; return st; }
+    if (mp > cur_mp) { cur_mp = mp; cur = c; }
+  }
+  const int wi = cur.bvh_width == 8 ? 1 : 0;
+  for (uint32_t tb : {(uint32_t)std::max(1, ctx->btrace[wi][0] / 2), (uint32_t)std::max(1, ctx->btrace[wi][0] * 3 / 4)}) {
+    GytBatchConfig c = cur;
+    c.trace_blocks_per_sm = tb;
+    float mp = 0.f;
+    st = trial(c, cur_scenes, &mp);
+    if (st) { ctx->bcfg = saved; return st; }
+    if (mp > cur_mp) { cur_mp = mp; cur = c; }
+  }
+  ctx->bcfg = cur;
+  *best = cur;
+  if (best_mpaths) *best_mpaths = cur_mp;
+  return GYT_OK;
+}
+
 namespace {
 
 constexpr size_t kNoAllocSlotBytes = 2 * (4 * sizeof(float4) + 8 + 3 * 4) + 7 * sizeof(float4);
@@ -1837,6 +2601,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   unsigned long long generated = 0;
   uint32_t active = 0, iters = 0, live = 0;
   int cur = 0;
+  GYT_CK(ctx, after_legacy_stream(ctx));
   while (generated < total || active > 0) {
     uint32_t n_new = (uint32_t)std::min<unsigned long long>(paths_in_flight - active, total - generated);
     GYT_CK(ctx, cudaMemsetAsync(q.counts, 0, 8 * sizeof(uint32_t), s));

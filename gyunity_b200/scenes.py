@@ -367,6 +367,91 @@ def mixed_materials_box(level=3, res=64, spp=4, max_depth=8, rr_depth=3, seed=11
                    sphere_material=np.array([mirror, glass], np.uint32), name="mixed_materials_box")
 
 
+# ------------------------------------------------- batched uneven workload ---
+
+def _smooth_normals(v: np.ndarray, f: np.ndarray) -> np.ndarray:
+    """Area-weighted vertex normals with one bincount per axis (the batch
+    workload's meshes; vertex_normals keeps the older summation order for the
+    scenes the golden fixtures were made from)."""
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    idx = f.reshape(-1)
+    n = np.stack([np.bincount(idx, np.repeat(fn[:, a], 3), minlength=v.shape[0]) for a in range(3)], 1)
+    return n / np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+
+
+_ICO_CACHE = {}
+
+
+def _unit_icosphere(level: int):
+    if level not in _ICO_CACHE:
+        _ICO_CACHE[level] = icosphere(level)
+    v, f = _ICO_CACHE[level]
+    return v.copy(), f
+
+
+def ring_torus(n_u: int, n_v: int, R=0.42, r=0.16):
+    """Ring torus around the y axis: 2 * n_u * n_v faces; returns vertices,
+    faces and the outward tube direction per vertex."""
+    u = np.arange(n_u) / n_u * 2 * np.pi
+    w = np.arange(n_v) / n_v * 2 * np.pi
+    cu, su, cw, sw = np.cos(u)[:, None], np.sin(u)[:, None], np.cos(w)[None, :], np.sin(w)[None, :]
+    dirs = np.stack([cu * cw, np.broadcast_to(sw, (n_u, n_v)), su * cw], -1).reshape(-1, 3)
+    center = np.stack([R * cu[:, 0], np.zeros(n_u), R * su[:, 0]], 1)
+    verts = (np.repeat(center, n_v, 0) + r * dirs)
+    iu, iv = np.meshgrid(np.arange(n_u), np.arange(n_v), indexing="ij")
+    a = iu * n_v + iv
+    b2 = ((iu + 1) % n_u) * n_v + iv
+    c2 = ((iu + 1) % n_u) * n_v + (iv + 1) % n_v
+    d = iu * n_v + (iv + 1) % n_v
+    faces = np.concatenate([np.stack([a, c2, b2], -1).reshape(-1, 3), np.stack([a, d, c2], -1).reshape(-1, 3)])
+    return verts, faces, dirs
+
+
+def batch_instance(seed: int, min_tris=10_000, max_tris=2_000_000, max_depth=16, rr_depth=5) -> SceneDesc:
+    """One instance of the uneven batch workload (seeded): a Cornell box
+    (walls and ceiling light as cornell_box, no spheres) holding a noise-
+    displaced icosphere or ring torus (coin flip) of log-uniform triangle count
+    in [min_tris, max_tris] (icospheres: the nearest subdivision level, tori:
+    a grid of about that many faces), diffuse or GGX-conductor (coin flip)
+    with albedo ~ U(0.2, 0.9) per channel and alpha ~ U(0.05, 0.5);
+    resolution uniform in {128, 256, 512, 1024} squared, spp uniform in 1..64."""
+    rng = np.random.default_rng(seed)
+    target = float(np.exp(rng.uniform(np.log(min_tris), np.log(max_tris))))
+    torus = bool(rng.integers(0, 2))
+    diffuse = bool(rng.integers(0, 2))
+    albedo = tuple(float(a) for a in rng.uniform(0.2, 0.9, 3))
+    alpha = float(rng.uniform(0.05, 0.5))
+    res = int(rng.choice([128, 256, 512, 1024]))
+    spp = int(rng.integers(1, 65))
+    b = _Builder()
+    _cornell_walls(b)
+    if torus:
+        n_u = max(8, int(round(math.sqrt(target))))
+        n_v = max(4, int(round(target / (2 * n_u))))
+        v, f, dirs = ring_torus(n_u, n_v)
+        d = value_noise(v, seed)
+        v = v + dirs * (0.16 * 0.05 * d)[:, None] + np.array([0.0, -0.55, 0.0])
+    else:
+        level = int(np.clip(round(math.log(target / 20.0, 4)), 2, 8))
+        v, f = _unit_icosphere(level)
+        d = value_noise(v, seed)
+        v = v * (0.42 * (1.0 + 0.05 * d))[:, None] + np.array([0.0, -0.5, 0.0])
+    v32 = v.astype(np.float32)
+    n = _smooth_normals(v32.astype(np.float64), f).astype(np.float32)
+    if diffuse:
+        m = b.material(*_mat(MAT_DIFFUSE, albedo))
+    else:
+        m = b.material(*_mat(MAT_CONDUCTOR, albedo, ax=alpha, ay=alpha))
+    b.tris(v32, n, f, np.full(f.shape[0], m, np.uint32))
+    return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
+                   name="batch_%d_%s_%d_%dx%d_%dspp" % (seed, "torus" if torus else "ico", f.shape[0], res, res, spp))
+
+
+def batch_workload(n=64, seed=1000, **kw):
+    """The uneven batch: instances seed, seed + 1, ..., seed + n - 1."""
+    return [batch_instance(seed + i, **kw) for i in range(n)]
+
+
 # ----------------------------------------------------------- environment ---
 
 def rgbe_quantize(img: np.ndarray) -> np.ndarray:

@@ -128,6 +128,15 @@ int32_t gyt_context_set_profile(gyt_context* ctx, int32_t mode);
  * (binary, two child boxes per 64-byte node; the default) or 8 (quantized
  * child boxes, 80-byte nodes). Both replace BVHAccel (accelerator/BVHAccel.cpp). */
 int32_t gyt_context_set_bvh_width(gyt_context* ctx, int32_t width);
+/* Where later gyt_scene_create calls build a binary (width 2) BVH:
+ * GYT_BVH_BUILD_DEVICE (the default) or GYT_BVH_BUILD_HOST. Both make the
+ * same tree: 16-bin SAH, at most 8 triangles per leaf, identical splits,
+ * leaves and child boxes (node numbering and the order inside a leaf differ).
+ * The 8-wide BVH is always built on the host. Replaces the BVHAccel
+ * constructor's build (accelerator/BVHAccel.cpp:154-200). */
+#define GYT_BVH_BUILD_HOST 0
+#define GYT_BVH_BUILD_DEVICE 1
+int32_t gyt_context_set_bvh_builder(gyt_context* ctx, int32_t builder);
 /* Copies the accumulated profile into *out and resets it. */
 int32_t gyt_profile_read(gyt_context* ctx, GytProfile* out);
 
@@ -137,6 +146,14 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* desc, gyt_scene**
 void gyt_scene_destroy(gyt_scene* scene);
 /* Triangle count, BVH node count and device bytes of a scene. */
 int32_t gyt_scene_info(const gyt_scene* scene, uint64_t* n_triangles, uint64_t* n_nodes, uint64_t* device_bytes);
+/* Copies a binary BVH to the host: node slots (16 floats each, the layout of
+ * the traversal kernels; slots a tree does not reach are left as found) and,
+ * per leaf-order position, the triangle's index in the scene description.
+ * *n_slots receives the slot count; with nodes == NULL only that is set.
+ * Capacities are in elements (floats, uint32s). GYT_ERR_UNSUPPORTED for an
+ * 8-wide BVH. Inspection and tests; no counterpart in the reference. */
+int32_t gyt_scene_read_bvh(const gyt_scene* scene, float* nodes, uint64_t node_capacity, uint32_t* tri_ids,
+                           uint64_t tri_capacity, uint64_t* n_slots);
 
 /* Integrator::Render: renders the full image and writes rgb_out (host,
  * res_x*res_y*3 floats, row-major from the top-left pixel) = colour/weight
@@ -177,6 +194,48 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 /* SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for n (s, x, y) triplets. */
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
+
+/* ---- Batched renders ------------------------------------------------------
+ * Many scenes and cameras of uneven sizes, resolutions and sample counts in
+ * one wavefront: one path pool refilled across the instances (instance after
+ * instance), each path carrying its instance, so the pool stays full until
+ * the last instance's tail. Each instance's film receives exactly what
+ * gyt_render_device would accumulate for it (the same paths; only the order
+ * of the FP64 additions differs). All scenes of a batch must have the same
+ * BVH width. No counterpart in the reference (its Integrator::Render takes
+ * one scene and one camera, integrator/Integrator.h:17-27). */
+typedef struct GytBatchConfig {
+  uint32_t paths_in_flight;      /* path pool size; 0 keeps the context's */
+  uint32_t stride_blocks_per_sm; /* blocks per SM of the refill, shade and finish kernels; 0 = 8 */
+  uint32_t trace_blocks_per_sm;  /* blocks per SM of the extend and shadow traversals; 0 = occupancy limit */
+  uint32_t use_graph;            /* 1: the render is one CUDA graph launch whose while-loop node runs
+                                    the wavefront iterations on the device; 0: a host loop */
+  uint32_t bvh_width;            /* set by gyt_batch_autotune: 2 or 8 */
+} GytBatchConfig;
+/* Configuration of later batched renders (NULL restores the defaults). */
+int32_t gyt_context_set_batch_config(gyt_context* ctx, const GytBatchConfig* config);
+int32_t gyt_context_get_batch_config(const gyt_context* ctx, GytBatchConfig* out);
+/* Renders n instances: scenes[i] seen through cameras[i] with params[i],
+ * accumulated into d_films[i] (device, res_x*res_y*4 doubles as in
+ * gyt_render_device; not cleared). stats (may be NULL) covers the batch;
+ * launches counts the kernels the batch ran, iterations the half-iterations
+ * (pool swaps). GYT_ERR_WATCHDOG if the device loop hit its iteration bound. */
+int32_t gyt_render_batch_device(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes,
+                                const GytCamera* cameras, const GytRenderParams* params, double* const* d_films,
+                                GytRenderStats* stats);
+/* The same with host images: rgb_out[i] receives res_x*res_y*3 floats as
+ * gyt_render writes them. */
+int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes, const GytCamera* cameras,
+                         const GytRenderParams* params, float* const* rgb_out);
+/* Autotuner: times batched renders of the given instances with at most
+ * sample_spp samples per pixel (0 = 1) over pool sizes, grid shapes and, when
+ * scenes_alt (the same scenes built with the other BVH width) is given, the
+ * BVH width; sets the fastest configuration on the context and returns it in
+ * *best with its throughput in *best_mpaths (Mpaths/s; may be NULL). */
+int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes,
+                           const gyt_scene* const* scenes_alt, const GytCamera* cameras,
+                           const GytRenderParams* params, uint32_t sample_spp, GytBatchConfig* best,
+                           float* best_mpaths);
 
 /* Render without allocating: the same render as gyt_render_device, for
  * callers that must not allocate GPU memory during the call (an engine that

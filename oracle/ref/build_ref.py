@@ -14,7 +14,7 @@ Recipe (no reference build system is run):
      submodules), plus ``oracle/ref/harness.cpp``;
   4. link ``oracle/_ref/gyref_harness``.
 
-Patches (P-numbers as in the survey of the reference):
+Patches (numbered P1-P8; each is an exact text replacement):
   P1 common/Core.h:42-43     int64/uint64 as long long so the Sampler override
                              at sampler/Sobol.h:70 matches sampler/Sampler.h:12
   P2 math/Linagl.h:155       dependent base-class name for GCC
