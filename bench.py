@@ -3,7 +3,9 @@
 Workload (default): a seeded noise-displaced icosphere of 1,310,720 triangles
 with 64 GGX-conductor material groups in the Cornell box, 1024x1024 film,
 64 spp Sobol', max depth 16 -> 67,108,864 camera paths per step. Synthetic
-seeded geometry stands in for the reference's mesh assets.
+seeded geometry stands in for the reference's mesh assets. After it, the
+uneven batch workload (64 seeded instances of 10k-2M triangles, 128^2-1024^2,
+1-64 spp) is timed per scene and as one batched render ("batched" object).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -45,6 +47,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bvh-width", type=int, default=None, choices=[2, 8])
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="instances of the uneven batch workload measured after the main render (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--adjoint-iters", type=int, default=200,
+                    help="Adam iterations of the inverse-rendering run after the adjoint timing (0 = skip the run)")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -65,30 +73,40 @@ def config(a, sd, extra=None):
 
 # ------------------------------------------------------------ dist setup ---
 class Dist:
-    def __init__(self, n):
+    """One process per GPU (torchrun environment). Every rank renders its own
+    full frame, so the only collectives are the barrier around the timed
+    region and the max-over-ranks reduction of the timings. NCCL on GPUs;
+    gloo where CUDA is absent (the CPU tests of this plumbing)."""
+
+    def __init__(self, n, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
         if self.world > 1:
             import datetime
+            import torch
             import torch.distributed as dist
             self.dist = dist
-            backend = "nccl"
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.pg = True
 
     def barrier(self):
         if self.pg:
             import torch
-            self.dist.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                self.dist.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.dist.barrier()
 
     def max(self, v):
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -303,10 +321,194 @@ def run_ours(a):
                 line["cpu_baseline"] = cpu_baseline(sd, spp=2)
             except Exception as e:  # reported, never fatal for the GPU numbers
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
-        print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
+    if a.batch_instances > 0:
+        b = measure_batch(a, d, g, torch)
+        if d.rank == 0:
+            line["batched"] = b
+    if not a.no_adjoint:
+        adj = measure_adjoint(a, d, g, torch)
+        if d.rank == 0:
+            line["adjoint"] = adj
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
     d.close()
+
+
+def measure_batch(a, d, g, torch):
+    """The uneven batch workload (64 seeded instances: Cornell boxes holding
+    displaced icospheres or tori of 10k-2M triangles, 128^2-1024^2 films,
+    1-64 spp, depth 16): every instance rendered on its own with
+    gyt_render_device (the per-scene integrator) against all of them in one
+    batched render (one graph launch, autotuned). Both render the same paths,
+    so their images have equal RMSE; the check reports the largest film
+    difference."""
+    from gyunity_b200 import scenes
+    t = time.perf_counter()
+    descs = scenes.batch_workload(a.batch_instances, seed=1000)
+    gen_s = time.perf_counter() - t
+    ctx = g.Context(d.local)
+    t = time.perf_counter()
+    scs = [g.Scene(sd, ctx) for sd in descs]
+    create_s = time.perf_counter() - t
+    cams = [sd.camera for sd in descs]
+    prms = [sd.params for sd in descs]
+    films = [torch.zeros(c.res_x * c.res_y * 4, dtype=torch.float64, device="cuda") for c in cams]
+    ptrs = [f.data_ptr() for f in films]
+    paths = sum(sd.n_paths() for sd in descs)
+
+    def per_scene():
+        ms = 0.0
+        for sc, c, p, f in zip(scs, cams, prms, ptrs):
+            ms += ctx.render_device(sc, c, p, f)["ms"]
+        return ms
+
+    for f in films:
+        f.zero_()
+    per_scene()  # warm-up pass (also the reference films)
+    ref = [f.clone() for f in films]
+    d.barrier()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    per_ms = per_scene()
+    torch.cuda.synchronize()
+    per_wall = time.perf_counter() - w0
+    per_ms = d.max(per_ms)
+
+    t = time.perf_counter()
+    cfg, tune_mp = ctx.batch_autotune(scs, cams, prms, sample_spp=1)
+    tune_s = time.perf_counter() - t
+    st = None
+    for _ in range(a.warmup):
+        st = ctx.render_batch_device(scs, cams, prms, ptrs)
+    d.barrier()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    b_ms = 0.0
+    launches = 0
+    for _ in range(a.batch_steps):
+        st = ctx.render_batch_device(scs, cams, prms, ptrs)
+        b_ms += st["ms"]
+        launches += st["launches"]
+    torch.cuda.synchronize()
+    b_wall = (time.perf_counter() - w0) / a.batch_steps
+    b_ms = d.max(b_ms / a.batch_steps)
+    # equal RMSE: one more batched render from zeroed films against the per-scene films
+    for f in films:
+        f.zero_()
+    ctx.render_batch_device(scs, cams, prms, ptrs)
+    torch.cuda.synchronize()
+    diff = max(float(((x - y).abs().max() / y.abs().max().clamp_min(1e-300)).item()) for x, y in zip(films, ref))
+    # end to end: the host-image batch call (images copied back every step)
+    imgs_bytes = sum(c.res_x * c.res_y * 3 * 4 for c in cams)
+    ctx.render_batch(scs, cams, prms)
+    t = time.perf_counter()
+    ctx.render_batch(scs, cams, prms)
+    e2e_s = d.max(time.perf_counter() - t)
+    out = {"workload": "uneven batch: %d instances, %d triangles, %d paths per step" % (
+               len(descs), sum(sd.n_triangles for sd in descs), paths),
+           "value": paths * d.world / (b_ms / 1e3) / 1e6, "unit": UNIT,
+           "ms_per_step": b_ms, "wall_ms_per_step": b_wall * 1e3, "steps": a.batch_steps,
+           "gpu_launches_per_step": launches // max(1, a.batch_steps), "graph_launches_per_step": 1,
+           "per_scene": {"value": paths * d.world / (per_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": per_ms,
+                         "wall_ms_per_step": per_wall * 1e3,
+                         "note": "gyt_render_device once per instance, events around each render"},
+           "speedup_vs_per_scene": per_ms / b_ms,
+           "equal_rmse": {"max_rel_film_diff": diff,
+                          "note": "same paths in both runs; only the order of the FP64 film sums differs"},
+           "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s},
+           "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": imgs_bytes,
+                   "note": "gyt_render_batch with the scenes resident, every image copied to host"},
+           "scene_generation_s": gen_s, "scene_create_s": create_s}
+    del films, ref
+    for sc in scs:
+        sc.close()
+    ctx.close()
+    return out
+
+
+def measure_adjoint(a, d, g, torch):
+    """Differentiable inverse rendering: a level-5 icosphere (20,480
+    triangles) in 256 GGX material groups and 4 emitter quads, 512x512, 32
+    spp, depth 8; P = 256 * (3 albedo + 1 alpha) + 4 * 3 radiance = 1036
+    parameters. Gradients per second by path replay (one primal + one adjoint
+    pass gives all P) against central finite differences (2P primal renders),
+    the FD check on 16 parameters (step 1e-3) and the Adam run from the
+    perturbed parameters."""
+    from gyunity_b200 import diff, scenes
+    ctx = g.Context(d.local)
+    hidden = scenes.inverse_params(groups=256, emitters=4, seed=7)
+    sd = scenes.inverse_box(hidden, level=5, res=512, spp=32, max_depth=8, rr_depth=8)
+    r = diff.DiffRenderer(ctx, sd)
+    target = r.forward(hidden).clone()
+    init = scenes.perturb_params(hidden, seed=8)
+    P = init.count
+    fwd, adj = [], []
+    for k in range(a.warmup + a.steps):
+        loss, grad = diff.loss_and_grad(r, init, target)
+        if k >= a.warmup:
+            fwd.append(r.last["forward_ms"])
+            adj.append(r.last["backward_ms"])
+    t_f = d.max(statistics.median(fwd))
+    t_a = d.max(statistics.median(adj))
+    # FD check: 8 albedo, 4 emitter (light sampling kept: exactly linear) and 4 alpha parameters
+    picks = [("albedo", i, c) for i, c in ((0, 0), (31, 1), (77, 2), (101, 0), (150, 1), (199, 2), (230, 0),
+                                           (255, 1))]
+    picks += [("radiance", i, c) for i, c in ((0, 0), (1, 1), (2, 2), (3, 0))]
+    picks += [("alpha", i, 0) for i in (5, 64, 128, 200)]
+
+    def get(p, kind, i, c):
+        return p.albedo[i, c] if kind == "albedo" else (p.alpha[i] if kind == "alpha" else p.radiance[i, c])
+
+    def put(p, kind, i, c, v):
+        q = scenes.InverseParams(p.albedo.copy(), p.alpha.copy(), p.radiance.copy())
+        if kind == "albedo":
+            q.albedo[i, c] = v
+        elif kind == "alpha":
+            q.alpha[i] = v
+        else:
+            q.radiance[i, c] = v
+        return q
+
+    checks = []
+    for kind, i, c in picks:
+        cur = get(init, kind, i, c)
+        keep = kind == "radiance"
+        up, dn = np.float32(cur + 1e-3), np.float32(cur - 1e-3)
+        fd = (diff.loss_at(r, put(init, kind, i, c, up), target, keep) -
+              diff.loss_at(r, put(init, kind, i, c, dn), target, keep)) / (float(up) - float(dn))
+        ad = float(get(grad, kind, i, c))
+        checks.append({"param": "%s[%d%s]" % (kind, i, "" if kind == "alpha" else ",%d" % c), "fd": fd,
+                       "adjoint": ad, "rel_err": abs(fd - ad) / max(abs(fd), 1e-30)})
+    out = {"workload": "inverse rendering: 20,480-triangle icosphere, 256 GGX groups, 4 emitters, 512x512, 32 spp, "
+                       "depth 8, %d parameters" % P,
+           "forward_ms": t_f, "adjoint_ms": t_a,
+           "grads_per_s": P / ((t_f + t_a) / 1e3), "fd_grads_per_s": P / (2 * P * t_f / 1e3),
+           "speedup_vs_fd": 2 * P * t_f / (t_f + t_a),
+           "paths_per_pass": int(sd.n_paths()),
+           "adjoint_mpaths_per_s": sd.n_paths() / t_a / 1e3,
+           "fd_check": checks,
+           "fd_check_max_rel_err": {k: max(x["rel_err"] for x in checks if x["param"].startswith(k))
+                                    for k in ("albedo", "radiance", "alpha")},
+           "fd_check_note": "central differences, step 1e-3; emitter steps keep the light-selection "
+                            "distribution; alpha moves the sampled directions, which fixed-sample differences "
+                            "follow and the detached adjoint does not"}
+    if a.adjoint_iters > 0:
+        t = time.perf_counter()
+        p, hist = diff.optimize(r, target, init, iterations=a.adjoint_iters, lr=0.02)
+        el = time.perf_counter() - t
+        err0 = float(np.abs(init.flat() - hidden.flat()).mean())
+        err1 = float(np.abs(p.flat() - hidden.flat()).mean())
+        out["optimization"] = {"iterations": a.adjoint_iters, "optimizer": "Adam lr 0.02", "loss_first": hist[0],
+                               "loss_last": hist[-1], "param_mae_first": err0, "param_mae_last": err1,
+                               "seconds": el,
+                               "e2e_grads_per_s": P * a.adjoint_iters / el,
+                               "note": "wall clock of the whole loop: parameter upload, primal, loss, adjoint, "
+                                       "gradient download and the Adam step through PathReplayRender"}
+    ctx.close()
+    return out
 
 
 # Algorithmic bytes per path slot and per ray:

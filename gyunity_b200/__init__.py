@@ -96,6 +96,46 @@ class Context:
         return self._lib.gyt_render_device_noalloc(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
                                                    ctypes.c_void_p(d_film_ptr), int(paths_in_flight))
 
+    # ---- differentiable rendering -----------------------------------------
+    def diff_forward(self, scene, camera, params, d_film_ptr, d_path_L_ptr):
+        """gyt_diff_forward: render into the device film and record every
+        path's radiance (res_x*res_y*spp*3 floats at d_path_L_ptr)."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_diff_forward(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                              ctypes.c_void_p(d_film_ptr), ctypes.c_void_p(d_path_L_ptr),
+                                              ctypes.byref(st)))
+        return {"paths": st.paths, "iterations": st.iterations, "launches": st.launches, "ms": st.ms}
+
+    def diff_backward(self, scene, camera, params, d_img_grad_ptr, d_film_ptr, d_path_L_ptr, d_grad_mat_ptr,
+                      d_grad_em_ptr):
+        """gyt_diff_backward: adds dLoss/dparams into the device gradient arrays."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_diff_backward(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                               ctypes.c_void_p(d_img_grad_ptr), ctypes.c_void_p(d_film_ptr),
+                                               ctypes.c_void_p(d_path_L_ptr), ctypes.c_void_p(d_grad_mat_ptr),
+                                               ctypes.c_void_p(d_grad_em_ptr), ctypes.byref(st)))
+        return {"paths": st.paths, "iterations": st.iterations, "launches": st.launches, "ms": st.ms}
+
+    def diff_backward_paths(self, scene, xys, delta, L_total, camera=None, params=None):
+        """gyt_diff_backward_paths: gradient sums (n_materials, 4) and
+        (n_emission, 3) of explicit paths with adjoint weights delta."""
+        cam = _c.camera_struct(camera or scene.desc.camera)
+        prm = _c.params_struct(params or scene.desc.params)
+        xys = np.ascontiguousarray(xys, np.uint32).reshape(-1, 3)
+        n = xys.shape[0]
+        d = np.ascontiguousarray(delta, np.float32).reshape(n, 3)
+        L = np.ascontiguousarray(L_total, np.float32).reshape(n, 3)
+        nm, ne = scene.desc.mat_type.shape[0], scene.desc.emission.shape[0]
+        gm = np.zeros((nm, 4), np.float64)
+        ge = np.zeros((max(ne, 1), 3), np.float64)
+        self.check(self._lib.gyt_diff_backward_paths(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                                     n, _c.ptr(xys), _c.ptr(d), _c.ptr(L), _c.ptr(gm), _c.ptr(ge)))
+        return gm, ge[:ne]
+
     # ---- batched renders ---------------------------------------------------
     def set_batch_config(self, paths_in_flight=0, stride_blocks_per_sm=0, trace_blocks_per_sm=0, use_graph=True):
         c = _c.GytBatchConfig(int(paths_in_flight), int(stride_blocks_per_sm), int(trace_blocks_per_sm),
@@ -186,6 +226,15 @@ class Scene:
         a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
         self.ctx.check(self.ctx._lib.gyt_scene_info(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return {"triangles": a.value, "bvh_nodes": b.value, "device_bytes": c.value}
+
+    def set_materials(self, mat_params=None, emission=None, keep_light_sampling=False):
+        """gyt_scene_set_materials: new material parameters (n_materials, 16)
+        and/or emission rows (n_emission, 3); geometry and BVH are kept. With
+        keep_light_sampling the light-selection distribution is not rebuilt."""
+        mp = None if mat_params is None else np.ascontiguousarray(mat_params, np.float32)
+        em = None if emission is None else np.ascontiguousarray(emission, np.float32)
+        flags = _c.KEEP_LIGHT_SAMPLING if keep_light_sampling else 0
+        self.ctx.check(self.ctx._lib.gyt_scene_set_materials(self.handle, _c.ptr(mp), _c.ptr(em), flags))
 
     def read_bvh(self):
         """The binary BVH on the host: node slots (n, 16) float32 in the

@@ -22,11 +22,15 @@ EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_c
            "gyt_scene_read_bvh", "gyt_render", "gyt_render_device",
            "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world",
            "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
-           "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune"]
+           "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune", "gyt_scene_set_materials",
+           "gyt_diff_forward", "gyt_diff_backward", "gyt_diff_backward_paths"]
 
 # BVH builders (GYT_BVH_BUILD_* in include/gyt.h)
 BVH_BUILD_HOST = 0
 BVH_BUILD_DEVICE = 1
+
+# gyt_scene_set_materials flags
+KEEP_LIGHT_SAMPLING = 1
 
 # Path slots of the library's built-in scratch array (GYT_NOALLOC_MAX_PATHS in include/gyt.h).
 NOALLOC_MAX_PATHS = 32768
@@ -116,6 +120,13 @@ def load():
     L.gyt_sobol.argtypes = [P, U64, P, P, P]
     L.gyt_sobol_enum_index.argtypes = [P, U32, U32, U64, P, P]
     L.gyt_camera_raster_to_world.argtypes = [ctypes.POINTER(GytCamera), P]
+    L.gyt_scene_set_materials.argtypes = [P, P, P, U32]
+    L.gyt_diff_forward.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, P,
+                                   ctypes.POINTER(GytRenderStats)]
+    L.gyt_diff_backward.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, P, P, P, P,
+                                    ctypes.POINTER(GytRenderStats)]
+    L.gyt_diff_backward_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P,
+                                          P, P, P, P]
     L.gyt_context_set_batch_config.argtypes = [P, ctypes.POINTER(GytBatchConfig)]
     L.gyt_context_get_batch_config.argtypes = [P, ctypes.POINTER(GytBatchConfig)]
     L.gyt_render_batch_device.argtypes = [P, U32, P, P, P, P, ctypes.POINTER(GytRenderStats)]

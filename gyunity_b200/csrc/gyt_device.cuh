@@ -203,7 +203,11 @@ __device__ __noinline__ bool wt_intersect_fp64(const WtRay& r, float3 p0, float3
   double Ax = (comp(p0, r.kx) - ox) - Sx * Akz, Ay = (comp(p0, r.ky) - oy) - Sy * Akz;
   double Bx = (comp(p1, r.kx) - ox) - Sx * Bkz, By = (comp(p1, r.ky) - oy) - Sy * Bkz;
   double Cx = (comp(p2, r.kx) - ox) - Sx * Ckz, Cy = (comp(p2, r.ky) - oy) - Sy * Ckz;
-  double U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+  // edge functions without contraction: a shared edge gives exactly opposite
+  // values in its two triangles (see wt_intersect)
+  double U = __dsub_rn(__dmul_rn(Cx, By), __dmul_rn(Cy, Bx));
+  double V = __dsub_rn(__dmul_rn(Ax, Cy), __dmul_rn(Ay, Cx));
+  double W = __dsub_rn(__dmul_rn(Bx, Ay), __dmul_rn(By, Ax));
   if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
   double det = U + V + W;
   if (det == 0) return false;
@@ -223,7 +227,14 @@ GYT_D bool wt_intersect(const WtRay& r, float3 p0, float3 p1, float3 p2, float t
   float Ax = comp(A, r.kx) - r.Sx * Akz, Ay = comp(A, r.ky) - r.Sy * Akz;
   float Bx = comp(B, r.kx) - r.Sx * Bkz, By = comp(B, r.ky) - r.Sy * Bkz;
   float Cx = comp(C, r.kx) - r.Sx * Ckz, Cy = comp(C, r.ky) - r.Sy * Ckz;
-  float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+  // Edge functions without FMA contraction: the two triangles of a shared
+  // edge evaluate it from the same two transformed vertices in swapped order,
+  // and only unfused products make the results exact negatives of each other,
+  // which is what makes the test watertight (a fused a*b - c*d rounds the
+  // two orders differently, and a ray exactly on the edge can miss both).
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
   if (U == 0.f || V == 0.f || W == 0.f) {
     U = (float)((double)Cx * By - (double)Cy * Bx);
     V = (float)((double)Ax * Cy - (double)Ay * Cx);
@@ -654,6 +665,36 @@ struct Bsdf {
 };
 
 GYT_D float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }  // Integrator.h:11-15
+
+// d log f / d alpha of the GGX reflection lobe (MicrofacetReflectionBSDF,
+// bsdf/BSDF.h:308-370) at local directions wo, wi, for ax = ay = alpha: the
+// factors that depend on alpha are D (Microfacet.cpp:232-252),
+//   D = 1 / (pi a^2 (c^2 + s^2 / a^2)^2),  d log D / da = -2/a + 4 s^2 / (a (a^2 c^2 + s^2)),
+// and the Smith terms G1 = 2 / (1 + S), S = sqrt(1 + a^2 tan^2) (:357-373),
+//   d log G1 / da = -a tan^2 / (S (1 + S)).
+// Where f = 0 (a grazing or back-facing direction) the derivative is 0.
+GYT_D float ggx_dlog_alpha(const GGX& g, float3 wo, float3 wi) {
+  float3 wh = wi + wo;
+  if (is_zero(wh)) return 0.f;
+  wh = norm(wh);
+  wh = wh * sgnf(wh.z);
+  const float a = g.ax;
+  const float c2 = wh.z * wh.z, s2 = wh.x * wh.x + wh.y * wh.y;
+  float d = -2.f / a + 4.f * s2 / (a * (a * a * c2 + s2));
+  const float3 vs[2] = {wo, wi};
+  for (int k = 0; k < 2; ++k) {
+    const float3 v = vs[k];
+    const float tanT = fabsf(sqrtf(fmaxf(0.f, 1.f - v.z * v.z)) / v.z);
+    if (tanT > 0.f && isfinite(tanT)) {
+      const float r = a * tanT;
+      const float S = sqrtf(1.f + r * r);
+      d -= a * tanT * tanT / (S * (1.f + S));
+    }
+  }
+  return isfinite(d) ? d : 0.f;
+}
+// The lobe's alpha derivative (0 for lobes without a differentiable alpha).
+GYT_D float lobe_dlog_alpha(const Lobe& l, float3 wo, float3 wi) { return l.type == 3 ? ggx_dlog_alpha(l.g, wo, wi) : 0.f; }
 
 // ----------------------------------------------------- environment light ---
 // EnvironmentMap (light/EnvMap.h) over a lat-long RGB image with the

@@ -23,6 +23,7 @@
 // paths stay dense and new paths fill the tail.
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 
 #include <algorithm>
 #include <cfloat>
@@ -65,7 +66,7 @@ struct DevScene {
 };
 
 // Light record (kLightRec float4): (p0, Le.r) (p1, Le.g) (p2, Le.b)
-// (n0, area) (n1, leaf index) (n2, original id) (face normal, -).
+// (n0, area) (n1, leaf index) (n2, original id) (face normal, emission row).
 constexpr int kLightRec = 7;
 
 struct PathBuf {
@@ -91,7 +92,24 @@ struct Queues {
   float4* mc;  // MIS ray: contribution, path slot bits
   float4* hit; // per path slot: t, b1, b2, prim bits
   uint32_t* counts;  // [0] shadow rays, [1] MIS rays, [2..4] fetch counters, [5] compaction
+  float4* sx;  // adjoint pass, shadow ray: material bits, d log f / d alpha, light bits, -
+  float4* mx;  // adjoint pass, MIS ray: material bits, d log f / d alpha, -, -
 };
+
+// Adjoint (path replay) state per path slot, ping-ponged with the pool.
+struct AdjBuf {
+  float4* delta;  // dLoss / d(path radiance), RGB
+  float4* Ltot;   // the path's radiance from the primal pass
+  uint2* pend;    // the last continuation: material | kPendValid, d log f / d alpha bits
+};
+
+// Parameter gradients (FP64): per material (dL/da.r, dL/da.g, dL/da.b,
+// dL/dalpha) and per emission row (dL/dLe.rgb).
+struct GradOut {
+  double* mat;
+  double* em;
+};
+constexpr uint32_t kPendValid = 1u << 31;
 
 struct Params {
   uint32_t spp, max_depth, rr_depth;
@@ -564,11 +582,61 @@ GYT_D uint32_t queue_slot(uint32_t* count) {
   return g.shfl(base, 0) + g.thread_rank();
 }
 
+// Gradient accumulation: lanes with the same key sum their values first
+// (FP64), one atomic per key and warp.
+GYT_D void grad_add(double* g, uint32_t key, int n, const double* v) {
+  cg::coalesced_group act = cg::coalesced_threads();
+  cg::coalesced_group grp = cg::labeled_partition(act, key);
+  for (int k = 0; k < n; ++k) {
+    const double r = cg::reduce(grp, v[k], cg::plus<double>());
+    if (grp.thread_rank() == 0) atomicAdd(g + (size_t)key * n + k, r);
+  }
+}
+
+// A contribution C (RGB) whose path carries the adjoint weight delta and
+// whose BSDF factor belongs to material m (albedo a, d log f / d alpha = da):
+// dL/da_c += delta_c C_c / a_c (f is linear in a for the diffuse and GGX
+// lobes), dL/dalpha += sum_c delta_c C_c da.
+GYT_D void grad_material(const GradOut& G, const DevScene& s, uint32_t m, float3 Cd, float da) {
+  const uint32_t type = __ldg(s.mtypes + m);
+  if (type != 0 && type != 3) return;
+  const float* a = s.mparams + 16u * m;
+  const float a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2);
+  double v[4];
+  v[0] = a0 != 0.f ? (double)Cd.x / a0 : 0.0;
+  v[1] = a1 != 0.f ? (double)Cd.y / a1 : 0.0;
+  v[2] = a2 != 0.f ? (double)Cd.z / a2 : 0.0;
+  v[3] = ((double)Cd.x + Cd.y + Cd.z) * da;
+  grad_add(G.mat, m, 4, v);
+}
+
+// Contribution through area light li: dL/dLe_c += delta_c C_c / Le_c into its emission row.
+GYT_D void grad_emitter(const GradOut& G, const DevScene& s, int li, float3 Cd) {
+  const float4* r = s.ltab + kLightRec * li;
+  const float l0 = __ldg(r).w, l1 = __ldg(r + 1).w, l2 = __ldg(r + 2).w;
+  const uint32_t row = __float_as_uint(__ldg(r + 6).w);
+  double v[3];
+  v[0] = l0 != 0.f ? (double)Cd.x / l0 : 0.0;
+  v[1] = l1 != 0.f ? (double)Cd.y / l1 : 0.0;
+  v[2] = l2 != 0.f ? (double)Cd.z / l2 : 0.0;
+  grad_add(G.em, row, 3, v);
+}
+
 // One bounce of path slot i (PathTracing::Li loop body, integrator/PT.cpp:14-63,
 // with Integrator::DirectIllumination, integrator/Integrator.cpp:9-107): emission,
 // light and BSDF samples queued as shadow and MIS rays, the continuation ray.
+//
+// ADJ (path replay backpropagation): the same bounce, replayed with the same
+// samples, also moves gradient into G. Sampling decisions are detached: the
+// BSDF and light sample pdfs, MIS weights, light selection and roulette
+// probabilities are constants of the derivative, which is then an unbiased
+// estimate of the gradient of the expected image. The radiance a BSDF factor
+// f_k scales is known from the primal radiance: everything after vertex k's
+// continuation is Ltot - (radiance gathered through vertex k), settled at the
+// next bounce.
+template <bool ADJ>
 GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
-                      SobolTables tab, const DebugOut& dbg) {
+                      SobolTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   float4 h4 = q.hit[i];
   int prim = __float_as_int(h4.w);
   uint32_t meta = cur.meta[i];
@@ -580,6 +648,17 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
   float3 L = f3(cur.L[i]);
   const uint32_t bounce = depth;
   bool alive = false;
+  float3 adj = mk(0.f, 0.f, 0.f);
+  uint2 pend_new = make_uint2(0u, 0u);
+  if (ADJ) {
+    adj = f3(A.delta[i]);
+    const uint2 pend = A.pend[i];
+    if (pend.x & kPendValid) {
+      // the previous continuation's BSDF factor scales all radiance after it
+      const float3 after = f3(A.Ltot[i]) - L;
+      grad_material(G, s, pend.x & ~kPendValid, adj * after, __uint_as_float(pend.y));
+    }
+  }
   if (prim < 0) {
     // PT.cpp:18-21: environment emission on the camera ray or after a delta bounce
     if ((depth == 0 || delta) && s.has_env) L = L + tp * env_lookup(s.env, rd);
@@ -610,7 +689,10 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     const bool emit = (depth == 0 || delta) && light >= 0;
     if (emit) {
       LightTri l = load_light(s, light);
-      if (dot(h.n, h.wo) > 0.f) L = L + tp * l.Le;  // AreaLight::Emission (AreaLight.h:40-43)
+      if (dot(h.n, h.wo) > 0.f) {
+        L = L + tp * l.Le;  // AreaLight::Emission (AreaLight.h:40-43)
+        if (ADJ) grad_emitter(G, s, light, adj * (tp * l.Le));
+      }
     } else {
       float vz = u10[0], vy = u10[1], vx = u10[2];
       float uy = u10[3], ux = u10[4];
@@ -670,6 +752,9 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
             q.so[j] = make_float4(so.x, so.y, so.z, dis - kShadowEps);
             q.sd[j] = make_float4(dd.x, dd.y, dd.z, __uint_as_float(i));
             q.sc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(bounce));
+            if (ADJ)
+              q.sx[j] = make_float4(__uint_as_float(mat), lobe_dlog_alpha(bsdf.lobe, bsdf.local(h.wo), bsdf.local(wi)),
+                                    __int_as_float(li), 0.f);
           }
         }
         // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
@@ -687,6 +772,9 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
             q.mo[j] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
             q.md[j] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
             q.mc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(i));
+            if (ADJ)
+              q.mx[j] = make_float4(__uint_as_float(mat), lobe_dlog_alpha(bsdf.lobe, bsdf.local(h.wo), bsdf.local(wi2)),
+                                    0.f, 0.f);
           }
         }
       }
@@ -718,18 +806,22 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
         cur.tp[i] = make_float4(tp.x, tp.y, tp.z, 0.f);
         depth += 1;
         alive = depth < prm.max_depth;
+        if (ADJ && alive)
+          pend_new = make_uint2(mat | kPendValid,
+                                __float_as_uint(lobe_dlog_alpha(bsdf.lobe, bsdf.local(h.wo), bsdf.local(wi))));
       }
     }
   }
   cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
   cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
+  if (ADJ) A.pend[i] = pend_new;
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
                                                   SobolTables tab, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  shade_path(cur, i, s, prm, q, tab, dbg);
+  shade_path<false>(cur, i, s, prm, q, tab, dbg);
 }
 
 // Next-event shadow rays (any hit): an unoccluded ray adds its contribution
@@ -760,8 +852,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow(PathBuf cur, DevScene s, Queu
 }
 
 // MIS-ray result of one queue entry (shared by both MIS kernels).
+template <bool ADJ = false>
 GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint32_t j, int prim, float b1, float b2,
-                    const DebugOut& dbg) {
+                    const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   const float4 md = q.md[j], mc = q.mc[j];
   const int li = __float_as_int(md.w);
   const uint32_t slot = __float_as_uint(mc.w);
@@ -785,6 +878,12 @@ GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint
   if (reach) {
     float4 l = cur.L[slot];
     cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
+    if (ADJ) {
+      const float3 Cd = f3(A.delta[slot]) * add;
+      const float4 x = q.mx[j];
+      grad_material(G, s, __float_as_uint(x.x), Cd, x.y);
+      if (li < s.n_area) grad_emitter(G, s, li, Cd);
+    }
     if (dbg.mis) {
       const uint32_t b = __float_as_uint(q.mo[j].w);
       if (b < 64) dbg.mis[cur.pid[slot]] |= 1ull << b;
@@ -860,6 +959,138 @@ __global__ void __launch_bounds__(kBlock) k_finish(PathBuf cur, PathBuf nxt, uin
   }
 }
 
+// ------------------------------------------------------- adjoint pass ---
+// Inputs of the path replay: the image gradient and the primal film (its
+// per-pixel weights) for full renders, or per-path adjoint weights for an
+// explicit path list; the primal radiance of every path.
+struct AdjIn {
+  const float* img_grad;    // dLoss/dImage, res_x * res_y * 3 (full renders)
+  const double* film;       // the primal film, res_x * res_y * 4 (weights in .w)
+  const float* path_delta;  // per path id, 3 floats (explicit lists)
+  const float* path_L;      // per path id, 3 floats: the primal radiance
+};
+
+__global__ void __launch_bounds__(kBlock) k_generate_adj(PathBuf dst, AdjBuf A, uint32_t base, uint32_t n_new,
+                                                         unsigned long long first, Cam cam, uint32_t spp,
+                                                         const uint32_t* __restrict__ list, SobolTables tab,
+                                                         AdjIn in) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_new) return;
+  const unsigned long long p = first + j;
+  uint32_t x, y, s;
+  if (list) {
+    x = __ldg(list + 3 * p);
+    y = __ldg(list + 3 * p + 1);
+    s = __ldg(list + 3 * p + 2);
+  } else {
+    const unsigned long long pixel = p / spp;
+    s = (uint32_t)(p - pixel * spp);
+    y = (uint32_t)(pixel / cam.res_x);
+    x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+  }
+  const uint32_t k = base + j;
+  gen_path(dst, k, x, y, s, cam, tab);
+  dst.pid[k] = (uint32_t)p;
+  float3 d = mk(0.f, 0.f, 0.f);
+  if (in.path_delta) {
+    d = mk(in.path_delta[3 * p], in.path_delta[3 * p + 1], in.path_delta[3 * p + 2]);
+  } else {
+    // the pixels the sample reaches (Film::AddSample's box filter, as
+    // k_finish splats it), each image value = colour / weight
+    const uint32_t pix = dst.pix[k];
+    const uint32_t q = pix & kPixMask;
+    const uint32_t py = q / cam.res_x, px = q - py * cam.res_x;
+    auto add = [&](uint32_t xx, uint32_t yy) {
+      const size_t o = (size_t)yy * cam.res_x + xx;
+      const double w = in.film[4 * o + 3];
+      if (w > 0.0) {
+        const float iw = (float)(1.0 / w);
+        d = d + mk(in.img_grad[3 * o], in.img_grad[3 * o + 1], in.img_grad[3 * o + 2]) * iw;
+      }
+    };
+    add(px, py);
+    if (pix & (1u << 30)) add(px - 1, py);
+    if (pix & (1u << 31)) add(px, py - 1);
+    if ((pix & (1u << 30)) && (pix & (1u << 31))) add(px - 1, py - 1);
+  }
+  A.delta[k] = make_float4(d.x, d.y, d.z, 0.f);
+  A.Ltot[k] = make_float4(in.path_L[3 * p], in.path_L[3 * p + 1], in.path_L[3 * p + 2], 0.f);
+  A.pend[k] = make_uint2(0u, 0u);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_adj(PathBuf cur, AdjBuf A, uint32_t n, DevScene s, Params prm,
+                                                      Queues q, SobolTables tab, GradOut G) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  shade_path<true>(cur, i, s, prm, q, tab, DebugOut{}, A, G);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_shadow_adj(PathBuf cur, AdjBuf A, DevScene s, Queues q, GradOut G) {
+  const uint32_t n = *(volatile uint32_t*)q.counts;
+  persistent_trace<W, true, false>(
+      s, q.counts + 3, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
+        const float4 a = q.so[j], b = q.sd[j];
+        o = f3(a);
+        d = f3(b);
+        tmax = a.w;
+      },
+      [&](uint32_t j, int prim, float, float, float) {
+        if (prim >= 0) return;
+        const uint32_t slot = __float_as_uint(q.sd[j].w);
+        const float4 c = q.sc[j], l = cur.L[slot];
+        cur.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.f);
+        const float3 Cd = f3(A.delta[slot]) * f3(c);
+        const float4 x = q.sx[j];
+        grad_material(G, s, __float_as_uint(x.x), Cd, x.y);
+        const int li = __float_as_int(x.z);
+        if (li < s.n_area) grad_emitter(G, s, li, Cd);
+      },
+      nullptr);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_mis_adj(PathBuf cur, AdjBuf A, DevScene s, Queues q, GradOut G) {
+  const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
+  persistent_trace<W, false, false>(
+      s, q.counts + 4, n,
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
+        o = f3(q.mo[j]);
+        d = f3(q.md[j]);
+        tmax = __int_as_float(0x7f800000);
+      },
+      [&](uint32_t j, int prim, float, float b1, float b2) {
+        mis_done<true>(cur, q, s, j, prim, b1, b2, DebugOut{}, A, G);
+      },
+      nullptr);
+}
+
+// Live paths (and their adjoint state) compacted; finished paths are done
+// (their gradient was moved at their last bounce).
+__global__ void __launch_bounds__(kBlock) k_finish_adj(PathBuf cur, PathBuf nxt, AdjBuf A, AdjBuf AN, uint32_t n,
+                                                       uint32_t* __restrict__ counter) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t meta = cur.meta[i];
+  if (!(meta & kAlive)) return;
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+  const uint32_t j = g.shfl(base, 0) + g.thread_rank();
+  nxt.o[j] = cur.o[i];
+  nxt.d[j] = cur.d[i];
+  nxt.tp[j] = cur.tp[i];
+  nxt.L[j] = cur.L[i];
+  nxt.sidx[j] = cur.sidx[i];
+  nxt.meta[j] = meta;
+  nxt.pix[j] = cur.pix[i];
+  nxt.pid[j] = cur.pid[i];
+  AN.delta[j] = A.delta[i];
+  AN.Ltot[j] = A.Ltot[i];
+  AN.pend[j] = A.pend[i];
+}
+
 // ------------------------------------------------------ batched renders ---
 // Many scenes, cameras and sample counts in one wavefront: the path pool is
 // refilled from the concatenation of all instances' paths (instance-major),
@@ -872,6 +1103,14 @@ struct Inst {
   double* film;
   unsigned long long first;  // first global path index of the instance
 };
+
+// The instance table lives in constant memory: warps almost always hold paths
+// of one instance (the pool is refilled instance after instance), so the
+// per-path reads of scene fields are uniform constant-cache hits and the
+// compiler can keep them out of the way of the kernels' global stores.
+// Larger batches run as consecutive groups of kMaxBatch instances.
+constexpr uint32_t kMaxBatch = 128;
+__constant__ Inst c_insts[kMaxBatch];
 
 // Device-side loop state of a batched render (one half-iteration moves the
 // pool from one buffer to the other).
@@ -898,7 +1137,7 @@ __global__ void k_batch_begin(IterState* __restrict__ st, uint32_t* __restrict__
 }
 
 __global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const IterState* __restrict__ st,
-                                                           const Inst* __restrict__ insts, SobolTables tab) {
+                                                           SobolTables tab) {
   const uint32_t n_new = st->n_new, base = st->active, ni = st->n_inst;
   const unsigned long long first = st->generated;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_new; j += gridDim.x * blockDim.x) {
@@ -907,9 +1146,9 @@ __global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const It
     uint32_t lo = 0, hi = ni;
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (insts[mid].first <= g) lo = mid; else hi = mid;
+      if (c_insts[mid].first <= g) lo = mid; else hi = mid;
     }
-    const Inst& I = insts[lo];
+    const Inst& I = c_insts[lo];
     const unsigned long long p = g - I.first;
     const unsigned long long pixel = p / I.prm.spp;
     const uint32_t s = (uint32_t)(p - pixel * I.prm.spp);
@@ -928,16 +1167,15 @@ GYT_D TraceGeo geo_of(const DevScene& s) {
 
 template <int W>
 __global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const IterState* __restrict__ st,
-                                                         const Inst* __restrict__ insts, float4* __restrict__ hits,
-                                                         uint32_t* __restrict__ fetch) {
+                                                         float4* __restrict__ hits, uint32_t* __restrict__ fetch) {
   const uint32_t n = st->n;
   persistent_trace<W, false, false, true>(
-      insts[0].s, fetch, n,
+      c_insts[0].s, fetch, n,
       [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo& g) {
         o = f3(cur.o[i]);
         d = f3(cur.d[i]);
         tmax = __int_as_float(0x7f800000);
-        g = geo_of(insts[cur.inst[i]].s);
+        g = geo_of(c_insts[cur.inst[i]].s);
       },
       [&](uint32_t i, int prim, float tmax, float b1, float b2) {
         hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
@@ -945,26 +1183,26 @@ __global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const Iter
       nullptr);
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st,
-                                                        const Inst* __restrict__ insts, Queues q, SobolTables tab) {
+__global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q,
+                                                        SobolTables tab) {
   const uint32_t n = st->n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const Inst& I = insts[cur.inst[i]];
-    shade_path(cur, i, I.s, I.prm, q, tab, DebugOut{});
+    const Inst& I = c_insts[cur.inst[i]];
+    shade_path<false>(cur, i, I.s, I.prm, q, tab, DebugOut{});
   }
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_shadow_batch(PathBuf cur, const Inst* __restrict__ insts, Queues q) {
+__global__ void __launch_bounds__(kBlock) k_shadow_batch(PathBuf cur, Queues q) {
   const uint32_t n = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, false, true>(
-      insts[0].s, q.counts + 3, n,
+      c_insts[0].s, q.counts + 3, n,
       [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
         const float4 a = q.so[j], b = q.sd[j];
         o = f3(a);
         d = f3(b);
         tmax = a.w;
-        g = geo_of(insts[cur.inst[__float_as_uint(b.w)]].s);
+        g = geo_of(c_insts[cur.inst[__float_as_uint(b.w)]].s);
       },
       [&](uint32_t j, int prim, float, float, float) {
         if (prim < 0) {
@@ -977,26 +1215,25 @@ __global__ void __launch_bounds__(kBlock) k_shadow_batch(PathBuf cur, const Inst
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_mis_batch(PathBuf cur, const Inst* __restrict__ insts, Queues q) {
+__global__ void __launch_bounds__(kBlock) k_mis_batch(PathBuf cur, Queues q) {
   const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
   persistent_trace<W, false, false, true>(
-      insts[0].s, q.counts + 4, n,
+      c_insts[0].s, q.counts + 4, n,
       [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
         o = f3(q.mo[j]);
         d = f3(q.md[j]);
         tmax = __int_as_float(0x7f800000);
-        g = geo_of(insts[cur.inst[__float_as_uint(q.mc[j].w)]].s);
+        g = geo_of(c_insts[cur.inst[__float_as_uint(q.mc[j].w)]].s);
       },
       [&](uint32_t j, int prim, float, float b1, float b2) {
         const uint32_t slot = __float_as_uint(q.mc[j].w);
-        mis_done(cur, q, insts[cur.inst[slot]].s, j, prim, b1, b2, DebugOut{});
+        mis_done(cur, q, c_insts[cur.inst[slot]].s, j, prim, b1, b2, DebugOut{});
       },
       nullptr);
 }
 
 // Finished paths to their instance's film, live paths compacted.
 __global__ void __launch_bounds__(kBlock) k_finish_batch(PathBuf cur, PathBuf nxt, const IterState* __restrict__ st,
-                                                         const Inst* __restrict__ insts,
                                                          uint32_t* __restrict__ counter) {
   const uint32_t n = st->n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1017,7 +1254,7 @@ __global__ void __launch_bounds__(kBlock) k_finish_batch(PathBuf cur, PathBuf nx
       nxt.pid[j] = cur.pid[i];
       nxt.inst[j] = cur.inst[i];
     } else {
-      const Inst& I = insts[cur.inst[i]];
+      const Inst& I = c_insts[cur.inst[i]];
       const float3 L = f3(L4);
       const uint32_t pix = cur.pix[i], res_x = I.cam.res_x;
       double* film = I.film;
@@ -1180,10 +1417,8 @@ struct gyt_context {
   unsigned long long* d_counters = nullptr;  // node visits and triangle tests per traversal kernel
   GytProfile prof = {};
   int sms = 0;
-  // batched renders: instance table, device loop state, configuration and
-  // the captured graph (rebuilt when its kernels' arguments change)
-  Inst* d_insts = nullptr;
-  uint32_t insts_cap = 0;
+  // batched renders: device loop state, configuration and the captured graph
+  // (rebuilt when its kernels' arguments change)
   IterState* d_iter = nullptr;
   IterState* h_iter = nullptr;  // pinned
   GytBatchConfig bcfg = {0, 0, 0, 1, 0};
@@ -1191,6 +1426,10 @@ struct gyt_context {
   cudaGraph_t bgraph = nullptr;
   cudaGraphExec_t bexec = nullptr;
   uint64_t bkey[6] = {};
+  // adjoint pass: replay state per path slot (two buffers) and queue payloads
+  AdjBuf adj[2] = {};
+  uint32_t adj_cap = 0;
+  std::vector<void*> adj_allocs;
 };
 
 struct gyt_scene {
@@ -1200,6 +1439,11 @@ struct gyt_scene {
   std::vector<void*> allocs;
   uint64_t n_tris = 0, n_nodes = 0, n_slots = 0, bytes = 0;
   uint32_t bvh_depth = 0;
+  // what gyt_scene_set_materials needs to rebuild the light tables
+  uint32_t n_materials = 0, n_emission = 0;
+  std::vector<float4> ltab;       // host copy of the light records
+  std::vector<float> light_area;  // per area light
+  std::vector<float> power;       // light powers (area lights, then the environment)
 };
 
 namespace {
@@ -1286,6 +1530,28 @@ int32_t make_cam(gyt_context* ctx, const GytCamera* c, Cam* out) {
   return GYT_OK;
 }
 
+// Distribution1D over light power (visual/Sampling.h:18-45), in float as the
+// reference builds it: returns the integral, fills the n + 1 CDF values.
+float light_distribution(const std::vector<float>& power, std::vector<float>* cdf_out) {
+  const int nl = (int)power.size();
+  std::vector<float>& cdf = *cdf_out;
+  cdf.assign(nl + 1, 0.f);
+  float fint = 0.f;
+  if (nl) {
+    for (int i = 1; i < nl + 1; ++i) cdf[i] = cdf[i - 1] + power[i - 1] / nl;
+    fint = cdf[nl];
+    if (fint == 0.f) {
+      for (int i = 1; i < nl + 1; ++i) cdf[i] = (float)i / (float)nl;
+    } else {
+      for (int i = 1; i < nl + 1; ++i) cdf[i] /= fint;
+    }
+  }
+  return fint;
+}
+
+// AreaLight::Power (light/AreaLight.h:45-48)
+float area_light_power(const float* em, float area) { return lum(mk(em[0], em[1], em[2]) * area * kPi); }
+
 int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
   if (!p) return fail(ctx, GYT_ERR_INVALID, "params: null");
   if (p->spp == 0) return fail(ctx, GYT_ERR_INVALID, "params: spp must be > 0");
@@ -1293,6 +1559,15 @@ int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
     return fail(ctx, GYT_ERR_UNSUPPORTED, "params: max_depth must be in [1, 100] (Sobol' has 1024 dimensions)");
   if (p->rr_depth > 255) return fail(ctx, GYT_ERR_INVALID, "params: rr_depth too large");
   if (p->flags != 0) return fail(ctx, GYT_ERR_INVALID, "params: flags must be 0");
+  return GYT_OK;
+}
+
+// Pools changed size: the adjoint buffers follow on their next use.
+int32_t ensure_adj_reset(gyt_context* ctx) {
+  for (void* p : ctx->adj_allocs) cudaFree(p);
+  ctx->adj_allocs.clear();
+  ctx->adj_cap = 0;
+  ctx->q.sx = ctx->q.mx = nullptr;
   return GYT_OK;
 }
 
@@ -1325,6 +1600,25 @@ int32_t ensure_pool(gyt_context* ctx) {
   GYT_CK(ctx, dalloc(L, &q.hit, n));
   GYT_CK(ctx, dalloc(L, &q.counts, 8));
   ctx->pool_cap = ctx->capacity;
+  return ensure_adj_reset(ctx);
+}
+
+int32_t ensure_adj(gyt_context* ctx) {
+  if (ctx->adj_cap == ctx->pool_cap && ctx->q.sx) return GYT_OK;
+  for (void* p : ctx->adj_allocs) cudaFree(p);
+  ctx->adj_allocs.clear();
+  ctx->adj_cap = 0;
+  ctx->q.sx = ctx->q.mx = nullptr;
+  const size_t n = ctx->pool_cap;
+  auto& L = ctx->adj_allocs;
+  for (int b = 0; b < 2; ++b) {
+    GYT_CK(ctx, dalloc(L, &ctx->adj[b].delta, n));
+    GYT_CK(ctx, dalloc(L, &ctx->adj[b].Ltot, n));
+    GYT_CK(ctx, dalloc(L, &ctx->adj[b].pend, n));
+  }
+  GYT_CK(ctx, dalloc(L, &ctx->q.sx, n));
+  GYT_CK(ctx, dalloc(L, &ctx->q.mx, n));
+  ctx->adj_cap = ctx->pool_cap;
   return GYT_OK;
 }
 
@@ -1438,6 +1732,69 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
   return GYT_OK;
 }
 
+// The path replay (adjoint) wavefront: the primal's paths again, with the
+// adjoint kernels moving gradient into G.
+int32_t run_adjoint(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, const GytRenderParams* p,
+                    unsigned long long total, const uint32_t* d_list, const AdjIn& in, GradOut G,
+                    GytRenderStats* stats) {
+  int32_t st = ensure_pool(ctx);
+  if (st) return st;
+  st = ensure_adj(ctx);
+  if (st) return st;
+  const Params prm{p->spp, p->max_depth, p->rr_depth};
+  const SobolTables tab = tables(ctx);
+  cudaStream_t s = ctx->stream;
+  const int W = scene->dev.wnodes ? 8 : 2;
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)],
+            g_mis = ctx->pgrid[pindex(kPMis, W, false)];
+  const DevScene& D = scene->dev;
+  const Queues q = ctx->q;
+  unsigned long long generated = 0;
+  uint32_t active = 0, iters = 0, launches = 0;
+  int cur = 0;
+  GYT_CK(ctx, after_legacy_stream(ctx));
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
+  while (generated < total || active > 0) {
+    const uint32_t n_new = (uint32_t)std::min<unsigned long long>(ctx->capacity - active, total - generated);
+    GYT_CK(ctx, cudaMemsetAsync(q.counts, 0, 8 * sizeof(uint32_t), s));
+    const PathBuf P = ctx->pool[cur], N = ctx->pool[cur ^ 1];
+    const AdjBuf A = ctx->adj[cur], AN = ctx->adj[cur ^ 1];
+    if (n_new) {
+      k_generate_adj<<<grid_for(n_new), kBlock, 0, s>>>(P, A, active, n_new, generated, cam, p->spp, d_list, tab, in);
+      ++launches;
+    }
+    generated += n_new;
+    active += n_new;
+    if (W == 8) k_extend<8, false><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+    else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+    k_shade_adj<<<grid_for(active), kBlock, 0, s>>>(P, A, active, D, prm, q, tab, G);
+    if (W == 8) k_shadow_adj<8><<<g_sh, kBlock, 0, s>>>(P, A, D, q, G);
+    else k_shadow_adj<2><<<g_sh, kBlock, 0, s>>>(P, A, D, q, G);
+    if (W == 8) k_mis_adj<8><<<g_mis, kBlock, 0, s>>>(P, A, D, q, G);
+    else k_mis_adj<2><<<g_mis, kBlock, 0, s>>>(P, A, D, q, G);
+    k_finish_adj<<<grid_for(active), kBlock, 0, s>>>(P, N, A, AN, active, q.counts + 5);
+    launches += 5;
+    GYT_CK(ctx, cudaGetLastError());
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, q.counts, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaStreamSynchronize(s));
+    active = ctx->h_counter[5];
+    cur ^= 1;
+    if (++iters > 100000) return fail(ctx, GYT_ERR_WATCHDOG, "adjoint: wavefront iteration cap reached");
+  }
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
+  GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
+  if (stats) {
+    stats->paths = total;
+    stats->path_slots = 0;
+    stats->iterations = iters;
+    stats->launches = launches;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->ms = ms;
+  }
+  return GYT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1518,6 +1875,7 @@ void gyt_context_destroy(gyt_context* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void* p : c->pool_allocs) cudaFree(p);
+  for (void* p : c->adj_allocs) cudaFree(p);
   cudaFree(c->d_counter);
   cudaFreeHost(c->h_counter);
   cudaFree(c->d_sobol);
@@ -1528,7 +1886,6 @@ void gyt_context_destroy(gyt_context* c) {
   cudaFree(c->d_rgb);
   if (c->bexec) cudaGraphExecDestroy(c->bexec);
   if (c->bgraph) cudaGraphDestroy(c->bgraph);
-  if (c->d_insts) cudaFree(c->d_insts);
   if (c->d_iter) cudaFree(c->d_iter);
   if (c->h_iter) cudaFreeHost(c->h_iter);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1614,8 +1971,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       const float* em = &d->emission[3 * e];
       const uint32_t* I = &d->indices[3 * t];
       float area = 0.5f * length(cross(vtx(I[1]) - vtx(I[0]), vtx(I[2]) - vtx(I[0])));
-      // AreaLight::Power (light/AreaLight.h:45-48)
-      power.push_back(lum(mk(em[0], em[1], em[2]) * area * kPi));
+      power.push_back(area_light_power(em, area));
     }
   }
   for (uint32_t k = 0; k < d->n_spheres; ++k)
@@ -1687,19 +2043,9 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     float3 mid = (a * (1.f - dt) + b2 * dt) * d->env_scale;
     power.push_back(lum(mid * kPi * env_radius * env_radius));
   }
-  // Distribution1D over light power (visual/Sampling.h:18-45), in float
-  int nl = (int)power.size();
-  std::vector<float> cdf(nl + 1, 0.f);
-  float fint = 0.f;
-  if (nl) {
-    for (int i = 1; i < nl + 1; ++i) cdf[i] = cdf[i - 1] + power[i - 1] / nl;
-    fint = cdf[nl];
-    if (fint == 0.f) {
-      for (int i = 1; i < nl + 1; ++i) cdf[i] = (float)i / (float)nl;
-    } else {
-      for (int i = 1; i < nl + 1; ++i) cdf[i] /= fint;
-    }
-  }
+  const int nl = (int)power.size();
+  std::vector<float> cdf;
+  const float fint = light_distribution(power, &cdf);
   // acceleration structure: binary (two child boxes per 64-byte node, built
   // on the device or the host) or 8-wide with quantized child boxes (80-byte
   // nodes, host), per context setting
@@ -1833,7 +2179,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     sc->n_slots = use_wide ? 0 : bin.nodes.size() / 16;
     sc->bvh_depth = use_wide ? wide.max_depth : bin.max_depth;
   }
-  // light records: (p0, Le.r) (p1, Le.g) (p2, Le.b) (n0, area) (n1, leaf) (n2, id) (face, -)
+  // light records: (p0, Le.r) (p1, Le.g) (p2, Le.b) (n0, area) (n1, leaf) (n2, id) (face, emission row)
   std::vector<float4> ltab((size_t)n_area * kLightRec);
   for (int li = 0; li < n_area; ++li) {
     const int t = light_tris[li];
@@ -1853,7 +2199,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     r[3] = make_float4(nc[0].x, nc[0].y, nc[0].z, area);
     r[4] = make_float4(nc[1].x, nc[1].y, nc[1].z, bits(k));
     r[5] = make_float4(nc[2].x, nc[2].y, nc[2].z, bits(t));
-    r[6] = make_float4(face.x, face.y, face.z, 0.f);
+    r[6] = make_float4(face.x, face.y, face.z, bits(d->tri_emission[t]));
   }
   std::vector<float4> sph(d->n_spheres);
   for (uint32_t k = 0; k < d->n_spheres; ++k)
@@ -1903,6 +2249,12 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   ds.n_tris = (int)d->n_triangles;
   ds.n_spheres = (int)d->n_spheres;
   sc->n_tris = d->n_triangles;
+  sc->n_materials = d->n_materials;
+  sc->n_emission = d->n_emission;
+  sc->ltab = ltab;
+  sc->power = power;
+  sc->light_area.resize(n_area);
+  for (int li = 0; li < n_area; ++li) sc->light_area[li] = ltab[(size_t)li * kLightRec + 3].w;
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // uploads are ordered on the context stream
   if (e != cudaSuccess) {
     gyt_scene_destroy(sc);
@@ -1925,6 +2277,48 @@ int32_t gyt_scene_info(const gyt_scene* s, uint64_t* nt, uint64_t* nn, uint64_t*
   if (nt) *nt = s->n_tris;
   if (nn) *nn = s->n_nodes;
   if (bytes) *bytes = s->bytes;
+  return GYT_OK;
+}
+
+int32_t gyt_scene_set_materials(gyt_scene* s, const float* mat_params, const float* emission, uint32_t flags) {
+  if (!s || !s->ctx) return GYT_ERR_INVALID;
+  gyt_context* ctx = s->ctx;
+  GYT_CK(ctx, cudaSetDevice(s->device));
+  cudaStream_t st = ctx->stream;
+  if (mat_params) {
+    for (size_t k = 0; k < (size_t)s->n_materials * 16; ++k)
+      if (!std::isfinite(mat_params[k])) return fail(ctx, GYT_ERR_INVALID, "set_materials: non-finite parameter");
+    GYT_CK(ctx, cudaMemcpyAsync((void*)s->dev.mparams, mat_params, (size_t)s->n_materials * 16 * sizeof(float),
+                                cudaMemcpyHostToDevice, st));
+  }
+  if (emission) {
+    for (size_t k = 0; k < (size_t)s->n_emission * 3; ++k)
+      if (!(emission[k] >= 0.f) || !std::isfinite(emission[k]))
+        return fail(ctx, GYT_ERR_INVALID, "set_materials: emission must be finite and >= 0");
+    const int n_area = s->dev.n_area;
+    for (int li = 0; li < n_area; ++li) {
+      float4* r = &s->ltab[(size_t)li * kLightRec];
+      int row;
+      std::memcpy(&row, &r[6].w, 4);
+      const float* em = emission + 3 * (size_t)row;
+      r[0].w = em[0];
+      r[1].w = em[1];
+      r[2].w = em[2];
+      s->power[li] = area_light_power(em, s->light_area[li]);
+    }
+    if (n_area)
+      GYT_CK(ctx, cudaMemcpyAsync((void*)s->dev.ltab, s->ltab.data(), s->ltab.size() * sizeof(float4),
+                                  cudaMemcpyHostToDevice, st));
+    std::vector<float> cdf;
+    const float fint = light_distribution(s->power, &cdf);
+    if (!s->power.empty() && !(flags & GYT_KEEP_LIGHT_SAMPLING)) {
+      GYT_CK(ctx, cudaMemcpyAsync((void*)s->dev.lcdf, cdf.data(), cdf.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+      GYT_CK(ctx, cudaMemcpyAsync((void*)s->dev.lfunc, s->power.data(), s->power.size() * sizeof(float),
+                                  cudaMemcpyHostToDevice, st));
+      s->dev.lfunc_int = fint;
+    }
+  }
+  GYT_CK(ctx, cudaStreamSynchronize(st));
   return GYT_OK;
 }
 
@@ -2028,6 +2422,86 @@ int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamer
   if (rr_out) GYT_CK(ctx, cudaMemcpy(rr_out, dm, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   if (occ_out) GYT_CK(ctx, cudaMemcpy(occ_out, dm + n, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   if (mis_out) GYT_CK(ctx, cudaMemcpy(mis_out, dm + 2 * n, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
+int32_t gyt_diff_forward(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                         const GytRenderParams* params, double* d_film, float* d_path_L, GytRenderStats* stats) {
+  if (!ctx || !scene || !d_film || !d_path_L) return fail(ctx, GYT_ERR_INVALID, "diff_forward: null argument");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "diff_forward: more than 2^32 paths");
+  return run_paths(ctx, scene, cam, params, total, nullptr, d_film, DebugOut{d_path_L, nullptr, nullptr, nullptr,
+                                                                            nullptr}, stats);
+}
+
+int32_t gyt_diff_backward(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, const float* d_image_grad, const double* d_film,
+                          const float* d_path_L, double* d_grad_mat, double* d_grad_em, GytRenderStats* stats) {
+  if (!ctx || !scene || !d_image_grad || !d_film || !d_path_L || !d_grad_mat || (scene->n_emission && !d_grad_em))
+    return fail(ctx, GYT_ERR_INVALID, "diff_backward: null argument");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "diff_backward: more than 2^32 paths");
+  const AdjIn in{d_image_grad, d_film, nullptr, d_path_L};
+  return run_adjoint(ctx, scene, cam, params, total, nullptr, in, GradOut{d_grad_mat, d_grad_em}, stats);
+}
+
+int32_t gyt_diff_backward_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                const GytRenderParams* params, uint64_t n, const uint32_t* xys, const float* delta,
+                                const float* L_total, double* grad_mat, double* grad_em) {
+  if (!ctx || !scene || !camera || !grad_mat || (scene->n_emission && !grad_em) ||
+      (n && (!xys || !delta || !L_total)))
+    return fail(ctx, GYT_ERR_INVALID, "diff_backward_paths: null argument");
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  Cam cam;
+  st = make_cam(ctx, camera, &cam);
+  if (st) return st;
+  if (n >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "diff_backward_paths: too many paths");
+  for (uint64_t i = 0; i < n; ++i)
+    if (xys[3 * i] >= camera->res_x || xys[3 * i + 1] >= camera->res_y)
+      return fail(ctx, GYT_ERR_INVALID, "diff_backward_paths: pixel outside the film");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() {
+      for (void* p : v) cudaFree(p);
+    }
+  } guard{tmp};
+  const size_t nm = (size_t)scene->n_materials * 4, ne = (size_t)scene->n_emission * 3;
+  uint32_t* dl = nullptr;
+  float *dd = nullptr, *dL = nullptr;
+  double *gm = nullptr, *ge = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dl, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dd, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dL, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &gm, nm));
+  GYT_CK(ctx, dalloc(tmp, &ge, ne));
+  GYT_CK(ctx, cudaMemcpyAsync(dl, xys, 3 * n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(dd, delta, 3 * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(dL, L_total, 3 * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemsetAsync(gm, 0, nm * sizeof(double), ctx->stream));
+  GYT_CK(ctx, cudaMemsetAsync(ge, 0, std::max<size_t>(ne, 1) * sizeof(double), ctx->stream));
+  if (n) {
+    const AdjIn in{nullptr, nullptr, dd, dL};
+    st = run_adjoint(ctx, scene, cam, params, n, dl, in, GradOut{gm, ge}, nullptr);
+    if (st) return st;
+  }
+  GYT_CK(ctx, cudaMemcpyAsync(grad_mat, gm, nm * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ne) GYT_CK(ctx, cudaMemcpyAsync(grad_em, ge, ne * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GYT_OK;
 }
 
@@ -2170,17 +2644,16 @@ cudaError_t enqueue_half(gyt_context* ctx, const BatchPlan& b, const PathBuf& P,
   const Queues q = ctx->q;
   const SobolTables tab = tables(ctx);
   IterState* st = ctx->d_iter;
-  const Inst* I = ctx->d_insts;
   k_batch_begin<<<1, 32, 0, s>>>(st, q.counts);
-  k_generate_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, I, tab);
-  if (b.W == 8) k_extend_batch<8><<<b.ext_grid, kBlock, 0, s>>>(P, st, I, q.hit, q.counts + 2);
-  else k_extend_batch<2><<<b.ext_grid, kBlock, 0, s>>>(P, st, I, q.hit, q.counts + 2);
-  k_shade_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, I, q, tab);
-  if (b.W == 8) k_shadow_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, I, q);
-  else k_shadow_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, I, q);
-  if (b.W == 8) k_mis_batch<8><<<b.mis_grid, kBlock, 0, s>>>(P, I, q);
-  else k_mis_batch<2><<<b.mis_grid, kBlock, 0, s>>>(P, I, q);
-  k_finish_batch<<<b.stride_grid, kBlock, 0, s>>>(P, N, st, I, q.counts + 5);
+  k_generate_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, tab);
+  if (b.W == 8) k_extend_batch<8><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
+  else k_extend_batch<2><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
+  k_shade_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, q, tab);
+  if (b.W == 8) k_shadow_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, q);
+  else k_shadow_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, q);
+  if (b.W == 8) k_mis_batch<8><<<b.mis_grid, kBlock, 0, s>>>(P, q);
+  else k_mis_batch<2><<<b.mis_grid, kBlock, 0, s>>>(P, q);
+  k_finish_batch<<<b.stride_grid, kBlock, 0, s>>>(P, N, st, q.counts + 5);
   k_batch_end<<<1, 32, 0, s>>>(st, q.counts, cond, in_graph);
   return cudaGetLastError();
 }
@@ -2190,8 +2663,7 @@ constexpr uint32_t kKernelsPerHalf = 8;
 // half-iterations (pool 0 -> 1 -> 0); k_batch_end sets the loop condition.
 int32_t ensure_batch_graph(gyt_context* ctx, const BatchPlan& b) {
   const uint64_t key[6] = {(uint64_t)b.W, (uint64_t)b.stride_grid, ((uint64_t)b.ext_grid << 32) | b.sh_grid,
-                           (uint64_t)(uintptr_t)ctx->d_insts, (uint64_t)(uintptr_t)ctx->pool[0].o,
-                           (uint64_t)ctx->pool_cap};
+                           (uint64_t)b.mis_grid, (uint64_t)(uintptr_t)ctx->pool[0].o, (uint64_t)ctx->pool_cap};
   if (ctx->bexec && std::memcmp(key, ctx->bkey, sizeof(key)) == 0) return GYT_OK;
   if (ctx->bexec) cudaGraphExecDestroy(ctx->bexec);
   if (ctx->bgraph) cudaGraphDestroy(ctx->bgraph);
@@ -2265,8 +2737,13 @@ int32_t batch_input(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes
   return GYT_OK;
 }
 
-// Runs a prepared batch: instance table and loop state to the device, then
-// the graph (or the host loop), timed with events on the context stream.
+// Runs a prepared batch: per group of at most kMaxBatch instances, the
+// instance table to constant memory and the loop state to the device, then
+// the graph (or the host loop); timed with events on the context stream. The
+// constant table is shared by every context of the process, so batched
+// renders are serialised.
+std::mutex g_batch_mutex;
+
 int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats) {
   const uint32_t n = (uint32_t)in.insts.size();
   if (stats) *stats = GytRenderStats{};
@@ -2277,60 +2754,63 @@ int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats)
   }
   int32_t st = ensure_pool(ctx);
   if (st) return st;
-  if (n > ctx->insts_cap) {
-    if (ctx->d_insts) cudaFree(ctx->d_insts);
-    ctx->d_insts = nullptr;
-    ctx->insts_cap = 0;
-    const uint32_t cap = std::max<uint32_t>(n, 64);
-    GYT_CK(ctx, cudaMalloc((void**)&ctx->d_insts, cap * sizeof(Inst)));
-    ctx->insts_cap = cap;
-  }
-  cudaStream_t s = ctx->stream;
-  GYT_CK(ctx, after_legacy_stream(ctx));
-  GYT_CK(ctx, cudaMemcpyAsync(ctx->d_insts, in.insts.data(), n * sizeof(Inst), cudaMemcpyHostToDevice, s));
-  IterState is = {};
-  is.total = in.total;
-  is.n_inst = n;
-  is.capacity = ctx->capacity;
-  // a path holds a slot for at most max_depth half-iterations and a full
-  // pool retires at least one slot per half-iteration: generous bound
-  const unsigned long long bound =
-      2ull * (in.total / ctx->capacity + 2) * ((unsigned long long)in.max_depth + 2) + 64;
-  is.max_iter = (uint32_t)std::min<unsigned long long>(bound, 1u << 30);
-  *ctx->h_iter = is;
-  GYT_CK(ctx, cudaMemcpyAsync(ctx->d_iter, ctx->h_iter, sizeof(IterState), cudaMemcpyHostToDevice, s));
   const BatchPlan b = batch_plan(ctx, in.W);
+  std::lock_guard<std::mutex> lock(g_batch_mutex);
   if (ctx->bcfg.use_graph) {
     st = ensure_batch_graph(ctx, b);
     if (st) return st;
   }
+  cudaStream_t s = ctx->stream;
+  GYT_CK(ctx, after_legacy_stream(ctx));
   GYT_CK(ctx, cudaEventRecord(ctx->ev0, s));
-  if (ctx->bcfg.use_graph) {
-    GYT_CK(ctx, cudaGraphLaunch(ctx->bexec, s));
-  } else {
-    for (;;) {
-      GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[0], ctx->pool[1], 0, 0));
-      GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[1], ctx->pool[0], 0, 0));
-      GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
-      GYT_CK(ctx, cudaStreamSynchronize(s));
-      const IterState& h = *ctx->h_iter;
-      if (h.watchdog || !(h.generated < h.total || h.active > 0)) break;
-      if (h.iter >= h.max_iter) break;
+  uint32_t halves = 0;
+  for (uint32_t g0 = 0; g0 < n; g0 += kMaxBatch) {
+    const uint32_t m = std::min(n - g0, kMaxBatch);
+    std::vector<Inst> grp(in.insts.begin() + g0, in.insts.begin() + g0 + m);
+    const unsigned long long base = grp[0].first;
+    const unsigned long long end = g0 + m < n ? in.insts[g0 + m].first : in.total;
+    for (Inst& I : grp) I.first -= base;
+    GYT_CK(ctx, cudaMemcpyToSymbolAsync(c_insts, grp.data(), m * sizeof(Inst), 0, cudaMemcpyHostToDevice, s));
+    IterState is = {};
+    is.total = end - base;
+    is.n_inst = m;
+    is.capacity = ctx->capacity;
+    // a path holds a slot for at most max_depth half-iterations and a full
+    // pool retires at least one slot per half-iteration: generous bound
+    const unsigned long long bound =
+        2ull * (is.total / ctx->capacity + 2) * ((unsigned long long)in.max_depth + 2) + 64;
+    is.max_iter = (uint32_t)std::min<unsigned long long>(bound, 1u << 30);
+    *ctx->h_iter = is;
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->d_iter, ctx->h_iter, sizeof(IterState), cudaMemcpyHostToDevice, s));
+    if (ctx->bcfg.use_graph) {
+      GYT_CK(ctx, cudaGraphLaunch(ctx->bexec, s));
+    } else {
+      for (;;) {
+        GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[0], ctx->pool[1], 0, 0));
+        GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[1], ctx->pool[0], 0, 0));
+        GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+        GYT_CK(ctx, cudaStreamSynchronize(s));
+        const IterState& h = *ctx->h_iter;
+        if (h.watchdog || !(h.generated < h.total || h.active > 0)) break;
+        if (h.iter >= h.max_iter) break;
+      }
     }
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+    GYT_CK(ctx, cudaStreamSynchronize(s));
+    const IterState h = *ctx->h_iter;
+    if (h.watchdog || h.generated < h.total || h.active > 0)
+      return fail(ctx, GYT_ERR_WATCHDOG, "batch: the device loop hit its iteration bound");
+    halves += h.iter;
   }
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
-  GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
-  GYT_CK(ctx, cudaStreamSynchronize(s));
-  const IterState h = *ctx->h_iter;
-  if (h.watchdog || h.generated < h.total || h.active > 0)
-    return fail(ctx, GYT_ERR_WATCHDOG, "batch: the device loop hit its iteration bound");
+  GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     stats->paths = in.total;
     stats->path_slots = 0;
-    stats->iterations = h.iter;
-    stats->launches = h.iter * kKernelsPerHalf;
+    stats->iterations = halves;
+    stats->launches = halves * kKernelsPerHalf;
     stats->ms = ms;
   }
   return GYT_OK;

@@ -163,10 +163,11 @@ class _Builder:
             **kw)
 
 
-def _cornell_walls(b: _Builder, light_radiance=(12.0, 12.0, 12.0), light_half=0.25):
+def _cornell_walls(b: _Builder, light_radiance=(12.0, 12.0, 12.0), light_half=0.25, light=True):
     """The +-1 Cornell box of CornellBoxMesh (Gyunity_exe/CornellBox.h:402-591):
-    left red, right blue, back/floor/ceiling grey 0.75, and a ceiling light quad
-    at y = 0.965 facing -y. Returns nothing; appends 12 triangles."""
+    left red, right blue, back/floor/ceiling grey 0.75, and (``light``) a
+    ceiling light quad at y = 0.965 facing -y. Returns nothing; appends 10
+    wall triangles and 2 light triangles."""
     grey = b.material(*_mat(MAT_DIFFUSE, (0.75, 0.75, 0.75)))
     red = b.material(*_mat(MAT_DIFFUSE, (0.75, 0.25, 0.25)))
     blue = b.material(*_mat(MAT_DIFFUSE, (0.25, 0.25, 0.75)))
@@ -190,6 +191,8 @@ def _cornell_walls(b: _Builder, light_radiance=(12.0, 12.0, 12.0), light_half=0.
         b.i.append(np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]], np.uint32))
         b.tm += [grey, grey]
         b.te += [-1, -1]
+    if not light:
+        return
     h = light_half
     l0, l1, l2, l3 = (h, 0.965, h), (h, 0.965, -h), (-h, 0.965, -h), (-h, 0.965, h)
     base = b.nv
@@ -365,6 +368,94 @@ def mixed_materials_box(level=3, res=64, spp=4, max_depth=8, rr_depth=3, seed=11
     return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
                    spheres=np.array([[-0.55, -0.7, -0.4, 0.25], [0.55, -0.7, 0.4, 0.25]], np.float32),
                    sphere_material=np.array([mirror, glass], np.uint32), name="mixed_materials_box")
+
+
+# ------------------------------------------------ differentiable rendering ---
+
+@dataclasses.dataclass
+class InverseParams:
+    """The optimised parameters of inverse_box: per material group albedo
+    (g, 3) and GGX alpha (g,), per emitter radiance (e, 3)."""
+    albedo: np.ndarray
+    alpha: np.ndarray
+    radiance: np.ndarray
+
+    def flat(self) -> np.ndarray:
+        return np.concatenate([self.albedo.ravel(), self.alpha.ravel(), self.radiance.ravel()]).astype(np.float64)
+
+    @property
+    def count(self) -> int:
+        return self.albedo.size + self.alpha.size + self.radiance.size
+
+
+def inverse_params(groups=256, emitters=4, seed=7) -> InverseParams:
+    """Hidden parameters (seeded): albedo ~ U(0.2, 0.9) per channel, alpha ~
+    U(0.05, 0.5), emitter radiance 4 * U(0.75, 1.25) per channel."""
+    rng = np.random.default_rng(seed)
+    return InverseParams(rng.uniform(0.2, 0.9, (groups, 3)), rng.uniform(0.05, 0.5, groups),
+                         4.0 * rng.uniform(0.75, 1.25, (emitters, 3)))
+
+
+def perturb_params(p: InverseParams, seed=8, spread=0.3) -> InverseParams:
+    """Initial parameters: every value times U(1 - spread, 1 + spread)."""
+    rng = np.random.default_rng(seed)
+    return InverseParams(p.albedo * rng.uniform(1 - spread, 1 + spread, p.albedo.shape),
+                         p.alpha * rng.uniform(1 - spread, 1 + spread, p.alpha.shape),
+                         p.radiance * rng.uniform(1 - spread, 1 + spread, p.radiance.shape))
+
+
+def inverse_box(params: InverseParams = None, level=5, res=512, spp=32, max_depth=8, rr_depth=8,
+                emitter_half=0.15) -> SceneDesc:
+    """Inverse-rendering scene: the Cornell walls (no central light), a level-
+    ``level`` icosphere (20 * 4**level faces; level 5 = 20,480) of radius 0.45
+    at (0, -0.4, 0) split into len(params.alpha) contiguous face groups, each a
+    GGX conductor (eta = k = 1.5) with its own albedo and alpha, and one
+    emitter quad per radiance row near each ceiling corner (both triangles of
+    a quad share one emission row). Roulette starts at rr_depth (>= max_depth:
+    none), so the estimator is smooth in the parameters."""
+    params = params or inverse_params()
+    groups = params.alpha.shape[0]
+    b = _Builder()
+    _cornell_walls(b, light=False)
+    v, n, f = displaced_icosphere(level, 0.45, (0.0, -0.4, 0.0), 5, amplitude=0.03)
+    first = len(b.mt)
+    for g in range(groups):
+        a = float(params.alpha[g])
+        b.material(*_mat(MAT_CONDUCTOR, tuple(float(x) for x in params.albedo[g]), ax=a, ay=a))
+    per = f.shape[0] // groups
+    grp = np.minimum(np.arange(f.shape[0]) // per, groups - 1)
+    b.tris(v, n, f, (first + grp).astype(np.uint32))
+    black = b.material(*_mat(MAT_DIFFUSE, (0.0, 0.0, 0.0)))
+    h = emitter_half
+    y = 0.965
+    corners = [(-0.6, -0.6), (0.6, -0.6), (0.6, 0.6), (-0.6, 0.6)]
+    for k, (cx, cz) in enumerate(corners[:params.radiance.shape[0]]):
+        q = [(cx + h, y, cz + h), (cx + h, y, cz - h), (cx - h, y, cz - h), (cx - h, y, cz + h)]
+        base = b.nv
+        b.v.append(np.array(q, np.float32))
+        b.n.append(np.array([(0, -1, 0)] * 4, np.float32))
+        b.nv += 4
+        b.i.append(np.array([[base, base + 1, base + 2], [base, base + 2, base + 3]], np.uint32))
+        b.tm += [black, black]
+        row = len(b.em)
+        b.em.append(tuple(float(x) for x in params.radiance[k]))
+        b.te += [row, row]
+    sd = b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
+                 name="inverse_box_L%d_%dgroups_%dx%d_%dspp" % (level, groups, res, res, spp))
+    sd.param_materials = np.arange(first, first + groups, dtype=np.int64)
+    return sd
+
+
+def apply_inverse_params(sd: SceneDesc, p: InverseParams):
+    """Material parameters (n_materials, 16) and emission (n_emission, 3) of
+    inverse_box's scene with the given optimised parameters."""
+    mp = sd.mat_params.copy()
+    m = sd.param_materials
+    mp[m, 0:3] = p.albedo
+    mp[m, 6] = p.alpha
+    mp[m, 7] = p.alpha
+    em = p.radiance.astype(np.float32).copy()
+    return np.ascontiguousarray(mp, np.float32), np.ascontiguousarray(em, np.float32)
 
 
 # ------------------------------------------------- batched uneven workload ---

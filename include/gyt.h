@@ -131,7 +131,8 @@ int32_t gyt_context_set_bvh_width(gyt_context* ctx, int32_t width);
 /* Where later gyt_scene_create calls build a binary (width 2) BVH:
  * GYT_BVH_BUILD_DEVICE (the default) or GYT_BVH_BUILD_HOST. Both make the
  * same tree: 16-bin SAH, at most 8 triangles per leaf, identical splits,
- * leaves and child boxes (node numbering and the order inside a leaf differ).
+ * leaves and child boxes, each leaf's triangles in ascending id order (only
+ * the node numbering differs).
  * The 8-wide BVH is always built on the host. Replaces the BVHAccel
  * constructor's build (accelerator/BVHAccel.cpp:154-200). */
 #define GYT_BVH_BUILD_HOST 0
@@ -194,6 +195,47 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 /* SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for n (s, x, y) triplets. */
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
+
+/* ---- Differentiable rendering (path replay backpropagation) ---------------
+ * Gradients of an image loss with respect to every material's albedo a
+ * (mat_params[0..2]) and GGX roughness alpha (mat_params[6] = [7]) and every
+ * emission row's radiance. The adjoint pass replays the primal's paths from
+ * their Sobol' indices (nothing per vertex is stored; the primal keeps one
+ * radiance value per path) with detached sampling: pdfs, MIS weights, light
+ * selection and roulette are constants of the derivative. Albedo gradients
+ * cover the diffuse and GGX-conductor lobes, alpha gradients the GGX lobe;
+ * other lobes pass radiance through without parameter gradients. Gradient
+ * sums are FP64. No counterpart in the reference (it has no derivatives). */
+
+/* Replaces the scene's material parameters (n_materials x 16 floats, the
+ * GytSceneDesc.mat_params layout; NULL keeps them) and emission rows
+ * (n_emission x 3; NULL keeps them). The light-selection distribution is
+ * rebuilt from the new powers unless flags holds GYT_KEEP_LIGHT_SAMPLING
+ * (sampling then stays that of the previous emission: the estimator remains
+ * unbiased and becomes linear in the emission, as a detached-sampling
+ * derivative assumes). Material types and geometry are unchanged. */
+#define GYT_KEEP_LIGHT_SAMPLING 1u
+int32_t gyt_scene_set_materials(gyt_scene* scene, const float* mat_params, const float* emission, uint32_t flags);
+/* Primal render for differentiation: gyt_render_device into d_film plus the
+ * radiance of every path (d_path_L: device, res_x*res_y*spp*3 floats,
+ * indexed by path id = pixel * spp + sample). */
+int32_t gyt_diff_forward(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                         const GytRenderParams* params, double* d_film, float* d_path_L, GytRenderStats* stats);
+/* Adjoint of the image (colour / weight per pixel, as gyt_render returns it):
+ * d_image_grad = dLoss/dImage (device, res_x*res_y*3 floats), d_film and
+ * d_path_L from gyt_diff_forward with the same parameters. Adds dLoss/dparam
+ * into d_grad_mat (device, n_materials*4 doubles: a.r, a.g, a.b, alpha) and
+ * d_grad_em (device, n_emission*3 doubles). */
+int32_t gyt_diff_backward(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, const float* d_image_grad, const double* d_film,
+                          const float* d_path_L, double* d_grad_mat, double* d_grad_em, GytRenderStats* stats);
+/* The adjoint of an explicit path list (host arrays): n (x, y, s) samples
+ * with their adjoint weights delta (n*3: dLoss/d(path radiance)) and primal
+ * radiance L_total (n*3, from gyt_trace_paths); grad_mat and grad_em (host)
+ * receive the gradient sums. For parity tests against an FP64 adjoint. */
+int32_t gyt_diff_backward_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                const GytRenderParams* params, uint64_t n, const uint32_t* xys, const float* delta,
+                                const float* L_total, double* grad_mat, double* grad_em);
 
 /* ---- Batched renders ------------------------------------------------------
  * Many scenes and cameras of uneven sizes, resolutions and sample counts in

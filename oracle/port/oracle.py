@@ -75,6 +75,15 @@ def lib():
         L.gyo_render.argtypes = [ctypes.c_void_p, ctypes.POINTER(CameraIn), ctypes.POINTER(ParamsIn),
                                  ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
         L.gyo_bsdf.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+        L.gyo_adjoint.argtypes = [ctypes.c_void_p, ctypes.POINTER(CameraIn), ctypes.POINTER(ParamsIn), ctypes.c_int64,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.gyo_set_sampling_materials.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.gyo_ggx_dlog_alpha.restype = ctypes.c_double
+        L.gyo_ggx_dlog_alpha.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+        L.gyo_ggx_log_f.restype = ctypes.c_double
+        L.gyo_ggx_log_f.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -167,6 +176,33 @@ class OracleScene:
             return L, cur, rr, occ, mis
         return (L, cur, rr) if return_rr else (L, cur)
 
+    def adjoint(self, x, y, s, delta, precision=64, threads=0, camera=None, params=None, force_rr=None,
+                force_occ=None, force_mis=None):
+        """Path replay adjoint of paths (x, y, s) with adjoint weights delta
+        (n, 3), replaying the given decisions. Returns the gradient sums per
+        material (n_materials, 4: a.r, a.g, a.b, alpha) and per emission row
+        (n_emission, 3), and the path radiance (n, 3)."""
+        x, y, s = (np.ascontiguousarray(np.asarray(a, np.uint32)) for a in (x, y, s))
+        n = x.shape[0]
+        d = np.ascontiguousarray(delta, np.float32).reshape(n, 3)
+        nm, ne = int(self.sd.mat_type.shape[0]), int(self.sd.emission.shape[0])
+        gm = np.zeros((nm, 4), np.float64)
+        ge = np.zeros((max(ne, 1), 3), np.float64)
+        L = np.empty((n, 3), np.float64)
+        f = [None if a is None else np.ascontiguousarray(np.asarray(a, np.uint64)) for a in (force_rr, force_occ,
+                                                                                           force_mis)]
+        c = camera_in(camera or self.sd.camera)
+        p = params_in(params or self.sd.params)
+        lib().gyo_adjoint(self.handle, ctypes.byref(c), ctypes.byref(p), n, _p(x), _p(y), _p(s), precision, _p(d),
+                          threads, _p(f[0]), _p(f[1]), _p(f[2]), nm, ne, _p(gm), _p(ge), _p(L))
+        return gm, ge[:ne], L
+
+    def set_sampling_materials(self, mat_params=None):
+        """Test hook: sample BSDFs (and their pdfs) with these parameters
+        while evaluating them with the scene's (None restores the scene's)."""
+        self._smp = None if mat_params is None else np.ascontiguousarray(mat_params, np.float32)
+        lib().gyo_set_sampling_materials(self.handle, _p(self._smp))
+
     def render(self, rows=None, precision=64, threads=0, camera=None, params=None):
         cam = camera or self.sd.camera
         c = camera_in(cam)
@@ -175,6 +211,18 @@ class OracleScene:
         r0, r1 = (0, cam.res_y) if rows is None else rows
         lib().gyo_render(self.handle, ctypes.byref(c), ctypes.byref(p), r0, r1, precision, _p(film), threads)
         return film
+
+
+def ggx_dlog_alpha(alpha, wo, wi):
+    """d log f / d alpha of the GGX reflection lobe (local directions)."""
+    a, b = np.ascontiguousarray(wo, np.float64), np.ascontiguousarray(wi, np.float64)
+    return lib().gyo_ggx_dlog_alpha(float(alpha), _p(a), _p(b))
+
+
+def ggx_log_f(alpha, wo, wi):
+    """log of the GGX reflection lobe's value (eta = k = 1.5, a = 1)."""
+    a, b = np.ascontiguousarray(wo, np.float64), np.ascontiguousarray(wi, np.float64)
+    return lib().gyo_ggx_log_f(float(alpha), _p(a), _p(b))
 
 
 def sobol(dims, indices):

@@ -302,8 +302,12 @@ template <typename T> struct Scene {
   std::vector<Tri<T>> tris;
   std::vector<Sph<T>> sph;
   std::vector<Material> mats;
+  // test hook: when not empty, BSDF sampling and pdfs use these materials
+  // while BSDF values use mats (sampling held fixed under a parameter change)
+  std::vector<Material> smats;
   std::vector<V3<T>> emission;     // per light (area lights only)
   std::vector<int> light_tri;      // light index -> triangle, -1 = environment
+  std::vector<int> light_row;      // light index -> emission row, -1 = environment
   Dist1D<T> light_power;
   bool has_env = false;
   Env<T> env;
@@ -916,10 +920,12 @@ template <typename T> Lobe<T> make_lobe(const Material& m) {
 // BSDF wrapper (bsdf/BSDF.cpp:58-119) for one lobe in the shading frame.
 template <typename T> struct Bsdf {
   Lobe<T> lobe;
+  Lobe<T> slobe;       // sampling lobe (the same as lobe unless the scene's smats are set)
+  bool split = false;
   V3<T> su, sv, n, gn;
   V3<T> to_local(const V3<T>& v) const { return V3<T>(dot(v, su), dot(v, sv), dot(v, n)); }
   V3<T> to_world(const V3<T>& v) const { return su * v.x + sv * v.y + n * v.z; }
-  T pdf(const V3<T>& wo, const V3<T>& wi) const { return lobe.pdf(to_local(wo), to_local(wi)); }
+  T pdf(const V3<T>& wo, const V3<T>& wi) const { return slobe.pdf(to_local(wo), to_local(wi)); }
   V3<T> eval(const V3<T>& wo, const V3<T>& wi) const {
     bool refl = dot(wi, gn) * dot(wo, gn) > 0;
     int f = lobe.flags();
@@ -928,7 +934,8 @@ template <typename T> struct Bsdf {
   }
   V3<T> sample(const V3<T>& wo, V3<T>* wi, T* pdf, T u0, T u1, T u2) const {
     V3<T> wl;
-    V3<T> f = lobe.sample(to_local(wo), &wl, pdf, u0, u1, u2);
+    V3<T> f = slobe.sample(to_local(wo), &wl, pdf, u0, u1, u2);
+    if (split && slobe.type == 3 && !f.zero()) f = lobe.eval(to_local(wo), wl);
     *wi = to_world(wl);
     return f;
   }
@@ -937,11 +944,76 @@ template <typename T> struct Bsdf {
 template <typename T> Bsdf<T> make_bsdf(const Scene<T>& sc, const Isect<T>& is, uint32_t mat) {
   Bsdf<T> b;
   b.lobe = make_lobe<T>(sc.mats[mat]);
+  b.split = !sc.smats.empty();
+  b.slobe = b.split ? make_lobe<T>(sc.smats[mat]) : b.lobe;
   b.su = is.su; b.sv = is.sv; b.n = is.n; b.gn = is.geo_n;
   return b;
 }
 
 template <typename T> T power_heuristic(T f, T g) { return (f * f) / (f * f + g * g); }  // Integrator.h:11-15
+
+// d log f / d alpha of the GGX reflection lobe for ax = ay = alpha at local
+// directions: D = 1 / (pi a^2 (c^2 + s^2/a^2)^2) and the Smith terms
+// G1 = 2 / (1 + sqrt(1 + a^2 tan^2)) are the factors that depend on alpha.
+template <typename T> T ggx_dlog_alpha(const GGX<T>& g, const V3<T>& wo, const V3<T>& wi) {
+  V3<T> wh = wi + wo;
+  if (wh.zero()) return 0;
+  wh = norm(wh);
+  wh = wh * sgn(wh.z);
+  const T a = g.ax;
+  const T c2 = wh.z * wh.z, s2 = wh.x * wh.x + wh.y * wh.y;
+  T d = -2 / a + 4 * s2 / (a * (a * a * c2 + s2));
+  const V3<T> vs[2] = {wo, wi};
+  for (const V3<T>& v : vs) {
+    const T tanT = std::abs(std::sqrt(std::max((T)0, 1 - v.z * v.z)) / v.z);
+    if (tanT > 0 && std::isfinite(tanT)) {
+      const T r = a * tanT, S = std::sqrt(1 + r * r);
+      d -= a * tanT * tanT / (S * (1 + S));
+    }
+  }
+  return std::isfinite(d) ? d : 0;
+}
+template <typename T> T lobe_dlog_alpha(const Lobe<T>& l, const V3<T>& wo, const V3<T>& wi) {
+  return l.type == 3 ? ggx_dlog_alpha(l.g, wo, wi) : (T)0;
+}
+
+// Path replay adjoint of one path (detached sampling: pdfs, MIS weights, light
+// selection and roulette are constants). Every radiance contribution C moves
+// gradient to each BSDF factor it contains: the continuation factors of the
+// earlier vertices, the own factor of a light or MIS sample, and the emitter.
+// f is linear in the albedo a of the diffuse and GGX lobes (dC/da_c = C_c/a_c)
+// and d log f / d alpha is the GGX term above.
+template <typename T> struct AdjAcc {
+  V3<T> delta;
+  std::vector<std::pair<uint32_t, T>> conts;
+  const Scene<T>* sc = nullptr;
+  double* gm = nullptr;  // per material: a.r, a.g, a.b, alpha
+  double* ge = nullptr;  // per emission row: r, g, b
+  void mat(uint32_t m, T da, const V3<T>& Cd) const {
+    const Material& mt = sc->mats[m];
+    if (mt.type != 0 && mt.type != 3) return;
+    for (int c = 0; c < 3; ++c)
+      if (mt.p[c] != 0.f) gm[4 * m + c] += (double)Cd[c] / (double)mt.p[c];
+    gm[4 * m + 3] += ((double)Cd.x + (double)Cd.y + (double)Cd.z) * (double)da;
+  }
+  void add(const V3<T>& C, int own_m, T own_da, int row, const V3<T>& Le) const {
+    const V3<T> Cd = delta * C;
+    for (const auto& k : conts) mat(k.first, k.second, Cd);
+    if (own_m >= 0) mat((uint32_t)own_m, own_da, Cd);
+    if (row >= 0)
+      for (int c = 0; c < 3; ++c)
+        if (Le[c] != 0) ge[3 * row + c] += (double)Cd[c] / (double)Le[c];
+  }
+};
+
+// The two halves of DirectIllumination for the adjoint.
+template <typename T> struct DirectParts {
+  bool has1 = false, has2 = false;
+  V3<T> C1, C2;  // (L1 w1 + L2 w2) / lightSel split into its halves
+  T da1 = 0, da2 = 0;
+  int row = -1;
+  V3<T> Le;
+};
 
 template <typename T> uint32_t prim_material(const Scene<T>& sc, int prim) {
   return prim < (int)sc.tris.size() ? sc.tris[prim].mat : sc.sph[prim - sc.tris.size()].mat;
@@ -981,11 +1053,12 @@ struct Replay {
 
 // Integrator::DirectIllumination (integrator/Integrator.cpp:9-107), surfaces only
 template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const Bsdf<T>& bsdf, T uLight,
-                                   T u0, T u1, T v0, T v1, T v2, Replay* rp) {
+                                   T u0, T u1, T v0, T v1, T v2, Replay* rp, DirectParts<T>* parts = nullptr) {
   T lightSel;
   int li = sc.light_power.sample_discrete(uLight, &lightSel);
   if (lightSel == 0) return V3<T>();
   int ltri = sc.light_tri[li];
+  V3<T> wi1, wi2;
   T w1 = 1, w2 = 1;
   V3<T> L1, L2;
   {
@@ -1035,6 +1108,7 @@ template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const
         }
         w1 = power_heuristic(pdf, spdf);
         L1 = Li * f * cosT / pdf;
+        wi1 = wi;
       }
     }
   }
@@ -1043,6 +1117,7 @@ template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const
     T pdf;
     V3<T> f = bsdf.sample(is.wo, &wi, &pdf, v0, v1, v2);
     T cosT = std::abs(dot(is.n, wi));
+    wi2 = wi;
     if (pdf != 0 && !f.zero()) {
       T lpdf = ltri >= 0 ? tri_light_pdf(sc.tris[ltri], is, wi) : sc.env.pdf_dir(wi);
       if (lpdf == 0) {
@@ -1086,6 +1161,16 @@ template <typename T> V3<T> direct(const Scene<T>& sc, const Isect<T>& is, const
   if (g_trace)
     std::fprintf(stderr, "    light %d sel %.9g L1 %.9g w1 %.9g L2 %.9g w2 %.9g\n", li, (double)lightSel, (double)L1.x,
                  (double)w1, (double)L2.x, (double)w2);
+  if (parts) {
+    parts->row = sc.light_row[li];
+    parts->Le = sc.emission[li];
+    parts->has1 = !L1.zero();
+    parts->has2 = !L2.zero();
+    parts->C1 = L1 * w1 / lightSel;
+    parts->C2 = L2 * w2 / lightSel;
+    parts->da1 = lobe_dlog_alpha(bsdf.lobe, bsdf.to_local(is.wo), bsdf.to_local(wi1));
+    parts->da2 = lobe_dlog_alpha(bsdf.lobe, bsdf.to_local(is.wo), bsdf.to_local(wi2));
+  }
   return (L1 * w1 + L2 * w2) / lightSel;
 }
 
@@ -1110,7 +1195,7 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
                                        const ParamsIn& pr, uint32_t x, uint32_t y, uint32_t s, int* cursor_out,
                                        float* u_out = nullptr, float* v_out = nullptr,
                                        const uint64_t* force_rr = nullptr, uint64_t* rr_out = nullptr,
-                                       Replay* rp_in = nullptr) {
+                                       Replay* rp_in = nullptr, AdjAcc<T>* adj = nullptr) {
   Replay rp_local;
   Replay* rp = rp_in ? rp_in : &rp_local;
   uint32_t m = log2_pow2_res(ci.res_x, ci.res_y);
@@ -1128,7 +1213,10 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
     Isect<T> is;
     int prim = closest_hit(sc, ray, &is);
     if (prim < 0) {
-      if ((i == 0 || delta) && sc.has_env) L = L + tp * sc.env.lookup(ray.d);
+      if ((i == 0 || delta) && sc.has_env) {
+        L = L + tp * sc.env.lookup(ray.d);
+        if (adj) adj->add(tp * sc.env.lookup(ray.d), -1, 0, -1, V3<T>());
+      }
       break;
     }
     complete_hit(sc, ray, &is);
@@ -1137,13 +1225,20 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
     if ((i == 0 || delta) && pl >= 0) {
       V3<T> e = dot(is.n, is.wo) > 0 ? sc.emission[pl] : V3<T>();  // AreaLight::Emission (AreaLight.h:40-43)
       L = L + tp * e;
+      if (adj && !e.zero()) adj->add(tp * e, -1, 0, sc.light_row[pl], sc.emission[pl]);
     } else {
       // argument evaluation order of PT.cpp:38 as compiled by GCC: v.z, v.y, v.x, u.y, u.x, uLight
       T vz = rnd.next(), vy = rnd.next(), vx = rnd.next();
       T uy = rnd.next(), ux = rnd.next();
       T ul = rnd.next();
       rp->bounce = i;
-      V3<T> di = direct(sc, is, bsdf, ul, ux, uy, vx, vy, vz, rp);
+      DirectParts<T> parts;
+      V3<T> di = direct(sc, is, bsdf, ul, ux, uy, vx, vy, vz, rp, adj ? &parts : nullptr);
+      if (adj) {
+        const int m = (int)prim_material(sc, prim);
+        if (parts.has1) adj->add(tp * parts.C1, m, parts.da1, parts.row, parts.Le);
+        if (parts.has2) adj->add(tp * parts.C2, m, parts.da2, parts.row, parts.Le);
+      }
       if (g_trace)
         std::fprintf(stderr, "  bounce %d prim %d pos (%.9g %.9g %.9g) DI (%.9g %.9g %.9g) tp %.9g\n", i, prim,
                      (double)is.pos.x, (double)is.pos.y, (double)is.pos.z, (double)di.x, (double)di.y, (double)di.z,
@@ -1170,6 +1265,8 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
     }
     tp = tp * est;
     ray = spawn_ray(is, wi);
+    if (adj)
+      adj->conts.push_back({prim_material(sc, prim), lobe_dlog_alpha(bsdf.lobe, bsdf.to_local(is.wo), bsdf.to_local(wi))});
   }
   if (cursor_out) *cursor_out = rnd.cursor;
   if (rr_out) *rr_out = rr_mask;
@@ -1272,6 +1369,7 @@ template <typename T> Scene<T>* make_scene(const SceneIn& in) {
     if (in.tri_emission[t] >= 0) {
       tr.light = (int)sc->light_tri.size();
       sc->light_tri.push_back((int)t);
+      sc->light_row.push_back(in.tri_emission[t]);
       V3<T> e = v3f<T>(&in.emission[3 * in.tri_emission[t]]);
       sc->emission.push_back(e);
       T area = (T)0.5 * length(cross(tr.p1 - tr.p0, tr.p2 - tr.p0));
@@ -1297,6 +1395,7 @@ template <typename T> Scene<T>* make_scene(const SceneIn& in) {
     V3<T> d((T)(bhi[0] - blo[0]), (T)(bhi[1] - blo[1]), (T)(bhi[2] - blo[2]));
     sc->env.radius = length(d) * (T)0.5;
     sc->light_tri.push_back(-1);
+    sc->light_row.push_back(-1);
     sc->emission.push_back(V3<T>());
     // EnvironmentLight::Power (EnvLight.cpp:59-62)
     power.push_back(lum(sc->env.lookup_radiance((T)0.5, (T)0.5) * K<T>::PI * sc->env.radius * sc->env.radius));
@@ -1499,6 +1598,94 @@ int gyo_paths(void* p, const CameraIn* c, const ParamsIn* pr, int64_t n, const u
     paths_impl<float>(h, c, pr, n, x, y, s, L, cursor, threads, force_rr, rr_out, force_occ, force_mis, occ_out,
                       mis_out);
   return 0;
+}
+
+// Path replay adjoint of n explicit paths with adjoint weights delta (n*3),
+// replaying the given decisions (any may be null): gradient sums into
+// grad_mat (n_materials*4: a.rgb, alpha) and grad_em (n_emission*3), path
+// radiance into L (n*3). Chunks of 256 paths accumulate separately and are
+// summed in chunk order, so the result does not depend on the thread count.
+int gyo_adjoint(void* p, const CameraIn* c, const ParamsIn* pr, int64_t n, const uint32_t* x, const uint32_t* y,
+                const uint32_t* s, int precision, const float* delta, int threads, const uint64_t* force_rr,
+                const uint64_t* force_occ, const uint64_t* force_mis, uint32_t n_materials, uint32_t n_emission,
+                double* grad_mat, double* grad_em, double* L) {
+  auto* h = (Handle*)p;
+  const int chunks = (int)((n + 255) / 256);
+  std::vector<double> gm((size_t)chunks * n_materials * 4, 0.0), ge((size_t)chunks * n_emission * 3, 0.0);
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    Scene<T>* sc = get<T>(h);
+    CamT<T> cam = make_cam<T>(*c);
+    parallel_rows(chunks, threads, [&](int ch) {
+      for (int64_t i = (int64_t)ch * 256; i < std::min<int64_t>(n, (int64_t)ch * 256 + 256); ++i) {
+        int cur = 0;
+        Replay rp;
+        rp.force_occ = force_occ ? &force_occ[i] : nullptr;
+        rp.force_mis = force_mis ? &force_mis[i] : nullptr;
+        AdjAcc<T> adj;
+        adj.delta = V3<T>((T)delta[3 * i], (T)delta[3 * i + 1], (T)delta[3 * i + 2]);
+        adj.sc = sc;
+        adj.gm = &gm[(size_t)ch * n_materials * 4];
+        adj.ge = n_emission ? &ge[(size_t)ch * n_emission * 3] : nullptr;
+        V3<T> l = trace_path(*sc, cam, *c, *pr, x[i], y[i], s[i], &cur, nullptr, nullptr,
+                             force_rr ? &force_rr[i] : nullptr, nullptr, &rp, &adj);
+        if (L) { L[3 * i] = (double)l.x; L[3 * i + 1] = (double)l.y; L[3 * i + 2] = (double)l.z; }
+      }
+    });
+  };
+  if (precision == 64) run(double());
+  else run(float());
+  for (size_t k = 0; k < (size_t)n_materials * 4; ++k) {
+    double v = 0;
+    for (int ch = 0; ch < chunks; ++ch) v += gm[(size_t)ch * n_materials * 4 + k];
+    grad_mat[k] = v;
+  }
+  for (size_t k = 0; k < (size_t)n_emission * 3; ++k) {
+    double v = 0;
+    for (int ch = 0; ch < chunks; ++ch) v += ge[(size_t)ch * n_emission * 3 + k];
+    grad_em[k] = v;
+  }
+  return 0;
+}
+
+// Test hook: BSDF sampling and pdfs from these material parameters (n*16,
+// the scene's material count) while BSDF values keep the scene's; null
+// restores the scene's own. A finite difference in a BSDF parameter with the
+// sampling held fixed is the derivative that path replay computes.
+int gyo_set_sampling_materials(void* p, const float* mat_params) {
+  auto* h = (Handle*)p;
+  auto set = [&](auto* sc) {
+    if (!sc) return;
+    sc->smats.clear();
+    if (!mat_params) return;
+    sc->smats = sc->mats;
+    for (size_t m = 0; m < sc->smats.size(); ++m) std::memcpy(sc->smats[m].p, &mat_params[m * 16], 16 * sizeof(float));
+  };
+  set(h->sf);
+  set(h->sd);
+  return 0;
+}
+
+// d log f / d alpha of the GGX lobe (alpha, local wo, wi), for a CPU check of
+// the derivative against finite differences of the lobe's value.
+double gyo_ggx_dlog_alpha(double alpha, const double* wo, const double* wi) {
+  GGX<double> g{alpha, alpha};
+  return ggx_dlog_alpha(g, V3<double>(wo[0], wo[1], wo[2]), V3<double>(wi[0], wi[1], wi[2]));
+}
+
+// log of the GGX lobe's value f (first channel) for alpha at local wo, wi
+// (eta = k = 1.5, a = 1), the function whose derivative the above is.
+double gyo_ggx_log_f(double alpha, const double* wo, const double* wi) {
+  Material m;
+  m.type = 3;
+  std::memset(m.p, 0, sizeof(m.p));
+  m.p[0] = m.p[1] = m.p[2] = 1.f;
+  Lobe<double> l = make_lobe<double>(m);
+  l.g = GGX<double>{alpha, alpha};
+  l.ceta = V3<double>(1.5, 1.5, 1.5);
+  l.ck = V3<double>(1.5, 1.5, 1.5);
+  V3<double> f = l.eval(V3<double>(wo[0], wo[1], wo[2]), V3<double>(wi[0], wi[1], wi[2]));
+  return std::log(f.x);
 }
 
 // Accumulates rows [row0, row1) of the image into film (res_x*res_y*4 doubles:

@@ -144,3 +144,12 @@ def test_batch_autotune(bctx, scs):
     got, _ = _batch(bctx, scs, DESCS)
     bctx.set_batch_config()
     _same(got, _per_scene(bctx, scs, DESCS))
+
+
+def test_batch_more_instances_than_one_group(bctx):
+    # more instances than the constant-memory table holds: consecutive groups
+    descs = [scenes.cornell_box(res=8, spp=1 + k % 3, max_depth=3, spheres=bool(k % 2)) for k in range(150)]
+    scs = [g.Scene(sd, bctx) for sd in descs]
+    got, st = _batch(bctx, scs, descs)
+    _same(got, _per_scene(bctx, scs, descs))
+    assert st["paths"] == sum(sd.n_paths() for sd in descs)

@@ -211,3 +211,22 @@ def test_edge_sizes(ctx):
     assert np.allclose(L, Lo, rtol=1e-4, atol=1e-6) and cur[0] == co[0]
     empty_L, _, _ = sc.trace_paths(np.zeros((0, 3), np.uint32))
     assert empty_L.shape == (0, 3)
+
+
+def test_rays_exactly_through_a_shared_edge_hit(ctx):
+    # from (0, 0, 3) the plane x = y holds the diagonal shared by the back
+    # wall's two triangles: every such ray meets the wall exactly on that
+    # edge, and a watertight test must report one of the two triangles
+    sd = scenes.cornell_box(res=32, spp=1, spheres=False)
+    sc = g.Scene(sd, ctx)
+    a = np.linspace(-0.22, 0.22, 401)
+    d = np.stack([a, a, -np.ones_like(a)], 1)
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    assert np.all(d[:, 0] == d[:, 1])
+    o = np.tile(np.array([0.0, 0.0, 3.0], np.float32), (a.shape[0], 1))
+    rays = np.concatenate([o, d, np.full((a.shape[0], 1), np.inf, np.float32)], 1)
+    prim, t, _, _ = sc.intersect(rays)
+    assert np.all(prim >= 0), int((prim < 0).sum())
+    oprim, ot, _, _ = orc.OracleScene(sd).closest_hit(rays, precision=32)
+    assert np.all(oprim >= 0)
+    np.testing.assert_allclose(t, ot, rtol=1e-6)
