@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gyunity", choices=["gyunity", "reference"])
+    ap.add_argument("--workload", default="mesh", choices=["mesh", "env", "cornell"],
+                    help="mesh: procedural mesh (default); env: environment-lit rough-glass torus knot "
+                         "(4M triangles, 1920x1080, 256 spp, depth 32); cornell: the Cornell box (256x256, 16 spp)")
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = 1.31M triangles)")
     ap.add_argument("--res", type=int, default=1024)
     ap.add_argument("--spp", type=int, default=64)
@@ -58,14 +61,27 @@ def parse():
 
 def workload(a):
     from gyunity_b200 import scenes
+    if a.workload == "env":
+        return scenes.env_torus_knot()
+    if a.workload == "cornell":
+        return scenes.cornell_box(res=256, spp=16, max_depth=8, rr_depth=3)
     return scenes.procedural_mesh_box(level=a.level, res=a.res, spp=a.spp, max_depth=a.depth)
 
 
 def config(a, sd, extra=None):
-    c = {"workload": "procedural_mesh_cornell", "triangles": int(sd.n_triangles), "material": "GGX conductor",
-         "groups": 64, "resolution": "%dx%d" % (a.res, a.res), "spp": a.spp, "max_depth": a.depth,
-         "rr_depth": sd.params.rr_depth, "sampler": "Sobol", "paths_per_step": int(sd.n_paths()),
-         "l2": "inputs larger than L2 (BVH + triangles exceed 126 MB); no flush"}
+    cam, prm = sd.camera, sd.params
+    if a.workload == "env":
+        c = {"workload": "env_lit_rough_glass_torus_knot", "material": "GGX rough dielectric alpha 0.1 IOR 1.5",
+             "env_map": "2048x1024 synthetic sky, RGBE-rounded", "l2": "inputs larger than L2; no flush"}
+    elif a.workload == "cornell":
+        c = {"workload": "cornell_box_spheres", "material": "diffuse walls, mirror and glass spheres",
+             "l2": "scene fits in L2 (the configuration's own size)"}
+    else:
+        c = {"workload": "procedural_mesh_cornell", "material": "GGX conductor", "groups": 64,
+             "l2": "inputs larger than L2 (BVH + triangles exceed 126 MB); no flush"}
+    c.update({"triangles": int(sd.n_triangles), "resolution": "%dx%d" % (cam.res_x, cam.res_y), "spp": prm.spp,
+              "max_depth": prm.max_depth, "rr_depth": prm.rr_depth, "sampler": "Sobol",
+              "paths_per_step": int(sd.n_paths())})
     if extra:
         c.update(extra)
     return c

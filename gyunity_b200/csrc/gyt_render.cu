@@ -1183,13 +1183,15 @@ __global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const Iter
       nullptr);
 }
 
+// One path per thread over a grid sized for the whole pool (threads past
+// the live count return at once): the work per path varies a lot, and the
+// block scheduler balances it far better than a grid-stride loop does.
 __global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q,
                                                         SobolTables tab) {
-  const uint32_t n = st->n;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const Inst& I = c_insts[cur.inst[i]];
-    shade_path<false>(cur, i, I.s, I.prm, q, tab, DebugOut{});
-  }
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= st->n) return;
+  const Inst& I = c_insts[cur.inst[i]];
+  shade_path<false>(cur, i, I.s, I.prm, q, tab, DebugOut{});
 }
 
 template <int W>
@@ -2617,7 +2619,7 @@ namespace {
 
 struct BatchPlan {
   int W = 2;
-  uint32_t stride_grid = 0, ext_grid = 0, sh_grid = 0, mis_grid = 0;
+  uint32_t stride_grid = 0, ext_grid = 0, sh_grid = 0, mis_grid = 0, shade_grid = 0;
 };
 
 BatchPlan batch_plan(const gyt_context* ctx, int W) {
@@ -2634,6 +2636,7 @@ BatchPlan batch_plan(const gyt_context* ctx, int W) {
   b.ext_grid = sms * std::max(1u, te);
   b.sh_grid = sms * std::max(1u, ts);
   b.mis_grid = sms;  // MIS rays are rare: one block per SM
+  b.shade_grid = grid_for(ctx->capacity);
   return b;
 }
 
@@ -2648,7 +2651,7 @@ cudaError_t enqueue_half(gyt_context* ctx, const BatchPlan& b, const PathBuf& P,
   k_generate_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, tab);
   if (b.W == 8) k_extend_batch<8><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
   else k_extend_batch<2><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
-  k_shade_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, q, tab);
+  k_shade_batch<<<b.shade_grid, kBlock, 0, s>>>(P, st, q, tab);
   if (b.W == 8) k_shadow_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, q);
   else k_shadow_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, q);
   if (b.W == 8) k_mis_batch<8><<<b.mis_grid, kBlock, 0, s>>>(P, q);
