@@ -132,6 +132,11 @@ constexpr uint32_t kPixMask = 0x0fffffffu;
 constexpr int kWStack = 48;  // node groups: one per level of the wide BVH
 constexpr int kBStack = 64;  // binary BVH: one entry per level
 constexpr int kBlock = 256;
+// Shadow-ray kernels are latency-bound (dependent node fetches): over the
+// binary BVH a register cap that fits four blocks per SM (a few spilled
+// values) beats two blocks; the 8-wide traversal needs its registers.
+template <int W>
+constexpr int shadow_blocks_per_sm() { return W == 8 ? 2 : 4; }
 
 GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive) {
   return (depth & 255u) | (delta ? 256u : 0u) | ((cursor & 2047u) << 9) | (alive ? kAlive : 0u);
@@ -189,8 +194,11 @@ GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count
   return false;
 }
 
-// Binary BVH (two child boxes per 64-byte node, gyt_bvh_host.h), one step =
-// one inner node or one leaf. The stack holds one far child per level.
+// Binary BVH (two child boxes per 64-byte node, gyt_bvh_host.h). One step =
+// the inner nodes down to the next leaf, then that leaf ("while-while"
+// traversal): the lanes of a warp stay on inner nodes together and test
+// their leaves together, instead of alternating between the two at every
+// step. The stack holds one far child per level.
 struct BinaryTraversal {
   int node, sp;
   int stack[kBStack];
@@ -201,7 +209,8 @@ struct BinaryTraversal {
   template <bool ANY, bool COUNT, class S>
   GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
-    if (node >= 0) {
+#pragma unroll 1
+    while (node >= 0) {
       if (COUNT) cnt->nodes++;
       const float4* n = s.nodes + 4 * (size_t)node;
       float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
@@ -221,7 +230,7 @@ struct BinaryTraversal {
       if (!h0 && !h1) {
         if (sp == 0) return true;
         node = stack[--sp];
-        return false;
+        continue;
       }
       if (h0 && h1) {
         int nearc = n3.x, farc = n3.y;
@@ -231,7 +240,6 @@ struct BinaryTraversal {
       } else {
         node = h0 ? n3.x : n3.y;
       }
-      return false;
     }
     uint32_t code = ~(uint32_t)node;
     if (test_tris<ANY, COUNT>(s, rc.wr, code >> 3, (code & 7u) + 1u, tmax, b1, b2, prim, cnt)) return true;
@@ -426,9 +434,10 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
     }
     if (__all_sync(0xffffffffu, ri == -2)) break;
     if (ri >= 0) {
-      // a few steps per fetch check keep the ballot cost small
+      // a few steps per fetch check keep the ballot cost small (a binary step
+      // already walks down to a leaf)
 #pragma unroll 1
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < (W == 8 ? 4 : 2); ++k) {
         const bool fin = BATCH ? tv.template step<ANY, COUNT>(lg, rc, o, tmax, b1, b2, prim, &cnt)
                                : tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, &cnt);
         if (fin) {
@@ -827,7 +836,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
 // Next-event shadow rays (any hit): an unoccluded ray adds its contribution
 // to its path's radiance (VisibilityTester::Unoccluded, Visibility.cpp:7-10).
 template <int W, bool COUNT>
-__global__ void __launch_bounds__(kBlock) k_shadow(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
+__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
                                                    unsigned long long* counters) {
   const uint32_t n = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, COUNT>(
@@ -1026,7 +1035,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_adj(PathBuf cur, AdjBuf A, uin
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_shadow_adj(PathBuf cur, AdjBuf A, DevScene s, Queues q, GradOut G) {
+__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow_adj(PathBuf cur, AdjBuf A, DevScene s, Queues q, GradOut G) {
   const uint32_t n = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, false>(
       s, q.counts + 3, n,
@@ -1195,7 +1204,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterS
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_shadow_batch(PathBuf cur, Queues q) {
+__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow_batch(PathBuf cur, Queues q) {
   const uint32_t n = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, false, true>(
       c_insts[0].s, q.counts + 3, n,
