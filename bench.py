@@ -540,7 +540,7 @@ def roofline(prof, cnt, stats, node_bytes=64):
     of its launches / their CUDA-event time; traversal bytes per ray = BVH
     nodes x node size + triangle tests x 48 B (counts from the counting pass)."""
     peak, src = peaks()
-    ms = prof["ms"]
+    ms = {k: v for k, v in prof["ms"].items() if k != "unused"}
     dom = max(ms, key=ms.get)
     launches = max(1, prof["launches"][dom])
     slots = stats[-1]["path_slots"]
@@ -552,8 +552,8 @@ def roofline(prof, cnt, stats, node_bytes=64):
 
     if dom == "extend":
         byts = rays["extend"] * (RAY + HIT + trav("extend"))
-    elif dom in ("shadow", "mis"):
-        byts = rays[dom] * (RAY + CONTRIB + 16 + trav(dom))
+    elif dom == "connect":
+        byts = sum(rays[k] * (RAY + CONTRIB + 16 + trav(k)) for k in ("shadow", "mis"))
     elif dom == "shade":
         byts = slots * (STATE_READ + HIT + STATE_WRITE) + (rays["shadow"] + rays["mis"]) * (RAY + CONTRIB)
     elif dom == "finish":

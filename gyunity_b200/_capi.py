@@ -79,7 +79,8 @@ class GytBatchConfig(ctypes.Structure):
                 ("bvh_width", ctypes.c_uint32)]
 
 
-KERNELS = ["generate", "extend", "shade", "shadow", "mis", "finish"]
+# profile slots (slot 4 is unused: the MIS rays are traced in the connect launch)
+KERNELS = ["generate", "extend", "shade", "connect", "unused", "finish"]
 TRAVERSALS = ["extend", "shadow", "mis"]
 
 

@@ -656,7 +656,10 @@ struct Bsdf {
     if ((refl && (f & kRefl)) || (!refl && (f & kTrans))) return lobe.eval(local(wo), local(wi));
     return mk(0.f, 0.f, 0.f);
   }
-  GYT_D float3 sample(float3 wo, float3* wi, float* pdf, float u0, float u1, float u2) const {
+  // Not inlined: the shading kernel samples the BSDF twice (the MIS half of
+  // direct lighting and the continuation), and one out-of-line copy keeps its
+  // instruction footprint small (it is instruction-bound).
+  __device__ __noinline__ float3 sample(float3 wo, float3* wi, float* pdf, float u0, float u1, float u2) const {
     float3 wl;
     float3 f = lobe.sample(local(wo), &wl, pdf, u0, u1, u2);
     *wi = world(wl);

@@ -92,6 +92,7 @@ struct Queues {
   float4* mc;  // MIS ray: contribution, path slot bits
   float4* hit; // per path slot: t, b1, b2, prim bits
   uint32_t* counts;  // [0] shadow rays, [1] MIS rays, [2..4] fetch counters, [5] compaction
+  float4* madd; // per path slot: its MIS ray's contribution (k_connect; added by k_finish)
   float4* sx;  // adjoint pass, shadow ray: material bits, d log f / d alpha, light bits, -
   float4* mx;  // adjoint pass, MIS ray: material bits, d log f / d alpha, -, -
 };
@@ -138,8 +139,12 @@ constexpr int kBlock = 256;
 template <int W>
 constexpr int shadow_blocks_per_sm() { return W == 8 ? 2 : 4; }
 
-GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive) {
-  return (depth & 255u) | (delta ? 256u : 0u) | ((cursor & 2047u) << 9) | (alive ? kAlive : 0u);
+// meta bit 20: the bounce queued an MIS ray whose contribution k_finish adds
+constexpr uint32_t kMisQueued = 1u << 20;
+
+GYT_D uint32_t meta_pack(uint32_t depth, bool delta, uint32_t cursor, bool alive, bool mis_queued = false) {
+  return (depth & 255u) | (delta ? 256u : 0u) | ((cursor & 2047u) << 9) | (alive ? kAlive : 0u) |
+         (mis_queued ? kMisQueued : 0u);
 }
 
 // ------------------------------------------------------------ traversal ---
@@ -643,7 +648,11 @@ GYT_D void grad_emitter(const GradOut& G, const DevScene& s, int li, float3 Cd) 
 // f_k scales is known from the primal radiance: everything after vertex k's
 // continuation is Ltot - (radiance gathered through vertex k), settled at the
 // next bounce.
-template <bool ADJ>
+//
+// DEFER: the MIS ray's contribution is added by k_finish (k_connect traces
+// the shadow and MIS rays in one launch and leaves it in q.madd), not by the
+// MIS kernel.
+template <bool ADJ, bool DEFER = false>
 GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
                       SobolTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   float4 h4 = q.hit[i];
@@ -659,6 +668,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
   bool alive = false;
   float3 adj = mk(0.f, 0.f, 0.f);
   uint2 pend_new = make_uint2(0u, 0u);
+  bool mis_queued = false;
   if (ADJ) {
     adj = f3(A.delta[i]);
     const uint2 pend = A.pend[i];
@@ -781,6 +791,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
             q.mo[j] = make_float4(o2.x, o2.y, o2.z, __uint_as_float(bounce));
             q.md[j] = make_float4(wi2.x, wi2.y, wi2.z, __int_as_float(li));
             q.mc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(i));
+            mis_queued = true;
             if (ADJ)
               q.mx[j] = make_float4(__uint_as_float(mat), lobe_dlog_alpha(bsdf.lobe, bsdf.local(h.wo), bsdf.local(wi2)),
                                     0.f, 0.f);
@@ -822,7 +833,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     }
   }
   cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
-  cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive);
+  cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive, DEFER && mis_queued);
   if (ADJ) A.pend[i] = pend_new;
 }
 
@@ -830,38 +841,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevSc
                                                   SobolTables tab, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  shade_path<false>(cur, i, s, prm, q, tab, dbg);
+  shade_path<false, true>(cur, i, s, prm, q, tab, dbg);
 }
 
-// Next-event shadow rays (any hit): an unoccluded ray adds its contribution
-// to its path's radiance (VisibilityTester::Unoccluded, Visibility.cpp:7-10).
-template <int W, bool COUNT>
-__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
-                                                   unsigned long long* counters) {
-  const uint32_t n = *(volatile uint32_t*)q.counts;
-  persistent_trace<W, true, COUNT>(
-      s, q.counts + 3, n,
-      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
-        float4 a = q.so[j], b = q.sd[j];
-        o = f3(a);
-        d = f3(b);
-        tmax = a.w;
-      },
-      [&](uint32_t j, int prim, float, float, float) {
-        const uint32_t slot = __float_as_uint(q.sd[j].w);
-        if (prim < 0) {
-          float4 c = q.sc[j], l = cur.L[slot];
-          cur.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.f);
-        } else if (dbg.occ) {
-          const uint32_t b = __float_as_uint(q.sc[j].w);
-          if (b < 64) dbg.occ[cur.pid[slot]] |= 1ull << b;
-        }
-      },
-      counters);
-}
-
-// MIS-ray result of one queue entry (shared by both MIS kernels).
-template <bool ADJ = false>
+// MIS-ray result of one queue entry (every MIS kernel). DEFER: the
+// contribution (zero when the light is missed) goes to the path's q.madd slot
+// for k_finish instead of into its radiance.
+template <bool ADJ = false, bool DEFER = false>
 GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint32_t j, int prim, float b1, float b2,
                     const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   const float4 md = q.md[j], mc = q.mc[j];
@@ -884,9 +870,12 @@ GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint
     }
     reach = true;
   }
+  if (DEFER) q.madd[slot] = make_float4(add.x, add.y, add.z, 0.f);
   if (reach) {
-    float4 l = cur.L[slot];
-    cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
+    if (!DEFER) {
+      float4 l = cur.L[slot];
+      cur.L[slot] = make_float4(l.x + add.x, l.y + add.y, l.z + add.z, 0.f);
+    }
     if (ADJ) {
       const float3 Cd = f3(A.delta[slot]) * add;
       const float4 x = q.mx[j];
@@ -900,21 +889,51 @@ GYT_D void mis_done(const PathBuf& cur, const Queues& q, const DevScene& s, uint
   }
 }
 
-// BSDF-sampled MIS rays (closest hit): the sampled light's emission where the
-// ray reaches it (Integrator.cpp:86-101).
+// The rays k_shade queued, in one persistent launch: first the next-event
+// shadow rays (any hit; an unoccluded ray adds its contribution to its path's
+// radiance, VisibilityTester::Unoccluded, Visibility.cpp:7-10), then the
+// BSDF-sampled MIS rays (closest hit; the sampled light's emission where the
+// ray reaches it, Integrator.cpp:86-101). The MIS rays are few: traced in the
+// same launch they fill the shadow rays' tail instead of paying a launch of
+// their own. Their contribution goes to q.madd (k_finish adds it), since the
+// path's radiance may still be in use by a shadow ray of another warp.
+// counters: node and triangle counts of the shadow rays, then of the MIS rays.
 template <int W, bool COUNT>
-__global__ void __launch_bounds__(kBlock) k_mis(PathBuf cur, DevScene s, Queues q, DebugOut dbg,
-                                                unsigned long long* counters) {
-  const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
+__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_connect(PathBuf cur, DevScene s, Queues q,
+                                                                                DebugOut dbg,
+                                                                                unsigned long long* counters) {
+  const uint32_t ns = *(volatile uint32_t*)q.counts;
+  persistent_trace<W, true, COUNT>(
+      s, q.counts + 3, ns,
+      [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
+        float4 a = q.so[j], b = q.sd[j];
+        o = f3(a);
+        d = f3(b);
+        tmax = a.w;
+      },
+      [&](uint32_t j, int prim, float, float, float) {
+        const uint32_t slot = __float_as_uint(q.sd[j].w);
+        if (prim < 0) {
+          float4 c = q.sc[j], l = cur.L[slot];
+          cur.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.f);
+        } else if (dbg.occ) {
+          const uint32_t b = __float_as_uint(q.sc[j].w);
+          if (b < 64) dbg.occ[cur.pid[slot]] |= 1ull << b;
+        }
+      },
+      counters);
+  const uint32_t nm = *(volatile uint32_t*)(q.counts + 1);
   persistent_trace<W, false, COUNT>(
-      s, q.counts + 4, n,
+      s, q.counts + 4, nm,
       [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo&) {
         o = f3(q.mo[j]);
         d = f3(q.md[j]);
         tmax = __int_as_float(0x7f800000);
       },
-      [&](uint32_t j, int prim, float, float b1, float b2) { mis_done(cur, q, s, j, prim, b1, b2, dbg); },
-      counters);
+      [&](uint32_t j, int prim, float, float b1, float b2) {
+        mis_done<false, true>(cur, q, s, j, prim, b1, b2, dbg);
+      },
+      COUNT ? counters + 2 : nullptr);
 }
 
 GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) {
@@ -928,11 +947,17 @@ GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) 
 // Finished paths go to the film (FP64 atomics, Film::AddSample with the box
 // filter, visual/Film.h:61-87); live paths are compacted into the next pool.
 __global__ void __launch_bounds__(kBlock) k_finish(PathBuf cur, PathBuf nxt, uint32_t n, double* __restrict__ film,
-                                                   uint32_t res_x, uint32_t* __restrict__ counter, DebugOut dbg) {
+                                                   uint32_t res_x, uint32_t* __restrict__ counter,
+                                                   const float4* __restrict__ madd, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t meta = cur.meta[i];
   float4 L4 = cur.L[i];
+  if (meta & kMisQueued) {  // the MIS contribution of this bounce (k_connect)
+    const float4 m = madd[i];
+    L4 = make_float4(L4.x + m.x, L4.y + m.y, L4.z + m.z, 0.f);
+    meta &= ~kMisQueued;
+  }
   if (meta & kAlive) {
     cg::coalesced_group g = cg::coalesced_threads();
     uint32_t base = 0;
@@ -1349,8 +1374,7 @@ inline int pindex(int kind, int w, bool count) { return (kind * 2 + (w == 8 ? 1 
 template <int W, bool C>
 const void* persistent_fn(int kind) {
   if (kind == kPExtend) return (const void*)k_extend<W, C>;
-  if (kind == kPShadow) return (const void*)k_shadow<W, C>;
-  return (const void*)k_mis<W, C>;
+  return (const void*)k_connect<W, C>;  // shadow and MIS rays (kPMis: grid of the adjoint's MIS kernel)
 }
 
 }  // namespace
@@ -1609,6 +1633,7 @@ int32_t ensure_pool(gyt_context* ctx) {
   GYT_CK(ctx, dalloc(L, &q.md, n));
   GYT_CK(ctx, dalloc(L, &q.mc, n));
   GYT_CK(ctx, dalloc(L, &q.hit, n));
+  GYT_CK(ctx, dalloc(L, &q.madd, n));
   GYT_CK(ctx, dalloc(L, &q.counts, 8));
   ctx->pool_cap = ctx->capacity;
   return ensure_adj_reset(ctx);
@@ -1650,8 +1675,7 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
   uint32_t launches = 0;
   unsigned long long slots = 0;
   const int W = scene->dev.wnodes ? 8 : 2;
-  const int g_ext = ctx->pgrid[pindex(kPExtend, W, cnt)], g_sh = ctx->pgrid[pindex(kPShadow, W, cnt)],
-            g_mis = ctx->pgrid[pindex(kPMis, W, cnt)];
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, cnt)], g_sh = ctx->pgrid[pindex(kPShadow, W, cnt)];
   Queues q = ctx->q;
   if (cnt) GYT_CK(ctx, cudaMemsetAsync(ctx->d_counters, 0, 6 * sizeof(unsigned long long), s));
   uint32_t hcounts[8];
@@ -1681,25 +1705,19 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[2], s));
     k_shade<<<grid_for(active), kBlock, 0, s>>>(P, active, D, prm, q, tab, dbg);
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[3], s));
+    // shadow and MIS rays in one launch (profile slot 3; slot 4 stays empty)
     if (W == 8) {
-      if (cnt) k_shadow<8, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
-      else k_shadow<8, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+      if (cnt) k_connect<8, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
+      else k_connect<8, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
     } else {
-      if (cnt) k_shadow<2, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
-      else k_shadow<2, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
+      if (cnt) k_connect<2, true><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, C + 2);
+      else k_connect<2, false><<<g_sh, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
     }
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[4], s));
-    if (W == 8) {
-      if (cnt) k_mis<8, true><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, C + 4);
-      else k_mis<8, false><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
-    } else {
-      if (cnt) k_mis<2, true><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, C + 4);
-      else k_mis<2, false><<<g_mis, kBlock, 0, s>>>(P, D, q, dbg, nullptr);
-    }
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[5], s));
-    k_finish<<<grid_for(active), kBlock, 0, s>>>(P, N, active, d_film, cam.res_x, q.counts + 5, dbg);
+    k_finish<<<grid_for(active), kBlock, 0, s>>>(P, N, active, d_film, cam.res_x, q.counts + 5, q.madd, dbg);
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[6], s));
-    launches += 5;
+    launches += 4;
     GYT_CK(ctx, cudaGetLastError());
     GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, q.counts, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GYT_CK(ctx, cudaStreamSynchronize(s));
@@ -1709,7 +1727,7 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->kev[k], ctx->kev[k + 1]);
         ctx->prof.ms[k] += ms;
-        if (k != 0 || n_new) ctx->prof.launches[k]++;
+        if ((k != 0 || n_new) && k != 4) ctx->prof.launches[k]++;
       }
       ctx->prof.rays[0] += active;
       ctx->prof.rays[1] += hcounts[0];
@@ -2996,7 +3014,7 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
 
 namespace {
 
-constexpr size_t kNoAllocSlotBytes = 2 * (4 * sizeof(float4) + 8 + 3 * 4) + 7 * sizeof(float4);
+constexpr size_t kNoAllocSlotBytes = 2 * (4 * sizeof(float4) + 8 + 3 * 4) + 8 * sizeof(float4);
 constexpr size_t kNoAllocAlign = 256;
 constexpr size_t align_up(size_t v) { return (v + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
 // per-array rounding adds at most one alignment unit per array (25 arrays)
@@ -3079,6 +3097,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   q.md = carve<float4>(c, n);
   q.mc = carve<float4>(c, n);
   q.hit = carve<float4>(c, n);
+  q.madd = carve<float4>(c, n);
   q.counts = carve<uint32_t>(c, 8);
   if ((size_t)(c - base) > kNoAllocBytes)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: scratch layout exceeds the array");
@@ -3087,8 +3106,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   SobolTables tab = tables(ctx);
   cudaStream_t s = ctx->stream;
   const int W = scene->dev.wnodes ? 8 : 2;
-  const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)],
-            g_mis = ctx->pgrid[pindex(kPMis, W, false)];
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)];
   const DevScene& D = scene->dev;
   unsigned long long generated = 0;
   uint32_t active = 0, iters = 0, live = 0;
@@ -3104,11 +3122,10 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
     if (W == 8) k_extend<8, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
     else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
     k_shade<<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, D, prm, q, tab, DebugOut{});
-    if (W == 8) k_shadow<8, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
-    else k_shadow<2, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
-    if (W == 8) k_mis<8, false><<<g_mis, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
-    else k_mis<2, false><<<g_mis, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    if (W == 8) k_connect<8, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
+    else k_connect<2, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
     k_finish<<<grid_for(active), kBlock, 0, s>>>(pool[cur], pool[cur ^ 1], active, d_film, cam.res_x, q.counts + 5,
+                                                q.madd,
                                                 DebugOut{});
     GYT_CK(ctx, cudaGetLastError());
     // pageable destination: the copy completes before cudaMemcpyAsync returns

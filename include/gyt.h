@@ -105,8 +105,9 @@ typedef struct {
 
 /* Kernel-level profile of the renders since the last gyt_profile_read.
  * Kernel slots: 0 generate, 1 extend (continuation rays), 2 shade,
- * 3 shadow (next-event shadow rays), 4 mis (BSDF-sampled MIS rays),
- * 5 finish (film and compaction). Traversal slots: 0 extend, 1 shadow, 2 mis. */
+ * 3 connect (next-event shadow rays, then the BSDF-sampled MIS rays, in one
+ * launch), 4 unused (0), 5 finish (film and compaction). Traversal slots:
+ * 0 extend, 1 shadow, 2 mis. */
 typedef struct {
   float ms[6];                    /* summed device time per kernel (CUDA events) */
   uint32_t launches[6];
@@ -284,7 +285,7 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
  * owns all device memory through its own allocator or a fixed budget, or code
  * running where cudaMalloc is not allowed). The paths in flight, their queues
  * and the compaction counter live in a scratch array built into the library
- * (GYT_NOALLOC_MAX_PATHS path slots, about 9 MB, reserved on every device that
+ * (GYT_NOALLOC_MAX_PATHS path slots, about 10 MB, reserved on every device that
  * loads the library until the process exits) instead of the context's pools,
  * which are allocated on first use. paths_in_flight (1..GYT_NOALLOC_MAX_PATHS)
  * sets how many paths share it; larger values are rejected with
