@@ -1,21 +1,28 @@
 """Benchmark of the path tracing hot path (the reference's PathTracing Render).
 
-Workload (default): a seeded noise-displaced icosphere of 1,310,720 triangles
-with 64 GGX-conductor material groups in the Cornell box, 1024x1024 film,
-64 spp Sobol', max depth 16 -> 67,108,864 camera paths per step. Synthetic
-seeded geometry stands in for the reference's mesh assets. After it, the
-uneven batch workload (64 seeded instances of 10k-2M triangles, 128^2-1024^2,
-1-64 spp) is timed per scene and as one batched render ("batched" object).
+Headline workload (default, --workload batch): the uneven batch: 64 seeded
+instances (Cornell boxes holding noise-displaced icospheres or tori of 10k-2M
+triangles, diffuse or GGX, 128^2-1024^2 films, 1-64 spp, depth 16; 834M
+camera paths per step). ``value`` is Mpaths/s of one batched render of all
+instances (one CUDA graph launch, autotuned); ``per_scene`` renders every
+instance with its own gyt_render_device call; both render the same paths, so
+the images have equal RMSE (``equal_rmse`` reports the largest film
+difference). ``single_scene`` is the procedural-mesh workload (a 1,310,720-
+triangle displaced icosphere, 1024x1024, 64 spp, depth 16) and ``adjoint`` the
+inverse-rendering workload (gradients per second against finite differences).
+--workload mesh | env | cornell make one of the single-scene workloads the
+headline instead.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-One JSON line on rank 0. ``value`` is Mpaths/s of whole renders with the
-scene resident on the device (CUDA-event time on the render stream, max over
-ranks); ``e2e`` is the same metric through the public Render call with the
-image read back to host memory. Multi-GPU runs are weak scaling: every rank
-renders its own full frame (independent frames, no collective on the data path).
+One JSON line on rank 0. Device times are CUDA events on the render stream,
+max over ranks; ``e2e`` is the same metric through the public host-image call.
+Multi-GPU runs are weak scaling: every rank renders the whole workload
+(independent renders, no collective on the data path). Synthetic seeded
+geometry stands in for the reference's mesh assets.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -30,7 +37,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "Mpaths/s (path-traced camera paths per second)"
+# the metric of the headline (batch) workload, and of the single-scene workloads
+METRIC = "batched vs per-scene Mpaths/s at equal RMSE; adjoint vs FD grads/s on 1 B200"
+METRIC_SINGLE = "Mpaths/s (path-traced camera paths per second)"
 UNIT = "Mpaths/s"
 
 
@@ -40,9 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gyunity", choices=["gyunity", "reference"])
-    ap.add_argument("--workload", default="mesh", choices=["mesh", "env", "cornell"],
-                    help="mesh: procedural mesh (default); env: environment-lit rough-glass torus knot "
-                         "(4M triangles, 1920x1080, 256 spp, depth 32); cornell: the Cornell box (256x256, 16 spp)")
+    ap.add_argument("--workload", default="batch", choices=["batch", "mesh", "env", "cornell"],
+                    help="batch: the uneven 64-instance batch (default); mesh: procedural mesh; env: "
+                         "environment-lit rough-glass torus knot (4M triangles, 1920x1080, 256 spp, depth 32); "
+                         "cornell: the Cornell box (256x256, 16 spp)")
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = 1.31M triangles)")
     ap.add_argument("--res", type=int, default=1024)
     ap.add_argument("--spp", type=int, default=64)
@@ -50,9 +60,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bvh-width", type=int, default=None, choices=[2, 8])
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
-    ap.add_argument("--batch-instances", type=int, default=64,
-                    help="instances of the uneven batch workload measured after the main render (0 = skip)")
-    ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--batch-instances", type=int, default=64, help="instances of the uneven batch workload")
+    ap.add_argument("--no-single-scene", action="store_true",
+                    help="batch workload: skip the single-scene (procedural mesh) measurement")
     ap.add_argument("--adjoint-iters", type=int, default=200,
                     help="Adam iterations of the inverse-rendering run after the adjoint timing (0 = skip the run)")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -60,6 +70,8 @@ def parse():
 
 
 def workload(a):
+    """The single-scene workload (--workload mesh, env, cornell; the batch
+    line's single_scene object uses mesh)."""
     from gyunity_b200 import scenes
     if a.workload == "env":
         return scenes.env_torus_knot()
@@ -190,13 +202,21 @@ def peaks():
 
 
 # ---------------------------------------------------------- CPU baseline ---
-def cpu_baseline(sd, spp, rows=None, threads=None):
-    """The reference CPU integrator (compiled from its sources, oracle/_ref)
-    or, when that binary is absent, the oracle's CPU restatement, on a bounded
-    sample of the same workload (full film at reduced spp). Returns a dict."""
+# The reference CPU integrator runs on a bounded sample of the batch: every
+# 16th instance (4 of 64: 158k, 33k, 1.05M and 473k triangles; 256^2 to
+# 1024^2 films) at up to 2 spp, about 8 s of single-core-equivalent work.
+BATCH_SAMPLE_STRIDE = 16
+BATCH_SAMPLE_SPP = 2
+
+
+def _cpu_render(sd, spp, rows=None, threads=None):
+    """One render of sd at spp by the reference CPU integrator (compiled from
+    its sources, oracle/_ref) or, where that binary is absent, by the
+    oracle's CPU restatement. Returns (paths, render seconds, kind, threads);
+    scene loading and the BVH build are outside the timed render."""
+    import copy
     from oracle import scene_io as io
     threads = threads or os.cpu_count() or 1
-    import copy
     s2 = copy.deepcopy(sd)
     s2.params.spp = spp
     if io.have_harness():
@@ -204,36 +224,71 @@ def cpu_baseline(sd, spp, rows=None, threads=None):
             path = os.path.join(tmp, "w.gyts")
             io.write_scene(path, s2)
             _, info = io.ref_render(tmp, path, rows=rows, spp=spp, threads=threads)
-        return {"value": info["mpaths_per_s"], "unit": UNIT, "cores": info["threads"], "kind": "reference",
-                "sample": "%d rows x %d px x %d spp of the same workload (TiledIntegrator::Render, BVH build excluded)"
-                          % (info["rows"], sd.camera.res_x, spp)}
+        return info["paths"], info["render_s"], "reference", info["threads"]
     from oracle.port import oracle as orc
     o = orc.OracleScene(s2)
-    t = time.perf_counter()
     r = rows or sd.camera.res_y
+    t = time.perf_counter()
     o.render(rows=(0, r), precision=32, threads=threads, params=s2.params)
-    dt = time.perf_counter() - t
-    return {"value": sd.camera.res_x * r * spp / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d rows x %d px x %d spp of the same workload (CPU restatement)" % (r, sd.camera.res_x, spp)}
+    return sd.camera.res_x * r * spp, time.perf_counter() - t, "port", threads
+
+
+def cpu_baseline(sd, spp, rows=None, threads=None):
+    """Single-scene CPU baseline: the full film of the same workload at spp."""
+    n, sec, kind, th = _cpu_render(sd, spp, rows, threads)
+    what = "TiledIntegrator::Render" if kind == "reference" else "CPU restatement"
+    return {"value": n / sec / 1e6, "unit": UNIT, "cores": th, "kind": kind,
+            "sample": "%d rows x %d px x %d spp of the same workload (%s, BVH build excluded)"
+                      % (n // (sd.camera.res_x * spp), sd.camera.res_x, spp, what)}
+
+
+def batch_sample(n):
+    from gyunity_b200 import scenes
+    return [(i, scenes.batch_instance(1000 + i)) for i in range(0, n, BATCH_SAMPLE_STRIDE)]
+
+
+def cpu_baseline_batch(sample, threads=None):
+    """Batch CPU baseline: the sampled instances one after another, each at
+    min(its spp, 2) over its full film; Mpaths/s = sample paths / the sum of
+    the render times."""
+    paths, secs, kind, th = 0, 0.0, None, None
+    for _, sd in sample:
+        n, sec, kind, th = _cpu_render(sd, min(sd.params.spp, BATCH_SAMPLE_SPP), threads=threads)
+        paths += n
+        secs += sec
+    what = "TiledIntegrator::Render" if kind == "reference" else "CPU restatement"
+    return {"value": paths / secs / 1e6, "unit": UNIT, "cores": th, "kind": kind,
+            "sample": "instances %s of the batch, full films at min(spp, %d): %d paths (%s, BVH build excluded)"
+                      % (",".join(str(i) for i, _ in sample), BATCH_SAMPLE_SPP, paths, what),
+            "paths": paths, "render_s": secs}
 
 
 def run_reference(a):
     # the reference is a CPU integrator: rank 0 runs it, other ranks exit at once
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    sd = workload(a)
-    spp = 1
-    vals = []
-    info = None
+    if a.workload == "batch":
+        sample = batch_sample(a.batch_instances)
+        step = lambda: cpu_baseline_batch(sample)  # noqa: E731
+        cfg = batch_config(a, None, {"reference_sample": "every %dth instance at min(spp, %d)"
+                                                          % (BATCH_SAMPLE_STRIDE, BATCH_SAMPLE_SPP)})
+        metric = METRIC
+    else:
+        sd = workload(a)
+        step = lambda: cpu_baseline(sd, 1)  # noqa: E731
+        cfg = config(a, sd, {"reference_sample_spp": 1})
+        metric = METRIC_SINGLE
+    vals, info = [], None
     for k in range(a.warmup + a.steps):
-        info = cpu_baseline(sd, spp)
+        info = step()
         if k >= a.warmup:
             vals.append(info["value"])
     v = statistics.median(vals)
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": sd.camera.res_x * sd.camera.res_y * spp / v / 1e3,
+    paths = info.get("paths") or (sd.camera.res_x * sd.camera.res_y)
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": paths / v / 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config(a, sd, {"reference_sample_spp": spp}),
+            "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                              "sample": info["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -246,6 +301,30 @@ def run_ours(a):
     d = Dist(a.gpus)
     torch.cuda.set_device(d.local)
     import gyunity_b200 as g
+    if a.workload == "batch":
+        line = measure_batch(a, d, g, torch)
+        if not a.no_single_scene:
+            a1 = argparse.Namespace(**vars(a))
+            a1.workload = "mesh"
+            single = measure_single(a1, d, g, torch)
+            if d.rank == 0:
+                for k in ("n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "dtype", "data"):
+                    single.pop(k, None)
+                line["single_scene"] = single
+    else:
+        line = measure_single(a, d, g, torch)
+    if not a.no_adjoint:
+        adj = measure_adjoint(a, d, g, torch)
+        if d.rank == 0:
+            line["adjoint"] = adj
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
+def measure_single(a, d, g, torch):
+    """One scene per step through gyt_render_device (--workload mesh, env,
+    cornell); returns the JSON line on rank 0."""
     sd = workload(a)
     ctx = g.Context(d.local, bvh_width=a.bvh_width, bvh_builder=a.bvh_builder)
     t0 = time.perf_counter()
@@ -301,21 +380,22 @@ def run_ours(a):
     other_s = time.perf_counter() - t
     ctx_o.close()
 
-    out = None
+    line = None
     if d.rank == 0:
         # kernel-level profile of one render (event timing) and traversal counts
         ctx.set_profile(1)
         film.zero_()
+        torch.cuda.nvtx.range_push("single_profile")  # the launch list's capture window
         ctx.render_device(scene, cam, prm, film.data_ptr())
+        torch.cuda.nvtx.range_pop()
         prof = ctx.read_profile()
         ctx.set_profile(2)
         film.zero_()
         ctx.render_device(scene, cam, prm, film.data_ptr())
         cnt = ctx.read_profile()
         ctx.set_profile(0)
-        out = roofline(prof, cnt, stats, node_bytes=80 if a.bvh_width == 8 else 64)
-        clocks = clk.summary()
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
+        out = roofline(prof, cnt, stats[-1]["path_slots"], node_bytes=80 if a.bvh_width == 8 else 64)
+        line = {"metric": METRIC_SINGLE, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh, no dataset)",
                 "config": config(a, sd, {"parallelism": "independent frames per GPU" if d.world > 1 else "1 GPU",
@@ -325,12 +405,12 @@ def run_ours(a):
                 "wall_ms_per_step": wall * 1e3 / a.steps,
                 "iterations_per_step": stats[-1]["iterations"],
                 "scene_upload_and_bvh_s": {a.bvh_builder: scene_s, other: other_s},
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 + 16,
-                        "d2h_bytes_per_step": W * H * 3 * 4,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": ctypes.sizeof(_c().GytCamera) +
+                        ctypes.sizeof(_c().GytRenderParams), "d2h_bytes_per_step": W * H * 3 * 4,
                         "note": "public Render call with the scene resident, image copied to host each step"},
                 "e2e_cold": {"value": paths / a.steps / cold_s / 1e6, "unit": UNIT,
                              "note": "scene upload from host arrays + BVH build + render + image readback"},
-                "gpu_launches": launches, "roofline": out, "clocks": clocks, "profile": prof,
+                "gpu_launches": launches, "roofline": out, "clocks": clk.summary(), "profile": prof,
                 "traversal_counts": cnt}
         if not a.no_cpu_baseline:
             try:
@@ -339,27 +419,34 @@ def run_ours(a):
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     scene.close()
     ctx.close()
-    if a.batch_instances > 0:
-        b = measure_batch(a, d, g, torch)
-        if d.rank == 0:
-            line["batched"] = b
-    if not a.no_adjoint:
-        adj = measure_adjoint(a, d, g, torch)
-        if d.rank == 0:
-            line["adjoint"] = adj
-    if d.rank == 0:
-        print(json.dumps(line), flush=True)
-    d.close()
+    return line
+
+
+def _c():
+    from gyunity_b200 import _capi
+    return _capi
+
+
+def batch_config(a, descs, extra=None):
+    c = {"workload": "uneven_batch_%d_instances" % a.batch_instances,
+         "instances": a.batch_instances, "instance_seeds": "1000..%d" % (1000 + a.batch_instances - 1),
+         "scenes": "Cornell boxes holding a noise-displaced icosphere or ring torus (10k-2M triangles, log-uniform), "
+                   "diffuse or GGX conductor; films 128^2-1024^2; 1-64 spp; depth 16, Russian roulette from 5",
+         "sampler": "Sobol", "l2": "inputs larger than L2 (26M triangles resident); no flush"}
+    if descs is not None:
+        c.update({"triangles": int(sum(sd.n_triangles for sd in descs)),
+                  "paths_per_step": int(sum(sd.n_paths() for sd in descs))})
+    if extra:
+        c.update(extra)
+    return c
 
 
 def measure_batch(a, d, g, torch):
-    """The uneven batch workload (64 seeded instances: Cornell boxes holding
-    displaced icospheres or tori of 10k-2M triangles, 128^2-1024^2 films,
-    1-64 spp, depth 16): every instance rendered on its own with
-    gyt_render_device (the per-scene integrator) against all of them in one
-    batched render (one graph launch, autotuned). Both render the same paths,
-    so their images have equal RMSE; the check reports the largest film
-    difference."""
+    """The headline: the uneven batch (64 seeded instances) rendered by the
+    per-scene integrator (gyt_render_device once per instance) and by the
+    batched one (gyt_render_batch_device: one graph launch, autotuned). Both
+    render the same paths, so the images have equal RMSE; the check reports
+    the largest film difference. Returns the JSON line on rank 0."""
     from gyunity_b200 import scenes
     t = time.perf_counter()
     descs = scenes.batch_workload(a.batch_instances, seed=1000)
@@ -395,54 +482,86 @@ def measure_batch(a, d, g, torch):
     t = time.perf_counter()
     cfg, tune_mp = ctx.batch_autotune(scs, cams, prms, sample_spp=1)
     tune_s = time.perf_counter() - t
-    st = None
     for _ in range(a.warmup):
-        st = ctx.render_batch_device(scs, cams, prms, ptrs)
+        ctx.render_batch_device(scs, cams, prms, ptrs)
     d.barrier()
     torch.cuda.synchronize()
-    w0 = time.perf_counter()
-    b_ms = 0.0
-    launches = 0
-    for _ in range(a.batch_steps):
-        st = ctx.render_batch_device(scs, cams, prms, ptrs)
-        b_ms += st["ms"]
-        launches += st["launches"]
-    torch.cuda.synchronize()
-    b_wall = (time.perf_counter() - w0) / a.batch_steps
-    b_ms = d.max(b_ms / a.batch_steps)
+    stats = []
+    with Clocks(d.local) as clk:
+        w0 = time.perf_counter()
+        for _ in range(a.steps):
+            stats.append(ctx.render_batch_device(scs, cams, prms, ptrs))
+        torch.cuda.synchronize()
+        b_wall = (time.perf_counter() - w0) / a.steps
+    d.barrier()
+    b_ms = d.max(sum(s["ms"] for s in stats)) / a.steps
+    launches = sum(s["launches"] for s in stats)
     # equal RMSE: one more batched render from zeroed films against the per-scene films
     for f in films:
         f.zero_()
     ctx.render_batch_device(scs, cams, prms, ptrs)
     torch.cuda.synchronize()
-    diff = max(float(((x - y).abs().max() / y.abs().max().clamp_min(1e-300)).item()) for x, y in zip(films, ref))
-    # end to end: the host-image batch call (images copied back every step)
+    fdiff = max(float(((x - y).abs().max() / y.abs().max().clamp_min(1e-300)).item()) for x, y in zip(films, ref))
+    del ref
+    # end to end: the host-image batch call (cameras and parameters in, every image out)
+    e2e_steps = max(1, min(a.steps, 2))
     imgs_bytes = sum(c.res_x * c.res_y * 3 * 4 for c in cams)
+    h2d = len(descs) * (ctypes.sizeof(_c().GytCamera) + ctypes.sizeof(_c().GytRenderParams))
     ctx.render_batch(scs, cams, prms)
+    d.barrier()
     t = time.perf_counter()
-    ctx.render_batch(scs, cams, prms)
-    e2e_s = d.max(time.perf_counter() - t)
-    out = {"workload": "uneven batch: %d instances, %d triangles, %d paths per step" % (
-               len(descs), sum(sd.n_triangles for sd in descs), paths),
-           "value": paths * d.world / (b_ms / 1e3) / 1e6, "unit": UNIT,
-           "ms_per_step": b_ms, "wall_ms_per_step": b_wall * 1e3, "steps": a.batch_steps,
-           "gpu_launches_per_step": launches // max(1, a.batch_steps), "graph_launches_per_step": 1,
-           "per_scene": {"value": paths * d.world / (per_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": per_ms,
-                         "wall_ms_per_step": per_wall * 1e3,
-                         "note": "gyt_render_device once per instance, events around each render"},
-           "speedup_vs_per_scene": per_ms / b_ms,
-           "equal_rmse": {"max_rel_film_diff": diff,
-                          "note": "same paths in both runs; only the order of the FP64 film sums differs"},
-           "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s},
-           "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
-                   "d2h_bytes_per_step": imgs_bytes,
-                   "note": "gyt_render_batch with the scenes resident, every image copied to host"},
-           "scene_generation_s": gen_s, "scene_create_s": create_s}
-    del films, ref
+    for _ in range(e2e_steps):
+        ctx.render_batch(scs, cams, prms)
+    e2e_s = d.max(time.perf_counter() - t) / e2e_steps
+
+    line = None
+    if d.rank == 0:
+        # per-kernel event timing of one batched render (host-driven loop),
+        # and traversal counts from the per-scene counting pass: both trace
+        # exactly the same rays
+        ctx.set_profile(1)
+        torch.cuda.nvtx.range_push("batch_profile")  # the launch list's capture window
+        ctx.render_batch_device(scs, cams, prms, ptrs)
+        torch.cuda.nvtx.range_pop()
+        prof = ctx.read_profile()
+        ctx.set_profile(2)
+        per_scene()
+        cnt = ctx.read_profile()
+        ctx.set_profile(0)
+        out = roofline(prof, cnt, prof["rays"]["extend"], node_bytes=80 if cfg["bvh_width"] == 8 else 64)
+        out["rays_match_counting_pass"] = prof["rays"] == cnt["rays"]
+        value = paths * d.world / (b_ms / 1e3) / 1e6
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": b_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes, no dataset)",
+                "config": batch_config(a, descs, {"parallelism": "independent batches per GPU" if d.world > 1
+                                                  else "1 GPU", "batch_config": cfg}),
+                "wall_ms_per_step": b_wall * 1e3,
+                "per_scene": {"value": paths * d.world / (per_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": per_ms,
+                              "wall_ms_per_step": per_wall * 1e3,
+                              "note": "gyt_render_device once per instance, events around each render"},
+                "speedup_vs_per_scene": per_ms / b_ms,
+                "equal_rmse": {"max_rel_film_diff": fdiff,
+                               "note": "same paths in both runs; only the order of the FP64 film sums differs"},
+                "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s},
+                "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": imgs_bytes, "steps": e2e_steps,
+                        "note": "gyt_render_batch with the scenes resident: cameras and parameters in, "
+                                "every image copied to host memory"},
+                "gpu_launches": launches, "graph_launches": a.steps,
+                "iterations_per_step": stats[-1]["iterations"],
+                "roofline": out, "clocks": clk.summary(), "profile": prof, "traversal_counts": cnt,
+                "scene_generation_s": gen_s, "scene_create_s": create_s}
+        if not a.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline_batch(batch_sample(a.batch_instances))
+            except Exception as e:  # reported, never fatal for the GPU numbers
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    del films
     for sc in scs:
         sc.close()
     ctx.close()
-    return out
+    return line
 
 
 def measure_adjoint(a, d, g, torch):
@@ -535,7 +654,7 @@ def measure_adjoint(a, d, g, torch):
 STATE_READ, STATE_WRITE, HIT, RAY, CONTRIB = 76, 68, 16, 32, 16
 
 
-def roofline(prof, cnt, stats, node_bytes=64):
+def roofline(prof, cnt, slots, node_bytes=64):
     """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
     of its launches / their CUDA-event time; traversal bytes per ray = BVH
     nodes x node size + triangle tests x 48 B (counts from the counting pass)."""
@@ -543,7 +662,6 @@ def roofline(prof, cnt, stats, node_bytes=64):
     ms = {k: v for k, v in prof["ms"].items() if k != "unused"}
     dom = max(ms, key=ms.get)
     launches = max(1, prof["launches"][dom])
-    slots = stats[-1]["path_slots"]
     rays = cnt["rays"]
 
     def trav(k):

@@ -1225,14 +1225,16 @@ __global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterS
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= st->n) return;
   const Inst& I = c_insts[cur.inst[i]];
-  shade_path<false>(cur, i, I.s, I.prm, q, tab, DebugOut{});
+  shade_path<false, true>(cur, i, I.s, I.prm, q, tab, DebugOut{});
 }
 
+// Shadow then MIS rays of the batch in one launch (k_connect, every ray with
+// its instance's geometry).
 template <int W>
-__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow_batch(PathBuf cur, Queues q) {
-  const uint32_t n = *(volatile uint32_t*)q.counts;
+__global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_connect_batch(PathBuf cur, Queues q) {
+  const uint32_t ns = *(volatile uint32_t*)q.counts;
   persistent_trace<W, true, false, true>(
-      c_insts[0].s, q.counts + 3, n,
+      c_insts[0].s, q.counts + 3, ns,
       [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
         const float4 a = q.so[j], b = q.sd[j];
         o = f3(a);
@@ -1248,13 +1250,9 @@ __global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_shadow_ba
         }
       },
       nullptr);
-}
-
-template <int W>
-__global__ void __launch_bounds__(kBlock) k_mis_batch(PathBuf cur, Queues q) {
-  const uint32_t n = *(volatile uint32_t*)(q.counts + 1);
+  const uint32_t nm = *(volatile uint32_t*)(q.counts + 1);
   persistent_trace<W, false, false, true>(
-      c_insts[0].s, q.counts + 4, n,
+      c_insts[0].s, q.counts + 4, nm,
       [&](uint32_t j, float3& o, float3& d, float& tmax, TraceGeo& g) {
         o = f3(q.mo[j]);
         d = f3(q.md[j]);
@@ -1263,18 +1261,24 @@ __global__ void __launch_bounds__(kBlock) k_mis_batch(PathBuf cur, Queues q) {
       },
       [&](uint32_t j, int prim, float, float b1, float b2) {
         const uint32_t slot = __float_as_uint(q.mc[j].w);
-        mis_done(cur, q, c_insts[cur.inst[slot]].s, j, prim, b1, b2, DebugOut{});
+        mis_done<false, true>(cur, q, c_insts[cur.inst[slot]].s, j, prim, b1, b2, DebugOut{});
       },
       nullptr);
 }
 
 // Finished paths to their instance's film, live paths compacted.
 __global__ void __launch_bounds__(kBlock) k_finish_batch(PathBuf cur, PathBuf nxt, const IterState* __restrict__ st,
-                                                         uint32_t* __restrict__ counter) {
+                                                         uint32_t* __restrict__ counter,
+                                                         const float4* __restrict__ madd) {
   const uint32_t n = st->n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t meta = cur.meta[i];
-    const float4 L4 = cur.L[i];
+    uint32_t meta = cur.meta[i];
+    float4 L4 = cur.L[i];
+    if (meta & kMisQueued) {  // the MIS contribution of this bounce (k_connect_batch)
+      const float4 m = madd[i];
+      L4 = make_float4(L4.x + m.x, L4.y + m.y, L4.z + m.z, 0.f);
+      meta &= ~kMisQueued;
+    }
     if (meta & kAlive) {
       cg::coalesced_group g = cg::coalesced_threads();
       uint32_t base = 0;
@@ -1865,8 +1869,8 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_iter, sizeof(IterState));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_iter, sizeof(IterState));
   if (e == cudaSuccess) {
-    const void* fns[2][2] = {{(const void*)k_extend_batch<2>, (const void*)k_shadow_batch<2>},
-                             {(const void*)k_extend_batch<8>, (const void*)k_shadow_batch<8>}};
+    const void* fns[2][2] = {{(const void*)k_extend_batch<2>, (const void*)k_connect_batch<2>},
+                             {(const void*)k_extend_batch<8>, (const void*)k_connect_batch<8>}};
     for (int w = 0; w < 2 && e == cudaSuccess; ++w)
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         int nb = 0;
@@ -2646,7 +2650,7 @@ namespace {
 
 struct BatchPlan {
   int W = 2;
-  uint32_t stride_grid = 0, ext_grid = 0, sh_grid = 0, mis_grid = 0, shade_grid = 0;
+  uint32_t stride_grid = 0, ext_grid = 0, sh_grid = 0, shade_grid = 0;
 };
 
 BatchPlan batch_plan(const gyt_context* ctx, int W) {
@@ -2662,38 +2666,43 @@ BatchPlan batch_plan(const gyt_context* ctx, int W) {
                                             : (uint32_t)ctx->btrace[wi][1];
   b.ext_grid = sms * std::max(1u, te);
   b.sh_grid = sms * std::max(1u, ts);
-  b.mis_grid = sms;  // MIS rays are rare: one block per SM
   b.shade_grid = grid_for(ctx->capacity);
   return b;
 }
 
 // One half-iteration of the batched wavefront: pool P (current) to N (next).
+// ev (profiling, host loop only): six events around generate, extend, shade,
+// connect and finish.
 cudaError_t enqueue_half(gyt_context* ctx, const BatchPlan& b, const PathBuf& P, const PathBuf& N,
-                         cudaGraphConditionalHandle cond, int in_graph) {
+                         cudaGraphConditionalHandle cond, int in_graph, cudaEvent_t* ev = nullptr) {
   cudaStream_t s = ctx->stream;
   const Queues q = ctx->q;
   const SobolTables tab = tables(ctx);
   IterState* st = ctx->d_iter;
   k_batch_begin<<<1, 32, 0, s>>>(st, q.counts);
+  if (ev) cudaEventRecord(ev[0], s);
   k_generate_batch<<<b.stride_grid, kBlock, 0, s>>>(P, st, tab);
+  if (ev) cudaEventRecord(ev[1], s);
   if (b.W == 8) k_extend_batch<8><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
   else k_extend_batch<2><<<b.ext_grid, kBlock, 0, s>>>(P, st, q.hit, q.counts + 2);
+  if (ev) cudaEventRecord(ev[2], s);
   k_shade_batch<<<b.shade_grid, kBlock, 0, s>>>(P, st, q, tab);
-  if (b.W == 8) k_shadow_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, q);
-  else k_shadow_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, q);
-  if (b.W == 8) k_mis_batch<8><<<b.mis_grid, kBlock, 0, s>>>(P, q);
-  else k_mis_batch<2><<<b.mis_grid, kBlock, 0, s>>>(P, q);
-  k_finish_batch<<<b.stride_grid, kBlock, 0, s>>>(P, N, st, q.counts + 5);
+  if (ev) cudaEventRecord(ev[3], s);
+  if (b.W == 8) k_connect_batch<8><<<b.sh_grid, kBlock, 0, s>>>(P, q);
+  else k_connect_batch<2><<<b.sh_grid, kBlock, 0, s>>>(P, q);
+  if (ev) cudaEventRecord(ev[4], s);
+  k_finish_batch<<<b.stride_grid, kBlock, 0, s>>>(P, N, st, q.counts + 5, q.madd);
+  if (ev) cudaEventRecord(ev[5], s);
   k_batch_end<<<1, 32, 0, s>>>(st, q.counts, cond, in_graph);
   return cudaGetLastError();
 }
-constexpr uint32_t kKernelsPerHalf = 8;
+constexpr uint32_t kKernelsPerHalf = 7;
 
 // The batched render as one graph: a while-loop node whose body is two
 // half-iterations (pool 0 -> 1 -> 0); k_batch_end sets the loop condition.
 int32_t ensure_batch_graph(gyt_context* ctx, const BatchPlan& b) {
   const uint64_t key[6] = {(uint64_t)b.W, (uint64_t)b.stride_grid, ((uint64_t)b.ext_grid << 32) | b.sh_grid,
-                           (uint64_t)b.mis_grid, (uint64_t)(uintptr_t)ctx->pool[0].o, (uint64_t)ctx->pool_cap};
+                           (uint64_t)b.shade_grid, (uint64_t)(uintptr_t)ctx->pool[0].o, (uint64_t)ctx->pool_cap};
   if (ctx->bexec && std::memcmp(key, ctx->bkey, sizeof(key)) == 0) return GYT_OK;
   if (ctx->bexec) cudaGraphExecDestroy(ctx->bexec);
   if (ctx->bgraph) cudaGraphDestroy(ctx->bgraph);
@@ -2786,7 +2795,10 @@ int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats)
   if (st) return st;
   const BatchPlan b = batch_plan(ctx, in.W);
   std::lock_guard<std::mutex> lock(g_batch_mutex);
-  if (ctx->bcfg.use_graph) {
+  // profiling (gyt_context_set_profile) times every kernel: host loop
+  const bool prof = ctx->profile > 0;
+  const bool graph = ctx->bcfg.use_graph && !prof;
+  if (graph) {
     st = ensure_batch_graph(ctx, b);
     if (st) return st;
   }
@@ -2812,8 +2824,30 @@ int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats)
     is.max_iter = (uint32_t)std::min<unsigned long long>(bound, 1u << 30);
     *ctx->h_iter = is;
     GYT_CK(ctx, cudaMemcpyAsync(ctx->d_iter, ctx->h_iter, sizeof(IterState), cudaMemcpyHostToDevice, s));
-    if (ctx->bcfg.use_graph) {
+    if (graph) {
       GYT_CK(ctx, cudaGraphLaunch(ctx->bexec, s));
+    } else if (prof) {
+      // one half at a time, every kernel between events; profile slots as
+      // gyt_render_device fills them (3 = connect, 4 unused)
+      for (int half = 0;; half ^= 1) {
+        GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[half], ctx->pool[half ^ 1], 0, 0, ctx->kev));
+        GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, ctx->q.counts, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GYT_CK(ctx, cudaMemcpyAsync(ctx->h_iter, ctx->d_iter, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+        GYT_CK(ctx, cudaStreamSynchronize(s));
+        const IterState& h = *ctx->h_iter;
+        static const int slot[5] = {0, 1, 2, 3, 5};
+        for (int k = 0; k < 5; ++k) {
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, ctx->kev[k], ctx->kev[k + 1]);
+          ctx->prof.ms[slot[k]] += ms;
+          ctx->prof.launches[slot[k]]++;
+        }
+        ctx->prof.rays[0] += h.n;
+        ctx->prof.rays[1] += ctx->h_counter[0];
+        ctx->prof.rays[2] += ctx->h_counter[1];
+        if (h.watchdog || !(h.generated < h.total || h.active > 0)) break;
+        if (h.iter >= h.max_iter) break;
+      }
     } else {
       for (;;) {
         GYT_CK(ctx, enqueue_half(ctx, b, ctx->pool[0], ctx->pool[1], 0, 0));

@@ -1,0 +1,41 @@
+"""bench.py's reference arm on the CPU: rank 0 times the reference integrator
+(or the restatement where the reference binary is absent) and prints one
+JSON line carrying the contract's keys."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+KEYS = {"impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+        "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"}
+
+
+def _run(*args):
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", *args], env=env,
+                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    return json.loads(lines[0])
+
+
+def test_reference_arm_single_scene_line():
+    line = _run("--workload", "cornell", "--steps", "1", "--warmup", "0")
+    assert KEYS <= set(line)
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_batch_sample_is_every_sixteenth_instance():
+    sys.path.insert(0, ROOT)
+    import bench
+    ids = [i for i, _ in bench.batch_sample(64)]
+    assert ids == [0, 16, 32, 48]
+    cfg = bench.batch_config(type("A", (), {"batch_instances": 64})(), None)
+    assert cfg["instances"] == 64 and cfg["workload"] == "uneven_batch_64_instances"
