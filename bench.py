@@ -40,6 +40,7 @@ sys.path.insert(0, ROOT)
 # the metric of the headline (batch) workload, and of the single-scene workloads
 METRIC = "batched vs per-scene Mpaths/s at equal RMSE; adjoint vs FD grads/s on 1 B200"
 METRIC_SINGLE = "Mpaths/s (path-traced camera paths per second)"
+SAMPLER_NAMES = {"sobol": "Sobol", "halton": "Halton (Faure permutations)"}
 UNIT = "Mpaths/s"
 
 
@@ -58,6 +59,8 @@ def parse():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--depth", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sampler", default="sobol", choices=["sobol", "halton"],
+                    help="sobol: SobolSampler + SobolEnum (default); halton: HaltonSampler (Faure) + HaltonEnum")
     ap.add_argument("--bvh-width", type=int, default=None, choices=[2, 8])
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
     ap.add_argument("--batch-instances", type=int, default=64, help="instances of the uneven batch workload")
@@ -74,10 +77,13 @@ def workload(a):
     line's single_scene object uses mesh)."""
     from gyunity_b200 import scenes
     if a.workload == "env":
-        return scenes.env_torus_knot()
-    if a.workload == "cornell":
-        return scenes.cornell_box(res=256, spp=16, max_depth=8, rr_depth=3)
-    return scenes.procedural_mesh_box(level=a.level, res=a.res, spp=a.spp, max_depth=a.depth)
+        sd = scenes.env_torus_knot()
+    elif a.workload == "cornell":
+        sd = scenes.cornell_box(res=256, spp=16, max_depth=8, rr_depth=3)
+    else:
+        sd = scenes.procedural_mesh_box(level=a.level, res=a.res, spp=a.spp, max_depth=a.depth)
+    sd.params.sampler = a.sampler
+    return sd
 
 
 def config(a, sd, extra=None):
@@ -92,7 +98,7 @@ def config(a, sd, extra=None):
         c = {"workload": "procedural_mesh_cornell", "material": "GGX conductor", "groups": 64,
              "l2": "inputs larger than L2 (BVH + triangles exceed 126 MB); no flush"}
     c.update({"triangles": int(sd.n_triangles), "resolution": "%dx%d" % (cam.res_x, cam.res_y), "spp": prm.spp,
-              "max_depth": prm.max_depth, "rr_depth": prm.rr_depth, "sampler": "Sobol",
+              "max_depth": prm.max_depth, "rr_depth": prm.rr_depth, "sampler": SAMPLER_NAMES[prm.sampler],
               "paths_per_step": int(sd.n_paths())})
     if extra:
         c.update(extra)
@@ -223,7 +229,7 @@ def _cpu_render(sd, spp, rows=None, threads=None):
         with tempfile.TemporaryDirectory() as tmp:
             path = os.path.join(tmp, "w.gyts")
             io.write_scene(path, s2)
-            _, info = io.ref_render(tmp, path, rows=rows, spp=spp, threads=threads)
+            _, info = io.ref_render(tmp, path, rows=rows, spp=spp, threads=threads, sampler=sd.params.sampler)
         return info["paths"], info["render_s"], "reference", info["threads"]
     from oracle.port import oracle as orc
     o = orc.OracleScene(s2)
@@ -242,9 +248,19 @@ def cpu_baseline(sd, spp, rows=None, threads=None):
                       % (n // (sd.camera.res_x * spp), sd.camera.res_x, spp, what)}
 
 
-def batch_sample(n):
+def batch_workload(n, sampler="sobol", stride=1):
+    """Instances 0, stride, 2 stride, ... < n of the uneven batch (seeds 1000 + i)."""
     from gyunity_b200 import scenes
-    return [(i, scenes.batch_instance(1000 + i)) for i in range(0, n, BATCH_SAMPLE_STRIDE)]
+    out = []
+    for i in range(0, n, stride):
+        sd = scenes.batch_instance(1000 + i)
+        sd.params.sampler = sampler
+        out.append((i, sd))
+    return out
+
+
+def batch_sample(n, sampler="sobol"):
+    return batch_workload(n, sampler, BATCH_SAMPLE_STRIDE)
 
 
 def cpu_baseline_batch(sample, threads=None):
@@ -268,7 +284,7 @@ def run_reference(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     if a.workload == "batch":
-        sample = batch_sample(a.batch_instances)
+        sample = batch_sample(a.batch_instances, a.sampler)
         step = lambda: cpu_baseline_batch(sample)  # noqa: E731
         cfg = batch_config(a, None, {"reference_sample": "every %dth instance at min(spp, %d)"
                                                           % (BATCH_SAMPLE_STRIDE, BATCH_SAMPLE_SPP)})
@@ -432,7 +448,7 @@ def batch_config(a, descs, extra=None):
          "instances": a.batch_instances, "instance_seeds": "1000..%d" % (1000 + a.batch_instances - 1),
          "scenes": "Cornell boxes holding a noise-displaced icosphere or ring torus (10k-2M triangles, log-uniform), "
                    "diffuse or GGX conductor; films 128^2-1024^2; 1-64 spp; depth 16, Russian roulette from 5",
-         "sampler": "Sobol", "l2": "inputs larger than L2 (26M triangles resident); no flush"}
+         "sampler": SAMPLER_NAMES[a.sampler], "l2": "inputs larger than L2 (26M triangles resident); no flush"}
     if descs is not None:
         c.update({"triangles": int(sum(sd.n_triangles for sd in descs)),
                   "paths_per_step": int(sum(sd.n_paths() for sd in descs))})
@@ -447,9 +463,8 @@ def measure_batch(a, d, g, torch):
     batched one (gyt_render_batch_device: one graph launch, autotuned). Both
     render the same paths, so the images have equal RMSE; the check reports
     the largest film difference. Returns the JSON line on rank 0."""
-    from gyunity_b200 import scenes
     t = time.perf_counter()
-    descs = scenes.batch_workload(a.batch_instances, seed=1000)
+    descs = [sd for _, sd in batch_workload(a.batch_instances, a.sampler)]
     gen_s = time.perf_counter() - t
     ctx = g.Context(d.local)
     t = time.perf_counter()
@@ -554,7 +569,7 @@ def measure_batch(a, d, g, torch):
                 "scene_generation_s": gen_s, "scene_create_s": create_s}
         if not a.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline_batch(batch_sample(a.batch_instances))
+                line["cpu_baseline"] = cpu_baseline_batch(batch_sample(a.batch_instances, a.sampler))
             except Exception as e:  # reported, never fatal for the GPU numbers
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     del films

@@ -192,6 +192,23 @@ class Context:
         self.check(self._lib.gyt_sobol(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
         return out
 
+    def halton(self, dims, indices):
+        """HaltonSampler with Faure permutations (sampler/Halton.h) for
+        (dimension, index) pairs; dimensions >= 256 give 0."""
+        d = np.ascontiguousarray(dims, np.uint32)
+        i = np.ascontiguousarray(indices, np.uint64)
+        out = np.empty(d.shape[0], np.float32)
+        self.check(self._lib.gyt_halton(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
+        return out
+
+    def halton_enum_index(self, res_x, res_y, s, x, y):
+        """HaltonEnum::GetIndex (sampler/HaltonEnum.h) for (s, x, y)."""
+        sxy = np.ascontiguousarray(np.stack([np.asarray(s), np.asarray(x), np.asarray(y)], 1), np.uint32)
+        out = np.empty(sxy.shape[0], np.uint64)
+        self.check(self._lib.gyt_halton_enum_index(self.handle, res_x, res_y, sxy.shape[0], _c.ptr(sxy),
+                                                   _c.ptr(out)))
+        return out
+
     def sobol_enum_index(self, res_x, res_y, s, x, y):
         """SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for (s, x, y)."""
         sxy = np.ascontiguousarray(np.stack([np.asarray(s), np.asarray(x), np.asarray(y)], 1), np.uint32)
@@ -325,12 +342,16 @@ class PinHoleCamera:
 
 
 class GpuPathTracing:
-    """Drop-in for PathTracing(spp, maxDepth, SobolSampler, SobolEnum)
+    """Drop-in for PathTracing(spp, maxDepth, sampler, samplerEnum)
     (integrator/PT.h:12). ``rr_depth``: roulette applies at bounce i > rr_depth
-    (the reference hard-codes 5, integrator/PT.cpp:53)."""
+    (the reference hard-codes 5, integrator/PT.cpp:53). ``sampler``: "sobol"
+    (SobolSampler + SobolEnum) or "halton" (HaltonSampler with Faure
+    permutations + HaltonEnum)."""
 
-    def __init__(self, spp, max_depth, rr_depth=5, ctx: Context = None):
-        self.params = RenderParams(int(spp), int(max_depth), int(rr_depth))
+    def __init__(self, spp, max_depth, rr_depth=5, ctx: Context = None, sampler="sobol"):
+        if sampler not in _c.SAMPLERS:
+            raise ValueError("sampler must be one of %s" % sorted(_c.SAMPLERS))
+        self.params = RenderParams(int(spp), int(max_depth), int(rr_depth), sampler)
         self.ctx = ctx
 
     def Render(self, scene: Scene, camera: PinHoleCamera):

@@ -20,7 +20,8 @@ EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_c
            "gyt_context_set_profile", "gyt_profile_read", "gyt_context_set_bvh_width",
            "gyt_context_set_bvh_builder", "gyt_scene_create", "gyt_scene_destroy", "gyt_scene_info",
            "gyt_scene_read_bvh", "gyt_render", "gyt_render_device",
-           "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_camera_raster_to_world",
+           "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_halton",
+           "gyt_halton_enum_index", "gyt_camera_raster_to_world",
            "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
            "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune", "gyt_scene_set_materials",
            "gyt_diff_forward", "gyt_diff_backward", "gyt_diff_backward_paths"]
@@ -31,6 +32,10 @@ BVH_BUILD_DEVICE = 1
 
 # gyt_scene_set_materials flags
 KEEP_LIGHT_SAMPLING = 1
+
+# GytRenderParams.flags: HaltonSampler + HaltonEnum instead of Sobol' (GYT_SAMPLER_HALTON).
+SAMPLER_HALTON = 1
+SAMPLERS = {"sobol": 0, "halton": SAMPLER_HALTON}
 
 # Path slots of the library's built-in scratch array (GYT_NOALLOC_MAX_PATHS in include/gyt.h).
 NOALLOC_MAX_PATHS = 32768
@@ -120,6 +125,8 @@ def load():
     L.gyt_intersect.argtypes = [P, P, U64, P, I32, P, P, P, P]
     L.gyt_sobol.argtypes = [P, U64, P, P, P]
     L.gyt_sobol_enum_index.argtypes = [P, U32, U32, U64, P, P]
+    L.gyt_halton.argtypes = [P, U64, P, P, P]
+    L.gyt_halton_enum_index.argtypes = [P, U32, U32, U64, P, P]
     L.gyt_camera_raster_to_world.argtypes = [ctypes.POINTER(GytCamera), P]
     L.gyt_scene_set_materials.argtypes = [P, P, P, U32]
     L.gyt_diff_forward.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, P,
@@ -159,7 +166,7 @@ def camera_struct(cam):
 
 
 def params_struct(p):
-    return GytRenderParams(p.spp, p.max_depth, p.rr_depth, 0)
+    return GytRenderParams(p.spp, p.max_depth, p.rr_depth, SAMPLERS[getattr(p, "sampler", "sobol")])
 
 
 def scene_struct(sd):

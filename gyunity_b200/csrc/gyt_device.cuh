@@ -62,11 +62,13 @@ GYT_D float next_down(float v) {
 }
 
 // ---------------------------------------------------------------- Sobol ---
-struct SobolTables {
+struct SamplerTables {
   const uint32_t* matrices;   // 1024 * 52 (+ padding) generator columns
   const uint64_t* vdc;        // m levels * 52
   const uint64_t* vdc_inv;    // m levels * 52
   const uint32_t* bits;       // transposed: column b of every dimension, kSobolRow per b
+  const uint16_t* hperm;      // Halton digit-block tables of dimensions 1..255, concatenated
+  const uint4* hdesc;         // per Halton dimension: table offset, block size, blocks, scale bits
 };
 
 // Transposed generator table: row b holds column b of dimensions 0..1039 (the
@@ -115,7 +117,7 @@ GYT_D float sobol_sample(const uint32_t* __restrict__ mat, uint64_t index, uint3
 }
 
 // SobolEnum::look_up (sampler/SobolEnum.h:42-72), zero scrambles.
-GYT_D uint64_t enum_index(const SobolTables& t, uint32_t m, uint32_t frame, uint32_t px, uint32_t py) {
+GYT_D uint64_t enum_index(const SamplerTables& t, uint32_t m, uint32_t frame, uint32_t px, uint32_t py) {
   if (m == 0) return 0;
   uint64_t index = (uint64_t)frame << (2u * m);
   const uint64_t* fw = t.vdc + (m - 1) * 52u;
@@ -132,13 +134,60 @@ GYT_D uint64_t enum_index(const SobolTables& t, uint32_t m, uint32_t frame, uint
   return index;
 }
 
+// --------------------------------------------------------------- Halton ---
+// HaltonSampler with Faure permutations (sampler/Halton.h): dimension d is
+// the radical inverse of the index in the d-th prime b with every digit
+// mapped through Faure's permutation of {0..b-1}. hdesc[d] = (offset of the
+// dimension's table in hperm, block size B = b^k, blocks n, scale bits): the
+// table maps k digits at once, least significant index digit to the most
+// significant place; the n block values are summed exactly (below 2^32) and
+// scaled by float((1 - 2^-23) / B^n). Dimension 0 (base 2) writes the
+// reversed index bits into a float mantissa; dimensions >= 256 give 0
+// (Halton.h:648-905).
+constexpr uint32_t kHaltonDims = 256;
+
+GYT_D float halton_sample(const SamplerTables& t, uint64_t index, uint32_t dim) {
+  if (dim == 0) return __fsub_rn(__uint_as_float(0x3f800000u | (uint32_t)(__brevll(index) >> 41)), 1.f);
+  if (dim >= kHaltonDims) return 0.f;
+  const uint4 d = __ldg(t.hdesc + dim);
+  const uint16_t* tab = t.hperm + d.x;
+  uint32_t v = 0;
+  if ((index >> 32) == 0) {
+    uint32_t q = (uint32_t)index;
+    for (uint32_t j = 0; j < d.z; ++j) {
+      const uint32_t nq = q / d.y;
+      v = v * d.y + __ldg(tab + (q - nq * d.y));
+      q = nq;
+    }
+  } else {
+    uint64_t q = index;
+    for (uint32_t j = 0; j < d.z; ++j) {
+      const uint64_t nq = q / d.y;
+      v = v * d.y + __ldg(tab + (uint32_t)(q - nq * d.y));
+      q = nq;
+    }
+  }
+  return __fmul_rn(__uint2float_rn(v), __uint_as_float(d.w));
+}
+
+// Ten consecutive Halton dimensions [c, c + 10) (RandomStateSequence's
+// >= 1 -> 0 rule applied).
+GYT_D void halton10(const SamplerTables& t, uint64_t index, uint32_t c, float out[10]) {
+#pragma unroll 1
+  for (int k = 0; k < 10; ++k) {
+    const float f = halton_sample(t, index, c + k);
+    out[k] = f >= 1.f ? 0.f : f;
+  }
+}
+
 // RandomStateSequence (sampler/Sampler.h:42-66): one dimension per call,
 // values >= 1 become 0.
 struct Rng {
   uint64_t index;
   uint32_t cursor;
-  GYT_D float next(const uint32_t* __restrict__ mat) {
-    float r = sobol_sample(mat, index, cursor++);
+  GYT_D float next(const SamplerTables& t, uint32_t sampler) {
+    float r = sampler ? halton_sample(t, index, cursor) : sobol_sample(t.matrices, index, cursor);
+    ++cursor;
     return r >= 1.f ? 0.f : r;
   }
 };
@@ -149,7 +198,27 @@ struct Cam {
   float3 pos;
   uint32_t res_x, res_y, log2_res;
   float res_pow2;   // SobolEnum's padded resolution (SobolEnum.h:17-21)
+  uint32_t sampler; // 0 SobolSampler + SobolEnum, 1 HaltonSampler + HaltonEnum
+  // HaltonEnum (sampler/HaltonEnum.h): 2^p2 >= res_x, 3^p3 >= res_y, the
+  // Chinese-remainder multipliers and the index increment 2^p2 3^p3
+  uint32_t h_p2, h_p3;
+  float h_sx, h_sy;  // 2^p2, 3^p3
+  unsigned long long h_mx, h_my, h_inc;
 };
+
+// HaltonEnum::get_index: the index congruent to the base-2 digit reversal of
+// x modulo 2^p2 and the base-3 digit reversal of y modulo 3^p3, plus s times
+// the increment.
+GYT_D uint64_t halton_enum_index(const Cam& c, uint32_t s, uint32_t x, uint32_t y) {
+  const uint64_t hx = c.h_p2 ? (__brevll((unsigned long long)x) >> (64u - c.h_p2)) : 0ull;
+  uint64_t hy = 0;
+  uint32_t q = y;
+  for (uint32_t d = 0; d < c.h_p3; ++d) {
+    hy = hy * 3u + q % 3u;
+    q /= 3u;
+  }
+  return (hx * c.h_mx + hy * c.h_my) % c.h_inc + (uint64_t)s * c.h_inc;
+}
 
 // PinHoleCamera::GenerateRay (camera/PinholeCamera.h:22-29) + the Ray
 // constructor's RayEps shift (math/Ray.h:17-18).

@@ -114,6 +114,7 @@ constexpr uint32_t kPendValid = 1u << 31;
 
 struct Params {
   uint32_t spp, max_depth, rr_depth;
+  uint32_t sampler;  // 0 Sobol', 1 Halton (GYT_SAMPLER_HALTON)
 };
 
 // Per-path replay record, indexed by path id (explicit path lists only).
@@ -532,13 +533,15 @@ GYT_D float tri_light_pdf(const LightTri& l, const Hit& h, float3 o, float3 wi) 
 // -------------------------------------------------------------- kernels ---
 // Camera path of sample s in pixel (x, y) into slot k (TiledIntegrator::Render
 // body, integrator/TiledIntegrator.cpp:37-48).
-GYT_D void gen_path(PathBuf& dst, uint32_t k, uint32_t x, uint32_t y, uint32_t s, const Cam& cam, SobolTables tab) {
-  uint64_t idx = enum_index(tab, cam.log2_res, s, x, y);
+GYT_D void gen_path(PathBuf& dst, uint32_t k, uint32_t x, uint32_t y, uint32_t s, const Cam& cam, SamplerTables tab) {
+  const bool halton = cam.sampler != 0;
+  uint64_t idx = halton ? halton_enum_index(cam, s, x, y) : enum_index(tab, cam.log2_res, s, x, y);
   Rng rng{idx, 0};
-  float su = rng.next(tab.matrices), sv = rng.next(tab.matrices);
-  // SobolEnum::SampleX/Y (SobolEnum.h:30-36), kept unfused as the reference
-  float u = __fsub_rn(__fmul_rn(cam.res_pow2, su), (float)x);
-  float v = __fsub_rn(__fmul_rn(cam.res_pow2, sv), (float)y);
+  float su = rng.next(tab, cam.sampler), sv = rng.next(tab, cam.sampler);
+  // SobolEnum::SampleX/Y (SobolEnum.h:30-36) or HaltonEnum::scale_x/y, kept
+  // unfused as the reference
+  float u = __fsub_rn(__fmul_rn(halton ? cam.h_sx : cam.res_pow2, su), (float)x);
+  float v = __fsub_rn(__fmul_rn(halton ? cam.h_sy : cam.res_pow2, sv), (float)y);
   float3 o, d;
   camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
   dst.o[k] = make_float4(o.x, o.y, o.z, 0.f);
@@ -553,7 +556,7 @@ GYT_D void gen_path(PathBuf& dst, uint32_t k, uint32_t x, uint32_t y, uint32_t s
 
 __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base, uint32_t n_new,
                                                      unsigned long long first, Cam cam, uint32_t spp,
-                                                     const uint32_t* __restrict__ list, SobolTables tab) {
+                                                     const uint32_t* __restrict__ list, SamplerTables tab) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_new) return;
   unsigned long long p = first + j;
@@ -654,7 +657,7 @@ GYT_D void grad_emitter(const GradOut& G, const DevScene& s, int li, float3 Cd) 
 // MIS kernel.
 template <bool ADJ, bool DEFER = false>
 GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
-                      SobolTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
+                      SamplerTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   float4 h4 = q.hit[i];
   int prim = __float_as_int(h4.w);
   uint32_t meta = cur.meta[i];
@@ -704,7 +707,8 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     // arguments in GCC's right-to-left order: v.z v.y v.x u.y u.x uLight), three
     // for the BSDF sample (PT.cpp:47, again z y x) and one for roulette
     float u10[10];
-    sobol10(tab.bits, rng.index, rng.cursor, u10);
+    if (prm.sampler) halton10(tab, rng.index, rng.cursor, u10);
+    else sobol10(tab.bits, rng.index, rng.cursor, u10);
     const bool emit = (depth == 0 || delta) && light >= 0;
     if (emit) {
       LightTri l = load_light(s, light);
@@ -838,7 +842,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
-                                                  SobolTables tab, DebugOut dbg) {
+                                                  SamplerTables tab, DebugOut dbg) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   shade_path<false, true>(cur, i, s, prm, q, tab, dbg);
@@ -1006,7 +1010,7 @@ struct AdjIn {
 
 __global__ void __launch_bounds__(kBlock) k_generate_adj(PathBuf dst, AdjBuf A, uint32_t base, uint32_t n_new,
                                                          unsigned long long first, Cam cam, uint32_t spp,
-                                                         const uint32_t* __restrict__ list, SobolTables tab,
+                                                         const uint32_t* __restrict__ list, SamplerTables tab,
                                                          AdjIn in) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_new) return;
@@ -1053,7 +1057,7 @@ __global__ void __launch_bounds__(kBlock) k_generate_adj(PathBuf dst, AdjBuf A, 
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade_adj(PathBuf cur, AdjBuf A, uint32_t n, DevScene s, Params prm,
-                                                      Queues q, SobolTables tab, GradOut G) {
+                                                      Queues q, SamplerTables tab, GradOut G) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   shade_path<true>(cur, i, s, prm, q, tab, DebugOut{}, A, G);
@@ -1171,7 +1175,7 @@ __global__ void k_batch_begin(IterState* __restrict__ st, uint32_t* __restrict__
 }
 
 __global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const IterState* __restrict__ st,
-                                                           SobolTables tab) {
+                                                           SamplerTables tab) {
   const uint32_t n_new = st->n_new, base = st->active, ni = st->n_inst;
   const unsigned long long first = st->generated;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_new; j += gridDim.x * blockDim.x) {
@@ -1221,7 +1225,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const Iter
 // the live count return at once): the work per path varies a lot, and the
 // block scheduler balances it far better than a grid-stride loop does.
 __global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q,
-                                                        SobolTables tab) {
+                                                        SamplerTables tab) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= st->n) return;
   const Inst& I = c_insts[cur.inst[i]];
@@ -1361,7 +1365,19 @@ __global__ void k_sobol(const uint32_t* __restrict__ mat, uint64_t n, const uint
   out[i] = sobol_sample(mat, idx[i], dims[i]);
 }
 
-__global__ void k_enum(SobolTables tab, uint32_t m, uint64_t n, const uint32_t* sxy, uint64_t* out) {
+__global__ void k_halton(SamplerTables tab, uint64_t n, const uint32_t* dims, const uint64_t* idx, float* out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = halton_sample(tab, idx[i], dims[i]);
+}
+
+__global__ void k_halton_enum(Cam cam, uint64_t n, const uint32_t* sxy, uint64_t* out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = halton_enum_index(cam, sxy[3 * i], sxy[3 * i + 1], sxy[3 * i + 2]);
+}
+
+__global__ void k_enum(SamplerTables tab, uint32_t m, uint64_t n, const uint32_t* sxy, uint64_t* out) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   out[i] = enum_index(tab, m, sxy[3 * i], sxy[3 * i + 1], sxy[3 * i + 2]);
@@ -1440,6 +1456,8 @@ struct gyt_context {
   uint32_t* h_counter = nullptr;
   uint32_t* d_sobol = nullptr;
   uint32_t* d_sobol_bits = nullptr;
+  uint16_t* d_hperm = nullptr;  // Halton digit-block tables (halton_tables)
+  uint4* d_hdesc = nullptr;
   uint64_t* d_vdc = nullptr;
   uint64_t* d_vdc_inv = nullptr;
   double* d_film = nullptr;
@@ -1517,7 +1535,13 @@ cudaError_t after_legacy_stream(gyt_context* ctx) {
   return e;
 }
 
-SobolTables tables(const gyt_context* c) { return SobolTables{c->d_sobol, c->d_vdc, c->d_vdc_inv, c->d_sobol_bits}; }
+SamplerTables tables(const gyt_context* c) {
+  return SamplerTables{c->d_sobol, c->d_vdc, c->d_vdc_inv, c->d_sobol_bits, c->d_hperm, c->d_hdesc};
+}
+
+Params make_params(const GytRenderParams* p) {
+  return Params{p->spp, p->max_depth, p->rr_depth, (p->flags & GYT_SAMPLER_HALTON) ? 1u : 0u};
+}
 
 // ProjectiveCamera::Initialize (camera/Camera.cpp:6-59): RasterToWorld in
 // closed form, in double. Raster (x, y, z, 1) -> NDC (2x/W - 1, 1 - 2y/H, z)
@@ -1552,15 +1576,104 @@ void raster_to_world(const GytCamera& c, double m[16]) {
     }
 }
 
-int32_t make_cam(gyt_context* ctx, const GytCamera* c, Cam* out) {
+// Digit-block tables of HaltonSampler with Faure permutations
+// (sampler/Halton.h:595-625 builds the permutations, :912-1435 the tables).
+// Faure's permutation of {0..b-1}: identity for b <= 3; for even b the
+// permutation of b/2 doubled into the even and the odd half; for odd b the
+// permutation of b - 1 with the middle value c = (b-1)/2 inserted at c (values
+// and positions from c on move up by one). Dimension d >= 1 uses the d-th
+// prime b, blocks of k digits (the largest k with b^k <= 512) through a table
+// of B = b^k entries, as many whole blocks n as keep B^n below 2^32.
+void halton_tables(std::vector<uint16_t>* perm_out, std::vector<uint4>* desc_out) {
+  constexpr uint32_t kMaxBase = 1619;  // the 256th prime
+  std::vector<std::vector<uint16_t>> fp(kMaxBase + 1);
+  for (uint32_t b = 1; b <= kMaxBase; ++b) {
+    std::vector<uint16_t>& q = fp[b];
+    q.resize(b);
+    if (b <= 3) {
+      for (uint32_t i = 0; i < b; ++i) q[i] = (uint16_t)i;
+    } else if (b % 2 == 0) {
+      const std::vector<uint16_t>& h = fp[b / 2];
+      for (uint32_t i = 0; i < b / 2; ++i) {
+        q[i] = (uint16_t)(2 * h[i]);
+        q[b / 2 + i] = (uint16_t)(2 * h[i] + 1);
+      }
+    } else {
+      const uint32_t c = b / 2;
+      const std::vector<uint16_t>& h = fp[b - 1];
+      for (uint32_t i = 0; i < b - 1; ++i) q[i < c ? i : i + 1] = (uint16_t)(h[i] < c ? h[i] : h[i] + 1);
+      q[c] = (uint16_t)c;
+    }
+  }
+  perm_out->clear();
+  desc_out->assign(kHaltonDims, make_uint4(0, 0, 0, 0));
+  uint32_t b = 2;
+  for (uint32_t d = 1; d < kHaltonDims; ++d) {
+    for (++b;; ++b) {
+      bool prime = true;
+      for (uint32_t f = 2; f * f <= b && prime; ++f) prime = b % f != 0;
+      if (prime) break;
+    }
+    uint32_t k = 1;
+    uint64_t B = b;
+    while (B * b <= 512) { B *= b; ++k; }
+    uint32_t n = 0;
+    uint64_t Bn = 1;
+    while (Bn * B < (1ull << 32)) { Bn *= B; ++n; }
+    const float scale = (float)(0x1.fffffcp-1 / (double)Bn);
+    uint32_t bits;
+    std::memcpy(&bits, &scale, 4);
+    (*desc_out)[d] = make_uint4((uint32_t)perm_out->size(), (uint32_t)B, n, bits);
+    for (uint32_t i = 0; i < B; ++i) {
+      uint32_t r = 0, q = i;
+      for (uint32_t j = 0; j < k; ++j, q /= b) r = r * b + fp[b][q % b];
+      perm_out->push_back((uint16_t)r);
+    }
+  }
+}
+
+// a^-1 mod m in [0, m), 0 for m == 1 (extended Euclidean algorithm)
+uint64_t inverse_mod(int64_t a, int64_t m) {
+  if (m == 1) return 0;
+  int64_t r0 = m, r1 = a % m, s0 = 0, s1 = 1;
+  while (r1) {
+    const int64_t q = r0 / r1;
+    int64_t t = r0 - q * r1;
+    r0 = r1;
+    r1 = t;
+    t = s0 - q * s1;
+    s0 = s1;
+    s1 = t;
+  }
+  return (uint64_t)(((s0 % m) + m) % m);
+}
+
+// The camera and the sample enumeration of the render's sampler
+// (params->flags: GYT_SAMPLER_HALTON selects HaltonSampler + HaltonEnum).
+int32_t make_cam(gyt_context* ctx, const GytCamera* c, const GytRenderParams* prm, Cam* out) {
   if (!c || c->res_x == 0 || c->res_y == 0) return fail(ctx, GYT_ERR_INVALID, "camera: empty film");
   if ((uint64_t)c->res_x * c->res_y > kPixMask) return fail(ctx, GYT_ERR_UNSUPPORTED, "camera: film too large");
+  *out = Cam{};
   double m[16];
   raster_to_world(*c, m);
   for (int i = 0; i < 16; ++i) out->m[i] = (float)m[i];
   out->pos = mk(c->pos[0], c->pos[1], c->pos[2]);
   out->res_x = c->res_x;
   out->res_y = c->res_y;
+  out->sampler = (prm && (prm->flags & GYT_SAMPLER_HALTON)) ? 1u : 0u;
+  if (out->sampler) {
+    // HaltonEnum::HaltonEnum (sampler/HaltonEnum.h): the film padded to 2^p2 x 3^p3
+    uint64_t w = 1, h = 1;
+    while (w < c->res_x) { w *= 2; ++out->h_p2; }
+    while (h < c->res_y) { h *= 3; ++out->h_p3; }
+    if (w * h >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "camera: film too large for HaltonEnum");
+    out->h_sx = (float)w;
+    out->h_sy = (float)h;
+    out->h_inc = w * h;
+    out->h_mx = h * inverse_mod((int64_t)h, (int64_t)w);
+    out->h_my = w * inverse_mod((int64_t)w, (int64_t)h);
+    return GYT_OK;
+  }
   uint32_t r = std::max(c->res_x, c->res_y), p = 1, lg = 0;
   while (p < r) { p <<= 1; ++lg; }
   if (lg > GYT_ENUM_M) return fail(ctx, GYT_ERR_UNSUPPORTED, "camera: resolution beyond the Sobol' enumeration tables");
@@ -1597,7 +1710,7 @@ int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
   if (p->max_depth == 0 || p->max_depth > 100)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "params: max_depth must be in [1, 100] (Sobol' has 1024 dimensions)");
   if (p->rr_depth > 255) return fail(ctx, GYT_ERR_INVALID, "params: rr_depth too large");
-  if (p->flags != 0) return fail(ctx, GYT_ERR_INVALID, "params: flags must be 0");
+  if (p->flags & ~GYT_SAMPLER_HALTON) return fail(ctx, GYT_ERR_INVALID, "params: unknown flags");
   return GYT_OK;
 }
 
@@ -1668,8 +1781,8 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
                   GytRenderStats* stats) {
   int32_t st = ensure_pool(ctx);
   if (st) return st;
-  Params prm{p->spp, p->max_depth, p->rr_depth};
-  SobolTables tab = tables(ctx);
+  Params prm = make_params(p);
+  SamplerTables tab = tables(ctx);
   cudaStream_t s = ctx->stream;
   unsigned long long generated = 0;
   uint32_t active = 0, iters = 0;
@@ -1774,8 +1887,8 @@ int32_t run_adjoint(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, co
   if (st) return st;
   st = ensure_adj(ctx);
   if (st) return st;
-  const Params prm{p->spp, p->max_depth, p->rr_depth};
-  const SobolTables tab = tables(ctx);
+  const Params prm = make_params(p);
+  const SamplerTables tab = tables(ctx);
   cudaStream_t s = ctx->stream;
   const int W = scene->dev.wnodes ? 8 : 2;
   const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)],
@@ -1856,6 +1969,15 @@ int32_t gyt_context_create(int32_t device, gyt_context** out) {
     e = cudaMalloc((void**)&c->d_sobol_bits, tr.size() * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_sobol_bits, tr.data(), tr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
   }
+  std::vector<uint16_t> hperm;
+  std::vector<uint4> hdesc;
+  halton_tables(&hperm, &hdesc);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_hperm, hperm.size() * sizeof(uint16_t));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->d_hperm, hperm.data(), hperm.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_hdesc, hdesc.size() * sizeof(uint4));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->d_hdesc, hdesc.data(), hdesc.size() * sizeof(uint4), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc, sizeof(gyt_vdc_sobol));
   if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_vdc, gyt_vdc_sobol, sizeof(gyt_vdc_sobol), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_vdc_inv, sizeof(gyt_vdc_sobol_inv));
@@ -1913,6 +2035,8 @@ void gyt_context_destroy(gyt_context* c) {
   cudaFreeHost(c->h_counter);
   cudaFree(c->d_sobol);
   cudaFree(c->d_sobol_bits);
+  cudaFree(c->d_hperm);
+  cudaFree(c->d_hdesc);
   cudaFree(c->d_vdc);
   cudaFree(c->d_vdc_inv);
   cudaFree(c->d_film);
@@ -2380,7 +2504,7 @@ int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCam
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
@@ -2425,7 +2549,7 @@ int32_t gyt_trace_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamer
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   if (n == 0) return GYT_OK;
   if (n >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "trace_paths: too many paths");
@@ -2464,7 +2588,7 @@ int32_t gyt_diff_forward(gyt_context* ctx, const gyt_scene* scene, const GytCame
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
@@ -2481,7 +2605,7 @@ int32_t gyt_diff_backward(gyt_context* ctx, const gyt_scene* scene, const GytCam
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
@@ -2499,7 +2623,7 @@ int32_t gyt_diff_backward_paths(gyt_context* ctx, const gyt_scene* scene, const 
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   if (n >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "diff_backward_paths: too many paths");
   for (uint64_t i = 0; i < n; ++i)
@@ -2598,6 +2722,63 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
   return GYT_OK;
 }
 
+int32_t gyt_halton(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out) {
+  if (!ctx || (n && (!dims || !indices || !out))) return fail(ctx, GYT_ERR_INVALID, "halton: null argument");
+  if (n == 0) return GYT_OK;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* p : v) cudaFree(p); }
+  } guard{tmp};
+  uint32_t* dd = nullptr;
+  uint64_t* di = nullptr;
+  float* dout = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dd, n));
+  GYT_CK(ctx, dalloc(tmp, &di, n));
+  GYT_CK(ctx, dalloc(tmp, &dout, n));
+  GYT_CK(ctx, cudaMemcpyAsync(dd, dims, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(di, indices, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  k_halton<<<grid_for(n), kBlock, 0, ctx->stream>>>(tables(ctx), n, dd, di, dout);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  GYT_CK(ctx, cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
+int32_t gyt_halton_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n, const uint32_t* sxy,
+                              uint64_t* out) {
+  if (!ctx || (n && (!sxy || !out))) return fail(ctx, GYT_ERR_INVALID, "halton_enum_index: null argument");
+  GytCamera c = {};
+  c.res_x = res_x;
+  c.res_y = res_y;
+  c.fovy = 53.13f;
+  c.film_distance = 1.f;
+  c.look_at[2] = -1.f;
+  c.up[1] = 1.f;
+  GytRenderParams prm = {1, 1, 0, GYT_SAMPLER_HALTON};
+  Cam cam;
+  int32_t st = make_cam(ctx, &c, &prm, &cam);
+  if (st) return st;
+  if (n == 0) return GYT_OK;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  uint32_t* ds = nullptr;
+  uint64_t* dout = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &ds, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dout, n));
+  GYT_CK(ctx, cudaMemcpyAsync(ds, sxy, 3 * n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  k_halton_enum<<<grid_for(n), kBlock, 0, ctx->stream>>>(cam, n, ds, dout);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  GYT_CK(ctx, cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n, const uint32_t* sxy,
                              uint64_t* out) {
   if (!ctx || (n && (!sxy || !out))) return fail(ctx, GYT_ERR_INVALID, "sobol_enum_index: null argument");
@@ -2677,7 +2858,7 @@ cudaError_t enqueue_half(gyt_context* ctx, const BatchPlan& b, const PathBuf& P,
                          cudaGraphConditionalHandle cond, int in_graph, cudaEvent_t* ev = nullptr) {
   cudaStream_t s = ctx->stream;
   const Queues q = ctx->q;
-  const SobolTables tab = tables(ctx);
+  const SamplerTables tab = tables(ctx);
   IterState* st = ctx->d_iter;
   k_batch_begin<<<1, 32, 0, s>>>(st, q.counts);
   if (ev) cudaEventRecord(ev[0], s);
@@ -2762,12 +2943,12 @@ int32_t batch_input(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes
     int32_t st = check_params(ctx, &params[i]);
     if (st) return st;
     Inst& I = in->insts[i];
-    st = make_cam(ctx, &cameras[i], &I.cam);
+    st = make_cam(ctx, &cameras[i], &params[i], &I.cam);
     if (st) return st;
     const unsigned long long np = (unsigned long long)cameras[i].res_x * cameras[i].res_y * params[i].spp;
     if (np >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: more than 2^32 paths in one instance");
     I.s = sc->dev;
-    I.prm = Params{params[i].spp, params[i].max_depth, params[i].rr_depth};
+    I.prm = make_params(&params[i]);
     I.film = films[i];
     I.first = in->total;
     in->total += np;
@@ -3102,7 +3283,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
-  st = make_cam(ctx, camera, &cam);
+  st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
@@ -3136,8 +3317,8 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   if ((size_t)(c - base) > kNoAllocBytes)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: scratch layout exceeds the array");
 
-  Params prm{params->spp, params->max_depth, params->rr_depth};
-  SobolTables tab = tables(ctx);
+  Params prm = make_params(params);
+  SamplerTables tab = tables(ctx);
   cudaStream_t s = ctx->stream;
   const int W = scene->dev.wnodes ? 8 : 2;
   const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)], g_sh = ctx->pgrid[pindex(kPShadow, W, false)];

@@ -61,6 +61,7 @@ class RenderParams:
     spp: int = 16
     max_depth: int = 8
     rr_depth: int = 5   # Russian roulette applies when bounce index i > rr_depth (reference: 5)
+    sampler: str = "sobol"  # "sobol" (SobolSampler + SobolEnum) or "halton" (HaltonSampler + HaltonEnum)
 
 
 @dataclasses.dataclass

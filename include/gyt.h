@@ -86,13 +86,19 @@ typedef struct {
   uint32_t res_x, res_y;
 } GytCamera;
 
-/* PathTracing(spp, maxDepth, SobolSampler, SobolEnum) (integrator/PT.h:12).
+/* PathTracing(spp, maxDepth, sampler, samplerEnum) (integrator/PT.h:12).
  * Russian roulette is applied at bounce i when i > rr_depth (the reference
- * hard-codes 5 at integrator/PT.cpp:53). */
+ * hard-codes 5 at integrator/PT.cpp:53). The sampler is SobolSampler +
+ * SobolEnum unless flags holds GYT_SAMPLER_HALTON. */
 typedef struct {
   uint32_t spp, max_depth, rr_depth;
-  uint32_t flags;                 /* reserved, must be 0 */
+  uint32_t flags;                 /* GYT_SAMPLER_* bits; other bits must be 0 */
 } GytRenderParams;
+
+/* HaltonSampler with Faure permutations + HaltonEnum (sampler/Halton.h,
+ * sampler/HaltonEnum.h), as the demo driver builds them
+ * (Gyunity_exe/main.cpp:134-137): 256 dimensions, later dimensions give 0. */
+#define GYT_SAMPLER_HALTON 1u
 
 /* Per-render statistics filled by gyt_render_device. */
 typedef struct {
@@ -196,6 +202,14 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 /* SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for n (s, x, y) triplets. */
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
+
+/* HaltonSampler::sample with Faure permutations (sampler/Halton.h:648-905)
+ * for n (dimension, index) pairs; dimensions >= 256 give 0. */
+int32_t gyt_halton(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out);
+
+/* HaltonEnum::GetIndex (sampler/HaltonEnum.h) for n (s, x, y) triplets. */
+int32_t gyt_halton_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
+                              const uint32_t* sxy, uint64_t* out);
 
 /* ---- Differentiable rendering (path replay backpropagation) ---------------
  * Gradients of an image loss with respect to every material's albedo a

@@ -44,7 +44,8 @@ class CameraIn(ctypes.Structure):
 
 
 class ParamsIn(ctypes.Structure):
-    _fields_ = [("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32)]
+    _fields_ = [("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32),
+                ("sampler", ctypes.c_uint32)]
 
 
 _lib = None
@@ -60,6 +61,10 @@ def lib():
         L.gyo_sobol.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
         L.gyo_enum_index.restype = ctypes.c_uint64
         L.gyo_enum_index.argtypes = [ctypes.c_uint32] * 5
+        L.gyo_halton.restype = ctypes.c_float
+        L.gyo_halton.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
+        L.gyo_halton_enum_index.restype = ctypes.c_uint64
+        L.gyo_halton_enum_index.argtypes = [ctypes.c_uint32] * 5
         L.gyo_raster_to_world.argtypes = [ctypes.POINTER(CameraIn), ctypes.c_void_p]
         L.gyo_scene_create.restype = ctypes.c_void_p
         L.gyo_scene_create.argtypes = [ctypes.POINTER(SceneIn)]
@@ -104,8 +109,11 @@ def camera_in(cam):
     return c
 
 
+SAMPLERS = {"sobol": 0, "halton": 1}
+
+
 def params_in(p):
-    return ParamsIn(p.spp, p.max_depth, p.rr_depth)
+    return ParamsIn(p.spp, p.max_depth, p.rr_depth, SAMPLERS[getattr(p, "sampler", "sobol")])
 
 
 class OracleScene:
@@ -233,6 +241,18 @@ def sobol(dims, indices):
 def enum_index(res_x, res_y, s, x, y):
     L = lib()
     return np.array([L.gyo_enum_index(res_x, res_y, int(a), int(b), int(c)) for a, b, c in zip(s, x, y)], np.uint64)
+
+
+def halton(dims, indices):
+    """HaltonSampler (Faure permutations) for (dim, index) pairs."""
+    L = lib()
+    return np.array([L.gyo_halton(int(d), int(i)) for d, i in zip(dims, indices)], np.float32)
+
+
+def halton_enum_index(res_x, res_y, s, x, y):
+    L = lib()
+    return np.array([L.gyo_halton_enum_index(res_x, res_y, int(a), int(b), int(c)) for a, b, c in zip(s, x, y)],
+                    np.uint64)
 
 
 def raster_to_world(cam):

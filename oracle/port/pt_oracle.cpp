@@ -115,13 +115,157 @@ inline uint32_t log2_pow2_res(uint32_t rx, uint32_t ry) {  // SobolEnum ctor, So
   return m;
 }
 
+// --------------------------------------------------------------- Halton ---
+// HaltonSampler with Faure permutations (sampler/Halton.h, generated code):
+// dimension d is the radical inverse in the d-th prime b with every digit
+// mapped through Faure's permutation of {0..b-1}. The digits are processed k
+// at a time through a table of b^k entries (k = 5, 3, 3, 2, 2, 2, 2 for
+// b = 3..19, else 1: the largest k with b^k <= 512, Halton.h:925-1435), n
+// blocks of k digits in all (the most whole blocks with b^(n k) < 2^32),
+// summed exactly in integers and scaled by float((1 - 2^-23) / b^(n k))
+// (Halton.h:1455-3308). Base 2 writes the reversed index bits into a float
+// mantissa (Halton.h:1441-1452). Dimensions >= 256 give 0 (Halton.h:648-905).
+struct HaltonDim {
+  uint32_t base = 0, block = 0, blocks = 0;
+  float scale = 0.f;
+  std::vector<uint16_t> table;
+};
+
+struct HaltonTables {
+  std::vector<HaltonDim> dims;
+  HaltonTables() {
+    const uint32_t max_base = 1619;  // the 256th prime
+    // Faure permutations (Halton.h:595-625): identity for b <= 3; an even b
+    // doubles the permutation of b/2 into its even and odd halves, an odd b
+    // inserts the middle digit into the permutation of b - 1
+    std::vector<std::vector<uint16_t>> perm(max_base + 1);
+    for (uint32_t b = 1; b <= 3; ++b)
+      for (uint32_t i = 0; i < b; ++i) perm[b].push_back((uint16_t)i);
+    for (uint32_t b = 4; b <= max_base; ++b) {
+      perm[b].assign(b, 0);
+      const uint32_t c = b / 2;
+      if (b % 2 == 0) {
+        for (uint32_t i = 0; i < c; ++i) {
+          perm[b][i] = (uint16_t)(2 * perm[c][i]);
+          perm[b][c + i] = (uint16_t)(2 * perm[c][i] + 1);
+        }
+      } else {
+        for (uint32_t i = 0; i + 1 < b; ++i) {
+          const uint32_t v = perm[b - 1][i];
+          perm[b][i + (i >= c ? 1 : 0)] = (uint16_t)(v + (v >= c ? 1 : 0));
+        }
+        perm[b][c] = (uint16_t)c;
+      }
+    }
+    dims.resize(256);
+    uint32_t b = 1;
+    for (uint32_t d = 0; d < 256; ++d) {
+      do {
+        ++b;
+      } while (!is_prime(b));
+      HaltonDim& h = dims[d];
+      h.base = b;
+      if (b == 2) continue;
+      uint32_t k = 1;
+      while (pow_u64(b, k + 1) <= 512) ++k;
+      uint32_t digits = 0;
+      while (pow_u64(b, digits + 1) < (1ull << 32)) ++digits;
+      h.blocks = digits / k;
+      h.block = (uint32_t)pow_u64(b, k);
+      h.scale = (float)(0x1.fffffcp-1 / (double)pow_u64(b, k * h.blocks));
+      h.table.resize(h.block);
+      for (uint32_t i = 0; i < h.block; ++i) {  // HaltonSampler::invert (Halton.h:912-923)
+        uint32_t r = 0, q = i;
+        for (uint32_t j = 0; j < k; ++j) {
+          r = r * b + perm[b][q % b];
+          q /= b;
+        }
+        h.table[i] = (uint16_t)r;
+      }
+    }
+  }
+  static bool is_prime(uint32_t n) {
+    for (uint32_t q = 2; q * q <= n; ++q)
+      if (n % q == 0) return false;
+    return n >= 2;
+  }
+  static uint64_t pow_u64(uint64_t b, uint32_t e) {
+    uint64_t r = 1;
+    while (e--) r *= b;
+    return r;
+  }
+};
+
+const HaltonTables& halton_tables() {
+  static const HaltonTables t;
+  return t;
+}
+
+inline uint64_t reverse_bits64(uint64_t v) {
+  uint64_t r = 0;
+  for (int i = 0; i < 64; ++i, v >>= 1) r = (r << 1) | (v & 1);
+  return r;
+}
+
+inline float halton_sample(uint64_t index, uint32_t dim) {
+  if (dim == 0) {
+    const uint32_t bits = 0x3f800000u | (uint32_t)(reverse_bits64(index) >> 41);
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f - 1.f;
+  }
+  if (dim >= 256) return 0.f;
+  const HaltonDim& h = halton_tables().dims[dim];
+  uint64_t v = 0, q = index;
+  for (uint32_t j = 0; j < h.blocks; ++j) {
+    v = v * h.block + h.table[q % h.block];
+    q /= h.block;
+  }
+  return (float)v * h.scale;
+}
+
+// HaltonEnum (sampler/HaltonEnum.h): the film is padded to 2^p2 x 3^p3 and
+// sample i of pixel (x, y) is the index congruent to the base-2 digit
+// reversal of x modulo 2^p2 and the base-3 digit reversal of y modulo 3^p3
+// (Chinese remainder theorem), plus i times 2^p2 3^p3.
+struct HaltonEnumC {
+  uint32_t p2 = 0, p3 = 0, w = 1, h = 1;
+  uint64_t mx = 0, my = 0, inc = 1;
+  HaltonEnumC(uint32_t width, uint32_t height) {
+    while (w < width) { w *= 2; ++p2; }
+    while (h < height) { h *= 3; ++p3; }
+    inc = (uint64_t)(uint32_t)(w * h);
+    mx = (uint64_t)h * inverse_mod(h, w);
+    my = (uint64_t)w * inverse_mod(w, h);
+  }
+  // a^-1 mod m in [0, m) (0 when m == 1), by the extended Euclidean algorithm
+  static uint64_t inverse_mod(int64_t a, int64_t m) {
+    if (m == 1) return 0;
+    int64_t r0 = m, r1 = a % m, s0 = 0, s1 = 1;
+    while (r1) {
+      const int64_t qq = r0 / r1;
+      int64_t t = r0 - qq * r1; r0 = r1; r1 = t;
+      t = s0 - qq * s1; s0 = s1; s1 = t;
+    }
+    return (uint64_t)(((s0 % m) + m) % m);
+  }
+  uint64_t index(uint32_t i, uint32_t x, uint32_t y) const {
+    const uint64_t hx = p2 ? reverse_bits64(x) >> (64 - p2) : 0;
+    uint64_t hy = 0;
+    for (uint32_t d = 0, q = y; d < p3; ++d, q /= 3) hy = hy * 3 + q % 3;
+    return (hx * mx + hy * my) % inc + (uint64_t)i * inc;
+  }
+};
+
 // RandomStateSequence::Sample (sampler/Sampler.h:52-64): cursor++ per call,
-// values >= 1 become 0.
+// values >= 1 become 0. halton selects HaltonSampler instead of SobolSampler.
 struct Rand {
   uint64_t index;
   int cursor = 0;
+  bool halton = false;
   float next() {
-    float r = sobol_sample(index, (uint32_t)cursor++);
+    const uint32_t d = (uint32_t)cursor++;
+    float r = halton ? halton_sample(index, d) : sobol_sample(index, d);
     return r >= 1.f ? 0.f : r;
   }
 };
@@ -152,6 +296,7 @@ struct CameraIn {
 
 struct ParamsIn {
   uint32_t spp, max_depth, rr_depth;
+  uint32_t sampler;  // 0 Sobol' + SobolEnum, 1 Halton (Faure) + HaltonEnum
 };
 
 struct Material {
@@ -1198,11 +1343,21 @@ template <typename T> V3<T> trace_path(const Scene<T>& sc, const CamT<T>& cam, c
                                        Replay* rp_in = nullptr, AdjAcc<T>* adj = nullptr) {
   Replay rp_local;
   Replay* rp = rp_in ? rp_in : &rp_local;
-  uint32_t m = log2_pow2_res(ci.res_x, ci.res_y);
-  Rand rnd{enum_index(m, s, x, y)};
-  float res = (float)(1u << m);
-  float u = res * rnd.next() - (float)x;  // SobolEnum::SampleX (SobolEnum.h:30-32)
-  float v = res * rnd.next() - (float)y;
+  float u, v;
+  Rand rnd{0};
+  if (pr.sampler == 1) {
+    // HaltonEnum::SampleX/Y (sampler/HaltonEnum.h): scale by 2^p2 and 3^p3
+    const HaltonEnumC he(ci.res_x, ci.res_y);
+    rnd = Rand{he.index(s, x, y), 0, true};
+    u = (float)he.w * rnd.next() - (float)x;
+    v = (float)he.h * rnd.next() - (float)y;
+  } else {
+    uint32_t m = log2_pow2_res(ci.res_x, ci.res_y);
+    rnd = Rand{enum_index(m, s, x, y)};
+    float res = (float)(1u << m);
+    u = res * rnd.next() - (float)x;  // SobolEnum::SampleX (SobolEnum.h:30-32)
+    v = res * rnd.next() - (float)y;
+  }
   if (u_out) *u_out = u;
   if (v_out) *v_out = v;
   Ray<T> ray = camera_ray(cam, (T)((float)x + u), (T)((float)y + v));
@@ -1526,6 +1681,10 @@ const char* gyo_tables_digest() { return GYT_TABLES_DIGEST; }
 void gyo_set_trace(int on) { g_trace = on; }
 
 float gyo_sobol(uint32_t dim, uint64_t index) { return sobol_sample(index, dim); }
+float gyo_halton(uint32_t dim, uint64_t index) { return halton_sample(index, dim); }
+uint64_t gyo_halton_enum_index(uint32_t res_x, uint32_t res_y, uint32_t s, uint32_t x, uint32_t y) {
+  return HaltonEnumC(res_x, res_y).index(s, x, y);
+}
 
 uint64_t gyo_enum_index(uint32_t res_x, uint32_t res_y, uint32_t s, uint32_t x, uint32_t y) {
   return enum_index(log2_pow2_res(res_x, res_y), s, x, y);

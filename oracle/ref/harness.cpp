@@ -5,12 +5,16 @@
 // Commands (all binary I/O is little-endian, see oracle/scene_io.py):
 //   sobol   <pairs.bin> <out.bin>             (u32 dim, u64 index) -> f32 sobol::sample
 //   enum    <resx> <resy> <trip.bin> <out.bin> (u32 s,x,y) -> u64 SobolEnum::GetIndex
+//   halton  <pairs.bin> <out.bin>             (u32 dim, u64 index) -> f32 HaltonSampler (Faure) Sample
+//   henum   <resx> <resy> <trip.bin> <out.bin> (u32 s,x,y) -> u64 HaltonEnum::GetIndex
 //   hits    <scene> <rays.bin> <out.bin>       closest-hit through BVHAccel::Intersect
 //   anyhit  <scene> <rays.bin> <out.bin>       occlusion through BVHAccel::Intersect(ray)
 //   paths   <scene> <trip.bin> <out.bin>       PathTracing::Li for (x,y,s) triplets
 //   render  <scene> <out.bin> [rows]           TiledIntegrator::Render, timed
 //   camera  <scene> <out.bin>                  RasterToWorld matrix (row-major f32)
 //   bsdf    <cases.bin> <out.bin>              BxDF Sample/Evaluate/Pdf tables
+// paths and render use SobolSampler + SobolEnum, or HaltonSampler (Faure
+// permutations) + HaltonEnum when GYREF_SAMPLER=halton.
 // Standard and shim headers first, so the access override below only reaches
 // the reference's own classes (Film's pixel buffer, Scene's counters).
 #include <algorithm>
@@ -35,6 +39,8 @@
 #include "accelerator/BVHAccel.h"
 #include "sampler/Sobol.h"
 #include "sampler/SobolEnum.h"
+#include "sampler/Halton.h"
+#include "sampler/HaltonEnum.h"
 #include "material/Diffuse.h"
 #include "material/Mirror.h"
 #include "material/Glass.h"
@@ -266,6 +272,42 @@ int cmd_enum(int argc, char** argv) {
   return 0;
 }
 
+// HaltonSampler(w, h) as the demo driver builds it (Gyunity_exe/main.cpp:134):
+// a non-zero first argument selects the Faure permutations.
+const HaltonSampler& faure_halton() {
+  static HaltonSampler h(true);
+  return h;
+}
+
+int cmd_halton(int argc, char** argv) {
+  std::vector<char> in = read_file(argv[2]);
+  size_t n = in.size() / 12;
+  std::vector<float> out(n);
+  const HaltonSampler& h = faure_halton();
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t dim; uint64_t idx;
+    std::memcpy(&dim, &in[12 * i], 4);
+    std::memcpy(&idx, &in[12 * i + 4], 8);
+    out[i] = h.sample(dim, idx);
+  }
+  write_file(argv[3], out.data(), out.size() * 4);
+  return 0;
+}
+
+int cmd_henum(int argc, char** argv) {
+  HaltonEnum e((uint32)std::atoi(argv[2]), (uint32)std::atoi(argv[3]));
+  std::vector<char> in = read_file(argv[4]);
+  size_t n = in.size() / 12;
+  std::vector<uint64_t> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t v[3];
+    std::memcpy(v, &in[12 * i], 12);
+    out[i] = e.GetIndex(v[0], v[1], v[2]);
+  }
+  write_file(argv[5], out.data(), out.size() * 8);
+  return 0;
+}
+
 int cmd_hits(int argc, char** argv, bool any) {
   LoadedScene ls = load_scene(argv[2]);
   std::vector<char> in = read_file(argv[3]);
@@ -295,8 +337,14 @@ int cmd_hits(int argc, char** argv, bool any) {
 
 std::shared_ptr<PathTracing> make_integrator(const LoadedScene& ls, std::shared_ptr<Sampler>* sampler,
                                              std::shared_ptr<SamplerEnum>* senum) {
-  *sampler = std::make_shared<SobolSampler>();
-  *senum = std::make_shared<SobolEnum>(ls.resX, ls.resY);
+  const char* kind = std::getenv("GYREF_SAMPLER");
+  if (kind && std::string(kind) == "halton") {
+    *sampler = std::make_shared<HaltonSampler>(faure_halton());
+    *senum = std::make_shared<HaltonEnum>(ls.resX, ls.resY);
+  } else {
+    *sampler = std::make_shared<SobolSampler>();
+    *senum = std::make_shared<SobolEnum>(ls.resX, ls.resY);
+  }
   return std::make_shared<PathTracing>(ls.spp, ls.maxDepth, *sampler, *senum);
 }
 
@@ -419,13 +467,15 @@ int cmd_bsdf(int argc, char** argv) {
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|hits|anyhit|paths|render|camera|bsdf> ...\n");
+    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|halton|henum|hits|anyhit|paths|render|camera|bsdf> ...\n");
     return 2;
   }
   try {
     std::string c = argv[1];
     if (c == "sobol") return cmd_sobol(argc, argv);
     if (c == "enum") return cmd_enum(argc, argv);
+    if (c == "halton") return cmd_halton(argc, argv);
+    if (c == "henum") return cmd_henum(argc, argv);
     if (c == "hits") return cmd_hits(argc, argv, false);
     if (c == "anyhit") return cmd_hits(argc, argv, true);
     if (c == "paths") return cmd_paths(argc, argv);

@@ -90,6 +90,30 @@ def ref_enum(tmp, res_x, res_y, s, x, y):
     return np.fromfile(b, np.uint64)
 
 
+def ref_halton(tmp, dims, indices):
+    """HaltonSampler with Faure permutations (sampler/Halton.h) for (dim, index) pairs."""
+    pairs = np.zeros(len(dims), np.dtype([("d", "<u4"), ("i", "<u8")]))
+    pairs["d"] = dims
+    pairs["i"] = indices
+    a, b = os.path.join(tmp, "halton_in.bin"), os.path.join(tmp, "halton_out.bin")
+    pairs.tofile(a)
+    run("halton", a, b)
+    return np.fromfile(b, np.float32)
+
+
+def ref_henum(tmp, res_x, res_y, s, x, y):
+    """HaltonEnum::GetIndex (sampler/HaltonEnum.h) for (s, x, y) triplets."""
+    trip = np.stack([np.asarray(s, np.uint32), np.asarray(x, np.uint32), np.asarray(y, np.uint32)], 1)
+    a, b = os.path.join(tmp, "henum_in.bin"), os.path.join(tmp, "henum_out.bin")
+    trip.astype(np.uint32).tofile(a)
+    run("henum", res_x, res_y, a, b)
+    return np.fromfile(b, np.uint64)
+
+
+def _sampler_env(sampler):
+    return {"GYREF_SAMPLER": sampler} if sampler and sampler != "sobol" else None
+
+
 def ref_hits(tmp, scene_path, rays, any_hit=False):
     a, b = os.path.join(tmp, "rays.bin"), os.path.join(tmp, "hits.bin")
     rays.astype(RAY_DTYPE).tofile(a)
@@ -97,11 +121,11 @@ def ref_hits(tmp, scene_path, rays, any_hit=False):
     return np.fromfile(b, HIT_DTYPE)
 
 
-def ref_paths(tmp, scene_path, x, y, s):
+def ref_paths(tmp, scene_path, x, y, s, sampler=None):
     trip = np.stack([np.asarray(x, np.uint32), np.asarray(y, np.uint32), np.asarray(s, np.uint32)], 1)
     a, b = os.path.join(tmp, "paths_in.bin"), os.path.join(tmp, "paths_out.bin")
     trip.astype(np.uint32).tofile(a)
-    run("paths", scene_path, a, b)
+    run("paths", scene_path, a, b, env=_sampler_env(sampler))
     return np.fromfile(b, np.float32).reshape(-1, 4)
 
 
@@ -111,7 +135,7 @@ def ref_camera(tmp, scene_path):
     return np.fromfile(b, np.float32).reshape(4, 4)
 
 
-def ref_render(tmp, scene_path, rows=None, spp=None, threads=None):
+def ref_render(tmp, scene_path, rows=None, spp=None, threads=None, sampler=None):
     import json
     b = os.path.join(tmp, "render.bin")
     args = ["render", scene_path, b]
@@ -119,7 +143,10 @@ def ref_render(tmp, scene_path, rows=None, spp=None, threads=None):
         args.append(rows if rows is not None else 0)
     if spp is not None:
         args.append(spp)
-    out = run(*args, env={"GYREF_THREADS": str(threads)} if threads else None)
+    env = dict(_sampler_env(sampler) or {})
+    if threads:
+        env["GYREF_THREADS"] = str(threads)
+    out = run(*args, env=env or None)
     info = json.loads(out.strip().splitlines()[-1])
     img = np.fromfile(b, np.float32).reshape(-1, 4)
     return img, info

@@ -5,7 +5,8 @@ oracle/ref/build_ref.py (``oracle/_ref/gyref_harness``) on seeded inputs and
 stores the inputs and the reference outputs as .npz fixtures. The reference
 checkout is only needed to regenerate; the tests read the fixtures.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py halton     # only the Halton fixtures
 """
 import os
 import sys
@@ -65,11 +66,54 @@ def bsdf_cases(rng, n_per=400):
     return np.concatenate(cases)
 
 
+def halton_golden(tmp):
+    """HaltonSampler (Faure permutations), HaltonEnum and PathTracing::Li with
+    the Halton sampler (GYREF_SAMPLER=halton selects it in the harness)."""
+    rng = np.random.default_rng(20261204)
+    # all 256 dimensions (and some beyond, which give 0) at small, 32-bit and 44-bit indices
+    dims = np.concatenate([np.arange(300), np.arange(300), rng.integers(0, 256, 3000)]).astype(np.uint32)
+    idx = np.concatenate([rng.integers(0, 1 << 20, 300), rng.integers(0, 1 << 44, 300),
+                          rng.integers(0, 1 << 32, 1500), rng.integers(0, 1 << 44, 1500)]).astype(np.uint64)
+    np.savez_compressed(os.path.join(HERE, "halton.npz"), dims=dims, indices=idx,
+                        values=io.ref_halton(tmp, dims, idx))
+    enum = {}
+    for rx, ry in ((256, 256), (1024, 1024), (1920, 1080), (100, 60), (1, 1), (7, 1), (1, 5)):
+        s = rng.integers(0, 300, 800).astype(np.uint32)
+        x = rng.integers(0, rx, 800).astype(np.uint32)
+        y = rng.integers(0, ry, 800).astype(np.uint32)
+        key = "%dx%d" % (rx, ry)
+        enum[key + "_sxy"] = np.stack([s, x, y], 1)
+        enum[key + "_index"] = io.ref_henum(tmp, rx, ry, s, x, y)
+    np.savez_compressed(os.path.join(HERE, "henum.npz"), **enum)
+    for name, sd in (("cornell_nospheres", scenes.cornell_box(spheres=False)),
+                     ("mixed", scenes.mixed_materials_box(level=3, res=64))):
+        sd.params.sampler = "halton"
+        path = os.path.join(tmp, name + "_h.gyts")
+        io.write_scene(path, sd)
+        n = 3000
+        x = rng.integers(0, sd.camera.res_x, n)
+        y = rng.integers(0, sd.camera.res_y, n)
+        s = rng.integers(0, sd.params.spp, n)
+        r = io.ref_paths(tmp, path, x, y, s, sampler="halton")
+        np.savez_compressed(os.path.join(HERE, "paths_%s_halton.npz" % name),
+                            xys=np.stack([x, y, s], 1).astype(np.uint32), L=r[:, :3], cursor=r[:, 3].astype(np.int32))
+    sd = scenes.cornell_box(res=64, spp=4)
+    sd.params.sampler = "halton"
+    path = os.path.join(tmp, "img_h.gyts")
+    io.write_scene(path, sd)
+    img, info = io.ref_render(tmp, path, sampler="halton")
+    np.savez_compressed(os.path.join(HERE, "image_cornell_64x64_4spp_halton.npz"), film=img)
+
+
 def main():
     if not io.have_harness():
         sys.exit("build the reference harness first: python oracle/ref/build_ref.py")
-    rng = np.random.default_rng(20261203)
     tmp = tempfile.mkdtemp()
+    if sys.argv[1:] == ["halton"]:
+        halton_golden(tmp)
+        print("Halton golden vectors written to", HERE)
+        return
+    rng = np.random.default_rng(20261203)
     out = {}
 
     # Sobol' points: sobol::sample over dimensions and 64-bit indices
@@ -146,6 +190,7 @@ def main():
     # BxDF tables in the local frame
     cases = bsdf_cases(rng)
     np.savez_compressed(os.path.join(HERE, "bsdf.npz"), cases=cases.view(np.uint8), out=io.ref_bsdf(tmp, cases))
+    halton_golden(tmp)
     print("golden vectors written to", HERE)
 
 

@@ -32,10 +32,15 @@ def test_reference_arm_single_scene_line():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
 
 
+def test_reference_arm_with_halton_sampler():
+    line = _run("--workload", "cornell", "--sampler", "halton", "--steps", "1", "--warmup", "0")
+    assert line["value"] > 0 and line["config"]["sampler"].startswith("Halton")
+
+
 def test_batch_sample_is_every_sixteenth_instance():
     sys.path.insert(0, ROOT)
     import bench
     ids = [i for i, _ in bench.batch_sample(64)]
     assert ids == [0, 16, 32, 48]
-    cfg = bench.batch_config(type("A", (), {"batch_instances": 64})(), None)
+    cfg = bench.batch_config(type("A", (), {"batch_instances": 64, "sampler": "sobol"})(), None)
     assert cfg["instances"] == 64 and cfg["workload"] == "uneven_batch_64_instances"
