@@ -221,6 +221,45 @@ Elem child_elem(const std::vector<float>& nodes, int node, int slot) {
   return e;
 }
 
+// Child slots as in Ylitie, Karras and Laine (HPG 2017): slot s faces the
+// octant direction d_s (component a is +1 when bit a of s is set, else -1);
+// greedily, the (child, free slot) pair whose child centre lies furthest along
+// d_s from the node centre is placed first. A ray whose negative direction
+// axes are the bits o then meets the children roughly in increasing order of
+// slot ^ o. Returns 8 entries; empty slots are leaves with no triangles.
+std::vector<Elem> slot_order(const std::vector<Elem>& ch) {
+  Box nb;
+  for (const Elem& e : ch) nb.grow(e.box);
+  float c[3];
+  for (int a = 0; a < 3; ++a) c[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
+  std::vector<Elem> slots(8);
+  for (Elem& e : slots) { e.node = -1; e.first = e.count = 0; }
+  std::vector<bool> placed(ch.size(), false), used(8, false);
+  for (size_t round = 0; round < ch.size(); ++round) {
+    float best = -INFINITY;
+    int bc = -1, bs = -1;
+    for (size_t k = 0; k < ch.size(); ++k) {
+      if (placed[k]) continue;
+      float off[3];
+      for (int a = 0; a < 3; ++a) off[a] = 0.5f * (ch[k].box.lo[a] + ch[k].box.hi[a]) - c[a];
+      for (int sl = 0; sl < 8; ++sl) {
+        if (used[sl]) continue;
+        float score = 0.f;
+        for (int a = 0; a < 3; ++a) score += ((sl >> a) & 1) ? off[a] : -off[a];
+        if (score > best) { best = score; bc = (int)k; bs = sl; }
+      }
+    }
+    if (bc < 0) {  // non-finite centres: first unplaced child into the first free slot
+      for (bc = 0; placed[bc]; ++bc) {}
+      for (bs = 0; used[bs]; ++bs) {}
+    }
+    placed[bc] = true;
+    used[bs] = true;
+    slots[bs] = ch[bc];
+  }
+  return slots;
+}
+
 }  // namespace
 
 bool build_wide_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_t nt, WideBvhHost* out) {
@@ -253,7 +292,7 @@ bool build_wide_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_
   todo.push_back(expand(root));
   depth.push_back(1);
   for (size_t w = 0; w < todo.size(); ++w) {
-    std::vector<Elem> ch = todo[w];
+    std::vector<Elem> ch = slot_order(todo[w]);
     // inner children first get consecutive node indices
     uint32_t child_base = (uint32_t)todo.size();
     uint32_t tri_base = (uint32_t)out->order.size();
@@ -293,6 +332,7 @@ bool build_wide_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_
     uint32_t inner_rank = 0;
     for (size_t k = 0; k < ch.size(); ++k) {
       const Elem& e = ch[k];
+      if (e.node < 0 && e.count == 0) continue;  // empty slot
       for (int a = 0; a < 3; ++a) {
         double lo = std::floor(((double)e.box.lo[a] - p[a]) / sc[a] * (1.0 - 1e-6) - 1e-6);
         double hi = std::ceil(((double)e.box.hi[a] - p[a]) / sc[a] * (1.0 + 1e-6) + 1e-6);
@@ -307,7 +347,7 @@ bool build_wide_bvh_host(const float* V, uint32_t nv, const uint32_t* I, uint32_
         ++inner_rank;
       } else {
         uint32_t off = (uint32_t)out->order.size() - tri_base;
-        if (e.count > 3 || off > 31) return false;
+        if (e.count > 3 || off + e.count > 32) return false;
         for (uint32_t t = 0; t < e.count; ++t) out->order.push_back(bin.order[e.first + t]);
         meta[k] = (uint8_t)((e.count << 5) | off);
       }

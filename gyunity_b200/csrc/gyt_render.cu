@@ -134,11 +134,14 @@ constexpr uint32_t kPixMask = 0x0fffffffu;
 constexpr int kWStack = 48;  // node groups: one per level of the wide BVH
 constexpr int kBStack = 64;  // binary BVH: one entry per level
 constexpr int kBlock = 256;
-// Shadow-ray kernels are latency-bound (dependent node fetches): over the
-// binary BVH a register cap that fits four blocks per SM (a few spilled
-// values) beats two blocks; the 8-wide traversal needs its registers.
+// Traversal kernels are latency-bound (dependent node fetches): a register
+// cap that fits four blocks per SM (a few spilled values) beats fewer blocks
+// for the closest-hit and the shadow/MIS kernels of both widths (measured on
+// the procedural mesh and the uneven batch).
 template <int W>
-constexpr int shadow_blocks_per_sm() { return W == 8 ? 2 : 4; }
+constexpr int shadow_blocks_per_sm() { return 4; }
+template <int W>
+constexpr int extend_blocks_per_sm() { return 4; }
 
 // meta bit 20: the bounce queued an MIS ray whose contribution k_finish adds
 constexpr uint32_t kMisQueued = 1u << 20;
@@ -209,7 +212,7 @@ struct BinaryTraversal {
   int node, sp;
   int stack[kBStack];
 
-  GYT_D void init() { node = 0; sp = 0; }
+  GYT_D void init(const RayConst&) { node = 0; sp = 0; }
 
   // Returns true when the traversal is finished (or, for ANY, on a hit).
   template <bool ANY, bool COUNT, class S>
@@ -259,47 +262,52 @@ struct BinaryTraversal {
 // subtraction removes 2^23 (both exact).
 GYT_D float qbyte(uint32_t w, int k) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440 + k)) - 8388608.f; }
 
-// 8-wide BVH with quantized child boxes (gyt_bvh_host.h); one step = one node
-// (its leaf children nearer than the first hit inner child are tested in
-// the same step) or one pending child of a group. Stack entries are child
-// groups, at most one per level: x = node whose children are pending, y =
-// inner mask (bits 0-7) | children left (bits 8-10) | their slots near to far
-// (3 bits each from bit 11), z = a lower bound of their entry distances.
+// 8-wide BVH with quantized child boxes (gyt_bvh_host.h), traversed as in
+// Ylitie, Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs
+// Through Compressed Wide BVHs" (HPG 2017). The builder puts the child whose
+// centre lies towards octant s of the node in slot s (axis a positive when
+// bit a of s is set); a ray whose direction has its negative axes in the bits
+// of `oct` meets the children roughly in increasing order of slot ^ oct. One
+// node group = the inner children of a node still to visit (bit slot ^ oct of
+// the hit mask) and the node's first inner child index: 8 bytes on the stack,
+// no per-node sort. A step tests the triangles of the last node's hit leaves,
+// then fetches the nearest pending inner child and tests its eight boxes.
 struct WideTraversal {
-  uint32_t node;
+  uint2 grp;        // .x first inner child; .y hit mask (bits 0-7) | inner-slot mask (bits 8-15)
+  uint32_t tri_base, tmask;  // the last node's hit leaf triangles (bit k = tri_base + k)
+  uint32_t oct;
   int sp;
-  bool have_node;
-  uint3 stack[kWStack];
+  uint2 stack[kWStack];
 
-  GYT_D void init() { node = 0; sp = 0; have_node = true; }
+  GYT_D void init(const RayConst& rc) {
+    grp = make_uint2(0u, 1u);  // the root as the single pending child of a virtual group
+    tri_base = tmask = 0u;
+    oct = (rc.ix < 0.f ? 1u : 0u) | (rc.iy < 0.f ? 2u : 0u) | (rc.iz < 0.f ? 4u : 0u);
+    sp = 0;
+  }
 
   template <bool ANY, bool COUNT, class S>
   GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
-    if (!have_node) {
-      // next pending child of the nearest group that can still be hit
-      while (sp > 0) {
-        uint3 e = stack[sp - 1];
-        if (__uint_as_float(e.z) > tmax) { --sp; continue; }
-        const uint32_t m = (e.y >> 8) & 7u, slot = (e.y >> 11) & 7u;
-        if (m == 1) --sp;
-        else stack[sp - 1].y = (e.y & 0xffu) | ((m - 1) << 8) | ((e.y >> 14) << 11);
-        const uint32_t emask = e.y & 0xffu;
-        const uint4 pw = __ldg(s.wnodes + 5 * (size_t)e.x + 1);
-        if ((emask >> slot) & 1u) {
-          node = pw.x + __popc(emask & ((1u << slot) - 1u));
-          have_node = true;
-          return false;
-        }
-        const uint32_t meta = ((slot < 4 ? pw.z : pw.w) >> (8 * (slot & 3u))) & 0xffu;
-        if (test_tris<ANY, COUNT>(s, rc.wr, pw.y + (meta & 31u), meta >> 5, tmax, b1, b2, prim, cnt)) return true;
-        return false;
-      }
-      return true;
+#pragma unroll 1
+    while (tmask) {
+      const uint32_t k = __ffs(tmask) - 1;
+      tmask &= tmask - 1u;
+      if (test_tris<ANY, COUNT>(s, rc.wr, tri_base + k, 1u, tmax, b1, b2, prim, cnt)) return true;
     }
+    if ((grp.y & 0xffu) == 0u) {
+      if (sp == 0) return true;
+      grp = stack[--sp];
+    }
+    const uint32_t p = __ffs(grp.y & 0xffu) - 1;
+    const uint32_t slot = p ^ oct;
+    // the virtual root group holds node 0 with an empty inner-slot mask
+    const uint32_t node = grp.x + __popc((grp.y >> 8) & ((1u << slot) - 1u));
+    grp.y &= ~(1u << p);
+    if (grp.y & 0xffu) stack[sp++] = grp;
     if (COUNT) cnt->nodes++;
     const uint4* n = s.wnodes + 5 * (size_t)node;
-    uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
+    const uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
     const float sx = __int_as_float(((int)(int8_t)(w0.w & 0xffu) + 127) << 23);
     const float sy = __int_as_float(((int)(int8_t)((w0.w >> 8) & 0xffu) + 127) << 23);
     const float sz = __int_as_float(((int)(int8_t)((w0.w >> 16) & 0xffu) + 127) << 23);
@@ -307,48 +315,30 @@ struct WideTraversal {
     const float ax = sx * rc.ix, ay = sy * rc.iy, az = sz * rc.iz;
     const float bx = (__uint_as_float(w0.x) - o.x) * rc.ix, by = (__uint_as_float(w0.y) - o.y) * rc.iy,
                 bz = (__uint_as_float(w0.z) - o.z) * rc.iz;
-    uint32_t key[8];
+    // near and far planes per axis by the direction's sign (t is monotone in
+    // the quantized coordinate, so this equals the min / max of the two)
+    const bool fx = oct & 1u, fy = oct & 2u, fz = oct & 4u;
+    const uint32_t nxa = fx ? w2.z : w2.x, nxb = fx ? w2.w : w2.y, fxa = fx ? w2.x : w2.z, fxb = fx ? w2.y : w2.w;
+    const uint32_t nya = fy ? w3.z : w3.x, nyb = fy ? w3.w : w3.y, fya = fy ? w3.x : w3.z, fyb = fy ? w3.y : w3.w;
+    const uint32_t nza = fz ? w4.z : w4.x, nzb = fz ? w4.w : w4.y, fza = fz ? w4.x : w4.z, fzb = fz ? w4.y : w4.w;
+    uint32_t hits = 0u, tm = 0u;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int k = i & 3;
-      const float t0x = fmaf(qbyte(i < 4 ? w2.x : w2.y, k), ax, bx), t1x = fmaf(qbyte(i < 4 ? w2.z : w2.w, k), ax, bx);
-      const float t0y = fmaf(qbyte(i < 4 ? w3.x : w3.y, k), ay, by), t1y = fmaf(qbyte(i < 4 ? w3.z : w3.w, k), ay, by);
-      const float t0z = fmaf(qbyte(i < 4 ? w4.x : w4.y, k), az, bz), t1z = fmaf(qbyte(i < 4 ? w4.z : w4.w, k), az, bz);
-      const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.f));
-      const float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tmax));
+      const float tn = fmaxf(fmaxf(fmaf(qbyte(i < 4 ? nxa : nxb, k), ax, bx), fmaf(qbyte(i < 4 ? nya : nyb, k), ay, by)),
+                             fmaxf(fmaf(qbyte(i < 4 ? nza : nzb, k), az, bz), 0.f));
+      const float tf = fminf(fminf(fmaf(qbyte(i < 4 ? fxa : fxb, k), ax, bx), fmaf(qbyte(i < 4 ? fya : fyb, k), ay, by)),
+                             fminf(fmaf(qbyte(i < 4 ? fza : fzb, k), az, bz), tmax));
       const uint32_t meta = ((i < 4 ? w1.z : w1.w) >> (8 * k)) & 0xffu;
-      const bool live = ((imask >> i) & 1u) || meta;
-      key[i] = (tn <= tf && live) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)i) : 0xffffffffu;
-    }
-#define GYT_CX(a, b) { uint32_t lo_ = min(key[a], key[b]), hi_ = max(key[a], key[b]); key[a] = lo_; key[b] = hi_; }
-    GYT_CX(0, 1) GYT_CX(2, 3) GYT_CX(4, 5) GYT_CX(6, 7)
-    GYT_CX(0, 2) GYT_CX(1, 3) GYT_CX(4, 6) GYT_CX(5, 7)
-    GYT_CX(1, 2) GYT_CX(5, 6) GYT_CX(0, 4) GYT_CX(3, 7)
-    GYT_CX(1, 5) GYT_CX(2, 6)
-    GYT_CX(1, 4) GYT_CX(3, 6)
-    GYT_CX(2, 4) GYT_CX(3, 5)
-    GYT_CX(3, 4)
-#undef GYT_CX
-    have_node = false;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (!have_node && key[k] != 0xffffffffu && __uint_as_float(key[k] & ~7u) <= tmax) {
-        const uint32_t slot = key[k] & 7u;
-        if ((imask >> slot) & 1u) {
-          uint32_t list = 0, m = 0;
-#pragma unroll
-          for (int j = k + 1; j < 8; ++j)
-            if (key[j] != 0xffffffffu) { list |= (key[j] & 7u) << (11 + 3 * m); ++m; }
-          if (m) stack[sp++] = make_uint3(node, imask | (m << 8) | list, key[k] & ~7u);
-          node = w1.x + __popc(imask & ((1u << slot) - 1u));
-          have_node = true;
-        } else {
-          const uint32_t meta = ((slot < 4 ? w1.z : w1.w) >> (8 * (slot & 3u))) & 0xffu;
-          if (test_tris<ANY, COUNT>(s, rc.wr, w1.y + (meta & 31u), meta >> 5, tmax, b1, b2, prim, cnt)) return true;
-        }
+      if (tn <= tf) {
+        if ((imask >> i) & 1u) hits |= 1u << (i ^ oct);
+        else if (meta) tm |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
       }
     }
-    return !have_node && sp == 0;
+    grp = make_uint2(w1.x, hits | (imask << 8));
+    tri_base = w1.y;
+    tmask = tm;
+    return false;
   }
 };
 
@@ -383,7 +373,7 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
   if (s.n_tris > 0) {
     RayConst rc = ray_const(o, d);
     typename TraversalOf<W>::type tv;
-    tv.init();
+    tv.init(rc);
     while (!tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, cnt)) {
     }
   }
@@ -426,7 +416,7 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
           b1 = b2 = 0.f;
           prim = -1;
           rc = ray_const(o, d);
-          tv.init();
+          tv.init(rc);
           if ((BATCH ? lg.n_tris : s.n_tris) == 0) {
             if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
             else trace_spheres<ANY>(s, o, d, tmax, prim);
@@ -576,8 +566,9 @@ __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base,
 }
 
 template <int W, bool COUNT>
-__global__ void __launch_bounds__(kBlock) k_extend(PathBuf cur, uint32_t n, DevScene s, float4* __restrict__ hits,
-                                                   uint32_t* __restrict__ fetch, unsigned long long* counters) {
+__global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
+    k_extend(PathBuf cur, uint32_t n, DevScene s, float4* __restrict__ hits, uint32_t* __restrict__ fetch,
+             unsigned long long* counters) {
   persistent_trace<W, false, COUNT>(
       s, fetch, n,
       [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo&) {
@@ -841,11 +832,41 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
   if (ADJ) A.pend[i] = pend_new;
 }
 
+// Shading classes: the lobe type of the surface hit (GYT_MAT_*), a miss, an
+// idle thread past the live paths.
+constexpr uint32_t kClassMiss = 5, kClassIdle = 6, kShadeClasses = 7;
+
+GYT_D uint32_t shade_class(const DevScene& s, const Queues& q, uint32_t i) {
+  const int prim = __float_as_int(q.hit[i].w);
+  if (prim < 0) return kClassMiss;
+  const uint32_t m = prim < s.n_tris ? (uint32_t)__float_as_int(__ldg(&s.tnrm[3 * prim].w))
+                                     : __ldg(s.sphere_mat + (prim - s.n_tris));
+  return min(__ldg(s.mtypes + m), 4u);
+}
+
+// Block-local counting sort of the block's path slots by shading class, so
+// that a warp shades surfaces of one kind (one BSDF branch) instead of a mix.
+// Returns the slot this thread shades, ~0u for none. Every thread of the
+// block must call it.
+GYT_D uint32_t coherent_slot(uint32_t i, uint32_t key) {
+  __shared__ uint32_t cnt[kShadeClasses];
+  __shared__ uint32_t order[kBlock];
+  if (threadIdx.x < kShadeClasses) cnt[threadIdx.x] = 0u;
+  __syncthreads();
+  const uint32_t rank = atomicAdd(&cnt[key], 1u);
+  __syncthreads();
+  uint32_t base = 0;
+  for (uint32_t c = 0; c < key; ++c) base += cnt[c];
+  order[base + rank] = key == kClassIdle ? ~0u : i;
+  __syncthreads();
+  return order[threadIdx.x];
+}
+
 __global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
                                                   SamplerTables tab, DebugOut dbg) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  shade_path<false, true>(cur, i, s, prm, q, tab, dbg);
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = coherent_slot(i, i < n ? shade_class(s, q, i) : kClassIdle);
+  if (j != ~0u) shade_path<false, true>(cur, j, s, prm, q, tab, dbg);
 }
 
 // MIS-ray result of one queue entry (every MIS kernel). DEFER: the
@@ -1204,8 +1225,9 @@ GYT_D TraceGeo geo_of(const DevScene& s) {
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const IterState* __restrict__ st,
-                                                         float4* __restrict__ hits, uint32_t* __restrict__ fetch) {
+__global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
+    k_extend_batch(PathBuf cur, const IterState* __restrict__ st, float4* __restrict__ hits,
+                   uint32_t* __restrict__ fetch) {
   const uint32_t n = st->n;
   persistent_trace<W, false, false, true>(
       c_insts[0].s, fetch, n,
@@ -1227,9 +1249,12 @@ __global__ void __launch_bounds__(kBlock) k_extend_batch(PathBuf cur, const Iter
 __global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q,
                                                         SamplerTables tab) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= st->n) return;
-  const Inst& I = c_insts[cur.inst[i]];
-  shade_path<false, true>(cur, i, I.s, I.prm, q, tab, DebugOut{});
+  const uint32_t n = st->n;
+  if (blockIdx.x * blockDim.x >= n) return;  // the whole block is idle
+  const uint32_t j = coherent_slot(i, i < n ? shade_class(c_insts[cur.inst[i]].s, q, i) : kClassIdle);
+  if (j == ~0u) return;
+  const Inst& I = c_insts[cur.inst[j]];
+  shade_path<false, true>(cur, j, I.s, I.prm, q, tab, DebugOut{});
 }
 
 // Shadow then MIS rays of the batch in one launch (k_connect, every ray with
