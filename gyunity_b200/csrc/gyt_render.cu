@@ -142,6 +142,12 @@ template <int W>
 constexpr int shadow_blocks_per_sm() { return 4; }
 template <int W>
 constexpr int extend_blocks_per_sm() { return 4; }
+// The shade kernels, once their blocks are sorted by lobe type, are bound by
+// latency at two blocks per SM (124 registers): a cap of 80 registers (three
+// blocks, some spilled values) shades 11-13% faster on the procedural mesh
+// and the uneven batch. 128-thread blocks at the same occupancy were slower:
+// the sort window is the block.
+constexpr int kShadeBlocksPerSm = 3;
 
 // meta bit 20: the bounce queued an MIS ray whose contribution k_finish adds
 constexpr uint32_t kMisQueued = 1u << 20;
@@ -862,8 +868,8 @@ GYT_D uint32_t coherent_slot(uint32_t i, uint32_t key) {
   return order[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
-                                                  SamplerTables tab, DebugOut dbg) {
+__global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm)
+    k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q, SamplerTables tab, DebugOut dbg) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t j = coherent_slot(i, i < n ? shade_class(s, q, i) : kClassIdle);
   if (j != ~0u) shade_path<false, true>(cur, j, s, prm, q, tab, dbg);
@@ -1246,8 +1252,8 @@ __global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
 // One path per thread over a grid sized for the whole pool (threads past
 // the live count return at once): the work per path varies a lot, and the
 // block scheduler balances it far better than a grid-stride loop does.
-__global__ void __launch_bounds__(kBlock) k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q,
-                                                        SamplerTables tab) {
+__global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm)
+    k_shade_batch(PathBuf cur, const IterState* __restrict__ st, Queues q, SamplerTables tab) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t n = st->n;
   if (blockIdx.x * blockDim.x >= n) return;  // the whole block is idle
