@@ -192,6 +192,19 @@ class Context:
         self.check(self._lib.gyt_sobol(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
         return out
 
+    def film_quantize(self, d_film_ptr, res_x, res_y, gamma=2.2):
+        """gyt_film_quantize: a device film (res_x*res_y*4 doubles) as 8-bit
+        RGB (res_y, res_x, 3), ImageIO::toInt on the GPU."""
+        out = np.empty((res_y, res_x, 3), np.uint8)
+        self.check(self._lib.gyt_film_quantize(self.handle, ctypes.c_void_p(int(d_film_ptr)), res_x, res_y,
+                                               float(gamma), _c.ptr(out)))
+        return out
+
+    def film_save(self, d_film_ptr, res_x, res_y, path):
+        """gyt_film_save: Film::SaveImage of a device film (.png .bmp .hdr)."""
+        self.check(self._lib.gyt_film_save(self.handle, ctypes.c_void_p(int(d_film_ptr)), res_x, res_y,
+                                           str(path).encode()))
+
     def halton(self, dims, indices):
         """HaltonSampler with Faure permutations (sampler/Halton.h) for
         (dimension, index) pairs; dimensions >= 256 give 0."""
@@ -318,6 +331,16 @@ class Film:
 
     def GetImage(self):
         return self.image
+
+    def SaveImage(self, filename, ctx=None):
+        """Film::SaveImage (visual/Film.cpp:6-9): the image (weight 1 per pixel,
+        as Film::SetImage) through gyt_film_save; .png, .bmp or .hdr."""
+        import torch
+        ctx = ctx or default_context()
+        film = np.ones((self.mResY, self.mResX, 4), np.float64)
+        film[..., :3] = self.image
+        d = torch.from_numpy(film.reshape(-1)).cuda()
+        ctx.film_save(d.data_ptr(), self.mResX, self.mResY, filename)
 
 
 class PinHoleCamera:

@@ -11,8 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgyunity_b200.so")
-SOURCES = ["gyt_render.cu", "gyt_bvh_gpu.cu", "gyt_bvh_host.cpp"]
-HEADERS = ["gyt_device.cuh", "gyt_bvh_host.h", "gyt_bvh_gpu.h"]
+SOURCES = ["gyt_render.cu", "gyt_bvh_gpu.cu", "gyt_bvh_host.cpp", "gyt_image.cpp", "gyt_obj.cpp"]
+HEADERS = ["gyt_device.cuh", "gyt_bvh_host.h", "gyt_bvh_gpu.h", "gyt_image.h", "gyt_obj.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]

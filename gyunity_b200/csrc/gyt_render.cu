@@ -39,6 +39,8 @@
 #include "gyt_bvh_gpu.h"
 #include "gyt_bvh_host.h"
 #include "gyt_device.cuh"
+#include "gyt_image.h"
+#include "gyt_obj.h"
 
 namespace cg = cooperative_groups;
 using namespace gyt;
@@ -1375,6 +1377,105 @@ __global__ void k_resolve(const double* __restrict__ film, float* __restrict__ r
   rgb[3ull * i + 2] = (float)(p[2] / w);
 }
 
+// ImageIO::toInt (image/ImageIO.cpp:66-68) in float as the reference
+// computes it: int(pow(Clamp(x, 0, 1), 1 / gamma) * 255 + 0.5). A pixel
+// without samples (weight 0, colour NaN) gives 0.
+GYT_D uint8_t to_int8(float x, float inv_gamma) {
+  const float c = x < 0.f ? 0.f : (x > 1.f ? 1.f : x);
+  const float v = __fadd_rn(__fmul_rn(powf(c, inv_gamma), 255.f), 0.5f);
+  return (v >= 0.f && v < 256.f) ? (uint8_t)(int)v : (uint8_t)0;
+}
+
+// Film::SaveImage for 8-bit formats: colour / weight per pixel
+// (Film::WriteToPixelBuffer, visual/Film.h:128-136), then toInt per channel.
+__global__ void k_film_rgb8(const double* __restrict__ film, uint8_t* __restrict__ rgb, uint32_t npix,
+                            float inv_gamma) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const double* p = film + 4ull * i;
+  const double w = p[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) rgb[3ull * i + k] = to_int8((float)(p[k] / w), inv_gamma);
+}
+
+// Film::SaveImage for .hdr: colour / weight in Ward's RGBE (shared exponent
+// e of the largest component m: frexp(m) = f * 2^e, each channel stored as
+// trunc(c * f * 256 / m), exponent byte e + 128; components below 1e-32 give
+// zero), as stbi_write_hdr stores the float image (image/ImageIO.cpp:121-131).
+__global__ void k_film_rgbe(const double* __restrict__ film, uint8_t* __restrict__ rgbe, uint32_t npix) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const double* p = film + 4ull * i;
+  const double w = p[3];
+  float c[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float v = (float)(p[k] / w);
+    c[k] = v > 0.f ? v : 0.f;  // negative or NaN: no light
+  }
+  const float m = fmaxf(fmaxf(c[0], c[1]), c[2]);
+  uint8_t* o = rgbe + 4ull * i;
+  if (!(m >= 1e-32f)) {
+    o[0] = o[1] = o[2] = o[3] = 0;
+    return;
+  }
+  int e;
+  const float f = frexpf(m, &e);
+  const float norm = __fdiv_rn(__fmul_rn(f, 256.f), m);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) o[k] = (uint8_t)(int)__fmul_rn(c[k], norm);
+  o[3] = (uint8_t)(e + 128);
+}
+
+// Scene::AddMesh's Triangle::SetTransform (shape/Triangle.h:78-88) per
+// vertex, in the reference's float arithmetic: a point is M (x, y, z, 1) with
+// the matrix applied column by column from the last (((M.3 + M.2 z) + M.1 y)
+// + M.0 x per row, unfused), divided by w unless w is 0 or 1
+// (math/Transform.h:106-115); a normal is M^-T (x, y, z, 0) the same way
+// (Transform::TransformNormal, math/Transform.h:247-251), then divided by its
+// length ((x x + y y) + z z).
+struct Xform {
+  float m[16], inv[16];  // row-major
+};
+
+__global__ void k_mesh_transform(float* __restrict__ pos, float* __restrict__ nrm, uint32_t nvert, Xform t) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nvert) return;
+  float* p = pos + 3ull * i;
+  const float x = p[0], y = p[1], z = p[2];
+  float r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float a = t.m[4 * k + 3];
+    a = __fadd_rn(__fmul_rn(t.m[4 * k + 2], z), a);
+    a = __fadd_rn(__fmul_rn(t.m[4 * k + 1], y), a);
+    r[k] = __fadd_rn(__fmul_rn(t.m[4 * k + 0], x), a);
+  }
+  if (r[3] == 1.f || r[3] == 0.f) {
+    p[0] = r[0];
+    p[1] = r[1];
+    p[2] = r[2];
+  } else {
+    p[0] = __fdiv_rn(r[0], r[3]);
+    p[1] = __fdiv_rn(r[1], r[3]);
+    p[2] = __fdiv_rn(r[2], r[3]);
+  }
+  float* n = nrm + 3ull * i;
+  const float nx = n[0], ny = n[1], nz = n[2];
+  float q[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float a = __fmul_rn(t.inv[12 + k], 0.f);
+    a = __fadd_rn(__fmul_rn(t.inv[8 + k], nz), a);
+    a = __fadd_rn(__fmul_rn(t.inv[4 + k], ny), a);
+    q[k] = __fadd_rn(__fmul_rn(t.inv[k], nx), a);
+  }
+  const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(q[0], q[0]), __fmul_rn(q[1], q[1])), __fmul_rn(q[2], q[2])));
+  n[0] = __fdiv_rn(q[0], len);
+  n[1] = __fdiv_rn(q[1], len);
+  n[2] = __fdiv_rn(q[2], len);
+}
+
 template <int W>
 __global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ rays, int any, int32_t* prim,
                             float* tout, float* b1out, float* b2out) {
@@ -1978,6 +2079,10 @@ int32_t run_adjoint(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, co
 
 }  // namespace
 
+struct gyt_mesh {
+  gyt::ObjMesh mesh;
+};
+
 extern "C" {
 
 int32_t gyt_context_create(int32_t device, gyt_context** out) {
@@ -2574,6 +2679,134 @@ int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaMemcpyAsync(rgb_out, ctx->d_rgb, rb, cudaMemcpyDeviceToHost, ctx->stream));
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_mesh_load_obj(const char* path, int32_t reverse_vertices, gyt_mesh** out, char* err, uint32_t err_len) {
+  auto report = [&](const std::string& m) {
+    if (err && err_len) {
+      std::strncpy(err, m.c_str(), err_len - 1);
+      err[err_len - 1] = '\0';
+    }
+  };
+  if (!path || !out) {
+    report("mesh_load_obj: null argument");
+    return GYT_ERR_INVALID;
+  }
+  *out = nullptr;
+  auto* m = new gyt_mesh();
+  std::string msg;
+  if (!load_obj(path, reverse_vertices != 0, &m->mesh, &msg)) {
+    delete m;
+    report(msg);
+    return GYT_ERR_INVALID;
+  }
+  *out = m;
+  return GYT_OK;
+}
+
+int32_t gyt_mesh_size(const gyt_mesh* mesh, uint32_t* n_triangles) {
+  if (!mesh || !n_triangles) return GYT_ERR_INVALID;
+  *n_triangles = mesh->mesh.triangles();
+  return GYT_OK;
+}
+
+int32_t gyt_mesh_read(const gyt_mesh* mesh, float* positions, float* normals, float* uvs) {
+  if (!mesh) return GYT_ERR_INVALID;
+  const ObjMesh& m = mesh->mesh;
+  if (positions) std::memcpy(positions, m.pos.data(), m.pos.size() * sizeof(float));
+  if (normals) std::memcpy(normals, m.nrm.data(), m.nrm.size() * sizeof(float));
+  if (uvs) std::memcpy(uvs, m.uv.data(), m.uv.size() * sizeof(float));
+  return GYT_OK;
+}
+
+int32_t gyt_mesh_transform(gyt_context* ctx, gyt_mesh* mesh, const float* matrix, const float* inverse) {
+  if (!ctx || !mesh || !matrix || !inverse) return fail(ctx, GYT_ERR_INVALID, "mesh_transform: null argument");
+  ObjMesh& m = mesh->mesh;
+  const uint64_t nvert = 3ull * m.triangles();
+  if (nvert == 0) return GYT_OK;
+  if (nvert >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "mesh_transform: mesh too large");
+  Xform t;
+  std::memcpy(t.m, matrix, sizeof(t.m));
+  std::memcpy(t.inv, inverse, sizeof(t.inv));
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  float *dp = nullptr, *dn = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dp, 3 * nvert));
+  GYT_CK(ctx, dalloc(tmp, &dn, 3 * nvert));
+  GYT_CK(ctx, cudaMemcpyAsync(dp, m.pos.data(), 3 * nvert * 4, cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(dn, m.nrm.data(), 3 * nvert * 4, cudaMemcpyHostToDevice, ctx->stream));
+  k_mesh_transform<<<grid_for(nvert), kBlock, 0, ctx->stream>>>(dp, dn, (uint32_t)nvert, t);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaMemcpyAsync(m.pos.data(), dp, 3 * nvert * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(m.nrm.data(), dn, 3 * nvert * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+void gyt_mesh_destroy(gyt_mesh* mesh) { delete mesh; }
+
+int32_t gyt_film_quantize(gyt_context* ctx, const double* d_film, uint32_t res_x, uint32_t res_y, float gamma,
+                          uint8_t* rgb8_out) {
+  if (!ctx || !d_film || !rgb8_out) return fail(ctx, GYT_ERR_INVALID, "film_quantize: null argument");
+  if (!(gamma > 0.f)) return fail(ctx, GYT_ERR_INVALID, "film_quantize: gamma must be positive");
+  const uint64_t npix = (uint64_t)res_x * res_y;
+  if (npix == 0 || npix > kPixMask) return fail(ctx, GYT_ERR_INVALID, "film_quantize: bad film size");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  uint8_t* d = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &d, 3 * npix));
+  GYT_CK(ctx, after_legacy_stream(ctx));
+  k_film_rgb8<<<grid_for(npix), kBlock, 0, ctx->stream>>>(d_film, d, (uint32_t)npix, 1.f / gamma);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaMemcpyAsync(rgb8_out, d, 3 * npix, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_film_save(gyt_context* ctx, const double* d_film, uint32_t res_x, uint32_t res_y, const char* path) {
+  if (!ctx || !d_film || !path) return fail(ctx, GYT_ERR_INVALID, "film_save: null argument");
+  const std::string name(path);
+  const std::string suffix = name.size() >= 4 ? name.substr(name.size() - 4) : std::string();
+  if (suffix != ".png" && suffix != ".bmp" && suffix != ".hdr")
+    return fail(ctx, GYT_ERR_INVALID, "film_save: the file name must end in .png, .bmp or .hdr");
+  const uint64_t npix = (uint64_t)res_x * res_y;
+  if (npix == 0 || npix > kPixMask) return fail(ctx, GYT_ERR_INVALID, "film_save: bad film size");
+  std::vector<uint8_t> host;
+  bool ok = false;
+  if (suffix == ".hdr") {
+    GYT_CK(ctx, cudaSetDevice(ctx->device));
+    std::vector<void*> tmp;
+    struct Guard {
+      std::vector<void*>& v;
+      ~Guard() { for (void* q : v) cudaFree(q); }
+    } guard{tmp};
+    uint8_t* d = nullptr;
+    GYT_CK(ctx, dalloc(tmp, &d, 4 * npix));
+    GYT_CK(ctx, after_legacy_stream(ctx));
+    k_film_rgbe<<<grid_for(npix), kBlock, 0, ctx->stream>>>(d_film, d, (uint32_t)npix);
+    GYT_CK(ctx, cudaGetLastError());
+    host.resize(4 * npix);
+    GYT_CK(ctx, cudaMemcpyAsync(host.data(), d, 4 * npix, cudaMemcpyDeviceToHost, ctx->stream));
+    GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    ok = write_hdr_rgbe(name, host.data(), res_x, res_y);
+  } else {
+    host.resize(3 * npix);
+    // ImageIO::WriteImage's default gamma (image/ImageIO.h:47)
+    const int32_t st = gyt_film_quantize(ctx, d_film, res_x, res_y, 2.2f, host.data());
+    if (st) return st;
+    ok = suffix == ".png" ? write_png_rgb8(name, host.data(), res_x, res_y)
+                          : write_bmp_rgb8(name, host.data(), res_x, res_y);
+  }
+  if (!ok) return fail(ctx, GYT_ERR_INVALID, "film_save: cannot write " + name);
   return GYT_OK;
 }
 

@@ -203,6 +203,49 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
 
+/* ---- Meshes from Wavefront OBJ files ---------------------------------------
+ * Mesh::LoadFromFile (mesh/Mesh.cpp:7-90) with the reference's vendored
+ * tinyobjloader (external/tinyobjloader, v2.0.0-rc) restated: its number
+ * parsing, face-index rules (1-based, negative = relative) and polygon
+ * triangulation (ear clipping). One record per triangle, three new vertices
+ * each; normals from the file, else the face normal Cross(p1 - p0, p2 - p0)
+ * normalised; reverse_vertices swaps the second and third vertex. Malformed
+ * input (index 0, out-of-range indices, a face with normals on some of its
+ * vertices only) fails with a message in err (err_len bytes, may be NULL).
+ * Host only: no GPU needed. */
+typedef struct gyt_mesh gyt_mesh;
+int32_t gyt_mesh_load_obj(const char* path, int32_t reverse_vertices, gyt_mesh** out, char* err, uint32_t err_len);
+int32_t gyt_mesh_size(const gyt_mesh* mesh, uint32_t* n_triangles);
+/* positions and normals: n_triangles*9 floats (p0 p1 p2, n0 n1 n2), uvs:
+ * n_triangles*6; any may be NULL. */
+int32_t gyt_mesh_read(const gyt_mesh* mesh, float* positions, float* normals, float* uvs);
+/* Scene::AddMesh's Triangle::SetTransform (visual/Scene.h:68-77,
+ * shape/Triangle.h:78-88) on the GPU of ctx: positions by matrix (w-divide
+ * unless w is 0 or 1), normals by the transpose of inverse, normalised; both
+ * 4x4 row-major, as Transform holds them (math/Transform.h). The mesh keeps
+ * the result. */
+int32_t gyt_mesh_transform(gyt_context* ctx, gyt_mesh* mesh, const float* matrix, const float* inverse);
+void gyt_mesh_destroy(gyt_mesh* mesh);
+
+/* ---- Film output ----------------------------------------------------------
+ * Film::SaveImage (visual/Film.cpp:6-9) on the GPU: colour / weight per pixel
+ * (Film::WriteToPixelBuffer, visual/Film.h:128-136) and ImageIO::toInt
+ * (image/ImageIO.cpp:66-68): int(pow(clamp(c, 0, 1), 1 / gamma) * 255 + 0.5)
+ * per channel, in float as the reference. d_film: res_x*res_y*4 doubles on
+ * the context's device (colour sums and weights, as gyt_render_device
+ * accumulates them); rgb8_out: host, res_x*res_y*3 bytes, row 0 = the top
+ * image row. Pixels of weight 0 give 0. */
+int32_t gyt_film_quantize(gyt_context* ctx, const double* d_film, uint32_t res_x, uint32_t res_y, float gamma,
+                          uint8_t* rgb8_out);
+
+/* ImageIO::WriteImage (image/ImageIO.cpp:117-149) of a device film by the
+ * file name's suffix: .png and .bmp with gyt_film_quantize's bytes at gamma
+ * 2.2, .hdr as Radiance RGBE of colour / weight (the RGBE encoding on the
+ * GPU). The containers are this library's own encoders (uncompressed PNG
+ * deflate blocks, 24-bit BMP, run-length-layout HDR); decoded pixels equal
+ * the reference's. */
+int32_t gyt_film_save(gyt_context* ctx, const double* d_film, uint32_t res_x, uint32_t res_y, const char* path);
+
 /* HaltonSampler::sample with Faure permutations (sampler/Halton.h:648-905)
  * for n (dimension, index) pairs; dimensions >= 256 give 0. */
 int32_t gyt_halton(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out);

@@ -74,7 +74,7 @@ SOURCES = [
     "math/LowDiscrepency.cpp", "visual/Medium.cpp", "system/Memory.cpp", "visual/Microfacet.cpp",
     "integrator/PT.cpp", "camera/PinholeCamera.cpp", "visual/Primitive.cpp", "math/Ray.cpp",
     "sampler/Sampler.cpp", "visual/Sampling.cpp", "visual/Scene.cpp", "shape/Shape.cpp",
-    "sampler/Sobol.cpp", "sampler/SobolEnum.cpp", "integrator/TiledIntegrator.cpp",
+    "sampler/Sobol.cpp", "sampler/SobolEnum.cpp", "integrator/TiledIntegrator.cpp", "mesh/Mesh.cpp",
     "math/Transform.cpp", "shape/Triangle.cpp", "visual/Film.cpp", "visual/Visibility.cpp",
 ]
 

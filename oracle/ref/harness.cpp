@@ -13,6 +13,11 @@
 //   render  <scene> <out.bin> [rows]           TiledIntegrator::Render, timed
 //   camera  <scene> <out.bin>                  RasterToWorld matrix (row-major f32)
 //   bsdf    <cases.bin> <out.bin>              BxDF Sample/Evaluate/Pdf tables
+//   toint   <in.bin> <gamma> <out.bin>         f32 -> i32 ImageIO::toInt
+//   image   <rgb.bin> <w> <h> <path>           f32 RGB -> ImageIO::WriteImage (.png .bmp .hdr)
+//   obj     <file.obj> <reverse> <spec> <out.bin>  Mesh::LoadFromFile, then Triangle::SetTransform
+//           by the transform of spec ("-": none; else "T x y z;S x y z;RX a;RY a;RZ a" composed
+//           left to right); 18 f32 per triangle: p0 p1 p2 n0 n1 n2
 // paths and render use SobolSampler + SobolEnum, or HaltonSampler (Faure
 // permutations) + HaltonEnum when GYREF_SAMPLER=halton.
 // Standard and shim headers first, so the access override below only reaches
@@ -50,6 +55,8 @@
 #include "light/EnvLight.h"
 #include "shape/Sphere.h"
 #include "system/Memory.h"
+#include "image/ImageIO.h"
+#include "mesh/Mesh.h"
 #undef private
 #undef protected
 
@@ -463,11 +470,74 @@ int cmd_bsdf(int argc, char** argv) {
   return 0;
 }
 
+int cmd_toint(int argc, char** argv) {
+  std::vector<char> in = read_file(argv[2]);
+  const float gamma = (float)std::atof(argv[3]);
+  size_t n = in.size() / 4;
+  std::vector<int32_t> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    float x;
+    std::memcpy(&x, &in[4 * i], 4);
+    out[i] = ImageIO::toInt(x, gamma);
+  }
+  write_file(argv[4], out.data(), out.size() * 4);
+  return 0;
+}
+
+int cmd_obj(int argc, char** argv) {
+  Mesh mesh;
+  mesh.LoadFromFile(argv[2], std::atoi(argv[3]) != 0);
+  const std::string spec = argv[4];
+  const bool apply = spec != "-";
+  Transform t;
+  if (apply) {
+    std::stringstream ss(spec);
+    std::string item;
+    while (std::getline(ss, item, ';')) {
+      std::stringstream is(item);
+      std::string op;
+      is >> op;
+      float a = 0, b = 0, c = 0;
+      is >> a >> b >> c;
+      Transform u;
+      if (op == "T") u = Transform::Translate(Vec3(a, b, c));
+      else if (op == "S") u = Transform::Scale(a, b, c);
+      else if (op == "RX") u = Transform::RotateX(a);
+      else if (op == "RY") u = Transform::RotateY(a);
+      else if (op == "RZ") u = Transform::RotateZ(a);
+      else throw std::runtime_error("bad transform " + op);
+      t = t * u;
+    }
+  }
+  std::vector<float> out;
+  for (const Triangle& src : mesh.untransformedTriangles) {
+    Triangle tri = src;
+    if (apply) tri.SetTransform(t);
+    const Vec3* v[6] = {&tri.p0, &tri.p1, &tri.p2, &tri.n0, &tri.n1, &tri.n2};
+    for (const Vec3* q : v) out.insert(out.end(), {q->x, q->y, q->z});
+  }
+  write_file(argv[5], out.data(), out.size() * 4);
+  return 0;
+}
+
+int cmd_image(int argc, char** argv) {
+  std::vector<char> in = read_file(argv[2]);
+  const uint32_t w = (uint32_t)std::atoi(argv[3]), h = (uint32_t)std::atoi(argv[4]);
+  std::vector<Vec3> img((size_t)w * h);
+  for (size_t i = 0; i < img.size(); ++i) {
+    float c[3];
+    std::memcpy(c, &in[12 * i], 12);
+    img[i] = Vec3(c[0], c[1], c[2]);
+  }
+  ImageIO::WriteImage(argv[5], img, w, h);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|halton|henum|hits|anyhit|paths|render|camera|bsdf> ...\n");
+    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|halton|henum|toint|image|obj|hits|anyhit|paths|render|camera|bsdf> ...\n");
     return 2;
   }
   try {
@@ -482,6 +552,9 @@ int main(int argc, char** argv) {
     if (c == "render") return cmd_render(argc, argv);
     if (c == "camera") return cmd_camera(argc, argv);
     if (c == "bsdf") return cmd_bsdf(argc, argv);
+    if (c == "toint") return cmd_toint(argc, argv);
+    if (c == "image") return cmd_image(argc, argv);
+    if (c == "obj") return cmd_obj(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", c.c_str());
     return 2;
   } catch (const std::exception& e) {

@@ -152,6 +152,31 @@ def ref_render(tmp, scene_path, rows=None, spp=None, threads=None, sampler=None)
     return img, info
 
 
+def ref_toint(tmp, x, gamma):
+    """ImageIO::toInt (image/ImageIO.cpp:66-68) of float values."""
+    a, b = os.path.join(tmp, "toint_in.bin"), os.path.join(tmp, "toint_out.bin")
+    np.ascontiguousarray(x, np.float32).tofile(a)
+    run("toint", a, repr(float(gamma)), b)
+    return np.fromfile(b, np.int32)
+
+
+def ref_write_image(tmp, rgb, path):
+    """ImageIO::WriteImage (image/ImageIO.cpp:117-149) of a float RGB image
+    (h, w, 3) to path (.png, .bmp or .hdr)."""
+    a = os.path.join(tmp, "image_in.bin")
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    rgb.tofile(a)
+    run("image", a, rgb.shape[1], rgb.shape[0], path)
+
+
+def ref_obj(tmp, obj_path, reverse, spec):
+    """Mesh::LoadFromFile of obj_path, then Triangle::SetTransform by the
+    transform spec ("-" for none): (n, 6, 3) float32 p0 p1 p2 n0 n1 n2."""
+    b = os.path.join(tmp, "obj_out.bin")
+    run("obj", obj_path, int(reverse), spec, b)
+    return np.fromfile(b, np.float32).reshape(-1, 6, 3)
+
+
 def ref_bsdf(tmp, cases):
     """cases: structured array with fields type (u4), params (16 f4), wo, u, we (3 f4)."""
     a, b = os.path.join(tmp, "bsdf_in.bin"), os.path.join(tmp, "bsdf_out.bin")

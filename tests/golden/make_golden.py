@@ -7,6 +7,8 @@ checkout is only needed to regenerate; the tests read the fixtures.
 
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py halton     # only the Halton fixtures
+    python tests/golden/make_golden.py film       # only the film-output fixtures
+    python tests/golden/make_golden.py obj        # only the OBJ-mesh fixtures
 """
 import os
 import sys
@@ -105,7 +107,126 @@ def halton_golden(tmp):
     np.savez_compressed(os.path.join(HERE, "image_cornell_64x64_4spp_halton.npz"), film=img)
 
 
+def film_output_golden(tmp):
+    """ImageIO::toInt at three gammas and ImageIO::WriteImage of one float
+    image to .png, .bmp and .hdr (decoded pixels stored)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from image_tools import read_hdr_rgbe, read_rgb8
+    rng = np.random.default_rng(20261205)
+    x = np.concatenate([rng.uniform(-0.2, 1.3, 15000), np.linspace(0.0, 1.0, 5001),
+                        np.array([0.0, 1.0, -0.0, 1e-30, 1e-7, 0.5, 2.0, -1.0])]).astype(np.float32)
+    out = {"x": x}
+    for g in (2.2, 1.8, 1.0):
+        out["toint_%g" % g] = io.ref_toint(tmp, x, g)
+    h, w = 23, 37  # odd sizes: BMP row padding, HDR run-length scanlines
+    img = np.zeros((h, w, 3), np.float32)
+    img[..., 0] = np.linspace(0, 1.2, w)[None, :]
+    img[..., 1] = np.linspace(-0.1, 1.0, h)[:, None]
+    img[..., 2] = rng.lognormal(-1.0, 1.5, (h, w))
+    img[0, 0] = 0.0
+    img[1, 1] = (5000.0, 0.25, 1e-3)
+    out["image"] = img
+    for ext in ("png", "bmp", "hdr"):
+        path = os.path.join(tmp, "ref." + ext)
+        io.ref_write_image(tmp, img, path)
+        out["decoded_" + ext] = read_hdr_rgbe(path) if ext == "hdr" else read_rgb8(path)
+    np.savez_compressed(os.path.join(HERE, "film_output.npz"), **out)
+
+
+OBJ_TRANSFORMS = ["T 0 -0.5 0;S 0.28 0.28 0.28",                       # CornellBox.h:534
+                  "T 0 -0.35 0;S 0.02 0.02 0.02;T -50 0 50;RX -90;S 1 2 1",  # CornellBox.h:1200-1208
+                  "RY 30;RZ 45;T 0.1 0.2 0.3;S 2 3 0.5;RX 17.5"]
+
+
+def obj_files(rng):
+    """Synthetic OBJ files for the loader: polygons (convex, concave,
+    collinear), every face-index form and number format, line endings."""
+    files = {}
+    # a 4x3 grid of quads with texture coordinates and normals, a pentagon, an
+    # L-shaped (concave) hexagon and a quad with three collinear vertices
+    lines = ["# quads and polygons", "o grid", "g grid"]
+    for j in range(4):
+        for i in range(5):
+            z = 0.05 * np.sin(i + 2 * j)
+            lines.append("v %.6f %.6f %.6f" % (i * 0.25, j * 0.3, z))
+            lines.append("vt %.4f %.4f" % (i / 4, j / 3))
+            lines.append("vn %.6f %.6f %.6f" % (0.1 * i, 0.05 * j, 1.0))
+    for j in range(3):
+        for i in range(4):
+            a = 1 + i + 5 * j
+            q = (a, a + 1, a + 6, a + 5)
+            lines.append("f " + " ".join("%d/%d/%d" % (k, k, k) for k in q))
+    lines.append("usemtl other")
+    base = 20
+    for ang in range(5):
+        t = 2 * np.pi * ang / 5
+        lines.append("v %.7f %.7f 1.5" % (np.cos(t), np.sin(t)))
+    lines.append("f %s" % " ".join(str(base + 1 + k) for k in range(5)))
+    lshape = [(0, 0), (2, 0), (2, 1), (1, 1), (1, 2), (0, 2)]
+    for x, y in lshape:
+        lines.append("v %g %g -1" % (x, y))
+    lines.append("f %s" % " ".join(str(base + 6 + k) for k in range(6)))
+    for x in (0, 1, 2):
+        lines.append("v %d 5 0.5" % x)
+    lines.append("v 1 6 0.5")
+    lines.append("f -4 -3 -2 -1")
+    files["polygons.obj"] = "\n".join(lines) + "\n"
+    # index forms (v, v/vt, v//vn, v/vt/vn, negative), number formats, CRLF
+    # line endings, tabs, comments, a face of two vertices (skipped)
+    body = ["# forms", "v 1e-3 .5 -.25", "v +2 3. 1.000000001", "v -0 1E+2 0.1234567890123",
+            "v\t0.5\t0.25\t-0.125  ", "vn 0 0 1", "vn 0 1 0", "vt 0.5 0.5", "vt 1 0",
+            "s off", "f 1 2 3", "f 1/1 2/2 3/1", "f 1//1 2//2 4//1", "f -4/-2/-2 -3/-1/-1 -1/-2/-2",
+            "f 1 2", "", "   # indented comment", "g second", "f\t2 3 4"]
+    files["forms.obj"] = "\r\n".join(body) + "\r\n"
+    # no normals anywhere (face normals generated), one zero-area triangle
+    ico = ["v 0 0 0", "v 1 0 0", "v 0 1 0", "v 0 0 1", "v 2 0 0", "v 3 0 0",
+           "f 1 2 3", "f 1 3 4", "f 1 4 2", "f 2 4 3", "f 2 5 6"]
+    files["generated_normals.obj"] = "\n".join(ico) + "\n"
+    # a seeded noisy sphere (latitude-longitude, quads at the poles become triangles)
+    sph = []
+    nu, nv = 24, 12
+    for j in range(nv + 1):
+        for i in range(nu):
+            th, ph = np.pi * j / nv, 2 * np.pi * i / nu
+            r = 1 + 0.05 * rng.standard_normal()
+            sph.append("v %.7f %.7f %.7f" % (r * np.sin(th) * np.cos(ph), r * np.cos(th), r * np.sin(th) * np.sin(ph)))
+    for j in range(nv):
+        for i in range(nu):
+            a, b = j * nu + i + 1, j * nu + (i + 1) % nu + 1
+            sph.append("f %d %d %d %d" % (a, b, b + nu, a + nu))
+    files["sphere.obj"] = "\n".join(sph) + "\n"
+    return files
+
+
+def obj_golden(tmp):
+    """Mesh::LoadFromFile of the synthetic OBJ files (both vertex orders) and
+    Triangle::SetTransform by three of the reference's own transforms."""
+    rng = np.random.default_rng(20261206)
+    odir = os.path.join(HERE, "obj")
+    os.makedirs(odir, exist_ok=True)
+    out = {}
+    for name, text in obj_files(rng).items():
+        path = os.path.join(odir, name)
+        with open(path, "w", newline="") as f:
+            f.write(text)
+        key = name[:-4]
+        for rev in (0, 1):
+            out["%s_rev%d" % (key, rev)] = io.ref_obj(tmp, path, rev, "-")
+        for k, spec in enumerate(OBJ_TRANSFORMS):
+            out["%s_t%d" % (key, k)] = io.ref_obj(tmp, path, 0, spec)
+    out["transforms"] = np.array(OBJ_TRANSFORMS)
+    np.savez_compressed(os.path.join(HERE, "obj_meshes.npz"), **out)
+
+
 def main():
+    if sys.argv[1:] == ["obj"]:
+        obj_golden(tempfile.mkdtemp())
+        print("OBJ golden vectors written to", HERE)
+        return
+    if sys.argv[1:] == ["film"]:
+        film_output_golden(tempfile.mkdtemp())
+        print("film-output golden vectors written to", HERE)
+        return
     if not io.have_harness():
         sys.exit("build the reference harness first: python oracle/ref/build_ref.py")
     tmp = tempfile.mkdtemp()
@@ -191,6 +312,8 @@ def main():
     cases = bsdf_cases(rng)
     np.savez_compressed(os.path.join(HERE, "bsdf.npz"), cases=cases.view(np.uint8), out=io.ref_bsdf(tmp, cases))
     halton_golden(tmp)
+    film_output_golden(tmp)
+    obj_golden(tmp)
     print("golden vectors written to", HERE)
 
 
