@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--adjoint-iters", type=int, default=200,
                     help="Adam iterations of the inverse-rendering run after the adjoint timing (0 = skip the run)")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-light-tracing", action="store_true",
+                    help="skip the light-tracing measurement (Cornell box, 512x512, 16 photons per pixel)")
     return ap.parse_args()
 
 
@@ -335,6 +337,10 @@ def run_ours(a):
         adj = measure_adjoint(a, d, g, torch)
         if d.rank == 0:
             line["adjoint"] = adj
+    if not a.no_light_tracing:
+        lt = measure_light_tracing(a, d, g, torch)
+        if d.rank == 0:
+            line["light_tracing"] = lt
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.close()
@@ -586,6 +592,47 @@ def measure_batch(a, d, g, torch):
         sc.close()
     ctx.close()
     return line
+
+
+def measure_light_tracing(a, d, g, torch):
+    """LightTracing (integrator/LT.h) on the Cornell box with its spheres,
+    512x512, 16 photons per pixel, depth 8: Mphotons/s on the GPU (device
+    time, median of the steps) and the reference's LightTracing::Render on
+    the host cores at 1 photon per pixel."""
+    from gyunity_b200 import scenes
+    sd = scenes.cornell_box(res=512, spp=16, max_depth=8)
+    ctx = g.Context(d.local)
+    sc = g.Scene(sd, ctx)
+    buf = torch.zeros(512 * 512 * 3, dtype=torch.float64, device="cuda")
+    ms = []
+    for k in range(a.warmup + a.steps):
+        st = ctx.render_light_tracing_device(sc, sd.camera, sd.params, buf.data_ptr())
+        if k >= a.warmup:
+            ms.append(st["ms"])
+    t = d.max(statistics.median(ms))
+    photons = 512 * 512 * 16
+    out = {"workload": "Cornell box with mirror and glass spheres, 512x512, 16 photons per pixel, depth 8",
+           "value": photons * d.world / (t / 1e3) / 1e6, "unit": "Mphotons/s", "ms_per_step": t,
+           "note": "one kernel launch per render (a photon per thread, closest-hit and camera-join rays traced "
+                   "inline); the splat buffer accumulates in FP64"}
+    if d.rank == 0 and not a.no_cpu_baseline:
+        try:
+            import copy
+            from oracle import scene_io as io
+            if io.have_harness():
+                s1 = copy.deepcopy(sd)
+                s1.params.spp = 1
+                with tempfile.TemporaryDirectory() as tmp:
+                    path = os.path.join(tmp, "lt.gyts")
+                    io.write_scene(path, s1)
+                    _, info = io.ref_light_render(tmp, path)
+                out["cpu_baseline"] = {"value": info["photons"] / info["render_s"] / 1e6, "unit": "Mphotons/s",
+                                       "cores": os.cpu_count(), "kind": "reference",
+                                       "sample": "LightTracing::Render of the same scene at 1 photon per pixel"}
+        except Exception as e:  # reported, never fatal for the GPU numbers
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    ctx.close()
+    return out
 
 
 def measure_adjoint(a, d, g, torch):

@@ -27,8 +27,8 @@ from ._capi import GytError, load
 from . import _capi as _c
 from .scenes import Camera, RenderParams, SceneDesc
 
-__all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "Renderer", "GytError", "SceneDesc",
-           "Camera", "RenderParams", "scenes", "default_context"]
+__all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "LightTracing", "Renderer", "GytError",
+           "SceneDesc", "Camera", "RenderParams", "scenes", "default_context"]
 
 
 class Context:
@@ -192,6 +192,17 @@ class Context:
         self.check(self._lib.gyt_sobol(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
         return out
 
+    def render_light_tracing_device(self, scene, camera, params, d_splat_ptr):
+        """gyt_render_light_tracing_device: LightTracing's splats accumulated
+        into a device buffer of res_x*res_y*3 doubles."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_render_light_tracing_device(self.handle, scene.handle, ctypes.byref(cam),
+                                                             ctypes.byref(prm), ctypes.c_void_p(int(d_splat_ptr)),
+                                                             ctypes.byref(st)))
+        return {"paths": st.paths, "ms": st.ms}
+
     def film_quantize(self, d_film_ptr, res_x, res_y, gamma=2.2):
         """gyt_film_quantize: a device film (res_x*res_y*4 doubles) as 8-bit
         RGB (res_y, res_x, 3), ImageIO::toInt on the GPU."""
@@ -300,6 +311,19 @@ class Scene:
                                                    _c.ptr(prim), _c.ptr(t), _c.ptr(b1), _c.ptr(b2)))
         return (prim.astype(bool),) if any_hit else (prim, t, b1, b2)
 
+    def trace_light_paths(self, photons, camera=None, params=None):
+        """LightTracing per photon index: (n, max_depth, 6) records of every
+        vertex's camera join (on film 1/0 or -1, X, Y, splatted RGB)."""
+        cam = _c.camera_struct(camera or self.desc.camera)
+        p = params or self.desc.params
+        prm = _c.params_struct(p)
+        ids = np.ascontiguousarray(photons, np.uint64)
+        out = np.empty((ids.shape[0], p.max_depth, 6), np.float32)
+        self.ctx.check(self.ctx._lib.gyt_trace_light_paths(self.ctx.handle, self.handle, ctypes.byref(cam),
+                                                           ctypes.byref(prm), ids.shape[0], _c.ptr(ids),
+                                                           _c.ptr(out)))
+        return out
+
     def trace_paths(self, xys, camera=None, params=None, decisions=False):
         """PathTracing::Li of explicit samples (n, 3) = x, y, s. Returns
         radiance (n, 3), Sobol' dimensions used and roulette-draw masks; with
@@ -315,6 +339,27 @@ class Scene:
                                                      ctypes.byref(prm), n, _c.ptr(xys), _c.ptr(L), _c.ptr(cur),
                                                      _c.ptr(rr), _c.ptr(occ), _c.ptr(mis)))
         return (L, cur, rr, occ, mis) if decisions else (L, cur, rr)
+
+
+class LightTracing:
+    """Drop-in for LightTracing(sampler, maxDepth, spp) (integrator/LT.h:14-15):
+    Render writes the splat image (Film::AddSplat) to the camera's film."""
+
+    def __init__(self, max_depth, spp, sampler="sobol"):
+        if sampler not in _c.SAMPLERS:
+            raise ValueError("sampler must be one of %s" % sorted(_c.SAMPLERS))
+        self.params = RenderParams(int(spp), int(max_depth), 5, sampler)
+
+    def Render(self, scene, camera):
+        ctx = scene.ctx
+        cam = _c.camera_struct(camera.cam)
+        prm = _c.params_struct(self.params)
+        film = camera.GetFilm()
+        rgb = np.empty((film.mResY, film.mResX, 3), np.float32)
+        ctx.check(ctx._lib.gyt_render_light_tracing(ctx.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                                    _c.ptr(rgb)))
+        film.SetImage(rgb)
+        return film
 
 
 class Film:

@@ -22,6 +22,7 @@ EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_c
            "gyt_scene_read_bvh", "gyt_render", "gyt_render_device",
            "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_halton",
            "gyt_halton_enum_index", "gyt_camera_raster_to_world", "gyt_film_quantize", "gyt_film_save",
+           "gyt_render_light_tracing", "gyt_render_light_tracing_device", "gyt_trace_light_paths",
            "gyt_mesh_load_obj", "gyt_mesh_size", "gyt_mesh_read", "gyt_mesh_transform", "gyt_mesh_destroy",
            "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
            "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune", "gyt_scene_set_materials",
@@ -130,6 +131,10 @@ def load():
     L.gyt_halton_enum_index.argtypes = [P, U32, U32, U64, P, P]
     L.gyt_film_quantize.argtypes = [P, P, U32, U32, ctypes.c_float, P]
     L.gyt_film_save.argtypes = [P, P, U32, U32, ctypes.c_char_p]
+    L.gyt_render_light_tracing.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P]
+    L.gyt_render_light_tracing_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams),
+                                                  P, ctypes.POINTER(GytRenderStats)]
+    L.gyt_trace_light_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P]
     L.gyt_mesh_load_obj.argtypes = [ctypes.c_char_p, I32, ctypes.POINTER(P), ctypes.c_char_p, U32]
     L.gyt_mesh_size.argtypes = [P, ctypes.POINTER(U32)]
     L.gyt_mesh_read.argtypes = [P, P, P, P]

@@ -537,6 +537,9 @@ struct Lobe {
   float3 a, b, ceta, ck;
   float eta, eta1;
   GGX g;
+  // TransportMode::Importance (light tracing): no eta^2 radiance scaling in
+  // the transmission lobes (bsdf/BSDF.h:266-271, 505, 608)
+  bool importance = false;
 
   GYT_D int flags() const { return (type == 0 || type == 1 || type == 3) ? kRefl : (kRefl | kTrans); }
   GYT_D bool delta() const { return type == 1 || type == 2; }
@@ -570,7 +573,7 @@ struct Lobe {
       wh = wh * sgnf(wh.z);
       float F = fr_dielectric(dot(wo, wh), 1.f, eta);
       float sd = dot(wo, wh) + e * dot(wi, wh);
-      float factor = 1.f / e;
+      float factor = importance ? 1.f : 1.f / e;
       float value = (1.f - F) * g.D(wh) * g.G(wo, wi, wh) * e * e * fabsf(dot(wi, wh)) * fabsf(dot(wo, wh)) /
                     fabsf(ci * co * sd * sd);
       return b * fabsf(value * factor * factor);
@@ -648,6 +651,7 @@ struct Lobe {
       if (!refract(wo, nf, eI / eT, wi)) return zero;
       *pdf = 1.f - P;
       float e = eI / eT;
+      if (importance) return b * (1.f - Re) / fabsf(wi->z);
       return b * (e * e) * (1.f - Re) / fabsf(wi->z);
     }
     if (type == 3) {  // MicrofacetReflectionBSDF::Sample (BSDF.h:331-346)
@@ -685,7 +689,7 @@ struct Lobe {
       *pdf = fabsf((1.f - P) * g.pdf(wo, wh) * dwh);
       float co = wo.z, ci = wi->z;
       if (ci == 0.f || co == 0.f) return zero;
-      float factor = 1.f / e;
+      float factor = importance ? 1.f : 1.f / e;
       float value = (1.f - F) * g.D(wh) * g.G(wo, *wi, wh) * e * e * fabsf(dot(*wi, wh)) * fabsf(dot(wo, wh)) /
                     fabsf(ci * co * sd * sd);
       return b * fabsf(value * factor * factor);

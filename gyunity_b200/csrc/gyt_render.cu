@@ -1427,6 +1427,185 @@ __global__ void k_film_rgbe(const double* __restrict__ film, uint8_t* __restrict
   o[3] = (uint8_t)(e + 128);
 }
 
+// --------------------------------------------------------- light tracing ---
+// LightTracing (integrator/LT.h:11-230): photon g (< spp * W * H) uses the
+// sampler index g with the dimension cursor at 0. The light path starts on a
+// power-sampled area light (Triangle::Sample + cosine hemisphere about the
+// interpolated normal, AreaLight::SampleOnLight, light/AreaLight.h:60-78),
+// follows BSDF samples in importance transport without roulette, and every
+// vertex is joined to the pinhole camera (ConnectToCamera): the light vertex
+// with its emission, the others with We * f * throughput * |cos| / pdfW.
+// Unoccluded joins whose truncated raster position lies in [0, W] x [0, H]
+// are splatted (Film::AddSplat, visual/Film.h:89-104) scaled by
+// W * H / total photons.
+struct LtCam {
+  float w2r[16];             // world to raster (CameraToRaster * WorldToCamera), row-major
+  float3 pos, cz;            // camera position and viewing direction (camera/Camera.cpp:8)
+  float film_dist, film_area;
+  uint32_t res_x, res_y;
+  float fx, fy, ftotal;      // the splat scale factors in float: res_x, res_y, total photons
+};
+
+// ConnectToCamera for a vertex at pos: returns whether it lands on the film
+// (pixel X, Y) and leaves the direction to the camera and its distance.
+template <int W>
+GYT_D bool lt_join(const DevScene& s, const LtCam& c, float3 pos, int* X, int* Y, float3* dir, float* dist) {
+  const float3 h2c = c.pos - pos;
+  const float len = length(h2c);
+  const float3 d = h2c / len;
+  *dir = d;
+  *dist = len;
+  if (dot(c.cz, -d) < 0.f) return false;
+  float r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = ((c.w2r[4 * k + 3] + c.w2r[4 * k + 2] * pos.z) + c.w2r[4 * k + 1] * pos.y) +
+                                     c.w2r[4 * k] * pos.x;
+  if (!(r[3] == 1.f || r[3] == 0.f)) {
+    r[0] = r[0] / r[3];
+    r[1] = r[1] / r[3];
+  }
+  const int xi = __float2int_rz(r[0]), yi = __float2int_rz(r[1]);
+  *X = xi;
+  *Y = yi;
+  if (!(xi >= 0 && xi <= (int)c.res_x && yi >= 0 && yi <= (int)c.res_y)) return false;
+  float tmax = len, b1 = 0.f, b2 = 0.f;  // Ray(pos, dir, len): the constructor's RayEps shift
+  return trace<W, true>(s, pos + d * kRayEps, d, tmax, b1, b2) < 0;
+}
+
+GYT_D void lt_splat(double* splat, const LtCam& c, int X, int Y, float3 L) {
+  X = min(max(X, 0), (int)c.res_x - 1);
+  Y = min(max(Y, 0), (int)c.res_y - 1);
+  double* p = splat + 3ull * ((unsigned long long)Y * c.res_x + X);
+  atomicAdd(p, (double)L.x);
+  atomicAdd(p + 1, (double)L.y);
+  atomicAdd(p + 2, (double)L.z);
+}
+
+// One thread per photon (grid-stride). rec (debug, may be null): per photon
+// max_depth records of (on film 1/0 or -1 for no vertex, X, Y, scaled L).
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_light_trace(DevScene s, LtCam c, Params prm, SamplerTables tab,
+                                                        unsigned long long n, const unsigned long long* __restrict__ ids,
+                                                        double* __restrict__ splat, float* __restrict__ rec) {
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long g = ids ? ids[t] : t;
+    float* out = rec ? rec + 6ull * prm.max_depth * t : nullptr;
+    if (out)
+      for (uint32_t k = 0; k < prm.max_depth; ++k) out[6 * k] = -1.f;
+    auto emit = [&](uint32_t k, bool on, int X, int Y, float3 L) {
+      L = ((L * c.fx) * c.fy) / c.ftotal;
+      if (out) {
+        out[6 * k] = on ? 1.f : 0.f;
+        out[6 * k + 1] = (float)X;
+        out[6 * k + 2] = (float)Y;
+        out[6 * k + 3] = L.x;
+        out[6 * k + 4] = L.y;
+        out[6 * k + 5] = L.z;
+      }
+      if (on && splat) lt_splat(splat, c, X, Y, L);
+    };
+    if (s.n_area <= 0) continue;
+    Rng rng{g, 0};
+    // GCC evaluates the arguments right to left: light choice, then v (y, x), then u (y, x)
+    const float ul = rng.next(tab, prm.sampler);
+    const float vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
+    const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
+    float lsel = 0.f;
+    const int li = sample_light(s, ul, &lsel);
+    if (li >= s.n_area) continue;  // environment light (rejected on the host)
+    const LightTri l = load_light(s, li);
+    const float su0 = sqrtf(ux);
+    const float b0 = 1.f - su0, b1 = uy * su0, b2 = 1.f - b0 - b1;
+    const float3 lpos = l.p0 * b0 + l.p1 * b1 + l.p2 * b2;
+    const float3 ln = l.n0 * b0 + l.n1 * b1 + l.n2 * b2;
+    // CoordinateSystem (math/GeometryUtils.h:11-17) and CosineSampleHemisphere
+    float3 ss;
+    {
+      const bool xz = fabsf(ln.x) > fabsf(ln.y);
+      const float den = xz ? sqrtf(ln.x * ln.x + ln.z * ln.z) : sqrtf(ln.y * ln.y + ln.z * ln.z);
+      ss = den == 0.f ? mk(0.f, 0.f, 0.f) : (xz ? mk(-ln.z, 0.f, ln.x) : mk(0.f, ln.z, -ln.y)) / den;  // Vector / 0 = 0
+    }
+    const float3 ts = cross(ln, ss);
+    float dx = 0.f, dy = 0.f;
+    {
+      const float ox = 2.f * vx - 1.f, oy = 2.f * vy - 1.f;
+      if (!(ox == 0.f && oy == 0.f)) {
+        float th, r;
+        if (fabsf(ox) > fabsf(oy)) { r = ox; th = kPiOver4 * (oy / ox); }
+        else { r = oy; th = kPiOver2 - kPiOver4 * (ox / oy); }
+        float sn, cs;
+        sincosf(th, &sn, &cs);
+        dx = r * cs;
+        dy = r * sn;
+      }
+    }
+    const float dz = sqrtf(fmaxf(0.f, 1.f - dx * dx - dy * dy));
+    const float3 dir = norm(ss * dx + ts * dy + ln * dz);
+    const float pdf_dir = dz * kInvPi, pdf_a = 1.f / l.area;
+    const float cos_l = fabsf(dot(ln, dir));
+    float3 tp = l.Le * cos_l / lsel / pdf_a / pdf_dir;
+    {
+      int X = 0, Y = 0;
+      float3 wd;
+      float dist;
+      const bool on = lt_join<W>(s, c, lpos, &X, &Y, &wd, &dist);
+      emit(0, on, X, Y, l.Le);
+    }
+    // a direction of pdf 0 (on the hemisphere's rim, where this GPU's cosine
+    // and the host library's can round differently) carries no flux
+    if (!(pdf_dir > 0.f)) continue;
+    float3 o = (lpos + dir * kRayEps) + dir * kRayEps, d = dir;
+    for (uint32_t bounce = 1; bounce < prm.max_depth;) {
+      float tmax = __int_as_float(0x7f800000), hb1 = 0.f, hb2 = 0.f;
+      const int prim = trace<W, false>(s, o, d, tmax, hb1, hb2);
+      if (prim < 0) break;
+      Hit h;
+      uint32_t mat;
+      if (prim < s.n_tris) {
+        float3 p0, p1, p2, n0, n1, n2, face;
+        int m, light;
+        load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, &light);
+        tri_hit(p0, p1, p2, n0, n1, n2, face, hb1, hb2, o, d, &h);
+        mat = (uint32_t)m;
+      } else {
+        const int k = prim - s.n_tris;
+        Ray r = sphere_object_ray(o, d, __int_as_float(0x7f800000), 0.f);
+        sphere_hit(__ldg(s.spheres + k), r, tmax, &h);
+        mat = __ldg(s.sphere_mat + k);
+      }
+      Bsdf bsdf;
+      bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
+      bsdf.lobe.importance = true;
+      bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+      {
+        int X = 0, Y = 0;
+        float3 wi;
+        float dist;
+        const bool on = lt_join<W>(s, c, h.pos, &X, &Y, &wi, &dist);
+        // PinHoleCamera::Sample_Wi and We (camera/PinholeCamera.h:31-49)
+        const float cos_c = dot(c.cz, -wi);
+        const float pdf_w = 1.f * (dist * dist) / cos_c;
+        const float c2 = cos_c * cos_c;
+        const float we = c.film_dist * c.film_dist * 1.f / (c.film_area * c2 * c2);
+        const float3 f = bsdf.eval(h.wo, wi);
+        const float3 L = mk(we, we, we) * f * tp * fabsf(dot(wi, h.n)) / pdf_w;
+        emit(bounce, on, X, Y, L);
+      }
+      ++bounce;
+      if (bounce >= prm.max_depth) break;
+      const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
+      float3 wi;
+      float pdf;
+      const float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
+      if (pdf == 0.f) break;  // the reference continues with an undefined direction here
+      o = (h.pos + wi * kRayEps) + wi * kRayEps;
+      d = wi;
+      tp = tp * f * fabsf(dot(wi, h.n)) / pdf;
+    }
+  }
+}
+
 // Scene::AddMesh's Triangle::SetTransform (shape/Triangle.h:78-88) per
 // vertex, in the reference's float arithmetic: a point is M (x, y, z, 1) with
 // the matrix applied column by column from the last (((M.3 + M.2 z) + M.1 y)
@@ -1847,6 +2026,99 @@ int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
     return fail(ctx, GYT_ERR_UNSUPPORTED, "params: max_depth must be in [1, 100] (Sobol' has 1024 dimensions)");
   if (p->rr_depth > 255) return fail(ctx, GYT_ERR_INVALID, "params: rr_depth too large");
   if (p->flags & ~GYT_SAMPLER_HALTON) return fail(ctx, GYT_ERR_INVALID, "params: unknown flags");
+  return GYT_OK;
+}
+
+// 4x4 inverse by Gauss-Jordan elimination with partial pivoting (double).
+bool invert4(const double a[16], double out[16]) {
+  double m[4][8];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? a[4 * i + j] : (j - 4 == i ? 1.0 : 0.0);
+  for (int c = 0; c < 4; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::fabs(m[r][c]) > std::fabs(m[piv][c])) piv = r;
+    if (m[piv][c] == 0.0) return false;
+    for (int j = 0; j < 8; ++j) std::swap(m[c][j], m[piv][j]);
+    const double d = m[c][c];
+    for (int j = 0; j < 8; ++j) m[c][j] /= d;
+    for (int r = 0; r < 4; ++r)
+      if (r != c) {
+        const double f = m[r][c];
+        for (int j = 0; j < 8; ++j) m[r][j] -= f * m[c][j];
+      }
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = m[i][4 + j];
+  return true;
+}
+
+// The camera quantities light tracing reads (camera/Camera.cpp:6-59) in float
+// as the reference computes them: mCz = -(pos - look).Norm(), the film plane
+// height 2 d tan(fovy / 2) and area; world to raster as the inverse of
+// RasterToWorld (in double, then float).
+int32_t make_lt_cam(gyt_context* ctx, const GytCamera* c, unsigned long long total, LtCam* out) {
+  double m[16], w[16];
+  raster_to_world(*c, m);
+  if (!invert4(m, w)) return fail(ctx, GYT_ERR_INVALID, "light_tracing: singular camera");
+  for (int i = 0; i < 16; ++i) out->w2r[i] = (float)w[i];
+  out->pos = mk(c->pos[0], c->pos[1], c->pos[2]);
+  const float dx = c->pos[0] - c->look_at[0], dy = c->pos[1] - c->look_at[1], dz = c->pos[2] - c->look_at[2];
+  const float len = std::sqrt((dx * dx + dy * dy) + dz * dz);
+  out->cz = mk(-(dx / len), -(dy / len), -(dz / len));
+  const float pi = (float)3.14159265358979;  // common/Core.h:185
+  const float height = c->film_distance * std::tan(c->fovy * 0.5f * pi / 180) * 2.f;
+  const float width = height * ((float)c->res_x / (float)c->res_y);
+  out->film_dist = c->film_distance;
+  out->film_area = width * height;
+  out->res_x = c->res_x;
+  out->res_y = c->res_y;
+  out->fx = (float)c->res_x;
+  out->fy = (float)c->res_y;
+  out->ftotal = (float)total;
+  return GYT_OK;
+}
+
+__global__ void k_splat_to_rgb(const double* __restrict__ splat, float* __restrict__ rgb, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rgb[i] = (float)splat[i];
+}
+
+// All photons of LightTracing::Render (n == 0: every photon, splatted into
+// d_splat) or the listed ones (ids, records only).
+int32_t run_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, uint64_t n, const unsigned long long* ids, double* d_splat,
+                          float* d_rec, GytRenderStats* stats) {
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  if (scene->dev.has_env)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "light_tracing: environment lights are not sampled (area lights only)");
+  Cam cam;
+  st = make_cam(ctx, camera, params, &cam);  // validates the film (and the sampler's enumeration limits)
+  if (st) return st;
+  const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  LtCam lc;
+  st = make_lt_cam(ctx, camera, total, &lc);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  GYT_CK(ctx, after_legacy_stream(ctx));
+  const Params prm = make_params(params);
+  const unsigned long long count = n ? n : total;
+  const uint32_t grid = (uint32_t)std::min<unsigned long long>((count + kBlock - 1) / kBlock,
+                                                                (unsigned long long)std::max(1, ctx->sms) * 8);
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  if (scene->dev.wnodes)
+    k_light_trace<8><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, lc, prm, tables(ctx), count, ids, d_splat, d_rec);
+  else
+    k_light_trace<2><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, lc, prm, tables(ctx), count, ids, d_splat, d_rec);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    *stats = GytRenderStats{count, 0, 1, 1, ms};
+  }
   return GYT_OK;
 }
 
@@ -2678,6 +2950,62 @@ int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
   k_resolve<<<grid_for(npix), kBlock, 0, ctx->stream>>>(ctx->d_film, ctx->d_rgb, (uint32_t)npix);
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaMemcpyAsync(rgb_out, ctx->d_rgb, rb, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_render_light_tracing_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                        const GytRenderParams* params, double* d_splat, GytRenderStats* stats) {
+  if (!ctx || !scene || !camera || !d_splat) return fail(ctx, GYT_ERR_INVALID, "light_tracing: null argument");
+  return run_light_tracing(ctx, scene, camera, params, 0, nullptr, d_splat, nullptr, stats);
+}
+
+int32_t gyt_render_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                 const GytRenderParams* params, float* rgb_out) {
+  if (!ctx || !scene || !camera || !rgb_out) return fail(ctx, GYT_ERR_INVALID, "light_tracing: null argument");
+  const uint64_t npix = (uint64_t)camera->res_x * camera->res_y;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  double* d = nullptr;
+  float* f = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &d, 3 * std::max<uint64_t>(npix, 1)));
+  GYT_CK(ctx, dalloc(tmp, &f, 3 * std::max<uint64_t>(npix, 1)));
+  GYT_CK(ctx, cudaMemsetAsync(d, 0, 3 * npix * sizeof(double), ctx->stream));
+  int32_t st = run_light_tracing(ctx, scene, camera, params, 0, nullptr, d, nullptr, nullptr);
+  if (st) return st;
+  k_splat_to_rgb<<<grid_for(3 * npix), kBlock, 0, ctx->stream>>>(d, f, 3 * npix);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaMemcpyAsync(rgb_out, f, 3 * npix * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                              const GytRenderParams* params, uint64_t n, const uint64_t* photons, float* records) {
+  if (!ctx || !scene || !camera || (n && (!photons || !records)))
+    return fail(ctx, GYT_ERR_INVALID, "trace_light_paths: null argument");
+  if (n == 0) return GYT_OK;
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  unsigned long long* di = nullptr;
+  float* dr = nullptr;
+  const uint64_t nrec = 6ull * params->max_depth * n;
+  GYT_CK(ctx, dalloc(tmp, &di, n));
+  GYT_CK(ctx, dalloc(tmp, &dr, nrec));
+  GYT_CK(ctx, cudaMemcpyAsync(di, photons, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  st = run_light_tracing(ctx, scene, camera, params, n, di, nullptr, dr, nullptr);
+  if (st) return st;
+  GYT_CK(ctx, cudaMemcpyAsync(records, dr, nrec * 4, cudaMemcpyDeviceToHost, ctx->stream));
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GYT_OK;
 }

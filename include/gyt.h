@@ -203,6 +203,30 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
 
+/* ---- Light tracing ---------------------------------------------------------
+ * LightTracing(sampler, maxDepth, spp) (integrator/LT.h:11-230) on the GPU:
+ * spp * res_x * res_y photons, photon g with sampler index g. Each light
+ * path starts on a power-sampled area light (cosine-weighted direction about
+ * the interpolated normal), follows BSDF samples in importance transport up
+ * to max_depth vertices (no roulette), and each vertex is joined to the
+ * pinhole camera; unoccluded joins are splatted (Film::AddSplat,
+ * visual/Film.h:89-104) scaled by res_x * res_y / photons. params: spp,
+ * max_depth and the sampler flag (rr_depth unused). Scenes with an
+ * environment light are refused (the reference samples area lights only).
+ * gyt_render_light_tracing: the splat image (res_x*res_y*3 floats, host);
+ * _device: accumulated into d_splat (res_x*res_y*3 doubles). Differences: a
+ * light direction or BSDF sample of pdf 0 ends the path (the reference
+ * divides by the zero pdf, or continues with an undefined direction). */
+int32_t gyt_render_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                 const GytRenderParams* params, float* rgb_out);
+int32_t gyt_render_light_tracing_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                        const GytRenderParams* params, double* d_splat, GytRenderStats* stats);
+/* Per-photon records for parity tests: for photons[i], max_depth records of
+ * 6 floats (on film 1 / 0, or -1 where the path has no such vertex; pixel X,
+ * Y; the splatted RGB), vertex 0 = the light vertex. */
+int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                              const GytRenderParams* params, uint64_t n, const uint64_t* photons, float* records);
+
 /* ---- Meshes from Wavefront OBJ files ---------------------------------------
  * Mesh::LoadFromFile (mesh/Mesh.cpp:7-90) with the reference's vendored
  * tinyobjloader (external/tinyobjloader, v2.0.0-rc) restated: its number

@@ -15,6 +15,9 @@
 //   bsdf    <cases.bin> <out.bin>              BxDF Sample/Evaluate/Pdf tables
 //   toint   <in.bin> <gamma> <out.bin>         f32 -> i32 ImageIO::toInt
 //   image   <rgb.bin> <w> <h> <path>           f32 RGB -> ImageIO::WriteImage (.png .bmp .hdr)
+//   lt      <scene> <photons.bin> <out.bin>    LightTracing: per photon (u64 index) max_depth records of
+//           (on film 1/0 or -1, X, Y, splatted RGB)
+//   ltrender <scene> <out.bin>                 LightTracing::Render, the film's splat buffer (W*H*3 f32)
 //   obj     <file.obj> <reverse> <spec> <out.bin>  Mesh::LoadFromFile, then Triangle::SetTransform
 //           by the transform of spec ("-": none; else "T x y z;S x y z;RX a;RY a;RZ a" composed
 //           left to right); 18 f32 per triangle: p0 p1 p2 n0 n1 n2
@@ -57,6 +60,7 @@
 #include "system/Memory.h"
 #include "image/ImageIO.h"
 #include "mesh/Mesh.h"
+#include "integrator/LT.h"
 #undef private
 #undef protected
 
@@ -484,6 +488,66 @@ int cmd_toint(int argc, char** argv) {
   return 0;
 }
 
+std::shared_ptr<Sampler> lt_sampler() {
+  const char* kind = std::getenv("GYREF_SAMPLER");
+  if (kind && std::string(kind) == "halton") return std::make_shared<HaltonSampler>(faure_halton());
+  return std::make_shared<SobolSampler>();
+}
+
+// LightTracing::Render's inner loop (integrator/LT.h:30-44) for listed photons.
+int cmd_lt(int argc, char** argv) {
+  LoadedScene ls = load_scene(argv[2]);
+  std::vector<char> in = read_file(argv[3]);
+  const size_t n = in.size() / 8;
+  std::shared_ptr<Sampler> sampler = lt_sampler();
+  LightTracing lt(sampler, ls.maxDepth, ls.spp);
+  const Camera& camera = *ls.camera;
+  const int64 resX = ls.resX, resY = ls.resY;
+  const int64 total = (int64)ls.spp * resX * resY;
+  std::vector<float> out(n * (size_t)ls.maxDepth * 6, 0.f);
+  MemoryPool arena;
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t g;
+    std::memcpy(&g, &in[8 * i], 8);
+    float* rec = &out[i * (size_t)ls.maxDepth * 6];
+    for (int k = 0; k < ls.maxDepth; ++k) rec[6 * k] = -1.f;
+    RandomStateSequence rand(sampler, g);
+    std::vector<PathVertex> lightPath(ls.maxDepth + 1);
+    int nv = lt.GenerateLightPath(*ls.scene, camera, rand, arena, lightPath);
+    for (int s = 0; s < nv && s < ls.maxDepth; ++s) {
+      Vec3 pRaster;
+      bool inScreen = false;
+      Vec3 L = lt.ConnectToCamera(*ls.scene, camera, rand, lightPath[s], s, &pRaster, &inScreen);
+      L = L * ls.film->mResX * ls.film->mResY / total;
+      rec[6 * s] = inScreen ? 1.f : 0.f;
+      rec[6 * s + 1] = pRaster.x;
+      rec[6 * s + 2] = pRaster.y;
+      rec[6 * s + 3] = L.x; rec[6 * s + 4] = L.y; rec[6 * s + 5] = L.z;
+    }
+    arena.Reset();
+  }
+  write_file(argv[4], out.data(), out.size() * 4);
+  return 0;
+}
+
+int cmd_ltrender(int argc, char** argv) {
+  LoadedScene ls = load_scene(argv[2]);
+  LightTracing lt(lt_sampler(), ls.maxDepth, ls.spp);
+  auto t0 = std::chrono::steady_clock::now();
+  lt.Render(*ls.scene, *ls.camera);
+  auto t1 = std::chrono::steady_clock::now();
+  const size_t npx = (size_t)ls.resX * ls.resY;
+  std::vector<float> img(npx * 3);
+  for (size_t i = 0; i < npx; ++i) {
+    const Pixel& p = ls.film->mPixelBuffer[i];
+    img[3 * i] = p.splat.x; img[3 * i + 1] = p.splat.y; img[3 * i + 2] = p.splat.z;
+  }
+  write_file(argv[3], img.data(), img.size() * 4);
+  const double sec = std::chrono::duration<double>(t1 - t0).count();
+  std::printf("{\"render_s\": %.6f, \"photons\": %.0f}\n", sec, (double)ls.spp * npx);
+  return 0;
+}
+
 int cmd_obj(int argc, char** argv) {
   Mesh mesh;
   mesh.LoadFromFile(argv[2], std::atoi(argv[3]) != 0);
@@ -537,7 +601,7 @@ int cmd_image(int argc, char** argv) {
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|halton|henum|toint|image|obj|hits|anyhit|paths|render|camera|bsdf> ...\n");
+    std::fprintf(stderr, "usage: gyref_harness <sobol|enum|halton|henum|toint|image|obj|lt|ltrender|hits|anyhit|paths|render|camera|bsdf> ...\n");
     return 2;
   }
   try {
@@ -555,6 +619,8 @@ int main(int argc, char** argv) {
     if (c == "toint") return cmd_toint(argc, argv);
     if (c == "image") return cmd_image(argc, argv);
     if (c == "obj") return cmd_obj(argc, argv);
+    if (c == "lt") return cmd_lt(argc, argv);
+    if (c == "ltrender") return cmd_ltrender(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", c.c_str());
     return 2;
   } catch (const std::exception& e) {

@@ -169,6 +169,24 @@ def ref_write_image(tmp, rgb, path):
     run("image", a, rgb.shape[1], rgb.shape[0], path)
 
 
+def ref_light_paths(tmp, scene_path, photons, sampler=None):
+    """LightTracing per photon: (n, max_depth, 6) records (on film 1/0 or -1,
+    X, Y, splatted RGB)."""
+    a, b = os.path.join(tmp, "lt_in.bin"), os.path.join(tmp, "lt_out.bin")
+    np.ascontiguousarray(photons, np.uint64).tofile(a)
+    run("lt", scene_path, a, b, env=_sampler_env(sampler))
+    return np.fromfile(b, np.float32).reshape(len(photons), -1, 6)
+
+
+def ref_light_render(tmp, scene_path, sampler=None):
+    """LightTracing::Render: the film's splat buffer (h, w, 3) and the timing."""
+    import json
+    b = os.path.join(tmp, "ltimg.bin")
+    out = run("ltrender", scene_path, b, env=_sampler_env(sampler))
+    info = json.loads(out.strip().splitlines()[-1])
+    return np.fromfile(b, np.float32), info
+
+
 def ref_obj(tmp, obj_path, reverse, spec):
     """Mesh::LoadFromFile of obj_path, then Triangle::SetTransform by the
     transform spec ("-" for none): (n, 6, 3) float32 p0 p1 p2 n0 n1 n2."""

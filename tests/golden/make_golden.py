@@ -9,6 +9,7 @@ checkout is only needed to regenerate; the tests read the fixtures.
     python tests/golden/make_golden.py halton     # only the Halton fixtures
     python tests/golden/make_golden.py film       # only the film-output fixtures
     python tests/golden/make_golden.py obj        # only the OBJ-mesh fixtures
+    python tests/golden/make_golden.py lt         # only the light-tracing fixtures
 """
 import os
 import sys
@@ -218,7 +219,31 @@ def obj_golden(tmp):
     np.savez_compressed(os.path.join(HERE, "obj_meshes.npz"), **out)
 
 
+def light_tracing_golden(tmp):
+    """LightTracing per photon (records of every vertex's camera join) and
+    LightTracing::Render of the Cornell box."""
+    rng = np.random.default_rng(20261207)
+    for name, sd in (("cornell_nospheres", scenes.cornell_box(res=64, spp=4, max_depth=6, spheres=False)),
+                     ("cornell", scenes.cornell_box(res=64, spp=4, max_depth=6)),
+                     ("mixed", scenes.mixed_materials_box(level=3, res=48, spp=4))):
+        path = os.path.join(tmp, "lt_%s.gyts" % name)
+        io.write_scene(path, sd)
+        total = sd.camera.res_x * sd.camera.res_y * sd.params.spp
+        ids = np.sort(rng.choice(total, 3000, replace=False)).astype(np.uint64)
+        np.savez_compressed(os.path.join(HERE, "lt_paths_%s.npz" % name), photons=ids,
+                            records=io.ref_light_paths(tmp, path, ids))
+    sd = scenes.cornell_box(res=64, spp=16, max_depth=6)
+    path = os.path.join(tmp, "lt_img.gyts")
+    io.write_scene(path, sd)
+    img, _ = io.ref_light_render(tmp, path)
+    np.savez_compressed(os.path.join(HERE, "image_lt_cornell_64x64_16spp.npz"), splat=img.reshape(64, 64, 3))
+
+
 def main():
+    if sys.argv[1:] == ["lt"]:
+        light_tracing_golden(tempfile.mkdtemp())
+        print("light-tracing golden vectors written to", HERE)
+        return
     if sys.argv[1:] == ["obj"]:
         obj_golden(tempfile.mkdtemp())
         print("OBJ golden vectors written to", HERE)
@@ -314,6 +339,7 @@ def main():
     halton_golden(tmp)
     film_output_golden(tmp)
     obj_golden(tmp)
+    light_tracing_golden(tmp)
     print("golden vectors written to", HERE)
 
 
