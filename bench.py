@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-light-tracing", action="store_true",
                     help="skip the light-tracing measurement (Cornell box, 512x512, 16 photons per pixel)")
+    ap.add_argument("--no-volume", action="store_true",
+                    help="skip the volumetric path-tracing measurement (Cornell box in fog, 512x512, 16 spp)")
     return ap.parse_args()
 
 
@@ -341,6 +343,10 @@ def run_ours(a):
         lt = measure_light_tracing(a, d, g, torch)
         if d.rank == 0:
             line["light_tracing"] = lt
+    if not a.no_volume:
+        vol = measure_volume(a, d, g, torch)
+        if d.rank == 0:
+            line["volume"] = vol
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.close()
@@ -629,6 +635,46 @@ def measure_light_tracing(a, d, g, torch):
                 out["cpu_baseline"] = {"value": info["photons"] / info["render_s"] / 1e6, "unit": "Mphotons/s",
                                        "cores": os.cpu_count(), "kind": "reference",
                                        "sample": "LightTracing::Render of the same scene at 1 photon per pixel"}
+        except Exception as e:  # reported, never fatal for the GPU numbers
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    ctx.close()
+    return out
+
+
+def measure_volume(a, d, g, torch):
+    """VolPathTracing (integrator/VPT.cpp) on the Cornell box filled with a
+    homogeneous medium (sigma_a 0.05, sigma_s 0.5, HG g 0.3) behind a
+    material-less front quad, with its mirror and glass spheres, 512x512,
+    16 spp, depth 8: Mpaths/s on the GPU (device time, median of the steps)
+    and the reference's TiledIntegrator::Render with VolPathTracing on the
+    host cores over the first 128 rows."""
+    from gyunity_b200 import scenes
+    sd = scenes.cornell_fog(res=512, spp=16, max_depth=8)
+    ctx = g.Context(d.local)
+    sc = g.Scene(sd, ctx)
+    film = torch.zeros(512 * 512 * 4, dtype=torch.float64, device="cuda")
+    ms = []
+    for k in range(a.warmup + a.steps):
+        st = ctx.render_volume_device(sc, sd.camera, sd.params, film.data_ptr())
+        if k >= a.warmup:
+            ms.append(st["ms"])
+    t = d.max(statistics.median(ms))
+    paths = 512 * 512 * 16
+    out = {"workload": "Cornell box in a homogeneous medium with mirror and glass spheres, 512x512, 16 spp, depth 8",
+           "value": paths * d.world / (t / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": t,
+           "note": "one kernel launch per render (a camera sample per thread; closest-hit, transmittance and "
+                   "shadow rays traced inline); FP64 film"}
+    if d.rank == 0 and not a.no_cpu_baseline:
+        try:
+            from oracle import scene_io as io
+            if io.have_harness():
+                with tempfile.TemporaryDirectory() as tmp:
+                    path = os.path.join(tmp, "vpt.gyts")
+                    io.write_scene(path, sd)
+                    _, info = io.ref_render(tmp, path, rows=128, integrator="vpt")
+                out["cpu_baseline"] = {"value": info["mpaths_per_s"], "unit": "Mpaths/s", "cores": info["threads"],
+                                       "kind": "reference",
+                                       "sample": "TiledIntegrator::Render with VolPathTracing, first 128 rows"}
         except Exception as e:  # reported, never fatal for the GPU numbers
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     ctx.close()

@@ -27,7 +27,8 @@ from ._capi import GytError, load
 from . import _capi as _c
 from .scenes import Camera, RenderParams, SceneDesc
 
-__all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "LightTracing", "Renderer", "GytError",
+__all__ = ["Context", "Scene", "Film", "PinHoleCamera", "GpuPathTracing", "LightTracing", "VolPathTracing", "Renderer",
+           "GytError",
            "SceneDesc", "Camera", "RenderParams", "scenes", "default_context"]
 
 
@@ -192,6 +193,16 @@ class Context:
         self.check(self._lib.gyt_sobol(self.handle, d.shape[0], _c.ptr(d), _c.ptr(i), _c.ptr(out)))
         return out
 
+    def render_volume_device(self, scene, camera, params, d_film_ptr):
+        """gyt_render_volume_device: VolPathTracing into a device film
+        (res_x*res_y*4 doubles, accumulated)."""
+        cam = _c.camera_struct(camera)
+        prm = _c.params_struct(params)
+        st = _c.GytRenderStats()
+        self.check(self._lib.gyt_render_volume_device(self.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                                      ctypes.c_void_p(int(d_film_ptr)), ctypes.byref(st)))
+        return {"paths": st.paths, "ms": st.ms}
+
     def render_light_tracing_device(self, scene, camera, params, d_splat_ptr):
         """gyt_render_light_tracing_device: LightTracing's splats accumulated
         into a device buffer of res_x*res_y*3 doubles."""
@@ -311,6 +322,20 @@ class Scene:
                                                    _c.ptr(prim), _c.ptr(t), _c.ptr(b1), _c.ptr(b2)))
         return (prim.astype(bool),) if any_hit else (prim, t, b1, b2)
 
+    def trace_volume_paths(self, xys, camera=None, params=None):
+        """VolPathTracing::Li of explicit samples (n, 3) = x, y, s: radiance
+        (n, 3) and the sampler dimensions each used."""
+        cam = _c.camera_struct(camera or self.desc.camera)
+        prm = _c.params_struct(params or self.desc.params)
+        xys = np.ascontiguousarray(xys, np.uint32).reshape(-1, 3)
+        n = xys.shape[0]
+        L = np.empty((n, 3), np.float32)
+        cur = np.empty(n, np.uint32)
+        self.ctx.check(self.ctx._lib.gyt_trace_volume_paths(self.ctx.handle, self.handle, ctypes.byref(cam),
+                                                            ctypes.byref(prm), n, _c.ptr(xys), _c.ptr(L),
+                                                            _c.ptr(cur)))
+        return L, cur
+
     def trace_light_paths(self, photons, camera=None, params=None):
         """LightTracing per photon index: (n, max_depth, 6) records of every
         vertex's camera join (on film 1/0 or -1, X, Y, splatted RGB)."""
@@ -339,6 +364,28 @@ class Scene:
                                                      ctypes.byref(prm), n, _c.ptr(xys), _c.ptr(L), _c.ptr(cur),
                                                      _c.ptr(rr), _c.ptr(occ), _c.ptr(mis)))
         return (L, cur, rr, occ, mis) if decisions else (L, cur, rr)
+
+
+class VolPathTracing:
+    """Drop-in for VolPathTracing(spp, maxDepth, sampler, samplerEnum, false)
+    (integrator/VPT.h:12-19): volumetric path tracing through the scene's
+    homogeneous media (SceneDesc.media, tri_medium)."""
+
+    def __init__(self, spp, max_depth, sampler="sobol"):
+        if sampler not in _c.SAMPLERS:
+            raise ValueError("sampler must be one of %s" % sorted(_c.SAMPLERS))
+        self.params = RenderParams(int(spp), int(max_depth), 5, sampler)
+
+    def Render(self, scene, camera):
+        ctx = scene.ctx
+        cam = _c.camera_struct(camera.cam)
+        prm = _c.params_struct(self.params)
+        film = camera.GetFilm()
+        rgb = np.empty((film.mResY, film.mResX, 3), np.float32)
+        ctx.check(ctx._lib.gyt_render_volume(ctx.handle, scene.handle, ctypes.byref(cam), ctypes.byref(prm),
+                                             _c.ptr(rgb)))
+        film.SetImage(rgb)
+        return film
 
 
 class LightTracing:

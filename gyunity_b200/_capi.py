@@ -23,6 +23,7 @@ EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_c
            "gyt_trace_paths", "gyt_intersect", "gyt_sobol", "gyt_sobol_enum_index", "gyt_halton",
            "gyt_halton_enum_index", "gyt_camera_raster_to_world", "gyt_film_quantize", "gyt_film_save",
            "gyt_render_light_tracing", "gyt_render_light_tracing_device", "gyt_trace_light_paths",
+           "gyt_render_volume", "gyt_render_volume_device", "gyt_trace_volume_paths",
            "gyt_mesh_load_obj", "gyt_mesh_size", "gyt_mesh_read", "gyt_mesh_transform", "gyt_mesh_destroy",
            "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
            "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune", "gyt_scene_set_materials",
@@ -56,7 +57,8 @@ class GytSceneDesc(ctypes.Structure):
                 ("tri_material", ctypes.c_void_p), ("tri_emission", ctypes.c_void_p), ("spheres", ctypes.c_void_p),
                 ("sphere_material", ctypes.c_void_p), ("mat_type", ctypes.c_void_p), ("mat_params", ctypes.c_void_p),
                 ("emission", ctypes.c_void_p), ("env_w", ctypes.c_uint32), ("env_h", ctypes.c_uint32),
-                ("env", ctypes.c_void_p), ("env_scale", ctypes.c_float)]
+                ("env", ctypes.c_void_p), ("env_scale", ctypes.c_float), ("n_media", ctypes.c_uint32),
+                ("media", ctypes.c_void_p), ("tri_medium", ctypes.c_void_p)]
 
 
 class GytCamera(ctypes.Structure):
@@ -135,6 +137,11 @@ def load():
     L.gyt_render_light_tracing_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams),
                                                   P, ctypes.POINTER(GytRenderStats)]
     L.gyt_trace_light_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P, P]
+    L.gyt_render_volume.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P]
+    L.gyt_render_volume_device.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P,
+                                           ctypes.POINTER(GytRenderStats)]
+    L.gyt_trace_volume_paths.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), U64, P,
+                                         P, P]
     L.gyt_mesh_load_obj.argtypes = [ctypes.c_char_p, I32, ctypes.POINTER(P), ctypes.c_char_p, U32]
     L.gyt_mesh_size.argtypes = [P, ctypes.POINTER(U32)]
     L.gyt_mesh_read.argtypes = [P, P, P, P]
@@ -191,7 +198,8 @@ def scene_struct(sd):
     keep = [c(sd.vertices, np.float32), c(sd.normals, np.float32), c(sd.indices, np.uint32),
             c(sd.tri_material, np.uint32), c(sd.tri_emission, np.int32), c(sd.spheres, np.float32),
             c(sd.sphere_material, np.uint32), c(sd.mat_type, np.uint32), c(sd.mat_params, np.float32),
-            c(sd.emission, np.float32), c(sd.env, np.float32)]
+            c(sd.emission, np.float32), c(sd.env, np.float32), c(getattr(sd, "media", None), np.float32),
+            c(getattr(sd, "tri_medium", None), np.int32)]
     s = GytSceneDesc()
     s.n_vertices, s.n_triangles = sd.vertices.shape[0], sd.n_triangles
     s.n_spheres, s.n_materials, s.n_emission = sd.n_spheres, sd.mat_type.shape[0], sd.emission.shape[0]
@@ -201,4 +209,9 @@ def scene_struct(sd):
         s.env_h, s.env_w = sd.env.shape[:2]
         s.env = keep[10].ctypes.data
     s.env_scale = sd.env_scale
+    if keep[11] is not None:
+        s.n_media = keep[11].reshape(-1, 7).shape[0]
+        s.media = keep[11].ctypes.data
+    if keep[12] is not None:
+        s.tri_medium = keep[12].ctypes.data
     return s, keep

@@ -65,6 +65,8 @@ struct DevScene {
   int n_area;        // area lights come first; light n_area is the environment
   int has_env;
   EnvDev env;
+  const float4* media;        // 2 float4 per medium: (sigma_a, g), (sigma_s, 0); or null
+  int n_media;
 };
 
 // Light record (kLightRec float4): (p0, Le.r) (p1, Le.g) (p2, Le.b)
@@ -1606,6 +1608,436 @@ __global__ void __launch_bounds__(kBlock) k_light_trace(DevScene s, LtCam c, Par
   }
 }
 
+// ------------------------------------------------ volumetric path tracing ---
+// VolPathTracing::Li without equi-angular sampling (integrator/VPT.cpp:7-104)
+// with HomogeneousMedium (volume/Homogeneous.cpp:7-35) and the
+// Henyey-Greenstein phase function (visual/Medium.cpp). One camera sample
+// per thread; the closest-hit, transmittance and shadow rays are traced
+// inline. A ray carries its medium (-1 none); a surface hit takes the
+// triangle's MediumInterface when it is a transition, else the ray's medium
+// (Primitive::Intersect, visual/Primitive.cpp:5-18); a ray leaving a surface
+// takes the outside medium when it leaves along the shading normal, else the
+// inside (Intersection::GetMedium, visual/Intersection.h:80-82).
+struct MediumDev {
+  float3 sa, ss, st;
+  float g;
+};
+
+GYT_D MediumDev load_medium(const DevScene& s, int m) {
+  const float4 a = __ldg(s.media + 2 * m), b = __ldg(s.media + 2 * m + 1);
+  MediumDev r;
+  r.sa = f3(a);
+  r.ss = f3(b);
+  r.st = r.ss + r.sa;
+  r.g = a.w;
+  return r;
+}
+
+// HomogeneousMedium::Tr over a segment of parametric length t of direction d
+GYT_D float3 medium_tr(const MediumDev& m, float t, float dlen) {
+  const float tt = fminf(t * dlen, FLT_MAX);
+  return mk(expf(-m.st.x * tt), expf(-m.st.y * tt), expf(-m.st.z * tt));
+}
+
+// PhaseHG (visual/Medium.h:20-23)
+GYT_D float phase_hg(float cos_t, float g) {
+  const float denom = 1.f + g * g + 2.f * g * cos_t;
+  return 0.07957747154594766788f * (1.f - g * g) / (denom * sqrtf(denom));
+}
+
+// CoordinateSystem (math/GeometryUtils.h:11-17): a zero denominator gives a
+// zero vector (Vector / 0 in math/Linagl.h:353-361)
+GYT_D void coord_system(float3 v, float3* a, float3* b) {
+  const bool xz = fabsf(v.x) > fabsf(v.y);
+  const float den = xz ? sqrtf(v.x * v.x + v.z * v.z) : sqrtf(v.y * v.y + v.z * v.z);
+  *a = den == 0.f ? mk(0.f, 0.f, 0.f) : (xz ? mk(-v.z, 0.f, v.x) : mk(0.f, v.z, -v.y)) / den;
+  *b = cross(v, *a);
+}
+
+// HenyeyGreenstein::Sample_p: returns the phase value, sets wi
+GYT_D float phase_sample(float g, float3 wo, float u0, float u1, float3* wi) {
+  float cos_t;
+  if (fabsf(g) < 1e-3f) {
+    cos_t = 1.f - 2.f * u0;
+  } else {
+    const float sq = (1.f - g * g) / (1.f - g + 2.f * g * u0);
+    cos_t = (1.f + g * g - sq * sq) / (2.f * g);
+  }
+  const float sin_t = sqrtf(fmaxf(0.f, 1.f - cos_t * cos_t));
+  const float phi = 2.f * (float)3.14159265358979 * u1;
+  float3 v1, v2;
+  coord_system(wo, &v1, &v2);
+  *wi = v1 * (sin_t * cosf(phi)) + v2 * (sin_t * sinf(phi)) + (-wo) * cos_t;
+  return phase_hg(-cos_t, g);
+}
+
+// A scattering point: a surface hit (its shading data and MediumInterface)
+// or a medium point (no normal, no position error, one medium both sides).
+struct VPoint {
+  float3 pos, perr, abs_n, n, wo;
+  int m_in, m_out;
+  bool surface;
+  GYT_D int medium_along(float3 w) const { return dot(w, n) > 0.f ? m_out : m_in; }
+};
+
+// The triangle's MediumInterface when it is a transition, else the ray's medium
+GYT_D void surface_media(const DevScene& s, int prim, int ray_medium, int* in, int* out) {
+  *in = *out = ray_medium;
+  if (!s.media || prim < 0 || prim >= s.n_tris) return;
+  const uint32_t packed = __float_as_uint(__ldg(&s.tnrm[3 * prim + 2].w));
+  const int a = (int)(packed & 0xffffu) - 1, b = (int)(packed >> 16) - 1;
+  if (a != b) {
+    *in = a;
+    *out = b;
+  }
+}
+
+GYT_D uint32_t material_type(const DevScene& s, int prim) {
+  const uint32_t m = prim < s.n_tris ? (uint32_t)__float_as_int(__ldg(&s.tnrm[3 * prim].w))
+                                     : __ldg(s.sphere_mat + (prim - s.n_tris));
+  return __ldg(s.mtypes + m);
+}
+
+// Full hit record of prim along (o, d) (Scene::QueryIntersectionInfo)
+GYT_D void vpt_hit(const DevScene& s, int prim, float t, float b1, float b2, float3 o, float3 d, Hit* h,
+                   uint32_t* mat, int* light) {
+  if (prim < s.n_tris) {
+    float3 p0, p1, p2, n0, n1, n2, face;
+    int m;
+    load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, light);
+    tri_hit(p0, p1, p2, n0, n1, n2, face, b1, b2, o, d, h);
+    *mat = (uint32_t)m;
+  } else {
+    const int k = prim - s.n_tris;
+    Ray r = sphere_object_ray(o, d, __int_as_float(0x7f800000), 0.f);
+    sphere_hit(__ldg(s.spheres + k), r, t, h);
+    *mat = __ldg(s.sphere_mat + k);
+    *light = -1;
+  }
+}
+
+// VisibilityTester::Tr (visual/Visibility.cpp:13-30): segments between the
+// point and the light point, through surfaces of no material, each
+// attenuated by its medium; a surface with a material blocks.
+template <int W>
+GYT_D float3 vpt_tr(const DevScene& s, const VPoint& p0, float3 lpos, float3 lerr, float3 labs) {
+  float3 tr = mk(1.f, 1.f, 1.f);
+  float3 pos = p0.pos, perr = p0.perr, abs_n = p0.abs_n, n = p0.n;
+  int m_in = p0.m_in, m_out = p0.m_out;
+#pragma unroll 1
+  for (int hop = 0; hop < 64; ++hop) {
+    // Intersection::SpawnTo (visual/Intersection.h:64-72)
+    const float3 org = offset_origin(pos, perr, abs_n, lpos - pos);
+    const float3 tgt = offset_origin(lpos, lerr, labs, org - lpos);
+    float3 d = tgt - org;
+    const float dis = length(d);
+    d = d / dis;
+    const int medium = dot(d, n) > 0.f ? m_out : m_in;
+    const float3 o = org + d * kRayEps;
+    const float seg = dis - kShadowEps;
+    float tmax = seg, b1 = 0.f, b2 = 0.f;
+    int prim = trace<W, false>(s, o, d, tmax, b1, b2);
+    // The segment ends on the light's surface: a hit at its very end is
+    // settled in FP64, as the occlusion test of path tracing settles it.
+    if (prim >= 0 && prim < s.n_tris && tmax >= seg * 0.999998f) {
+      const float4* tv = s.tris + 3 * (size_t)prim;
+      if (!wt_intersect_fp64(wt_setup(o, d), f3(__ldg(tv)), f3(__ldg(tv + 1)), f3(__ldg(tv + 2)), seg)) {
+        prim = -1;
+        tmax = seg;
+      }
+    }
+    if (prim >= 0 && material_type(s, prim) != 5u) return mk(0.f, 0.f, 0.f);
+    if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
+    if (prim < 0) return tr;
+    Hit h;
+    uint32_t mat;
+    int light;
+    vpt_hit(s, prim, tmax, b1, b2, o, d, &h, &mat, &light);
+    surface_media(s, prim, medium, &m_in, &m_out);
+    pos = h.pos;
+    perr = h.perr;
+    abs_n = h.abs_n;
+    n = h.n;
+  }
+  return mk(0.f, 0.f, 0.f);
+}
+
+// Scene::IntersectTr (visual/Scene.cpp:14-26): the first surface with a
+// material along the ray and the transmittance up to it. The segment after a
+// surface of no material starts at its hit position (Triangle::Intersect's
+// barycentric point, no offset) in the inside medium of its interface, as
+// the reference's record of an unqueried hit gives.
+template <int W>
+GYT_D bool vpt_intersect_tr(const DevScene& s, float3 o, float3 d, int medium, int* prim_out, float* t_out,
+                            float* b1_out, float* b2_out, float3* o_out, float3* tr_out) {
+  float3 tr = mk(1.f, 1.f, 1.f);
+#pragma unroll 1
+  for (int hop = 0; hop < 64; ++hop) {
+    float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
+    const int prim = trace<W, false>(s, o, d, tmax, b1, b2);
+    if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
+    if (prim < 0) {
+      *tr_out = tr;
+      return false;
+    }
+    if (material_type(s, prim) != 5u || prim >= s.n_tris) {
+      *prim_out = prim;
+      *t_out = tmax;
+      *b1_out = b1;
+      *b2_out = b2;
+      *o_out = o;
+      *tr_out = tr;
+      return true;
+    }
+    float3 p0, p1, p2, n0, n1, n2, face;
+    int m, light;
+    load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, &light);
+    const float3 pos = p0 * (1.f - b1 - b2) + p1 * b1 + p2 * b2;
+    int in, out;
+    surface_media(s, prim, medium, &in, &out);
+    medium = in;
+    o = pos + d * kRayEps;
+  }
+  *tr_out = mk(0.f, 0.f, 0.f);
+  return false;
+}
+
+// Integrator::DirectIllumination with handleMedia (integrator/Integrator.cpp:9-107)
+// for a surface point (bsdf) or a medium point (phase g). u: uLight, u.y, u.x,
+// v.z, v.y, v.x as the caller draws them.
+template <int W>
+GYT_D float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, const Hit* h, float ul,
+                        float ux, float uy, float vx, float vy, float vz) {
+  if (s.n_lights <= 0) return mk(0.f, 0.f, 0.f);
+  float lsel = 0.f;
+  const int li = sample_light(s, ul, &lsel);
+  if (!(lsel > 0.f) || li >= s.n_area) return mk(0.f, 0.f, 0.f);
+  const LightTri l = load_light(s, li);
+  float3 L1 = mk(0.f, 0.f, 0.f), L2 = mk(0.f, 0.f, 0.f);
+  float w1 = 1.f, w2 = 1.f;
+  {
+    // AreaLight::Sample_Li -> Shape::Sample(ref) -> Triangle::Sample
+    const float su0 = sqrtf(ux);
+    const float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
+    const float3 lpos = l.p0 * bb0 + l.p1 * bb1 + l.p2 * bb2;
+    const float3 ln = l.n0 * bb0 + l.n1 * bb1 + l.n2 * bb2;
+    const float3 lerr = (vabs(l.p0 * bb0) + vabs(l.p1 * bb1) + vabs(l.p2 * bb2)) * gammaf(6);
+    float pdf = 1.f / l.area;
+    float3 w = p.pos - lpos;
+    if (length(w) == 0.f) {
+      pdf = 0.f;
+    } else {
+      w = norm(w);
+      pdf *= dot(p.pos - lpos, p.pos - lpos) / fabsf(dot(ln, -w));
+      if (isinf(pdf)) pdf = 0.f;
+    }
+    const float3 wi = norm(lpos - p.pos);
+    const float3 Li = dot(ln, -wi) > 0.f ? l.Le : mk(0.f, 0.f, 0.f);
+    if (pdf > 0.f && !is_zero(Li)) {
+      float spdf, cos_t = 1.f;
+      float3 f;
+      if (p.surface) {
+        spdf = bsdf->pdf(p.wo, wi);
+        f = bsdf->eval(p.wo, wi);
+        cos_t = fabsf(dot(p.n, wi));
+      } else {
+        const float ph = phase_hg(dot(p.wo, wi), g);
+        f = mk(ph, ph, ph);
+        spdf = ph;
+      }
+      if (!is_zero(f)) {
+        const float3 tr = vpt_tr<W>(s, p, lpos, lerr, l.face);
+        w1 = power_heuristic(pdf, spdf);
+        L1 = Li * tr * f * cos_t / pdf;
+      }
+    }
+  }
+  {
+    float3 wi, f;
+    float pdf, cos_t = 1.f;
+    if (p.surface) {
+      f = bsdf->sample(p.wo, &wi, &pdf, vx, vy, vz);
+      cos_t = fabsf(dot(p.n, wi));
+    } else {
+      const float ph = phase_sample(g, p.wo, vx, vy, &wi);
+      f = mk(ph, ph, ph);
+      pdf = ph;
+    }
+    if (pdf != 0.f && !is_zero(f)) {
+      // Intersection::SpawnRay (visual/Intersection.h:74-78)
+      const float3 o2 = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
+      Hit hh;
+      hh.pos = p.pos;
+      hh.perr = p.perr;
+      hh.abs_n = p.abs_n;
+      hh.n = p.n;
+      const float lpdf = tri_light_pdf(l, hh, o2, wi);
+      if (lpdf == 0.f) {
+        w2 = 0.f;
+      } else {
+        w2 = power_heuristic(pdf, lpdf);
+        int prim = -1;
+        float t = 0.f, b1 = 0.f, b2 = 0.f;
+        float3 ro, tr;
+        if (vpt_intersect_tr<W>(s, o2, wi, p.medium_along(wi), &prim, &t, &b1, &b2, &ro, &tr) && prim < s.n_tris &&
+            __float_as_int(__ldg(&s.tnrm[3 * prim + 1].w)) == li) {
+          Hit lh;
+          uint32_t mat;
+          int light;
+          vpt_hit(s, prim, t, b1, b2, ro, wi, &lh, &mat, &light);
+          if (dot(lh.n, -wi) > 0.f) L2 = l.Le * f * tr * cos_t / pdf;  // AreaLight::Emission(isect, -wi)
+        }
+      }
+    }
+  }
+  (void)h;
+  return (L1 * w1 + L2 * w2) / lsel;
+}
+
+// One camera sample per thread (grid-stride over the render's samples, or the
+// listed (x, y, s) of xys); film as gyt_render_device's, L_out/cursor_out for
+// parity tests.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
+                                                unsigned long long n, const uint32_t* __restrict__ xys,
+                                                double* __restrict__ film, float* __restrict__ L_out,
+                                                uint32_t* __restrict__ cursor_out) {
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t x, y, sm;
+    if (xys) {
+      x = xys[3 * t];
+      y = xys[3 * t + 1];
+      sm = xys[3 * t + 2];
+    } else {
+      const unsigned long long pixel = t / prm.spp;
+      sm = (uint32_t)(t - pixel * prm.spp);
+      y = (uint32_t)(pixel / cam.res_x);
+      x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+    }
+    // the camera sample (TiledIntegrator::Render, integrator/TiledIntegrator.cpp:40-47)
+    const bool halton = cam.sampler != 0;
+    const uint64_t idx = halton ? halton_enum_index(cam, sm, x, y) : enum_index(tab, cam.log2_res, sm, x, y);
+    Rng rng{idx, 0};
+    const float su = rng.next(tab, cam.sampler), sv = rng.next(tab, cam.sampler);
+    const float u = __fsub_rn(__fmul_rn(halton ? cam.h_sx : cam.res_pow2, su), (float)x);
+    const float v = __fsub_rn(__fmul_rn(halton ? cam.h_sy : cam.res_pow2, sv), (float)y);
+    float3 o, d;
+    camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
+    int medium = -1;  // the camera's medium (PinHoleCamera::GenerateRay: none)
+    float3 tp = mk(1.f, 1.f, 1.f), L = mk(0.f, 0.f, 0.f);
+    bool delta = false;
+    int crossings = 0;
+    for (int i = 0; i < (int)prm.max_depth; ++i) {
+      if (rng.cursor + 16u > (prm.sampler ? kHaltonDims : 1024u)) break;  // the sampler's dimensions are spent
+      float tmax = __int_as_float(0x7f800000), hb1 = 0.f, hb2 = 0.f;
+      const int prim = trace<W, false>(s, o, d, tmax, hb1, hb2);
+      bool scattered = false;
+      float3 mpos;
+      MediumDev md;
+      if (medium >= 0) {
+        // HomogeneousMedium::Sample (volume/Homogeneous.cpp:12-30)
+        md = load_medium(s, medium);
+        const float uc = rng.next(tab, prm.sampler), ud = rng.next(tab, prm.sampler);
+        const int ch = min((int)(uc * 3.f), 2);
+        const float sc = ch == 0 ? md.st.x : (ch == 1 ? md.st.y : md.st.z);
+        const float dist = -logf(1.f - ud) / sc;
+        const float dl = length(d);
+        const float tt = fminf(dist / dl, tmax);
+        scattered = tt < tmax;
+        const float tc = fminf(tt, FLT_MAX);  // Exp(-sigma_t * min(t, MaxReal) * |d|)
+        const float3 tr = mk(expf((-md.st.x * tc) * dl), expf((-md.st.y * tc) * dl), expf((-md.st.z * tc) * dl));
+        const float3 dens = scattered ? md.st * tr : tr;
+        float pdf = ((0.f + dens.x) + dens.y) + dens.z;
+        pdf *= 1.f / 3.f;
+        if (pdf == 0.f) pdf = 1.f;
+        tp = tp * (scattered ? tr * md.ss / pdf : tr / pdf);
+        if (scattered) mpos = o + d * tt;
+      }
+      if (is_zero(tp)) break;
+      if (scattered) {
+        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
+        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
+        const float ul = rng.next(tab, prm.sampler);
+        VPoint p;
+        p.pos = mpos;
+        p.perr = p.abs_n = p.n = mk(0.f, 0.f, 0.f);
+        p.wo = -d;
+        p.m_in = p.m_out = medium;
+        p.surface = false;
+        L = L + tp * vpt_direct<W>(s, p, nullptr, md.g, nullptr, ul, ux, uy, vx, vy, vz);
+        const float py = rng.next(tab, prm.sampler), px = rng.next(tab, prm.sampler);
+        float3 wi;
+        phase_sample(md.g, -d, px, py, &wi);
+        o = mpos + wi * kRayEps;  // MediumIntersection::SpawnRay: no offset
+        d = wi;
+        delta = false;
+        continue;
+      }
+      if (prim < 0) break;  // no environment light with media
+      Hit h;
+      uint32_t mat;
+      int light;
+      vpt_hit(s, prim, tmax, hb1, hb2, o, d, &h, &mat, &light);
+      int m_in, m_out;
+      surface_media(s, prim, medium, &m_in, &m_out);
+      const uint32_t mtype = __ldg(s.mtypes + mat);
+      if (mtype == 5u) {
+        // no BSDF: pass through without using a bounce (VPT.cpp:70-75)
+        o = offset_origin(h.pos, h.perr, h.abs_n, d) + d * kRayEps;
+        medium = dot(d, h.n) > 0.f ? m_out : m_in;
+        --i;
+        if (++crossings > 64) break;
+        continue;
+      }
+      Bsdf bsdf;
+      bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
+      bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+      if ((i == 0 || delta) && light >= 0) {
+        if (dot(h.n, h.wo) > 0.f) L = L + tp * load_light(s, light).Le;
+      } else {
+        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
+        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
+        const float ul = rng.next(tab, prm.sampler);
+        VPoint p;
+        p.pos = h.pos;
+        p.perr = h.perr;
+        p.abs_n = h.abs_n;
+        p.n = h.n;
+        p.wo = h.wo;
+        p.m_in = m_in;
+        p.m_out = m_out;
+        p.surface = true;
+        L = L + tp * vpt_direct<W>(s, p, &bsdf, 0.f, &h, ul, ux, uy, vx, vy, vz);
+      }
+      const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
+      float3 wi;
+      float pdf;
+      const float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
+      if (is_zero(f) || pdf == 0.f) break;
+      const float3 est = f * fabsf(dot(h.n, wi)) / pdf;
+      delta = bsdf.lobe.delta();
+      tp = tp * est;
+      o = offset_origin(h.pos, h.perr, h.abs_n, wi) + wi * kRayEps;
+      d = wi;
+      medium = dot(wi, h.n) > 0.f ? m_out : m_in;
+    }
+    if (L_out) {
+      L_out[3 * t] = L.x;
+      L_out[3 * t + 1] = L.y;
+      L_out[3 * t + 2] = L.z;
+    }
+    if (cursor_out) cursor_out[t] = rng.cursor;
+    if (film) {
+      const uint32_t pix_x = x, pix_y = y;
+      film_add(film, cam.res_x, pix_x, pix_y, L);
+      if (u == 0.f && x > 0) film_add(film, cam.res_x, pix_x - 1, pix_y, L);
+      if (v == 0.f && y > 0) film_add(film, cam.res_x, pix_x, pix_y - 1, L);
+      if (u == 0.f && x > 0 && v == 0.f && y > 0) film_add(film, cam.res_x, pix_x - 1, pix_y - 1, L);
+    }
+  }
+}
+
 // Scene::AddMesh's Triangle::SetTransform (shape/Triangle.h:78-88) per
 // vertex, in the reference's float arithmetic: a point is M (x, y, z, 1) with
 // the matrix applied column by column from the last (((M.3 + M.2 z) + M.1 y)
@@ -1717,13 +2149,13 @@ const void* persistent_fn(int kind) {
 // Leaf-order triangle data of a device-built BVH, the same records the host
 // path writes: tris[3k + c] = (p_c, triangle id bits for c = 0) and
 // tnrm[3k + c] = (vertex normal, or the face normal without normals; material
-// bits for c = 0, light bits for c = 1). The face normal is computed with the
+// bits for c = 0, light bits for c = 1, the packed medium interface for c = 2). The face normal is computed with the
 // host's IEEE operations in the host's order (no contraction), so both paths
 // store identical floats. leaf_of[t] = k.
 __global__ void k_leaf_data(uint32_t nt, const uint32_t* __restrict__ order, const float* __restrict__ V,
                             const uint32_t* __restrict__ I, const float* __restrict__ N,
-                            const int2* __restrict__ info, float4* __restrict__ tris, float4* __restrict__ tnrm,
-                            int* __restrict__ leaf_of) {
+                            const int2* __restrict__ info, const uint32_t* __restrict__ tmed, float4* __restrict__ tris,
+                            float4* __restrict__ tnrm, int* __restrict__ leaf_of) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   const uint32_t t = order[k];
@@ -1746,7 +2178,7 @@ __global__ void k_leaf_data(uint32_t nt, const uint32_t* __restrict__ order, con
   for (int c = 0; c < 3; ++c) {
     tris[3 * (size_t)k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? __int_as_float((int)t) : 0.f);
     const float3 n = N ? mk(N[3 * (size_t)vi[c]], N[3 * (size_t)vi[c] + 1], N[3 * (size_t)vi[c] + 2]) : face;
-    const float w = c == 0 ? __int_as_float(in.x) : (c == 1 ? __int_as_float(in.y) : 0.f);
+    const float w = c == 0 ? __int_as_float(in.x) : (c == 1 ? __int_as_float(in.y) : __uint_as_float(tmed ? tmed[t] : 0u));
     tnrm[3 * (size_t)k + c] = make_float4(n.x, n.y, n.z, w);
   }
 }
@@ -2111,6 +2543,41 @@ int32_t run_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCam
     k_light_trace<8><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, lc, prm, tables(ctx), count, ids, d_splat, d_rec);
   else
     k_light_trace<2><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, lc, prm, tables(ctx), count, ids, d_splat, d_rec);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    *stats = GytRenderStats{count, 0, 1, 1, ms};
+  }
+  return GYT_OK;
+}
+
+// VolPathTracing (n == 0: every sample of the render into d_film; else the
+// listed (x, y, s) samples, radiance and dimensions used out).
+int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
+                   uint64_t n, const uint32_t* xys, double* d_film, float* L_out, uint32_t* cursor_out,
+                   GytRenderStats* stats) {
+  int32_t st = check_params(ctx, params);
+  if (st) return st;
+  if (scene->dev.has_env)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "render_volume: environment lights are not supported with media");
+  Cam cam;
+  st = make_cam(ctx, camera, params, &cam);
+  if (st) return st;
+  const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
+  const unsigned long long count = n ? n : total;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  GYT_CK(ctx, after_legacy_stream(ctx));
+  const Params prm = make_params(params);
+  const uint32_t grid = (uint32_t)std::min<unsigned long long>((count + kBlock - 1) / kBlock,
+                                                                (unsigned long long)std::max(1, ctx->sms) * 8);
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  if (scene->dev.wnodes)
+    k_vpt<8><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
+  else
+    k_vpt<2><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
@@ -2520,7 +2987,20 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: environment map too large");
   if ((uint64_t)d->n_triangles >= (1ull << 28)) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many triangles");
   for (uint32_t m = 0; m < d->n_materials; ++m)
-    if (d->mat_type[m] > 4) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
+    if (d->mat_type[m] > GYT_MAT_NONE) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
+  if (d->n_media && !d->media) return fail(ctx, GYT_ERR_INVALID, "scene_create: media array missing");
+  if (d->n_media >= 0xffffu) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many media");
+  // the triangles' medium interfaces, packed (inside + 1) | (outside + 1) << 16
+  std::vector<uint32_t> tmed;
+  if (d->tri_medium) {
+    tmed.resize(d->n_triangles);
+    for (uint32_t t = 0; t < d->n_triangles; ++t) {
+      const int32_t a = d->tri_medium[2 * t], b = d->tri_medium[2 * t + 1];
+      if (a < -1 || b < -1 || a >= (int32_t)d->n_media || b >= (int32_t)d->n_media)
+        return fail(ctx, GYT_ERR_INVALID, "scene_create: medium index out of range");
+      tmed[t] = (uint32_t)(a + 1) | ((uint32_t)(b + 1) << 16);
+    }
+  }
   std::vector<int2> info(d->n_triangles);
   std::vector<int> light_tris;
   std::vector<float> power;
@@ -2663,6 +3143,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     if (e == cudaSuccess) e = tup(&dI, d->indices, (size_t)nt * 3);
     if (e == cudaSuccess && d->normals) e = tup(&dN, d->normals, (size_t)d->n_vertices * 3);
     if (e == cudaSuccess) e = tup(&dInfo, info.data(), info.size());
+    uint32_t* dTmed = nullptr;
+    if (e == cudaSuccess && !tmed.empty()) e = tup(&dTmed, tmed.data(), tmed.size());
     if (e == cudaSuccess) e = tup(&dLeafOf, (const int*)nullptr, nt);
     if (e == cudaSuccess && n_area) e = tup(&dLights, light_tris.data(), light_tris.size());
     if (e == cudaSuccess && n_area) e = tup(&dLightLeaf, (const int*)nullptr, light_tris.size());
@@ -2680,7 +3162,7 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     if (e == cudaSuccess) e = dalloc(sc->allocs, &dn, (size_t)nt * 3);
     if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
     sc->bytes += (uint64_t)nt * 3 * 2 * sizeof(float4);
-    k_leaf_data<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(nt, g.order, dV, dI, dN, dInfo, dtris, dn, dLeafOf);
+    k_leaf_data<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(nt, g.order, dV, dI, dN, dInfo, dTmed, dtris, dn, dLeafOf);
     if (n_area)
       k_gather_int<<<(n_area + 255) / 256, 256, 0, ctx->stream>>>((uint32_t)n_area, dLights, dLeafOf, dLightLeaf);
     e = cudaGetLastError();
@@ -2722,7 +3204,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       for (int c = 0; c < 3; ++c) {
         tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : 0.f);
         float3 n = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
-        float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : 0.f);
+        uint32_t mw = tmed.empty() ? 0u : tmed[t];
+        float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : bits((int)mw));
         tnrm[3 * k + c] = make_float4(n.x, n.y, n.z, w);
       }
     }
@@ -2797,6 +3280,19 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   ds.lfunc_int = fint;
   ds.n_lights = nl;
   ds.n_area = n_area;
+  ds.media = nullptr;
+  ds.n_media = (int)d->n_media;
+  if (d->n_media) {
+    std::vector<float4> mrec(2 * (size_t)d->n_media);
+    for (uint32_t k = 0; k < d->n_media; ++k) {
+      const float* q = &d->media[7 * (size_t)k];
+      mrec[2 * k] = make_float4(q[0], q[1], q[2], q[6]);
+      mrec[2 * k + 1] = make_float4(q[3], q[4], q[5], 0.f);
+    }
+    float4* dm = nullptr;
+    if (e == cudaSuccess) e = up(&dm, mrec.data(), mrec.size());
+    ds.media = dm;
+  }
   ds.has_env = has_env ? 1 : 0;
   if (has_env) {
     EnvDev& ev = ds.env;
@@ -3006,6 +3502,64 @@ int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const Gy
   st = run_light_tracing(ctx, scene, camera, params, n, di, nullptr, dr, nullptr);
   if (st) return st;
   GYT_CK(ctx, cudaMemcpyAsync(records, dr, nrec * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_render_volume_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                 const GytRenderParams* params, double* d_film, GytRenderStats* stats) {
+  if (!ctx || !scene || !camera || !d_film) return fail(ctx, GYT_ERR_INVALID, "render_volume: null argument");
+  return run_volume(ctx, scene, camera, params, 0, nullptr, d_film, nullptr, nullptr, stats);
+}
+
+int32_t gyt_render_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, float* rgb_out) {
+  if (!ctx || !scene || !camera || !rgb_out) return fail(ctx, GYT_ERR_INVALID, "render_volume: null argument");
+  const uint64_t npix = (uint64_t)camera->res_x * camera->res_y;
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  double* d = nullptr;
+  float* f = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &d, 4 * std::max<uint64_t>(npix, 1)));
+  GYT_CK(ctx, dalloc(tmp, &f, 3 * std::max<uint64_t>(npix, 1)));
+  GYT_CK(ctx, cudaMemsetAsync(d, 0, 4 * npix * sizeof(double), ctx->stream));
+  int32_t st = run_volume(ctx, scene, camera, params, 0, nullptr, d, nullptr, nullptr, nullptr);
+  if (st) return st;
+  k_resolve<<<grid_for(npix), kBlock, 0, ctx->stream>>>(d, f, (uint32_t)npix);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaMemcpyAsync(rgb_out, f, 3 * npix * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GYT_OK;
+}
+
+int32_t gyt_trace_volume_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                               const GytRenderParams* params, uint64_t n, const uint32_t* xys, float* L_out,
+                               uint32_t* cursor_out) {
+  if (!ctx || !scene || !camera || (n && !xys)) return fail(ctx, GYT_ERR_INVALID, "trace_volume_paths: null argument");
+  if (n == 0) return GYT_OK;
+  for (uint64_t i = 0; i < n; ++i)
+    if (xys[3 * i] >= camera->res_x || xys[3 * i + 1] >= camera->res_y)
+      return fail(ctx, GYT_ERR_INVALID, "trace_volume_paths: pixel outside the film");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* q : v) cudaFree(q); }
+  } guard{tmp};
+  uint32_t *dx = nullptr, *dc = nullptr;
+  float* dl = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dx, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dl, 3 * n));
+  GYT_CK(ctx, dalloc(tmp, &dc, n));
+  GYT_CK(ctx, cudaMemcpyAsync(dx, xys, 3 * n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  int32_t st = run_volume(ctx, scene, camera, params, n, dx, nullptr, dl, dc, nullptr);
+  if (st) return st;
+  if (L_out) GYT_CK(ctx, cudaMemcpyAsync(L_out, dl, 3 * n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (cursor_out) GYT_CK(ctx, cudaMemcpyAsync(cursor_out, dc, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
   GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GYT_OK;
 }

@@ -39,7 +39,7 @@ from typing import Optional
 
 import numpy as np
 
-MAT_DIFFUSE, MAT_MIRROR, MAT_GLASS, MAT_CONDUCTOR, MAT_DIELECTRIC = 0, 1, 2, 3, 4
+MAT_DIFFUSE, MAT_MIRROR, MAT_GLASS, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_NONE = 0, 1, 2, 3, 4, 5
 
 # fovy of the reference's Cornell-box camera (Gyunity_exe/main.cpp:712)
 CORNELL_FOVY = 53.13010235415597
@@ -78,6 +78,8 @@ class SceneDesc:
     sphere_material: Optional[np.ndarray] = None  # (ns,) uint32
     env: Optional[np.ndarray] = None     # (h, w, 3) float32, row 0 = top (theta = 0)
     env_scale: float = 1.0
+    media: Optional[np.ndarray] = None   # (nmed, 7) float32: sigma_a rgb, sigma_s rgb, HG g
+    tri_medium: Optional[np.ndarray] = None  # (nt, 2) int32: medium inside, outside (-1 none)
     camera: Camera = dataclasses.field(default_factory=Camera)
     params: RenderParams = dataclasses.field(default_factory=RenderParams)
     name: str = ""
@@ -220,6 +222,34 @@ def cornell_box(res=256, spp=16, max_depth=8, rr_depth=3, spheres=True) -> Scene
         kw["sphere_material"] = np.array([mirror, glass], np.uint32)
     return b.build(camera=Camera(res_x=res, res_y=res), params=RenderParams(spp, max_depth, rr_depth),
                    name="cornell_box_%dx%d_%dspp" % (res, res, spp), **kw)
+
+
+def cornell_fog(res=128, spp=8, max_depth=8, sigma_a=0.05, sigma_s=0.5, g=0.3, spheres=True) -> SceneDesc:
+    """CornellBoxMedium (Gyunity_exe/CornellBox.h:1631-1700): the Cornell box
+    filled with one homogeneous medium, closed at z = 1 by a front quad of no
+    material whose MediumInterface is (inside: the medium, outside: none);
+    the walls keep the ray's medium. The reference's medium is sigma_s = 1,
+    sigma_a = 0, g = 0; here thinner and forward-scattering, with the
+    mirror and glass spheres of cornell_box."""
+    sd = cornell_box(res=res, spp=spp, max_depth=max_depth, rr_depth=5, spheres=spheres)
+    nv = sd.vertices.shape[0]
+    front = np.array([[-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], np.float32)
+    none = sd.mat_type.shape[0]
+    nt = sd.n_triangles
+    tri_medium = np.full((nt + 2, 2), -1, np.int32)
+    tri_medium[nt:] = (0, -1)
+    return dataclasses.replace(
+        sd,
+        vertices=np.concatenate([sd.vertices, front]),
+        normals=np.concatenate([sd.normals, np.tile(np.array([[0, 0, 1]], np.float32), (4, 1))]),
+        indices=np.concatenate([sd.indices, np.array([[nv, nv + 1, nv + 2], [nv, nv + 2, nv + 3]], np.uint32)]),
+        tri_material=np.concatenate([sd.tri_material, np.array([none, none], np.uint32)]),
+        tri_emission=np.concatenate([sd.tri_emission, np.array([-1, -1], np.int32)]),
+        mat_type=np.concatenate([sd.mat_type, np.array([MAT_NONE], np.uint32)]),
+        mat_params=np.concatenate([sd.mat_params, np.zeros((1, 16), np.float32)]),
+        media=np.array([[sigma_a] * 3 + [sigma_s] * 3 + [g]], np.float32),
+        tri_medium=tri_medium,
+        name="cornell_fog_%dx%d_%dspp" % (res, res, spp))
 
 
 # ---------------------------------------------------------------- meshes ----

@@ -54,7 +54,8 @@ enum {
  *   4 GGX dielectric   (material/RoughDielectric.h:21-41) [0:3] kr [3:6] kt [6] alpha_x [7] alpha_y [8] eta
  * Alpha is the GGX alpha (the reference maps roughness to alpha with
  * GGXDistribution::RoughnessToAlpha, visual/Microfacet.h:49-54, before this). */
-enum { GYT_MAT_DIFFUSE = 0, GYT_MAT_MIRROR = 1, GYT_MAT_GLASS = 2, GYT_MAT_CONDUCTOR = 3, GYT_MAT_DIELECTRIC = 4 };
+enum { GYT_MAT_DIFFUSE = 0, GYT_MAT_MIRROR = 1, GYT_MAT_GLASS = 2, GYT_MAT_CONDUCTOR = 3, GYT_MAT_DIELECTRIC = 4,
+       GYT_MAT_NONE = 5 /* no material: a GeometryPrimitive with a null material (a medium boundary) */ };
 
 /* Scene description (all host pointers; copied by gyt_scene_create).
  * Primitive ids: triangle t has id t, sphere s has id n_triangles + s, the
@@ -76,6 +77,15 @@ typedef struct {
   uint32_t env_w, env_h;          /* lat-long environment map, 0 if none */
   const float* env;               /* env_h * env_w * 3, row 0 = top (theta = 0) */
   float env_scale;
+  /* Participating media for volumetric path tracing (HomogeneousMedium,
+   * volume/Homogeneous.h): n_media * 7 floats (sigma_a rgb, sigma_s rgb,
+   * Henyey-Greenstein g); tri_medium: n_triangles * 2 (medium inside,
+   * outside; -1 none), the triangle's MediumInterface (visual/Medium.h), or
+   * NULL. A triangle whose inside and outside differ is a medium boundary;
+   * one of material GYT_MAT_NONE has no BSDF (rays pass through it). */
+  uint32_t n_media;
+  const float* media;
+  const int32_t* tri_medium;
 } GytSceneDesc;
 
 /* PinHoleCamera(film, position, lookAt, up, fovy, filmDistance) on a
@@ -226,6 +236,32 @@ int32_t gyt_render_light_tracing_device(gyt_context* ctx, const gyt_scene* scene
  * Y; the splatted RGB), vertex 0 = the light vertex. */
 int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
                               const GytRenderParams* params, uint64_t n, const uint64_t* photons, float* records);
+
+/* ---- Volumetric path tracing -----------------------------------------------
+ * VolPathTracing(spp, maxDepth, sampler, samplerEnum, false)
+ * (integrator/VPT.cpp:7-104, the estimator without equi-angular sampling)
+ * with the scene's homogeneous media (GytSceneDesc::media, tri_medium):
+ * camera rays start in no medium; a ray through a medium samples a
+ * scattering distance (HomogeneousMedium::Sample, volume/Homogeneous.cpp);
+ * at a medium point light is gathered with the Henyey-Greenstein phase
+ * function (both halves of the MIS estimate, transmittance along shadow
+ * rays) and the path continues in a phase-sampled direction; surfaces of
+ * GYT_MAT_NONE are passed through without using a bounce. No Russian
+ * roulette (the reference's test is always false). Environment lights are
+ * refused. _device accumulates into a film as gyt_render_device; the
+ * reference's VolPathTracing needs its BSDF pointer initialised to null to
+ * pass through surfaces of no material (it reads it uninitialised). A hit
+ * at the very end of a shadow segment (the light's own surface) is settled
+ * in FP64, as in the path tracer's occlusion test. */
+int32_t gyt_render_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                          const GytRenderParams* params, float* rgb_out);
+int32_t gyt_render_volume_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                                 const GytRenderParams* params, double* d_film, GytRenderStats* stats);
+/* VolPathTracing::Li for listed samples (xys: n triplets x, y, s): radiance
+ * (n*3 floats) and the sampler dimensions each used (n). */
+int32_t gyt_trace_volume_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
+                               const GytRenderParams* params, uint64_t n, const uint32_t* xys, float* L_out,
+                               uint32_t* cursor_out);
 
 /* ---- Meshes from Wavefront OBJ files ---------------------------------------
  * Mesh::LoadFromFile (mesh/Mesh.cpp:7-90) with the reference's vendored

@@ -14,7 +14,7 @@ Recipe (no reference build system is run):
      submodules), plus ``oracle/ref/harness.cpp``;
   4. link ``oracle/_ref/gyref_harness``.
 
-Patches (numbered P1-P8; each is an exact text replacement):
+Patches (numbered P1-P9; each is an exact text replacement):
   P1 common/Core.h:42-43     int64/uint64 as long long so the Sampler override
                              at sampler/Sobol.h:70 matches sampler/Sampler.h:12
   P2 math/Linagl.h:155       dependent base-class name for GCC
@@ -28,6 +28,10 @@ Patches (numbered P1-P8; each is an exact text replacement):
   P8 integrator/PT.cpp:53    Russian roulette start depth (hard-coded 5) made
                              a global so configurations that ask for another
                              start depth can be reproduced; default stays 5.
+  P9 visual/Intersection.h:23 the BSDF pointer starts null: VolPathTracing
+                             tests it to pass through surfaces of no material
+                             (integrator/VPT.cpp:70-75) but the constructor
+                             leaves it uninitialised.
 """
 import os
 import shutil
@@ -65,6 +69,7 @@ PATCHES = [
     ("shape/Sphere.h", "\t\tWorldToObject(ray);\n\n\t\tVec3 op", "\t\tr = WorldToObject(ray);\n\n\t\tVec3 op"),
     ("integrator/PT.cpp", "if (p < 1 && i > 5) {", "if (p < 1 && i > gyref_rr_start_depth) {"),
     ("integrator/PT.cpp", "GYT_NAMESPACE_BEGIN\n", "int gyref_rr_start_depth = 5;\nGYT_NAMESPACE_BEGIN\n"),
+    ("visual/Intersection.h", "\tBSDF* mpBSDF;\n", "\tBSDF* mpBSDF = nullptr;\n"),
 ]
 
 SOURCES = [
@@ -75,6 +80,7 @@ SOURCES = [
     "integrator/PT.cpp", "camera/PinholeCamera.cpp", "visual/Primitive.cpp", "math/Ray.cpp",
     "sampler/Sampler.cpp", "visual/Sampling.cpp", "visual/Scene.cpp", "shape/Shape.cpp",
     "sampler/Sobol.cpp", "sampler/SobolEnum.cpp", "integrator/TiledIntegrator.cpp", "mesh/Mesh.cpp",
+    "integrator/VPT.cpp", "volume/Homogeneous.cpp",
     "math/Transform.cpp", "shape/Triangle.cpp", "visual/Film.cpp", "visual/Visibility.cpp",
 ]
 

@@ -22,7 +22,8 @@
 //           by the transform of spec ("-": none; else "T x y z;S x y z;RX a;RY a;RZ a" composed
 //           left to right); 18 f32 per triangle: p0 p1 p2 n0 n1 n2
 // paths and render use SobolSampler + SobolEnum, or HaltonSampler (Faure
-// permutations) + HaltonEnum when GYREF_SAMPLER=halton.
+// permutations) + HaltonEnum when GYREF_SAMPLER=halton; PathTracing, or
+// VolPathTracing (without equi-angular sampling) when GYREF_INTEGRATOR=vpt.
 // Standard and shim headers first, so the access override below only reaches
 // the reference's own classes (Film's pixel buffer, Scene's counters).
 #include <algorithm>
@@ -61,6 +62,8 @@
 #include "image/ImageIO.h"
 #include "mesh/Mesh.h"
 #include "integrator/LT.h"
+#include "integrator/VPT.h"
+#include "volume/Homogeneous.h"
 #undef private
 #undef protected
 
@@ -157,7 +160,7 @@ LoadedScene load_scene(const char* path) {
   Reader r{buf.data(), buf.data() + buf.size()};
   if (r.get<uint32_t>() != 0x53545947u) throw std::runtime_error("bad scene magic");
   uint32_t version = r.get<uint32_t>();
-  if (version != 1) throw std::runtime_error("bad scene version");
+  if (version != 1 && version != 2) throw std::runtime_error("bad scene version");
   uint32_t nv = r.get<uint32_t>(), nt = r.get<uint32_t>(), ns = r.get<uint32_t>();
   uint32_t nm = r.get<uint32_t>(), ne = r.get<uint32_t>(), has_normals = r.get<uint32_t>();
   uint32_t env_w = r.get<uint32_t>(), env_h = r.get<uint32_t>();
@@ -180,6 +183,20 @@ LoadedScene load_scene(const char* path) {
   std::vector<float> MP = r.arr<float>((size_t)nm * 16);
   std::vector<float> EM = r.arr<float>((size_t)ne * 3);
   std::vector<float> ENV = r.arr<float>((size_t)env_w * env_h * 3);
+  // version 2: homogeneous media (sigma_a, sigma_s, g) and the triangles'
+  // MediumInterface (inside, outside; -1 none)
+  std::vector<const Medium*> media;
+  std::vector<int32_t> TMED;
+  if (version == 2) {
+    const uint32_t n_media = r.get<uint32_t>(), has_tmed = r.get<uint32_t>();
+    std::vector<float> MD = r.arr<float>((size_t)n_media * 7);
+    for (uint32_t k = 0; k < n_media; ++k) {
+      const float* q = &MD[7 * k];
+      media.push_back(new HomogeneousMedium(Vec3(q[0], q[1], q[2]), Vec3(q[3], q[4], q[5]), q[6]));
+    }
+    if (has_tmed) TMED = r.arr<int32_t>((size_t)nt * 2);
+  }
+  auto medium_of = [&](int32_t k) -> const Medium* { return k < 0 ? nullptr : media.at((size_t)k); };
 
   std::vector<std::shared_ptr<Material>> mats;
   for (uint32_t m = 0; m < nm; ++m) {
@@ -192,6 +209,7 @@ LoadedScene load_scene(const char* path) {
                                                                       Vec3(p[9], p[10], p[11]), Vec3(p[12], p[13], p[14]))); break;
       case 4: mats.push_back(std::make_shared<AlphaDielectricMaterial>(Vec3(p[0], p[1], p[2]), Vec3(p[3], p[4], p[5]),
                                                                        p[6], p[7], p[8])); break;
+      case 5: mats.push_back(nullptr); break;  // no material: a medium boundary
       default: throw std::runtime_error("unknown material type");
     }
   }
@@ -218,7 +236,9 @@ LoadedScene load_scene(const char* path) {
       light = std::make_shared<AreaLight>(shape, Vec3(e[0], e[1], e[2]));
       out.scene->AddLight(light);
     }
-    out.scene->AddPrimitive(std::make_shared<Primitive>(shape, mats[TM[t]], light));
+    MediumInterface mi;
+    if (!TMED.empty()) mi = MediumInterface(medium_of(TMED[2 * t]), medium_of(TMED[2 * t + 1]));
+    out.scene->AddPrimitive(std::make_shared<Primitive>(shape, mats[TM[t]], light, mi));
   }
   for (uint32_t s = 0; s < ns; ++s) {
     auto shape = std::make_shared<Sphere>(Transform(), Transform(), SP[4 * s + 3],
@@ -346,8 +366,8 @@ int cmd_hits(int argc, char** argv, bool any) {
   return 0;
 }
 
-std::shared_ptr<PathTracing> make_integrator(const LoadedScene& ls, std::shared_ptr<Sampler>* sampler,
-                                             std::shared_ptr<SamplerEnum>* senum) {
+std::shared_ptr<TiledIntegrator> make_integrator(const LoadedScene& ls, std::shared_ptr<Sampler>* sampler,
+                                                 std::shared_ptr<SamplerEnum>* senum) {
   const char* kind = std::getenv("GYREF_SAMPLER");
   if (kind && std::string(kind) == "halton") {
     *sampler = std::make_shared<HaltonSampler>(faure_halton());
@@ -356,12 +376,15 @@ std::shared_ptr<PathTracing> make_integrator(const LoadedScene& ls, std::shared_
     *sampler = std::make_shared<SobolSampler>();
     *senum = std::make_shared<SobolEnum>(ls.resX, ls.resY);
   }
+  const char* integ = std::getenv("GYREF_INTEGRATOR");
+  if (integ && std::string(integ) == "vpt")  // the estimator without equi-angular sampling
+    return std::make_shared<VolPathTracing>(ls.spp, ls.maxDepth, *sampler, *senum, false);
   return std::make_shared<PathTracing>(ls.spp, ls.maxDepth, *sampler, *senum);
 }
 
 // One sample of TiledIntegrator::Render's inner loop
 // (integrator/TiledIntegrator.cpp:40-47) for pixel (x, y), sample s.
-Vec3 one_path(const LoadedScene& ls, PathTracing& pt, const std::shared_ptr<Sampler>& sampler,
+Vec3 one_path(const LoadedScene& ls, const TiledIntegrator& pt, const std::shared_ptr<Sampler>& sampler,
               const SamplerEnum& senum, uint32_t x, uint32_t y, uint32_t s, MemoryPool& arena, int* cursor) {
   uint64 instance = senum.GetIndex(s, x, y);
   RandomStateSequence rand(sampler, instance);

@@ -30,8 +30,11 @@ def write_scene(path, sd):
     env_h, env_w = (0, 0) if env is None else env.shape[:2]
     c = sd.camera
     p = sd.params
+    media = getattr(sd, "media", None)
+    tri_medium = getattr(sd, "tri_medium", None)
+    version = 2 if media is not None else 1
     with open(path, "wb") as f:
-        f.write(struct.pack("<2I", 0x53545947, 1))
+        f.write(struct.pack("<2I", 0x53545947, version))
         f.write(struct.pack("<8I", sd.vertices.shape[0], sd.n_triangles, ns, sd.mat_type.shape[0],
                             sd.emission.shape[0], 0 if sd.normals is None else 1, env_w, env_h))
         f.write(struct.pack("<5I", c.res_x, c.res_y, p.spp, p.max_depth, p.rr_depth))
@@ -51,6 +54,13 @@ def write_scene(path, sd):
         f.write(np.ascontiguousarray(sd.emission, np.float32).tobytes())
         if env is not None:
             f.write(np.ascontiguousarray(env, np.float32).tobytes())
+        if version == 2:
+            # version 2: homogeneous media and per-triangle medium interfaces
+            m = np.ascontiguousarray(media, np.float32).reshape(-1, 7)
+            f.write(struct.pack("<2I", m.shape[0], 0 if tri_medium is None else 1))
+            f.write(m.tobytes())
+            if tri_medium is not None:
+                f.write(np.ascontiguousarray(tri_medium, np.int32).reshape(-1, 2).tobytes())
 
 
 def have_harness():
@@ -110,8 +120,13 @@ def ref_henum(tmp, res_x, res_y, s, x, y):
     return np.fromfile(b, np.uint64)
 
 
-def _sampler_env(sampler):
-    return {"GYREF_SAMPLER": sampler} if sampler and sampler != "sobol" else None
+def _sampler_env(sampler, integrator=None):
+    env = {}
+    if sampler and sampler != "sobol":
+        env["GYREF_SAMPLER"] = sampler
+    if integrator and integrator != "pt":
+        env["GYREF_INTEGRATOR"] = integrator
+    return env or None
 
 
 def ref_hits(tmp, scene_path, rays, any_hit=False):
@@ -121,11 +136,12 @@ def ref_hits(tmp, scene_path, rays, any_hit=False):
     return np.fromfile(b, HIT_DTYPE)
 
 
-def ref_paths(tmp, scene_path, x, y, s, sampler=None):
+def ref_paths(tmp, scene_path, x, y, s, sampler=None, integrator=None):
+    """Li of PathTracing (or VolPathTracing with integrator="vpt") for (x, y, s)."""
     trip = np.stack([np.asarray(x, np.uint32), np.asarray(y, np.uint32), np.asarray(s, np.uint32)], 1)
     a, b = os.path.join(tmp, "paths_in.bin"), os.path.join(tmp, "paths_out.bin")
     trip.astype(np.uint32).tofile(a)
-    run("paths", scene_path, a, b, env=_sampler_env(sampler))
+    run("paths", scene_path, a, b, env=_sampler_env(sampler, integrator))
     return np.fromfile(b, np.float32).reshape(-1, 4)
 
 
@@ -135,7 +151,7 @@ def ref_camera(tmp, scene_path):
     return np.fromfile(b, np.float32).reshape(4, 4)
 
 
-def ref_render(tmp, scene_path, rows=None, spp=None, threads=None, sampler=None):
+def ref_render(tmp, scene_path, rows=None, spp=None, threads=None, sampler=None, integrator=None):
     import json
     b = os.path.join(tmp, "render.bin")
     args = ["render", scene_path, b]
@@ -143,7 +159,7 @@ def ref_render(tmp, scene_path, rows=None, spp=None, threads=None, sampler=None)
         args.append(rows if rows is not None else 0)
     if spp is not None:
         args.append(spp)
-    env = dict(_sampler_env(sampler) or {})
+    env = dict(_sampler_env(sampler, integrator) or {})
     if threads:
         env["GYREF_THREADS"] = str(threads)
     out = run(*args, env=env or None)

@@ -10,6 +10,7 @@ checkout is only needed to regenerate; the tests read the fixtures.
     python tests/golden/make_golden.py film       # only the film-output fixtures
     python tests/golden/make_golden.py obj        # only the OBJ-mesh fixtures
     python tests/golden/make_golden.py lt         # only the light-tracing fixtures
+    python tests/golden/make_golden.py vpt        # only the volume fixtures
 """
 import os
 import sys
@@ -239,7 +240,34 @@ def light_tracing_golden(tmp):
     np.savez_compressed(os.path.join(HERE, "image_lt_cornell_64x64_16spp.npz"), splat=img.reshape(64, 64, 3))
 
 
+def volume_golden(tmp):
+    """VolPathTracing (without equi-angular sampling) per path and rendered,
+    on the Cornell box filled with fog (scenes.cornell_fog)."""
+    rng = np.random.default_rng(20261208)
+    for name, sd in (("fog", scenes.cornell_fog(res=48, spp=4, max_depth=6)),
+                     ("fog_thick", scenes.cornell_fog(res=48, spp=4, max_depth=6, sigma_a=0.2, sigma_s=1.5, g=-0.4,
+                                                      spheres=False))):
+        path = os.path.join(tmp, "vpt_%s.gyts" % name)
+        io.write_scene(path, sd)
+        n = 3000
+        x = rng.integers(0, sd.camera.res_x, n)
+        y = rng.integers(0, sd.camera.res_y, n)
+        s = rng.integers(0, sd.params.spp, n)
+        r = io.ref_paths(tmp, path, x, y, s, integrator="vpt")
+        np.savez_compressed(os.path.join(HERE, "vpt_paths_%s.npz" % name), xys=np.stack([x, y, s], 1).astype(np.uint32),
+                            L=r[:, :3], cursor=r[:, 3].astype(np.int32))
+    sd = scenes.cornell_fog(res=64, spp=8, max_depth=6)
+    path = os.path.join(tmp, "vpt_img.gyts")
+    io.write_scene(path, sd)
+    img, _ = io.ref_render(tmp, path, integrator="vpt")
+    np.savez_compressed(os.path.join(HERE, "image_vpt_fog_64x64_8spp.npz"), film=img)
+
+
 def main():
+    if sys.argv[1:] == ["vpt"]:
+        volume_golden(tempfile.mkdtemp())
+        print("volume golden vectors written to", HERE)
+        return
     if sys.argv[1:] == ["lt"]:
         light_tracing_golden(tempfile.mkdtemp())
         print("light-tracing golden vectors written to", HERE)
@@ -340,6 +368,7 @@ def main():
     film_output_golden(tmp)
     obj_golden(tmp)
     light_tracing_golden(tmp)
+    volume_golden(tmp)
     print("golden vectors written to", HERE)
 
 

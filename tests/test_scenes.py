@@ -36,3 +36,15 @@ def test_procedural_mesh_is_deterministic():
 def test_roughness_to_alpha():
     assert abs(scenes.roughness_to_alpha(0.5) - 1.62142 - 0.819955 * np.log(0.5) - 0.1734 * np.log(0.5) ** 2
                - 0.0171201 * np.log(0.5) ** 3 - 0.000640711 * np.log(0.5) ** 4) < 1e-5
+
+
+def test_cornell_fog_layout():
+    sd = scenes.cornell_fog(res=32, spp=2)
+    nt = sd.n_triangles
+    assert nt == 14 and sd.media.shape == (1, 7) and sd.tri_medium.shape == (nt, 2)
+    # only the front quad is a medium boundary, and it has no material
+    inside = np.nonzero(sd.tri_medium[:, 0] >= 0)[0]
+    assert list(inside) == [12, 13]
+    assert np.all(sd.mat_type[sd.tri_material[inside]] == scenes.MAT_NONE)
+    assert np.all(sd.tri_medium[:12] == -1) and np.all(sd.tri_medium[12:, 1] == -1)
+    assert np.all(sd.vertices[sd.indices[12:]][..., 2] == 1.0)
