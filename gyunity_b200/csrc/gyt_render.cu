@@ -1618,6 +1618,18 @@ __global__ void __launch_bounds__(kBlock) k_light_trace(DevScene s, LtCam c, Par
 // (Primitive::Intersect, visual/Primitive.cpp:5-18); a ray leaving a surface
 // takes the outside medium when it leaves along the shading normal, else the
 // inside (Intersection::GetMedium, visual/Intersection.h:80-82).
+// The volume kernel's one traversal, called from its three ray sites (closest
+// hit, transmittance hops, shadow segments) rather than inlined at each: the
+// inlined copies kept the path state and three traversal states live at once
+// (128 registers with spills for the binary BVH, 212 for the 8-wide one);
+// called, 64 against 49 Mpaths/s on the Cornell box in fog (binary BVH);
+// with vpt_direct called too and three blocks per SM, 69.
+template <int W>
+__device__ __noinline__ int vpt_trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1,
+                                       float& b2) {
+  return trace<W, false>(s, o, d, tmax, b1, b2);
+}
+
 struct MediumDev {
   float3 sa, ss, st;
   float g;
@@ -1736,7 +1748,7 @@ GYT_D float3 vpt_tr(const DevScene& s, const VPoint& p0, float3 lpos, float3 ler
     const float3 o = org + d * kRayEps;
     const float seg = dis - kShadowEps;
     float tmax = seg, b1 = 0.f, b2 = 0.f;
-    int prim = trace<W, false>(s, o, d, tmax, b1, b2);
+    int prim = vpt_trace<W>(s, o, d, tmax, b1, b2);
     // The segment ends on the light's surface: a hit at its very end is
     // settled in FP64, as the occlusion test of path tracing settles it.
     if (prim >= 0 && prim < s.n_tris && tmax >= seg * 0.999998f) {
@@ -1774,7 +1786,7 @@ GYT_D bool vpt_intersect_tr(const DevScene& s, float3 o, float3 d, int medium, i
 #pragma unroll 1
   for (int hop = 0; hop < 64; ++hop) {
     float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
-    const int prim = trace<W, false>(s, o, d, tmax, b1, b2);
+    const int prim = vpt_trace<W>(s, o, d, tmax, b1, b2);
     if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
     if (prim < 0) {
       *tr_out = tr;
@@ -1802,11 +1814,13 @@ GYT_D bool vpt_intersect_tr(const DevScene& s, float3 o, float3 d, int medium, i
   return false;
 }
 
-// Integrator::DirectIllumination with handleMedia (integrator/Integrator.cpp:9-107)
+// Integrator::DirectIllumination with handleMedia (integrator/Integrator.cpp:9-107),
+// called (not inlined) from the medium and the surface branch: one copy of its
+// code, which the instruction cache holds better.
 // for a surface point (bsdf) or a medium point (phase g). u: uLight, u.y, u.x,
 // v.z, v.y, v.x as the caller draws them.
 template <int W>
-GYT_D float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, const Hit* h, float ul,
+__device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, const Hit* h, float ul,
                         float ux, float uy, float vx, float vy, float vz) {
   if (s.n_lights <= 0) return mk(0.f, 0.f, 0.f);
   float lsel = 0.f;
@@ -1896,9 +1910,11 @@ GYT_D float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, fl
 
 // One camera sample per thread (grid-stride over the render's samples, or the
 // listed (x, y, s) of xys); film as gyt_render_device's, L_out/cursor_out for
-// parity tests.
+// parity tests. Capped at three blocks per SM (80 registers, a few spills):
+// the kernel is bound by divergence and instruction fetch, not by memory
+// (ncu: 10 of 32 lanes active per instruction; no_instruction the top stall).
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
+__global__ void __launch_bounds__(kBlock, 3) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
                                                 unsigned long long n, const uint32_t* __restrict__ xys,
                                                 double* __restrict__ film, float* __restrict__ L_out,
                                                 uint32_t* __restrict__ cursor_out) {
@@ -1931,7 +1947,7 @@ __global__ void __launch_bounds__(kBlock) k_vpt(DevScene s, Cam cam, Params prm,
     for (int i = 0; i < (int)prm.max_depth; ++i) {
       if (rng.cursor + 16u > (prm.sampler ? kHaltonDims : 1024u)) break;  // the sampler's dimensions are spent
       float tmax = __int_as_float(0x7f800000), hb1 = 0.f, hb2 = 0.f;
-      const int prim = trace<W, false>(s, o, d, tmax, hb1, hb2);
+      const int prim = vpt_trace<W>(s, o, d, tmax, hb1, hb2);
       bool scattered = false;
       float3 mpos;
       MediumDev md;
