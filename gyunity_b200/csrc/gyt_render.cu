@@ -1622,8 +1622,7 @@ __global__ void __launch_bounds__(kBlock) k_light_trace(DevScene s, LtCam c, Par
 // hit, transmittance hops, shadow segments) rather than inlined at each: the
 // inlined copies kept the path state and three traversal states live at once
 // (128 registers with spills for the binary BVH, 212 for the 8-wide one);
-// called, 64 against 49 Mpaths/s on the Cornell box in fog (binary BVH);
-// with vpt_direct called too and three blocks per SM, 69.
+// called, 64 against 49 Mpaths/s on the Cornell box in fog (binary BVH).
 template <int W>
 __device__ __noinline__ int vpt_trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1,
                                        float& b2) {
@@ -1910,50 +1909,73 @@ __device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, co
 
 // One camera sample per thread (grid-stride over the render's samples, or the
 // listed (x, y, s) of xys); film as gyt_render_device's, L_out/cursor_out for
-// parity tests. Capped at three blocks per SM (80 registers, a few spills):
-// the kernel is bound by divergence and instruction fetch, not by memory
-// (ncu: 10 of 32 lanes active per instruction; no_instruction the top stall).
+// parity tests. Capped at four blocks per SM (64 registers, a few spills) and
+// launched as one persistent wave: the kernel is bound by divergence and
+// instruction fetch, not by memory. On the Cornell box in fog (binary BVH):
+// 69 Mpaths/s with a whole path per loop pass, 89 with regeneration, 112 with
+// four blocks per SM in a single wave.
 template <int W>
-__global__ void __launch_bounds__(kBlock, 3) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
+__global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
                                                 unsigned long long n, const uint32_t* __restrict__ xys,
                                                 double* __restrict__ film, float* __restrict__ L_out,
                                                 uint32_t* __restrict__ cursor_out) {
-  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (unsigned long long)gridDim.x * blockDim.x) {
-    uint32_t x, y, sm;
-    if (xys) {
-      x = xys[3 * t];
-      y = xys[3 * t + 1];
-      sm = xys[3 * t + 2];
-    } else {
-      const unsigned long long pixel = t / prm.spp;
-      sm = (uint32_t)(t - pixel * prm.spp);
-      y = (uint32_t)(pixel / cam.res_x);
-      x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+  // Path regeneration: every pass of the loop is one bounce of each lane's
+  // path; a lane whose path ended starts its next sample (grid stride) on the
+  // next pass instead of idling until the warp's longest path is done.
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t dim_limit = prm.sampler ? kHaltonDims : 1024u;
+  bool alive = false;
+  uint32_t x = 0, y = 0;
+  bool u_zero = false, v_zero = false;
+  Rng rng{0, 0};
+  float3 o = mk(0.f, 0.f, 0.f), d = o, tp = o, L = o;
+  int medium = -1, i = 0, crossings = 0;
+  bool delta = false;
+  for (;;) {
+    if (!alive) {
+      if (t >= n) break;
+      uint32_t sm;
+      if (xys) {
+        x = xys[3 * t];
+        y = xys[3 * t + 1];
+        sm = xys[3 * t + 2];
+      } else {
+        const unsigned long long pixel = t / prm.spp;
+        sm = (uint32_t)(t - pixel * prm.spp);
+        y = (uint32_t)(pixel / cam.res_x);
+        x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+      }
+      // the camera sample (TiledIntegrator::Render, integrator/TiledIntegrator.cpp:40-47)
+      const bool halton = cam.sampler != 0;
+      const uint64_t idx = halton ? halton_enum_index(cam, sm, x, y) : enum_index(tab, cam.log2_res, sm, x, y);
+      rng = Rng{idx, 0};
+      const float su = rng.next(tab, cam.sampler), sv = rng.next(tab, cam.sampler);
+      const float u = __fsub_rn(__fmul_rn(halton ? cam.h_sx : cam.res_pow2, su), (float)x);
+      const float v = __fsub_rn(__fmul_rn(halton ? cam.h_sy : cam.res_pow2, sv), (float)y);
+      u_zero = u == 0.f;
+      v_zero = v == 0.f;
+      camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
+      medium = -1;  // the camera's medium (PinHoleCamera::GenerateRay: none)
+      tp = mk(1.f, 1.f, 1.f);
+      L = mk(0.f, 0.f, 0.f);
+      delta = false;
+      i = 0;
+      crossings = 0;
+      alive = true;
     }
-    // the camera sample (TiledIntegrator::Render, integrator/TiledIntegrator.cpp:40-47)
-    const bool halton = cam.sampler != 0;
-    const uint64_t idx = halton ? halton_enum_index(cam, sm, x, y) : enum_index(tab, cam.log2_res, sm, x, y);
-    Rng rng{idx, 0};
-    const float su = rng.next(tab, cam.sampler), sv = rng.next(tab, cam.sampler);
-    const float u = __fsub_rn(__fmul_rn(halton ? cam.h_sx : cam.res_pow2, su), (float)x);
-    const float v = __fsub_rn(__fmul_rn(halton ? cam.h_sy : cam.res_pow2, sv), (float)y);
-    float3 o, d;
-    camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
-    int medium = -1;  // the camera's medium (PinHoleCamera::GenerateRay: none)
-    float3 tp = mk(1.f, 1.f, 1.f), L = mk(0.f, 0.f, 0.f);
-    bool delta = false;
-    int crossings = 0;
-    for (int i = 0; i < (int)prm.max_depth; ++i) {
-      if (rng.cursor + 16u > (prm.sampler ? kHaltonDims : 1024u)) break;  // the sampler's dimensions are spent
+    // one bounce of VolPathTracing::Li (integrator/VPT.cpp:13-101)
+    bool end = rng.cursor + 16u > dim_limit;  // the sampler's dimensions are spent
+    if (!end) {
       float tmax = __int_as_float(0x7f800000), hb1 = 0.f, hb2 = 0.f;
       const int prim = vpt_trace<W>(s, o, d, tmax, hb1, hb2);
       bool scattered = false;
-      float3 mpos;
-      MediumDev md;
+      float3 mpos = o;
+      float g = 0.f;
       if (medium >= 0) {
         // HomogeneousMedium::Sample (volume/Homogeneous.cpp:12-30)
-        md = load_medium(s, medium);
+        const MediumDev md = load_medium(s, medium);
+        g = md.g;
         const float uc = rng.next(tab, prm.sampler), ud = rng.next(tab, prm.sampler);
         const int ch = min((int)(uc * 3.f), 2);
         const float sc = ch == 0 ? md.st.x : (ch == 1 ? md.st.y : md.st.z);
@@ -1970,86 +1992,96 @@ __global__ void __launch_bounds__(kBlock, 3) k_vpt(DevScene s, Cam cam, Params p
         tp = tp * (scattered ? tr * md.ss / pdf : tr / pdf);
         if (scattered) mpos = o + d * tt;
       }
-      if (is_zero(tp)) break;
-      if (scattered) {
-        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
-        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
-        const float ul = rng.next(tab, prm.sampler);
-        VPoint p;
+      VPoint p;
+      Bsdf bsdf;
+      bool gather = false, pass = false;
+      if (is_zero(tp)) {
+        end = true;
+      } else if (scattered) {
         p.pos = mpos;
         p.perr = p.abs_n = p.n = mk(0.f, 0.f, 0.f);
         p.wo = -d;
         p.m_in = p.m_out = medium;
         p.surface = false;
-        L = L + tp * vpt_direct<W>(s, p, nullptr, md.g, nullptr, ul, ux, uy, vx, vy, vz);
-        const float py = rng.next(tab, prm.sampler), px = rng.next(tab, prm.sampler);
-        float3 wi;
-        phase_sample(md.g, -d, px, py, &wi);
-        o = mpos + wi * kRayEps;  // MediumIntersection::SpawnRay: no offset
-        d = wi;
-        delta = false;
-        continue;
-      }
-      if (prim < 0) break;  // no environment light with media
-      Hit h;
-      uint32_t mat;
-      int light;
-      vpt_hit(s, prim, tmax, hb1, hb2, o, d, &h, &mat, &light);
-      int m_in, m_out;
-      surface_media(s, prim, medium, &m_in, &m_out);
-      const uint32_t mtype = __ldg(s.mtypes + mat);
-      if (mtype == 5u) {
-        // no BSDF: pass through without using a bounce (VPT.cpp:70-75)
-        o = offset_origin(h.pos, h.perr, h.abs_n, d) + d * kRayEps;
-        medium = dot(d, h.n) > 0.f ? m_out : m_in;
-        --i;
-        if (++crossings > 64) break;
-        continue;
-      }
-      Bsdf bsdf;
-      bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
-      bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
-      if ((i == 0 || delta) && light >= 0) {
-        if (dot(h.n, h.wo) > 0.f) L = L + tp * load_light(s, light).Le;
+        gather = true;
+      } else if (prim < 0) {
+        end = true;  // no environment light with media
       } else {
-        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
-        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
-        const float ul = rng.next(tab, prm.sampler);
-        VPoint p;
+        Hit h;
+        uint32_t mat;
+        int light;
+        vpt_hit(s, prim, tmax, hb1, hb2, o, d, &h, &mat, &light);
+        surface_media(s, prim, medium, &p.m_in, &p.m_out);
         p.pos = h.pos;
         p.perr = h.perr;
         p.abs_n = h.abs_n;
         p.n = h.n;
         p.wo = h.wo;
-        p.m_in = m_in;
-        p.m_out = m_out;
         p.surface = true;
-        L = L + tp * vpt_direct<W>(s, p, &bsdf, 0.f, &h, ul, ux, uy, vx, vy, vz);
+        if (__ldg(s.mtypes + mat) == 5u) {
+          // no BSDF: pass through without using a bounce (VPT.cpp:70-75)
+          pass = true;
+          o = offset_origin(h.pos, h.perr, h.abs_n, d) + d * kRayEps;
+          medium = dot(d, h.n) > 0.f ? p.m_out : p.m_in;
+          if (++crossings > 64) end = true;
+        } else {
+          bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
+          bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+          if ((i == 0 || delta) && light >= 0) {
+            if (dot(h.n, h.wo) > 0.f) L = L + tp * load_light(s, light).Le;
+          } else {
+            gather = true;
+          }
+        }
       }
-      const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
-      float3 wi;
-      float pdf;
-      const float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
-      if (is_zero(f) || pdf == 0.f) break;
-      const float3 est = f * fabsf(dot(h.n, wi)) / pdf;
-      delta = bsdf.lobe.delta();
-      tp = tp * est;
-      o = offset_origin(h.pos, h.perr, h.abs_n, wi) + wi * kRayEps;
-      d = wi;
-      medium = dot(wi, h.n) > 0.f ? m_out : m_in;
+      if (gather) {
+        // one call site for surface and medium points
+        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
+        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
+        const float ul = rng.next(tab, prm.sampler);
+        L = L + tp * vpt_direct<W>(s, p, scattered ? nullptr : &bsdf, g, nullptr, ul, ux, uy, vx, vy, vz);
+      }
+      if (!end && !pass) {
+        if (scattered) {
+          const float py = rng.next(tab, prm.sampler), px = rng.next(tab, prm.sampler);
+          float3 wi;
+          phase_sample(g, -d, px, py, &wi);
+          o = mpos + wi * kRayEps;  // MediumIntersection::SpawnRay: no offset
+          d = wi;
+          delta = false;
+        } else {
+          const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
+          float3 wi;
+          float pdf;
+          const float3 f = bsdf.sample(p.wo, &wi, &pdf, rx, ry, rz);
+          if (is_zero(f) || pdf == 0.f) {
+            end = true;
+          } else {
+            tp = tp * (f * fabsf(dot(p.n, wi)) / pdf);
+            delta = bsdf.lobe.delta();
+            o = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
+            d = wi;
+            medium = dot(wi, p.n) > 0.f ? p.m_out : p.m_in;
+          }
+        }
+        if (!end && ++i >= (int)prm.max_depth) end = true;
+      }
     }
-    if (L_out) {
-      L_out[3 * t] = L.x;
-      L_out[3 * t + 1] = L.y;
-      L_out[3 * t + 2] = L.z;
-    }
-    if (cursor_out) cursor_out[t] = rng.cursor;
-    if (film) {
-      const uint32_t pix_x = x, pix_y = y;
-      film_add(film, cam.res_x, pix_x, pix_y, L);
-      if (u == 0.f && x > 0) film_add(film, cam.res_x, pix_x - 1, pix_y, L);
-      if (v == 0.f && y > 0) film_add(film, cam.res_x, pix_x, pix_y - 1, L);
-      if (u == 0.f && x > 0 && v == 0.f && y > 0) film_add(film, cam.res_x, pix_x - 1, pix_y - 1, L);
+    if (end) {
+      if (L_out) {
+        L_out[3 * t] = L.x;
+        L_out[3 * t + 1] = L.y;
+        L_out[3 * t + 2] = L.z;
+      }
+      if (cursor_out) cursor_out[t] = rng.cursor;
+      if (film) {
+        film_add(film, cam.res_x, x, y, L);
+        if (u_zero && x > 0) film_add(film, cam.res_x, x - 1, y, L);
+        if (v_zero && y > 0) film_add(film, cam.res_x, x, y - 1, L);
+        if (u_zero && x > 0 && v_zero && y > 0) film_add(film, cam.res_x, x - 1, y - 1, L);
+      }
+      alive = false;
+      t += stride;
     }
   }
 }
@@ -2587,8 +2619,10 @@ int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   GYT_CK(ctx, after_legacy_stream(ctx));
   const Params prm = make_params(params);
+  // persistent: the four resident blocks per SM of k_vpt, each lane taking
+  // samples until the grid stride runs past the end
   const uint32_t grid = (uint32_t)std::min<unsigned long long>((count + kBlock - 1) / kBlock,
-                                                                (unsigned long long)std::max(1, ctx->sms) * 8);
+                                                                (unsigned long long)std::max(1, ctx->sms) * 4);
   GYT_CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   if (scene->dev.wnodes)
     k_vpt<8><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
