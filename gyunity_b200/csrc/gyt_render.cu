@@ -149,9 +149,10 @@ constexpr int extend_blocks_per_sm() { return 4; }
 // The shade kernels, once their blocks are sorted by lobe type, are bound by
 // latency at two blocks per SM (124 registers): a cap of 80 registers (three
 // blocks, some spilled values) shades 11-13% faster on the procedural mesh
-// and the uneven batch. 128-thread blocks at the same occupancy were slower:
+// and the uneven batch, and 64 registers (four blocks) another 3% (2% of the
+// whole render on both). 128-thread blocks at the same occupancy were slower:
 // the sort window is the block.
-constexpr int kShadeBlocksPerSm = 3;
+constexpr int kShadeBlocksPerSm = 4;
 
 // meta bit 20: the bounce queued an MIS ray whose contribution k_finish adds
 constexpr uint32_t kMisQueued = 1u << 20;
