@@ -252,6 +252,34 @@ def cornell_fog(res=128, spp=8, max_depth=8, sigma_a=0.05, sigma_s=0.5, g=0.3, s
         name="cornell_fog_%dx%d_%dspp" % (res, res, spp))
 
 
+def fog_ball_box(res=48, spp=4, max_depth=6, level=2, sigma_a=0.1, sigma_s=2.0, g=0.5) -> SceneDesc:
+    """The Cornell box (no spheres, no fog in the box) holding a ball of fog:
+    a level-``level`` icosphere of radius 0.45 at (0, -0.45, 0) with no
+    material whose MediumInterface is (inside: the medium, outside: none),
+    outward normals. Camera rays and light paths enter and leave the medium
+    through it repeatedly; shadow rays cross it."""
+    sd = cornell_box(res=res, spp=spp, max_depth=max_depth, rr_depth=5, spheres=False)
+    v, f = icosphere(level)
+    nv = sd.vertices.shape[0]
+    none = sd.mat_type.shape[0]
+    nt = sd.n_triangles
+    ball = (v * 0.45 + np.array([0.0, -0.45, 0.0])).astype(np.float32)
+    tri_medium = np.full((nt + f.shape[0], 2), -1, np.int32)
+    tri_medium[nt:] = (0, -1)
+    return dataclasses.replace(
+        sd,
+        vertices=np.concatenate([sd.vertices, ball]),
+        normals=np.concatenate([sd.normals, v.astype(np.float32)]),
+        indices=np.concatenate([sd.indices, (f + nv).astype(np.uint32)]),
+        tri_material=np.concatenate([sd.tri_material, np.full(f.shape[0], none, np.uint32)]),
+        tri_emission=np.concatenate([sd.tri_emission, np.full(f.shape[0], -1, np.int32)]),
+        mat_type=np.concatenate([sd.mat_type, np.array([MAT_NONE], np.uint32)]),
+        mat_params=np.concatenate([sd.mat_params, np.zeros((1, 16), np.float32)]),
+        media=np.array([[sigma_a] * 3 + [sigma_s] * 3 + [g]], np.float32),
+        tri_medium=tri_medium,
+        name="fog_ball_box_%dx%d_%dspp" % (res, res, spp))
+
+
 # ---------------------------------------------------------------- meshes ----
 
 def _hash3(ix, iy, iz, seed):

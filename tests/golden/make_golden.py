@@ -12,6 +12,7 @@ checkout is only needed to regenerate; the tests read the fixtures.
     python tests/golden/make_golden.py lt         # only the light-tracing fixtures
     python tests/golden/make_golden.py vpt        # only the volume fixtures
 """
+import dataclasses
 import os
 import sys
 import tempfile
@@ -242,18 +243,24 @@ def light_tracing_golden(tmp):
 
 def volume_golden(tmp):
     """VolPathTracing (without equi-angular sampling) per path and rendered,
-    on the Cornell box filled with fog (scenes.cornell_fog)."""
+    on the Cornell box filled with fog (scenes.cornell_fog, also with the
+    Halton sampler) and on the box holding a ball of fog
+    (scenes.fog_ball_box)."""
     rng = np.random.default_rng(20261208)
+    halton = scenes.cornell_fog(res=48, spp=4, max_depth=6)
+    halton = dataclasses.replace(halton, params=dataclasses.replace(halton.params, sampler="halton"))
     for name, sd in (("fog", scenes.cornell_fog(res=48, spp=4, max_depth=6)),
                      ("fog_thick", scenes.cornell_fog(res=48, spp=4, max_depth=6, sigma_a=0.2, sigma_s=1.5, g=-0.4,
-                                                      spheres=False))):
+                                                      spheres=False)),
+                     ("fog_ball", scenes.fog_ball_box(res=48, spp=4, max_depth=6)),
+                     ("fog_halton", halton)):
         path = os.path.join(tmp, "vpt_%s.gyts" % name)
         io.write_scene(path, sd)
         n = 3000
         x = rng.integers(0, sd.camera.res_x, n)
         y = rng.integers(0, sd.camera.res_y, n)
         s = rng.integers(0, sd.params.spp, n)
-        r = io.ref_paths(tmp, path, x, y, s, integrator="vpt")
+        r = io.ref_paths(tmp, path, x, y, s, sampler=sd.params.sampler, integrator="vpt")
         np.savez_compressed(os.path.join(HERE, "vpt_paths_%s.npz" % name), xys=np.stack([x, y, s], 1).astype(np.uint32),
                             L=r[:, :3], cursor=r[:, 3].astype(np.int32))
     sd = scenes.cornell_fog(res=64, spp=8, max_depth=6)

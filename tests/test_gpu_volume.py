@@ -7,6 +7,8 @@ Per path the radiance must agree within relative 1e-4 of max(|L|, 1e-3) and
 the path must use the same number of sampler dimensions. A path can branch
 differently where a rounding decides (a scattering distance that lands on a
 surface, a grazing shadow ray); those are counted and bounded."""
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -17,9 +19,18 @@ from gyunity_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 
+def _halton_fog():
+    sd = scenes.cornell_fog(res=48, spp=4, max_depth=6)
+    return dataclasses.replace(sd, params=dataclasses.replace(sd.params, sampler="halton"))
+
+
+# the fog ball: a closed material-less icosphere whose inside is the medium,
+# entered and left through its faces (medium transitions both ways)
 CASES = {"fog": lambda: scenes.cornell_fog(res=48, spp=4, max_depth=6),
          "fog_thick": lambda: scenes.cornell_fog(res=48, spp=4, max_depth=6, sigma_a=0.2, sigma_s=1.5, g=-0.4,
-                                                 spheres=False)}
+                                                 spheres=False),
+         "fog_ball": lambda: scenes.fog_ball_box(res=48, spp=4, max_depth=6),
+         "fog_halton": _halton_fog}
 
 
 @pytest.mark.parametrize("name", list(CASES))

@@ -48,3 +48,14 @@ def test_cornell_fog_layout():
     assert np.all(sd.mat_type[sd.tri_material[inside]] == scenes.MAT_NONE)
     assert np.all(sd.tri_medium[:12] == -1) and np.all(sd.tri_medium[12:, 1] == -1)
     assert np.all(sd.vertices[sd.indices[12:]][..., 2] == 1.0)
+
+
+def test_fog_ball_layout():
+    sd = scenes.fog_ball_box(level=2)
+    ball = np.arange(12, sd.n_triangles)
+    assert ball.shape[0] == 320 and sd.media.shape == (1, 7)
+    assert np.all(sd.tri_medium[ball] == (0, -1)) and np.all(sd.tri_medium[:12] == -1)
+    assert np.all(sd.mat_type[sd.tri_material[ball]] == scenes.MAT_NONE)
+    # outward shading normals: leaving along the normal enters the outside (no medium)
+    c = sd.vertices[sd.indices[ball]].mean(1) - np.array([0.0, -0.45, 0.0])
+    assert np.all(np.einsum("ij,ij->i", c, sd.normals[sd.indices[ball, 0]]) > 0)
