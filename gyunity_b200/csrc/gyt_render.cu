@@ -668,7 +668,12 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
   Rng rng{cur.sidx[i], (meta >> 9) & 2047u};
   float3 ro = f3(cur.o[i]), rd = f3(cur.d[i]);
   float3 tp = f3(cur.tp[i]);
-  float3 L = f3(cur.L[i]);
+  // the path's radiance changes only on emission (a light or the environment
+  // seen directly): added to the stored sum there, not carried through
+  auto add_L = [&](float3 v) {
+    const float3 L = f3(cur.L[i]) + v;
+    cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
+  };
   const uint32_t bounce = depth;
   bool alive = false;
   float3 adj = mk(0.f, 0.f, 0.f);
@@ -679,13 +684,13 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     const uint2 pend = A.pend[i];
     if (pend.x & kPendValid) {
       // the previous continuation's BSDF factor scales all radiance after it
-      const float3 after = f3(A.Ltot[i]) - L;
+      const float3 after = f3(A.Ltot[i]) - f3(cur.L[i]);
       grad_material(G, s, pend.x & ~kPendValid, adj * after, __uint_as_float(pend.y));
     }
   }
   if (prim < 0) {
     // PT.cpp:18-21: environment emission on the camera ray or after a delta bounce
-    if ((depth == 0 || delta) && s.has_env) L = L + tp * env_lookup(s.env, rd);
+    if ((depth == 0 || delta) && s.has_env) add_L(tp * env_lookup(s.env, rd));
   } else {
     Hit h;
     uint32_t mat;
@@ -715,7 +720,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     if (emit) {
       LightTri l = load_light(s, light);
       if (dot(h.n, h.wo) > 0.f) {
-        L = L + tp * l.Le;  // AreaLight::Emission (AreaLight.h:40-43)
+        add_L(tp * l.Le);  // AreaLight::Emission (AreaLight.h:40-43)
         if (ADJ) grad_emitter(G, s, light, adj * (tp * l.Le));
       }
     } else {
@@ -789,7 +794,9 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
         float cos2 = fabsf(dot(h.n, wi2));
         if (pdf2 != 0.f && !is_zero(f2)) {
           float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
-          float lpdf = env_light ? env_pdf_dir(s.env, wi2) : tri_light_pdf(l, h, o2, wi2);
+          // the light triangle again from the light table rather than kept live
+          // across the BSDF evaluation and sampling
+          float lpdf = env_light ? env_pdf_dir(s.env, wi2) : tri_light_pdf(load_light(s, li), h, o2, wi2);
           if (lpdf != 0.f) {
             float w2 = power_heuristic(pdf2, lpdf);
             float3 c = tp * (f2 * cos2 / pdf2) * w2 / lsel;
@@ -838,7 +845,6 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
       }
     }
   }
-  cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
   cur.meta[i] = meta_pack(depth, delta, rng.cursor, alive, DEFER && mis_queued);
   if (ADJ) A.pend[i] = pend_new;
 }
