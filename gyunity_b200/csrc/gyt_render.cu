@@ -1492,8 +1492,10 @@ GYT_D void lt_splat(double* splat, const LtCam& c, int X, int Y, float3 L) {
 
 // One thread per photon (grid-stride). rec (debug, may be null): per photon
 // max_depth records of (on film 1/0 or -1 for no vertex, X, Y, scaled L).
+// Capped at four blocks per SM (64 registers; spills, but more warps to hide
+// the dependent node fetches): 446 -> 462 Mphotons/s on the Cornell box.
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_light_trace(DevScene s, LtCam c, Params prm, SamplerTables tab,
+__global__ void __launch_bounds__(kBlock, 4) k_light_trace(DevScene s, LtCam c, Params prm, SamplerTables tab,
                                                         unsigned long long n, const unsigned long long* __restrict__ ids,
                                                         double* __restrict__ splat, float* __restrict__ rec) {
   for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
