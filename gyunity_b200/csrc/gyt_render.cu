@@ -1828,8 +1828,8 @@ GYT_D bool vpt_intersect_tr(const DevScene& s, float3 o, float3 d, int medium, i
 // for a surface point (bsdf) or a medium point (phase g). u: uLight, u.y, u.x,
 // v.z, v.y, v.x as the caller draws them.
 template <int W>
-__device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, const Hit* h, float ul,
-                        float ux, float uy, float vx, float vy, float vz) {
+__device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, float ul, float ux,
+                                          float uy, float vx, float vy, float vz) {
   if (s.n_lights <= 0) return mk(0.f, 0.f, 0.f);
   float lsel = 0.f;
   const int li = sample_light(s, ul, &lsel);
@@ -1912,7 +1912,6 @@ __device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, co
       }
     }
   }
-  (void)h;
   return (L1 * w1 + L2 * w2) / lsel;
 }
 
@@ -2048,7 +2047,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params p
         const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
         const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
         const float ul = rng.next(tab, prm.sampler);
-        L = L + tp * vpt_direct<W>(s, p, scattered ? nullptr : &bsdf, g, nullptr, ul, ux, uy, vx, vy, vz);
+        L = L + tp * vpt_direct<W>(s, p, scattered ? nullptr : &bsdf, g, ul, ux, uy, vx, vy, vz);
       }
       if (!end && !pass) {
         if (scattered) {
