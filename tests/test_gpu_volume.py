@@ -99,3 +99,22 @@ def test_volume_edge_sizes(ctx):
     assert L.shape == (0, 3) and cur.shape == (0,)
     L, cur = sc.trace_volume_paths(np.array([[0, 0, 0], [15, 15, 0]], np.uint32))
     assert L.shape == (2, 3) and np.isfinite(L).all() and np.all(cur >= 2)
+
+
+def test_volume_rejects_bad_input(ctx):
+    """Errors come back as status codes: an environment light is refused, a
+    medium index out of range and a sample off the film are rejected."""
+    sd = scenes.cornell_fog(res=16, spp=1, max_depth=3)
+    d = torch.zeros(16 * 16 * 4, dtype=torch.float64, device="cuda")
+    env = g.Scene(scenes.env_knot_small(), ctx)
+    with pytest.raises(g.GytError):
+        ctx.render_volume_device(env, sd.camera, sd.params, d.data_ptr())
+    bad = dataclasses.replace(sd, tri_medium=np.where(sd.tri_medium >= 0, 1, -1).astype(np.int32))
+    with pytest.raises(g.GytError):
+        g.Scene(bad, ctx)
+    sc = g.Scene(sd, ctx)
+    with pytest.raises(g.GytError):
+        sc.trace_volume_paths(np.array([[16, 0, 0]], np.uint32))
+    # the context stays usable after the errors
+    L, cur = sc.trace_volume_paths(np.array([[3, 4, 0]], np.uint32))
+    assert np.isfinite(L).all() and cur[0] >= 2
