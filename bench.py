@@ -22,6 +22,7 @@ Multi-GPU runs are weak scaling: every rank renders the whole workload
 geometry stands in for the reference's mesh assets.
 """
 import argparse
+import dataclasses
 import ctypes
 import json
 import os
@@ -214,11 +215,11 @@ def peaks():
 
 
 # ---------------------------------------------------------- CPU baseline ---
-# The reference CPU integrator runs on a bounded sample of the batch: every
-# 16th instance (4 of 64: 158k, 33k, 1.05M and 473k triangles; 256^2 to
-# 1024^2 films) at up to 2 spp, about 8 s of single-core-equivalent work.
-BATCH_SAMPLE_STRIDE = 16
-BATCH_SAMPLE_SPP = 2
+# The reference CPU integrator on the batch's own path mix: every instance, on
+# a regular grid of every 16th column and 32nd row of its film with all of its
+# samples per pixel, i.e. 1/512 of each instance's paths (1.6M of the 834M),
+# so that each instance weighs in the sample as it weighs in the batch.
+BATCH_GRID = (16, 32)
 
 
 def _cpu_render(sd, spp, rows=None, threads=None):
@@ -265,24 +266,57 @@ def batch_workload(n, sampler="sobol", stride=1):
     return out
 
 
-def batch_sample(n, sampler="sobol"):
-    return batch_workload(n, sampler, BATCH_SAMPLE_STRIDE)
+def batch_grid_samples(sd, i):
+    """Instance i's share of the CPU sample: pixels on a grid of every
+    BATCH_GRID[0]th column and BATCH_GRID[1]th row (offset by the instance
+    index), every sample of each: (n, 3) uint32 x, y, s."""
+    gx, gy = BATCH_GRID
+    W, H, S = sd.camera.res_x, sd.camera.res_y, sd.params.spp
+    xs = np.arange(i % gx, W, gx)
+    ys = np.arange((i // gx) % gy, H, gy)
+    X, Y = np.meshgrid(xs, ys)
+    px = np.stack([X.ravel(), Y.ravel()], 1)
+    return np.concatenate([np.repeat(px, S, axis=0), np.tile(np.arange(S), len(px))[:, None]], 1).astype(np.uint32)
 
 
-def cpu_baseline_batch(sample, threads=None):
-    """Batch CPU baseline: the sampled instances one after another, each at
-    min(its spp, 2) over its full film; Mpaths/s = sample paths / the sum of
-    the render times."""
-    paths, secs, kind, th = 0, 0.0, None, None
-    for _, sd in sample:
-        n, sec, kind, th = _cpu_render(sd, min(sd.params.spp, BATCH_SAMPLE_SPP), threads=threads)
-        paths += n
-        secs += sec
-    what = "TiledIntegrator::Render" if kind == "reference" else "CPU restatement"
-    return {"value": paths / secs / 1e6, "unit": UNIT, "cores": th, "kind": kind,
-            "sample": "instances %s of the batch, full films at min(spp, %d): %d paths (%s, BVH build excluded)"
-                      % (",".join(str(i) for i, _ in sample), BATCH_SAMPLE_SPP, paths, what),
-            "paths": paths, "render_s": secs}
+def cpu_reference_batch(descs, warmup, steps, threads=None):
+    """The batch CPU baseline: the reference's PathTracing::Li over every
+    instance's grid sample (batch_grid_samples), instance after instance,
+    scene loading and the reference's BVH build untimed; warmup + steps
+    passes. Returns (Mpaths/s of each step, description). Without the
+    reference binary the oracle's CPU restatement traces the same samples."""
+    from oracle import scene_io as io
+    sample = [(sd, batch_grid_samples(sd, i)) for i, sd in enumerate(descs)]
+    paths = int(sum(len(x) for _, x in sample))
+    total = int(sum(sd.n_paths() for sd in descs))
+    if io.have_harness():
+        with tempfile.TemporaryDirectory() as tmp:
+            items = []
+            for i, (sd, xys) in enumerate(sample):
+                path = os.path.join(tmp, "inst%d.gyts" % i)
+                io.write_scene(path, sd)
+                items.append((path, xys))
+            rec = io.ref_sample(tmp, items, warmup, steps, sampler=descs[0].params.sampler, threads=threads)
+        vals = [rec["paths_per_step"] / t / 1e6 for t in rec["step_s"]]
+        kind, cores, what = "reference", rec["threads"], "PathTracing::Li of the reference"
+    else:
+        from oracle.port import oracle as orc
+        cores = threads or os.cpu_count() or 1
+        secs = [0.0] * steps
+        for sd, xys in sample:
+            o = orc.OracleScene(sd)
+            for k in range(warmup + steps):
+                t = time.perf_counter()
+                o.paths(xys[:, 0], xys[:, 1], xys[:, 2], precision=32, threads=cores)
+                if k >= warmup:
+                    secs[k - warmup] += time.perf_counter() - t
+        vals = [paths / t / 1e6 for t in secs]
+        kind, what = "port", "the CPU restatement"
+    desc = ("all %d instances, every %dth column and %dth row of each film with all its samples per pixel: %d of "
+            "the batch's %d paths (1/%d of every instance, the batch's own mix), %s, scene loading and BVH build "
+            "untimed" % (len(descs), BATCH_GRID[0], BATCH_GRID[1], paths, total, BATCH_GRID[0] * BATCH_GRID[1],
+                         what))
+    return vals, {"kind": kind, "cores": cores, "sample": desc, "paths": paths}
 
 
 def run_reference(a):
@@ -290,23 +324,22 @@ def run_reference(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     if a.workload == "batch":
-        sample = batch_sample(a.batch_instances, a.sampler)
-        step = lambda: cpu_baseline_batch(sample)  # noqa: E731
-        cfg = batch_config(a, None, {"reference_sample": "every %dth instance at min(spp, %d)"
-                                                          % (BATCH_SAMPLE_STRIDE, BATCH_SAMPLE_SPP)})
+        descs = [sd for _, sd in batch_workload(a.batch_instances, a.sampler)]
+        vals, info = cpu_reference_batch(descs, a.warmup, a.steps)
+        cfg = batch_config(a, descs)
         metric = METRIC
     else:
         sd = workload(a)
-        step = lambda: cpu_baseline(sd, 1)  # noqa: E731
+        vals, info = [], None
+        for k in range(a.warmup + a.steps):
+            info = cpu_baseline(sd, 1)
+            if k >= a.warmup:
+                vals.append(info["value"])
+        info["paths"] = sd.camera.res_x * sd.camera.res_y
         cfg = config(a, sd, {"reference_sample_spp": 1})
         metric = METRIC_SINGLE
-    vals, info = [], None
-    for k in range(a.warmup + a.steps):
-        info = step()
-        if k >= a.warmup:
-            vals.append(info["value"])
     v = statistics.median(vals)
-    paths = info.get("paths") or (sd.camera.res_x * sd.camera.res_y)
+    paths = info["paths"]
     line = {"impl": "reference", "metric": metric, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": paths / v / 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -447,8 +480,8 @@ def measure_single(a, d, g, torch):
                         "note": "public Render call with the scene resident, image copied to host each step"},
                 "e2e_cold": {"value": paths / a.steps / cold_s / 1e6, "unit": UNIT,
                              "note": "scene upload from host arrays + BVH build + render + image readback"},
-                "gpu_launches": launches, "roofline": out, "clocks": clk.summary(), "profile": prof,
-                "traversal_counts": cnt}
+                "gpu_launches": launches, "roofline": out, "rays_per_s": rays_per_s(prof, dev_ms / a.steps),
+                "clocks": clk.summary(), "profile": prof, "traversal_counts": cnt}
         if not a.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(sd, spp=2)
@@ -489,13 +522,25 @@ def measure_batch(a, d, g, torch):
     gen_s = time.perf_counter() - t
     ctx = g.Context(d.local)
     t = time.perf_counter()
-    scs = [g.Scene(sd, ctx) for sd in descs]
+    scs2 = [g.Scene(sd, ctx) for sd in descs]
     create_s = time.perf_counter() - t
+    # the same scenes with the 8-wide BVH (built on the device too), so that
+    # the autotuner can pick the width
+    ctx8 = g.Context(d.local, bvh_width=8)
+    t = time.perf_counter()
+    scs8 = [g.Scene(sd, ctx8) for sd in descs]
+    create8_s = time.perf_counter() - t
     cams = [sd.camera for sd in descs]
     prms = [sd.params for sd in descs]
     films = [torch.zeros(c.res_x * c.res_y * 4, dtype=torch.float64, device="cuda") for c in cams]
     ptrs = [f.data_ptr() for f in films]
     paths = sum(sd.n_paths() for sd in descs)
+
+    t = time.perf_counter()
+    cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=1)
+    tune_s = time.perf_counter() - t
+    # both integrators render the scenes of the width the autotuner chose
+    scs = scs8 if cfg["bvh_width"] == 8 else scs2
 
     def per_scene():
         ms = 0.0
@@ -515,9 +560,6 @@ def measure_batch(a, d, g, torch):
     per_wall = time.perf_counter() - w0
     per_ms = d.max(per_ms)
 
-    t = time.perf_counter()
-    cfg, tune_mp = ctx.batch_autotune(scs, cams, prms, sample_spp=1)
-    tune_s = time.perf_counter() - t
     for _ in range(a.warmup):
         ctx.render_batch_device(scs, cams, prms, ptrs)
     d.barrier()
@@ -570,8 +612,8 @@ def measure_batch(a, d, g, torch):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": b_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes, no dataset)",
-                "config": batch_config(a, descs, {"parallelism": "independent batches per GPU" if d.world > 1
-                                                  else "1 GPU", "batch_config": cfg}),
+                "config": batch_config(a, descs),
+                "parallelism": "independent batches per GPU" if d.world > 1 else "1 GPU", "batch_config": cfg,
                 "wall_ms_per_step": b_wall * 1e3,
                 "per_scene": {"value": paths * d.world / (per_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": per_ms,
                               "wall_ms_per_step": per_wall * 1e3,
@@ -579,23 +621,31 @@ def measure_batch(a, d, g, torch):
                 "speedup_vs_per_scene": per_ms / b_ms,
                 "equal_rmse": {"max_rel_film_diff": fdiff,
                                "note": "same paths in both runs; only the order of the FP64 film sums differs"},
-                "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s},
+                "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s,
+                             "widths_tried": [2, 8],
+                             "note": "coordinate search over BVH width (binary and 8-wide scenes, both built on "
+                                     "the device), pool size, grid-stride and traversal blocks per SM on a 1-spp "
+                                     "sample; the per-scene renders use the chosen width too"},
                 "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": imgs_bytes, "steps": e2e_steps,
                         "note": "gyt_render_batch with the scenes resident: cameras and parameters in, "
                                 "every image copied to host memory"},
                 "gpu_launches": launches, "graph_launches": a.steps,
                 "iterations_per_step": stats[-1]["iterations"],
-                "roofline": out, "clocks": clk.summary(), "profile": prof, "traversal_counts": cnt,
-                "scene_generation_s": gen_s, "scene_create_s": create_s}
+                "roofline": out, "rays_per_s": rays_per_s(prof, b_ms / d.world),
+                "clocks": clk.summary(), "profile": prof, "traversal_counts": cnt,
+                "scene_generation_s": gen_s, "scene_create_s": create_s, "scene_create_8wide_s": create8_s}
         if not a.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline_batch(batch_sample(a.batch_instances, a.sampler))
+                vals, info = cpu_reference_batch(descs, 0, 1)
+                line["cpu_baseline"] = {"value": vals[0], "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                                        "sample": info["sample"]}
             except Exception as e:  # reported, never fatal for the GPU numbers
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     del films
-    for sc in scs:
+    for sc in scs2 + scs8:
         sc.close()
+    ctx8.close()
     ctx.close()
     return line
 
@@ -664,19 +714,33 @@ def measure_volume(a, d, g, torch):
            "value": paths * d.world / (t / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": t,
            "note": "one kernel launch per render (a camera sample per thread; closest-hit, transmittance and "
                    "shadow rays traced inline); FP64 film"}
+    # the same render with equi-angular sampling (VolPathTracing's default)
+    sde = dataclasses.replace(sd, params=dataclasses.replace(sd.params, equi_angular=True))
+    ms = []
+    film.zero_()
+    for k in range(a.warmup + a.steps):
+        st = ctx.render_volume_device(sc, sde.camera, sde.params, film.data_ptr())
+        if k >= a.warmup:
+            ms.append(st["ms"])
+    te = d.max(statistics.median(ms))
+    out["equi_angular"] = {"value": paths * d.world / (te / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": te,
+                           "note": "VolPathTracing with equalAngular = true: one light point per bounce, "
+                                   "equi-angular distances in the medium, the connection to that point"}
     if d.rank == 0 and not a.no_cpu_baseline:
-        try:
-            from oracle import scene_io as io
-            if io.have_harness():
-                with tempfile.TemporaryDirectory() as tmp:
-                    path = os.path.join(tmp, "vpt.gyts")
-                    io.write_scene(path, sd)
-                    _, info = io.ref_render(tmp, path, rows=128, integrator="vpt")
-                out["cpu_baseline"] = {"value": info["mpaths_per_s"], "unit": "Mpaths/s", "cores": info["threads"],
-                                       "kind": "reference",
-                                       "sample": "TiledIntegrator::Render with VolPathTracing, first 128 rows"}
-        except Exception as e:  # reported, never fatal for the GPU numbers
-            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        for integ, key, dst in (("vpt", "cpu_baseline", out), ("vpt_eq", "cpu_baseline", out["equi_angular"])):
+            try:
+                from oracle import scene_io as io
+                if io.have_harness():
+                    with tempfile.TemporaryDirectory() as tmp:
+                        path = os.path.join(tmp, "vpt.gyts")
+                        io.write_scene(path, sd)
+                        _, info = io.ref_render(tmp, path, rows=128, integrator=integ)
+                    dst[key] = {"value": info["mpaths_per_s"], "unit": "Mpaths/s", "cores": info["threads"],
+                                "kind": "reference",
+                                "sample": "TiledIntegrator::Render with VolPathTracing (%s), first 128 rows" %
+                                          ("equalAngular = true" if integ == "vpt_eq" else "equalAngular = false")}
+            except Exception as e:  # reported, never fatal for the GPU numbers
+                dst[key] = {"value": None, "error": str(e)[:200]}
     ctx.close()
     return out
 
@@ -724,16 +788,23 @@ def measure_adjoint(a, d, g, torch):
             q.radiance[i, c] = v
         return q
 
-    checks = []
+    checks, free = [], []
     for kind, i, c in picks:
         cur = get(init, kind, i, c)
         keep = kind == "radiance"
         up, dn = np.float32(cur + 1e-3), np.float32(cur - 1e-3)
-        fd = (diff.loss_at(r, put(init, kind, i, c, up), target, keep) -
-              diff.loss_at(r, put(init, kind, i, c, dn), target, keep)) / (float(up) - float(dn))
+        # alpha: BSDF sampling and pdfs frozen at the unstepped parameters, so
+        # that the difference quotient is the detached-sampling derivative
+        frozen = init if kind == "alpha" else None
+        fd = (diff.loss_at(r, put(init, kind, i, c, up), target, keep, frozen) -
+              diff.loss_at(r, put(init, kind, i, c, dn), target, keep, frozen)) / (float(up) - float(dn))
         ad = float(get(grad, kind, i, c))
-        checks.append({"param": "%s[%d%s]" % (kind, i, "" if kind == "alpha" else ",%d" % c), "fd": fd,
-                       "adjoint": ad, "rel_err": abs(fd - ad) / max(abs(fd), 1e-30)})
+        name = "%s[%d%s]" % (kind, i, "" if kind == "alpha" else ",%d" % c)
+        checks.append({"param": name, "fd": fd, "adjoint": ad, "rel_err": abs(fd - ad) / max(abs(fd), 1e-30)})
+        if kind == "alpha":
+            fd_free = (diff.loss_at(r, put(init, kind, i, c, up), target) -
+                       diff.loss_at(r, put(init, kind, i, c, dn), target)) / (float(up) - float(dn))
+            free.append({"param": name, "fd": fd_free, "adjoint": ad})
     out = {"workload": "inverse rendering: 20,480-triangle icosphere, 256 GGX groups, 4 emitters, 512x512, 32 spp, "
                        "depth 8, %d parameters" % P,
            "forward_ms": t_f, "adjoint_ms": t_a,
@@ -744,9 +815,15 @@ def measure_adjoint(a, d, g, torch):
            "fd_check": checks,
            "fd_check_max_rel_err": {k: max(x["rel_err"] for x in checks if x["param"].startswith(k))
                                     for k in ("albedo", "radiance", "alpha")},
-           "fd_check_note": "central differences, step 1e-3; emitter steps keep the light-selection "
-                            "distribution; alpha moves the sampled directions, which fixed-sample differences "
-                            "follow and the detached adjoint does not"}
+           "fd_check_note": "central differences of the full loss, step 1e-3; emitter steps keep the "
+                            "light-selection distribution; alpha steps hold BSDF sampling and pdfs at the "
+                            "unstepped parameters (gyt_scene_freeze_sampling), whose difference quotient is the "
+                            "detached-sampling derivative",
+           "fd_free_alpha": free,
+           "fd_free_alpha_note": "the same alpha steps with sampling free: the sampled directions move with "
+                                 "alpha, a far noisier estimator of the same derivative (one sample set; "
+                                 "tests/test_gpu_adjoint.py checks its mean over 32 disjoint sample sets "
+                                 "against the adjoint)"}
     if a.adjoint_iters > 0:
         t = time.perf_counter()
         p, hist = diff.optimize(r, target, init, iterations=a.adjoint_iters, lr=0.02)
@@ -771,47 +848,77 @@ def measure_adjoint(a, d, g, torch):
 STATE_READ, STATE_WRITE, HIT, RAY, CONTRIB = 76, 68, 16, 32, 16
 
 
-def roofline(prof, cnt, slots, node_bytes=64):
-    """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
-    of its launches / their CUDA-event time; traversal bytes per ray = BVH
-    nodes x node size + triangle tests x 48 B (counts from the counting pass)."""
-    peak, src = peaks()
-    ms = {k: v for k, v in prof["ms"].items() if k != "unused"}
-    dom = max(ms, key=ms.get)
-    launches = max(1, prof["launches"][dom])
+def kernel_bytes(kernel, prof, cnt, slots, node_bytes):
+    """Algorithmic bytes of all launches of one kernel in a profiled render:
+    traversal bytes per ray = BVH nodes x node size + triangle tests x 48 B
+    (counts from the counting pass) on top of the ray and hit records; the
+    shade, finish and generate kernels by their path-state records."""
     rays = cnt["rays"]
 
     def trav(k):
         r = max(1, rays[k])
         return cnt["node_visits"][k] / r * node_bytes + cnt["tri_tests"][k] / r * 48
 
-    if dom == "extend":
-        byts = rays["extend"] * (RAY + HIT + trav("extend"))
-    elif dom == "connect":
-        byts = sum(rays[k] * (RAY + CONTRIB + 16 + trav(k)) for k in ("shadow", "mis"))
-    elif dom == "shade":
-        byts = slots * (STATE_READ + HIT + STATE_WRITE) + (rays["shadow"] + rays["mis"]) * (RAY + CONTRIB)
-    elif dom == "finish":
-        byts = slots * (STATE_READ + 4) + slots * (STATE_READ + 8)
-    else:
-        byts = slots * STATE_WRITE
+    if kernel == "extend":
+        return rays["extend"] * (RAY + HIT + trav("extend"))
+    if kernel == "connect":
+        return sum(rays[k] * (RAY + CONTRIB + 16 + trav(k)) for k in ("shadow", "mis"))
+    if kernel == "shade":
+        return slots * (STATE_READ + HIT + STATE_WRITE) + (rays["shadow"] + rays["mis"]) * (RAY + CONTRIB)
+    if kernel == "finish":
+        return slots * (STATE_READ + 4) + slots * (STATE_READ + 8)
+    return slots * STATE_WRITE
+
+
+def roofline(prof, cnt, slots, node_bytes=64):
+    """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
+    of its launches / their CUDA-event time (kernel_bytes); the same figures
+    for every kernel under "kernels", and the ncu issue utilisation and SIMD
+    efficiency of the captured kernels (profiles/traffic.json) under "ncu"."""
+    peak, src = peaks()
+    ms = {k: v for k, v in prof["ms"].items() if k != "unused"}
+    dom = max(ms, key=ms.get)
+    launches = max(1, prof["launches"][dom])
+    rays = cnt["rays"]
+    byts = kernel_bytes(dom, prof, cnt, slots, node_bytes)
     achieved = byts / (ms[dom] / 1e3) / 1e9
-    traffic = None
+    traffic, ncu = None, {}
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            rec = json.load(open(tf)).get("k_" + dom)
-            if rec:
+            recs = json.load(open(tf))
+            rec = recs.get("k_" + dom)
+            if rec and "bytes_per_slot" in rec:
                 traffic = rec["bytes_per_slot"] * slots / launches
+            ncu = {k: {f: v[f] for f in ("issue_active", "threads_per_inst", "source") if f in v}
+                   for k, v in recs.items() if "issue_active" in v}
         except Exception:
             traffic = None
+    kernels = {}
+    for k, t in ms.items():
+        n = max(1, prof["launches"][k])
+        b = kernel_bytes(k, prof, cnt, slots, node_bytes)
+        kernels["k_" + k] = {"share": t / sum(ms.values()), "launches": n, "avg_launch_ms": t / n,
+                             "algorithmic_bytes_per_launch": b / n,
+                             "achieved_gbs": b / (t / 1e3) / 1e9 if t > 0 else None,
+                             "frac": b / (t / 1e3) / 1e9 / peak if t > 0 else None}
     per_ray = {k: {"nodes": cnt["node_visits"][k] / max(1, rays[k]), "tris": cnt["tri_tests"][k] / max(1, rays[k]),
                    "rays": rays[k]} for k in rays}
     return {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic,
             "algorithmic_bytes_per_launch": byts / launches, "launches": launches,
             "avg_launch_ms": ms[dom] / launches, "traversal": per_ray,
-            "share": {k: v / sum(ms.values()) for k, v in ms.items()}}
+            "share": {k: v / sum(ms.values()) for k, v in ms.items()}, "kernels": kernels, "ncu": ncu}
+
+
+def rays_per_s(prof, step_ms):
+    """Extend, shadow and MIS rays traced per second of the timed step (the
+    profiled render traces the same rays as each timed step)."""
+    r = prof["rays"]
+    out = {k: r[k] / (step_ms / 1e3) for k in ("extend", "shadow", "mis")}
+    out["total"] = sum(out.values())
+    out["unit"] = "rays/s"
+    return out
 
 
 def main():

@@ -185,6 +185,19 @@ class Context:
         return {f: getattr(best, f) for f, _ in _c.GytBatchConfig._fields_}, mp.value
 
     # ---- parity / debug entry points --------------------------------------
+    def bsdf_table(self, types, params, wo, u, we):
+        """gyt_bsdf_table: the GPU's BxDF lobes for n cases (kind, 16
+        parameters, wo, u, we): (n, 11) = sampled f, wi, pdf, then f and pdf
+        toward we."""
+        t = np.ascontiguousarray(types, np.uint32)
+        n = t.shape[0]
+        p = np.ascontiguousarray(params, np.float32).reshape(n, 16)
+        v = np.ascontiguousarray(np.concatenate([np.reshape(wo, (n, 3)), np.reshape(u, (n, 3)),
+                                                 np.reshape(we, (n, 3))], 1), np.float32)
+        out = np.empty((n, 11), np.float32)
+        self.check(self._lib.gyt_bsdf_table(self.handle, n, _c.ptr(t), _c.ptr(p), _c.ptr(v), _c.ptr(out)))
+        return out
+
     def sobol(self, dims, indices):
         """sobol::sample (sampler/Sobol.h:46-61) for (dimension, index) pairs."""
         d = np.ascontiguousarray(dims, np.uint32)
@@ -288,6 +301,13 @@ class Scene:
         flags = _c.KEEP_LIGHT_SAMPLING if keep_light_sampling else 0
         self.ctx.check(self.ctx._lib.gyt_scene_set_materials(self.handle, _c.ptr(mp), _c.ptr(em), flags))
 
+    def freeze_sampling(self, mat_params=None):
+        """gyt_scene_freeze_sampling: BSDF sampling and pdfs from mat_params
+        (n_materials, 16) while the GGX BSDF values follow the current
+        parameters; None ends it. For difference checks of the adjoint."""
+        mp = None if mat_params is None else np.ascontiguousarray(mat_params, np.float32)
+        self.ctx.check(self.ctx._lib.gyt_scene_freeze_sampling(self.handle, _c.ptr(mp)))
+
     def read_bvh(self):
         """The binary BVH on the host: node slots (n, 16) float32 in the
         traversal layout and the scene triangle id of each leaf-order position."""
@@ -299,6 +319,18 @@ class Scene:
         self.ctx.check(lib.gyt_scene_read_bvh(self.handle, _c.ptr(nodes), nodes.size, _c.ptr(ids), ids.size,
                                               ctypes.byref(n)))
         return nodes, ids
+
+    def read_wide_bvh(self):
+        """The 8-wide BVH on the host: nodes (n, 20) uint32 in the traversal
+        layout and the scene triangle id of each leaf-order position."""
+        n = ctypes.c_uint64()
+        lib = self.ctx._lib
+        self.ctx.check(lib.gyt_scene_read_wide_bvh(self.handle, None, 0, None, 0, ctypes.byref(n)))
+        words = np.zeros((n.value, 20), np.uint32)
+        ids = np.zeros(self.info()["triangles"], np.uint32)
+        self.ctx.check(lib.gyt_scene_read_wide_bvh(self.handle, _c.ptr(words), words.size, _c.ptr(ids), ids.size,
+                                                   ctypes.byref(n)))
+        return words, ids
 
     def close(self):
         if getattr(self, "handle", None):
@@ -367,14 +399,16 @@ class Scene:
 
 
 class VolPathTracing:
-    """Drop-in for VolPathTracing(spp, maxDepth, sampler, samplerEnum, false)
-    (integrator/VPT.h:12-19): volumetric path tracing through the scene's
-    homogeneous media (SceneDesc.media, tri_medium)."""
+    """Drop-in for VolPathTracing(spp, maxDepth, sampler, samplerEnum,
+    equalAngular = true) (integrator/VPT.h:12-19): volumetric path tracing
+    through the scene's homogeneous media (SceneDesc.media, tri_medium);
+    equal_angular selects equi-angular distance sampling about one light
+    point per bounce, the reference constructor's default."""
 
-    def __init__(self, spp, max_depth, sampler="sobol"):
+    def __init__(self, spp, max_depth, sampler="sobol", equal_angular=True):
         if sampler not in _c.SAMPLERS:
             raise ValueError("sampler must be one of %s" % sorted(_c.SAMPLERS))
-        self.params = RenderParams(int(spp), int(max_depth), 5, sampler)
+        self.params = RenderParams(int(spp), int(max_depth), 5, sampler, bool(equal_angular))
 
     def Render(self, scene, camera):
         ctx = scene.ctx

@@ -27,6 +27,7 @@ EXPORTS = ["gyt_context_create", "gyt_context_destroy", "gyt_last_error", "gyt_c
            "gyt_mesh_load_obj", "gyt_mesh_size", "gyt_mesh_read", "gyt_mesh_transform", "gyt_mesh_destroy",
            "gyt_render_device_noalloc", "gyt_context_set_batch_config", "gyt_context_get_batch_config",
            "gyt_render_batch_device", "gyt_render_batch", "gyt_batch_autotune", "gyt_scene_set_materials",
+           "gyt_scene_freeze_sampling", "gyt_scene_read_wide_bvh", "gyt_bsdf_table",
            "gyt_diff_forward", "gyt_diff_backward", "gyt_diff_backward_paths"]
 
 # BVH builders (GYT_BVH_BUILD_* in include/gyt.h)
@@ -39,6 +40,10 @@ KEEP_LIGHT_SAMPLING = 1
 # GytRenderParams.flags: HaltonSampler + HaltonEnum instead of Sobol' (GYT_SAMPLER_HALTON).
 SAMPLER_HALTON = 1
 SAMPLERS = {"sobol": 0, "halton": SAMPLER_HALTON}
+
+# GytRenderParams.flags of the volumetric entry points: equi-angular sampling
+# (VolPathTracing's equalAngular, GYT_VOLUME_EQUI_ANGULAR).
+VOLUME_EQUI_ANGULAR = 2
 
 # Path slots of the library's built-in scratch array (GYT_NOALLOC_MAX_PATHS in include/gyt.h).
 NOALLOC_MAX_PATHS = 32768
@@ -116,6 +121,7 @@ def load():
     L.gyt_context_set_bvh_width.argtypes = [P, I32]
     L.gyt_context_set_bvh_builder.argtypes = [P, I32]
     L.gyt_scene_read_bvh.argtypes = [P, P, U64, P, U64, ctypes.POINTER(U64)]
+    L.gyt_scene_read_wide_bvh.argtypes = [P, P, U64, P, U64, ctypes.POINTER(U64)]
     L.gyt_scene_create.argtypes = [P, ctypes.POINTER(GytSceneDesc), ctypes.POINTER(P)]
     L.gyt_scene_destroy.argtypes = [P]
     L.gyt_scene_destroy.restype = None
@@ -150,6 +156,8 @@ def load():
     L.gyt_mesh_destroy.restype = None
     L.gyt_camera_raster_to_world.argtypes = [ctypes.POINTER(GytCamera), P]
     L.gyt_scene_set_materials.argtypes = [P, P, P, U32]
+    L.gyt_scene_freeze_sampling.argtypes = [P, P]
+    L.gyt_bsdf_table.argtypes = [P, U64, P, P, P, P]
     L.gyt_diff_forward.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, P,
                                    ctypes.POINTER(GytRenderStats)]
     L.gyt_diff_backward.argtypes = [P, P, ctypes.POINTER(GytCamera), ctypes.POINTER(GytRenderParams), P, P, P, P, P,
@@ -187,7 +195,10 @@ def camera_struct(cam):
 
 
 def params_struct(p):
-    return GytRenderParams(p.spp, p.max_depth, p.rr_depth, SAMPLERS[getattr(p, "sampler", "sobol")])
+    flags = SAMPLERS[getattr(p, "sampler", "sobol")]
+    if getattr(p, "equi_angular", False):
+        flags |= VOLUME_EQUI_ANGULAR
+    return GytRenderParams(p.spp, p.max_depth, p.rr_depth, flags)
 
 
 def scene_struct(sd):

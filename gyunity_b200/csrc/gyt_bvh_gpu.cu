@@ -451,11 +451,12 @@ __device__ void leaf_sort(uint32_t* __restrict__ idx, uint32_t start, uint32_t c
 }
 
 // One thread per small task: the host builder's recursion on the task's
-// range (leaf at <= 2 triangles, or at <= kMaxLeaf when no split beats the
+// range (leaf at <= 2 triangles, or at <= max_leaf when no split beats the
 // leaf cost), depth-first, nodes from the task's reserved range.
 __global__ void k_small(uint32_t nsmall, const Task* __restrict__ small, uint32_t* __restrict__ idx,
                         const float4* __restrict__ blo, const float4* __restrict__ bhi,
-                        const float4* __restrict__ cen, float4* __restrict__ nodes, Counters* __restrict__ cnt) {
+                        const float4* __restrict__ cen, float4* __restrict__ nodes, Counters* __restrict__ cnt,
+                        uint32_t max_leaf) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsmall) return;
   struct Job {
@@ -474,7 +475,7 @@ __global__ void k_small(uint32_t nsmall, const Task* __restrict__ small, uint32_
   while (sp) {
     const Job j = stack[--sp];
     maxd = max(maxd, j.depth + 1);
-    if (j.count <= 2u) {
+    if (j.count <= min(2u, max_leaf)) {
       leaf_sort(idx, j.start, j.count);
       set_link(nodes, j.parent, j.slot, leaf_code(j.start, j.count));
       continue;
@@ -530,7 +531,7 @@ __global__ void k_small(uint32_t nsmall, const Task* __restrict__ small, uint32_
       }
     }
     const float an = area_rn(nlo, nhi);
-    if (j.count <= (uint32_t)kMaxLeaf && (bax < 0 || __fadd_rn(best, an) >= __fmul_rn(an, (float)j.count))) {
+    if (j.count <= max_leaf && (bax < 0 || __fadd_rn(best, an) >= __fmul_rn(an, (float)j.count))) {
       leaf_sort(idx, j.start, j.count);
       set_link(nodes, j.parent, j.slot, leaf_code(j.start, j.count));
       continue;
@@ -616,9 +617,11 @@ struct Bufs {
     }                                                                               \
   } while (0)
 
-int build_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t nt, GpuBvh* out, std::string* err) {
+int build_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t nt, GpuBvh* out, std::string* err,
+                  int max_leaf_in) {
   *out = GpuBvh{};
   if (nt == 0) return 0;
+  const uint32_t max_leaf = (uint32_t)std::min(kMaxLeaf, std::max(1, max_leaf_in));
   if ((uint64_t)nt >= (1ull << 28)) {
     *err = "build_bvh_gpu: more than 2^28 triangles";
     return 4;
@@ -669,7 +672,7 @@ int build_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t
   GYT_BCK(cudaMemcpyAsync(rh, root, sizeof(rh), cudaMemcpyDeviceToHost, st));
   GYT_BCK(cudaStreamSynchronize(st));
 
-  if (nt <= (uint32_t)kMaxLeaf) {
+  if (nt <= max_leaf) {
     // one leaf under the root and an inverted (never hit) box in the other
     // slot, as the host builder makes it
     float lo[3], hi[3], m = 0.f;
@@ -757,7 +760,8 @@ int build_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t
     nsmall = ch.nsmall;
     if (ntasks) k_cb_final<<<blocks(ntasks, kTB), kTB, 0, st>>>(ntasks, ta, next_cb);
   }
-  if (nsmall) k_small<<<blocks(nsmall, 64), 64, 0, st>>>(nsmall, small, idx_cur, blo, bhi, cen, nodes, cnt);
+  if (nsmall)
+    k_small<<<blocks(nsmall, 64), 64, 0, st>>>(nsmall, small, idx_cur, blo, bhi, cen, nodes, cnt, max_leaf);
   GYT_BCK(cudaGetLastError());
   Counters ch;
   GYT_BCK(cudaMemcpyAsync(&ch, cnt, sizeof(ch), cudaMemcpyDeviceToHost, st));
@@ -773,6 +777,317 @@ int build_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t
   out->n_slots = ch.nodes;
   out->n_inner = ch.inner;
   out->max_depth = ch.depth;
+  return 0;
+}
+
+
+// ------------------------------------------------ 8-wide collapse ---
+namespace {
+
+// A child of a binary node: its box (the padded box its parent stores) and
+// either the inner node it is or the leaf range it holds.
+struct WElem {
+  float lo[3], hi[3];
+  int node;  // binary inner node, or -1 for a leaf (or an empty slot)
+  uint32_t first, count;
+};
+
+__device__ WElem welem_child(const float4* __restrict__ nodes, int node, int slot) {
+  const float4* n = nodes + (size_t)node * 4;
+  const float4 a = n[slot], z = n[2];
+  const int4 l = *reinterpret_cast<const int4*>(n + 3);
+  WElem e;
+  e.lo[0] = a.x; e.hi[0] = a.y; e.lo[1] = a.z; e.hi[1] = a.w;
+  e.lo[2] = slot == 0 ? z.x : z.z;
+  e.hi[2] = slot == 0 ? z.y : z.w;
+  const int c = slot == 0 ? l.x : l.y;
+  if (c >= 0) {
+    e.node = c;
+    e.first = e.count = 0;
+  } else {
+    const uint32_t code = ~(uint32_t)c;
+    e.node = -1;
+    e.first = code >> 3;
+    e.count = (code & 7u) + 1u;
+  }
+  return e;
+}
+
+__device__ __forceinline__ void welem_empty(WElem& e) {
+  for (int a = 0; a < 3; ++a) {
+    e.lo[a] = FLT_MAX;
+    e.hi[a] = -FLT_MAX;
+  }
+  e.node = -1;
+  e.first = e.count = 0;
+}
+
+// One wide node from its seed (the binary node whose two children it starts
+// from), as build_wide_bvh_host makes it: ch receives the eight child slots
+// in slot order, boxes widened by the node's margin; words the node's 20
+// words with child_base and tri_base still to fill. Returns the number of
+// inner children; *ntris the triangles of its leaves. root: the binary root,
+// whose second child is dropped when it is the inverted box of a one-leaf
+// tree. Float and double operations as the host's (no contraction).
+__device__ uint32_t wide_node(const float4* __restrict__ bin, int seed, bool root, WElem ch[8], uint32_t words[20],
+                              uint32_t* ntris, bool* bad) {
+  // the greedy expansion: the inner child of largest surface area is replaced
+  // by its two children until there are eight
+  int n = 2;
+  ch[0] = welem_child(bin, seed, 0);
+  ch[1] = welem_child(bin, seed, 1);
+  if (root && ch[1].node < 0 && ch[1].count > 0 && !(ch[1].lo[0] <= ch[1].hi[0])) n = 1;
+  while (n < 8) {
+    int best = -1;
+    float area = -1.f;
+    for (int k = 0; k < n; ++k)
+      if (ch[k].node >= 0) {
+        const float ak = area_rn(ch[k].lo, ch[k].hi);
+        if (ak > area) {
+          area = ak;
+          best = k;
+        }
+      }
+    if (best < 0) break;
+    const int b = ch[best].node;
+    const WElem c = welem_child(bin, b, 1);
+    ch[best] = welem_child(bin, b, 0);
+    if (c.node >= 0 || c.count > 0) ch[n++] = c;
+  }
+  // slot order: the (child, free slot) pair whose child centre lies furthest
+  // along the slot's octant direction from the node centre goes first
+  float nlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, nhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int k = 0; k < n; ++k)
+    for (int a = 0; a < 3; ++a) {
+      nlo[a] = fminf(nlo[a], ch[k].lo[a]);
+      nhi[a] = fmaxf(nhi[a], ch[k].hi[a]);
+    }
+  float cc[3];
+  for (int a = 0; a < 3; ++a) cc[a] = __fmul_rn(0.5f, __fadd_rn(nlo[a], nhi[a]));
+  WElem sl[8];
+  for (int k = 0; k < 8; ++k) welem_empty(sl[k]);
+  uint32_t placed = 0u, used = 0u;
+  for (int round = 0; round < n; ++round) {
+    float best = -INFINITY;
+    int bc = -1, bs = -1;
+    for (int k = 0; k < n; ++k) {
+      if ((placed >> k) & 1u) continue;
+      float off[3];
+      for (int a = 0; a < 3; ++a) off[a] = __fsub_rn(__fmul_rn(0.5f, __fadd_rn(ch[k].lo[a], ch[k].hi[a])), cc[a]);
+      for (int q = 0; q < 8; ++q) {
+        if ((used >> q) & 1u) continue;
+        float score = 0.f;
+        for (int a = 0; a < 3; ++a) score = __fadd_rn(score, ((q >> a) & 1) ? off[a] : -off[a]);
+        if (score > best) {
+          best = score;
+          bc = k;
+          bs = q;
+        }
+      }
+    }
+    if (bc < 0) {  // non-finite centres: first unplaced child into the first free slot
+      for (bc = 0; (placed >> bc) & 1u; ++bc) {}
+      for (bs = 0; (used >> bs) & 1u; ++bs) {}
+    }
+    placed |= 1u << bc;
+    used |= 1u << bs;
+    sl[bs] = ch[bc];
+  }
+  // margin of the node's size so that FP32 rounding in the slab test can
+  // never cull a boundary hit (every slot, empty ones included, as the host)
+  float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int k = 0; k < 8; ++k)
+    for (int a = 0; a < 3; ++a) {
+      rlo[a] = fminf(rlo[a], sl[k].lo[a]);
+      rhi[a] = fmaxf(rhi[a], sl[k].hi[a]);
+    }
+  float mext = 0.f, mabs = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    mext = fmaxf(mext, __fsub_rn(rhi[a], rlo[a]));
+    mabs = fmaxf(mabs, fmaxf(fabsf(rlo[a]), fabsf(rhi[a])));
+  }
+  const float margin = __fadd_rn(__fadd_rn(__fmul_rn(1e-5f, mext), __fmul_rn(1e-6f, mabs)), 1e-30f);
+  for (int k = 0; k < 8; ++k)
+    for (int a = 0; a < 3; ++a) {
+      sl[k].lo[a] = __fsub_rn(sl[k].lo[a], margin);
+      sl[k].hi[a] = __fadd_rn(sl[k].hi[a], margin);
+    }
+  float blo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int k = 0; k < 8; ++k)
+    for (int a = 0; a < 3; ++a) {
+      blo[a] = fminf(blo[a], sl[k].lo[a]);
+      bhi[a] = fmaxf(bhi[a], sl[k].hi[a]);
+    }
+  // per axis the power-of-two scale: the smallest e (at least -100) with
+  // 255 2^e >= extent (1 + 1e-6), which is what the host's log2 estimate and
+  // its correction loop give
+  double p[3], sc[3];
+  int ex[3];
+  for (int a = 0; a < 3; ++a) {
+    p[a] = (double)blo[a];
+    const double ext = __dsub_rn((double)bhi[a], (double)blo[a]);
+    const double need = __dmul_rn(ext, 1.0 + 1e-6);
+    int e = ext > 0 ? (int)ceil(log2(__ddiv_rn(ext, 255.0))) : -100;
+    if (e < -100) e = -100;
+    while (ldexp(255.0, e) < need) ++e;
+    while (e > -100 && ldexp(255.0, e - 1) >= need) --e;
+    ex[a] = e;
+    sc[a] = ldexp(1.0, e);
+  }
+  for (int k = 0; k < 20; ++k) words[k] = 0u;
+  words[0] = __float_as_uint(blo[0]);
+  words[1] = __float_as_uint(blo[1]);
+  words[2] = __float_as_uint(blo[2]);
+  uint32_t imask = 0u, inner = 0u, tris = 0u;
+  for (int k = 0; k < 8; ++k) {
+    const WElem& e = sl[k];
+    if (e.node < 0 && e.count == 0) continue;  // empty slot
+    for (int a = 0; a < 3; ++a) {
+      const double lo = floor(__dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)e.lo[a], p[a]), sc[a]), 1.0 - 1e-6), 1e-6));
+      const double hi = ceil(__dadd_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)e.hi[a], p[a]), sc[a]), 1.0 + 1e-6), 1e-6));
+      const uint32_t ql = (uint32_t)fmin(255.0, fmax(0.0, lo)), qh = (uint32_t)fmin(255.0, fmax(0.0, hi));
+      words[8 + 4 * a + (k >> 2)] |= ql << (8 * (k & 3));
+      words[10 + 4 * a + (k >> 2)] |= qh << (8 * (k & 3));
+    }
+    if (e.node >= 0) {
+      imask |= 1u << k;
+      ++inner;
+    } else {
+      if (e.count > 3 || tris + e.count > 32) *bad = true;
+      const uint32_t meta = (e.count << 5) | tris;
+      words[6 + (k >> 2)] |= (meta & 0xffu) << (8 * (k & 3));
+      tris += e.count;
+    }
+  }
+  words[3] = (uint32_t)(uint8_t)(int8_t)ex[0] | ((uint32_t)(uint8_t)(int8_t)ex[1] << 8) |
+             ((uint32_t)(uint8_t)(int8_t)ex[2] << 16) | (imask << 24);
+  for (int k = 0; k < 8; ++k) ch[k] = sl[k];
+  *ntris = tris;
+  return inner;
+}
+
+// Pass 1 of a level: inner children and leaf triangles of every wide node,
+// packed (inner << 32 | triangles) for one prefix sum.
+__global__ void k_wide_count(const float4* __restrict__ bin, const int* __restrict__ seeds, uint32_t n, bool root,
+                             unsigned long long* __restrict__ counts, uint32_t* __restrict__ bad) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n) return;
+  WElem ch[8];
+  uint32_t words[20], tris;
+  bool b = false;
+  const uint32_t inner = wide_node(bin, seeds[w], root, ch, words, &tris, &b);
+  counts[w] = ((unsigned long long)inner << 32) | tris;
+  if (b) atomicOr(bad, 1u);
+}
+
+// Pass 2: the node words, the next level's seeds (inner children in slot
+// order from child_base) and the leaves' triangles (from tri_base). first_node
+// is the level's first node index, next_first the next level's.
+__global__ void k_wide_write(const float4* __restrict__ bin, const uint32_t* __restrict__ bin_order,
+                             const int* __restrict__ seeds, uint32_t n, bool root,
+                             const unsigned long long* __restrict__ excl, uint32_t first_node, uint32_t next_first,
+                             uint32_t tri_first, uint4* __restrict__ out, int* __restrict__ next_seeds,
+                             uint32_t* __restrict__ order) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n) return;
+  WElem ch[8];
+  uint32_t words[20], tris;
+  bool b = false;
+  wide_node(bin, seeds[w], root, ch, words, &tris, &b);
+  const uint32_t ibase = (uint32_t)(excl[w] >> 32), tbase = tri_first + (uint32_t)(excl[w] & 0xffffffffull);
+  words[4] = next_first + ibase;
+  words[5] = tbase;
+  uint32_t rank = 0, t = 0;
+  for (int k = 0; k < 8; ++k) {
+    const WElem& e = ch[k];
+    if (e.node >= 0) {
+      next_seeds[ibase + rank++] = e.node;
+    } else {
+      for (uint32_t j = 0; j < e.count; ++j) order[tbase + t + j] = bin_order[e.first + j];
+      t += e.count;
+    }
+  }
+  uint4* o = out + 5 * (size_t)(first_node + w);
+  for (int q = 0; q < 5; ++q) o[q] = make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+}
+
+}  // namespace
+
+int build_wide_bvh_gpu(cudaStream_t st, const float* dV, const uint32_t* dI, uint32_t nt, GpuWideBvh* out,
+                       std::string* err) {
+  *out = GpuWideBvh{};
+  if (nt == 0) return 0;
+  GpuBvh g;
+  int rc = build_bvh_gpu(st, dV, dI, nt, &g, err, 3);
+  if (rc) return rc;
+  Bufs B;
+  B.v.push_back(g.nodes);
+  B.v.push_back(g.order);
+  // every wide node has its own binary inner node as seed
+  const uint32_t cap = std::max<uint32_t>(g.n_inner, 1);
+  uint4* wn;
+  uint32_t *order, *bad;
+  int *seeds0, *seeds1;
+  unsigned long long *counts, *excl;
+  GYT_BCK(B.get(&wn, 5 * (size_t)cap));
+  GYT_BCK(B.get(&order, nt));
+  GYT_BCK(B.get(&seeds0, cap));
+  GYT_BCK(B.get(&seeds1, cap));
+  GYT_BCK(B.get(&counts, (size_t)cap + 1));
+  GYT_BCK(B.get(&excl, (size_t)cap + 1));
+  GYT_BCK(B.get(&bad, 1));
+  size_t scan_bytes = 0;
+  GYT_BCK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, excl, (int)cap + 1, st));
+  uint8_t* scan_tmp;
+  GYT_BCK(B.get(&scan_tmp, scan_bytes));
+  GYT_BCK(cudaMemsetAsync(seeds0, 0, sizeof(int), st));  // the binary root
+  GYT_BCK(cudaMemsetAsync(bad, 0, sizeof(uint32_t), st));
+  uint32_t level_first = 0, level_n = 1, tri_first = 0, levels = 0;
+  int *cur = seeds0, *nxt = seeds1;
+  while (level_n > 0) {
+    if (++levels > 64 || level_first + level_n > cap) {
+      *err = "build_wide_bvh_gpu: node capacity or depth exceeded";
+      return 4;
+    }
+    const bool root = level_first == 0;
+    k_wide_count<<<blocks(level_n, 128), 128, 0, st>>>(g.nodes, cur, level_n, root, counts, bad);
+    GYT_BCK(cudaMemsetAsync(counts + level_n, 0, sizeof(unsigned long long), st));
+    GYT_BCK(cudaGetLastError());
+    GYT_BCK(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, excl, (int)level_n + 1, st));
+    unsigned long long tot;
+    GYT_BCK(cudaMemcpyAsync(&tot, excl + level_n, sizeof(tot), cudaMemcpyDeviceToHost, st));
+    GYT_BCK(cudaStreamSynchronize(st));
+    const uint32_t next_n = (uint32_t)(tot >> 32), ntris = (uint32_t)(tot & 0xffffffffull);
+    if ((uint64_t)level_first + level_n + next_n > cap || (uint64_t)tri_first + ntris > nt) {
+      *err = "build_wide_bvh_gpu: node or triangle capacity exceeded";
+      return 4;
+    }
+    k_wide_write<<<blocks(level_n, 128), 128, 0, st>>>(g.nodes, g.order, cur, level_n, root, excl, level_first,
+                                                        level_first + level_n, tri_first, wn, nxt, order);
+    GYT_BCK(cudaGetLastError());
+    level_first += level_n;
+    tri_first += ntris;
+    level_n = next_n;
+    std::swap(cur, nxt);
+  }
+  uint32_t hbad = 0;
+  GYT_BCK(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, st));
+  GYT_BCK(cudaStreamSynchronize(st));
+  if (hbad || tri_first != nt) {
+    *err = "build_wide_bvh_gpu: a leaf does not fit the 8-wide node layout";
+    return 4;
+  }
+  // the exact node count: move the nodes into an allocation of that size
+  uint4* exact;
+  GYT_BCK(B.get(&exact, 5 * (size_t)level_first));
+  GYT_BCK(cudaMemcpyAsync(exact, wn, 5 * (size_t)level_first * sizeof(uint4), cudaMemcpyDeviceToDevice, st));
+  GYT_BCK(cudaStreamSynchronize(st));
+  B.release(exact);
+  B.release(order);
+  out->nodes = exact;
+  out->order = order;
+  out->n_nodes = level_first;
+  out->max_depth = levels;
   return 0;
 }
 

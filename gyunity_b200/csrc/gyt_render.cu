@@ -67,6 +67,9 @@ struct DevScene {
   EnvDev env;
   const float4* media;        // 2 float4 per medium: (sigma_a, g), (sigma_s, 0); or null
   int n_media;
+  // BSDF sampling parameters (16 floats per material) while sampling is
+  // frozen by gyt_scene_freeze_sampling; null otherwise
+  const float* sparams;
 };
 
 // Light record (kLightRec float4): (p0, Le.r) (p1, Le.g) (p2, Le.b)
@@ -137,7 +140,27 @@ constexpr uint32_t kAlive = 1u << 31;
 constexpr uint32_t kPixMask = 0x0fffffffu;
 constexpr int kWStack = 48;  // node groups: one per level of the wide BVH
 constexpr int kBStack = 64;  // binary BVH: one entry per level
-constexpr int kBlock = 256;
+constexpr int kBlock = 256;  // every kernel that traverses the BVH runs blocks of kBlock threads
+
+// Traversal stacks live in a per-warp slab of shared memory: each lane keeps
+// its top kBStackSh binary entries (4 bytes) or kWStackSh wide node groups
+// (8 bytes) there, deeper entries in a local-memory tail that only deep
+// traversals reach. The slab is [warp][entry][lane]: entry k of lane l sits
+// at word 32 k + l of the binary view (bank l) or at element 32 k + l of the
+// 8-byte view, so a warp's pushes and pops never conflict in the binary view
+// and take the two phases any 8-byte warp access takes in the wide one,
+// whatever depth each lane is at. 64 bytes per lane: 16 KB per block of 256.
+constexpr int kBStackSh = 16;
+constexpr int kWStackSh = 8;
+constexpr int kSlabWarps = kBlock / 32;
+__shared__ uint2 g_trav_slab[kSlabWarps * kWStackSh * 32];
+
+// Entry k of this lane's stack in the slab (binary and 8-byte views).
+GYT_D uint32_t& slab_b(int k) {
+  return reinterpret_cast<uint32_t*>(g_trav_slab)[(threadIdx.x >> 5) * (kBStackSh * 32) + k * 32 + (threadIdx.x & 31)];
+}
+GYT_D uint2& slab_w(int k) { return g_trav_slab[(threadIdx.x >> 5) * (kWStackSh * 32) + k * 32 + (threadIdx.x & 31)]; }
+static_assert(kBStackSh * 4 == kWStackSh * 8, "both views cover the same slab");
 // Traversal kernels are latency-bound (dependent node fetches): a register
 // cap that fits four blocks per SM (a few spilled values) beats fewer blocks
 // for the closest-hit and the shadow/MIS kernels of both widths (measured on
@@ -221,9 +244,18 @@ GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count
 // step. The stack holds one far child per level.
 struct BinaryTraversal {
   int node, sp;
-  int stack[kBStack];
+  int tail[kBStack - kBStackSh];  // entries past the lane's part of the shared slab
 
   GYT_D void init(const RayConst&) { node = 0; sp = 0; }
+  GYT_D void push(int v) {
+    if (sp < kBStackSh) slab_b(sp) = (uint32_t)v;
+    else tail[sp - kBStackSh] = v;
+    ++sp;
+  }
+  GYT_D int pop() {
+    --sp;
+    return sp < kBStackSh ? (int)slab_b(sp) : tail[sp - kBStackSh];
+  }
 
   // Returns true when the traversal is finished (or, for ANY, on a hit).
   template <bool ANY, bool COUNT, class S>
@@ -249,13 +281,13 @@ struct BinaryTraversal {
       bool h0 = lo0 <= hi0, h1 = lo1 <= hi1;
       if (!h0 && !h1) {
         if (sp == 0) return true;
-        node = stack[--sp];
+        node = pop();
         continue;
       }
       if (h0 && h1) {
         int nearc = n3.x, farc = n3.y;
         if (lo1 < lo0) { nearc = n3.y; farc = n3.x; }
-        stack[sp++] = farc;
+        push(farc);
         node = nearc;
       } else {
         node = h0 ? n3.x : n3.y;
@@ -264,7 +296,7 @@ struct BinaryTraversal {
     uint32_t code = ~(uint32_t)node;
     if (test_tris<ANY, COUNT>(s, rc.wr, code >> 3, (code & 7u) + 1u, tmax, b1, b2, prim, cnt)) return true;
     if (sp == 0) return true;
-    node = stack[--sp];
+    node = pop();
     return false;
   }
 };
@@ -288,7 +320,17 @@ struct WideTraversal {
   uint32_t tri_base, tmask;  // the last node's hit leaf triangles (bit k = tri_base + k)
   uint32_t oct;
   int sp;
-  uint2 stack[kWStack];
+  uint2 tail[kWStack - kWStackSh];  // node groups past the lane's part of the shared slab
+
+  GYT_D void push(uint2 v) {
+    if (sp < kWStackSh) slab_w(sp) = v;
+    else tail[sp - kWStackSh] = v;
+    ++sp;
+  }
+  GYT_D uint2 pop() {
+    --sp;
+    return sp < kWStackSh ? slab_w(sp) : tail[sp - kWStackSh];
+  }
 
   GYT_D void init(const RayConst& rc) {
     grp = make_uint2(0u, 1u);  // the root as the single pending child of a virtual group
@@ -308,14 +350,14 @@ struct WideTraversal {
     }
     if ((grp.y & 0xffu) == 0u) {
       if (sp == 0) return true;
-      grp = stack[--sp];
+      grp = pop();
     }
     const uint32_t p = __ffs(grp.y & 0xffu) - 1;
     const uint32_t slot = p ^ oct;
     // the virtual root group holds node 0 with an empty inner-slot mask
     const uint32_t node = grp.x + __popc((grp.y >> 8) & ((1u << slot) - 1u));
     grp.y &= ~(1u << p);
-    if (grp.y & 0xffu) stack[sp++] = grp;
+    if (grp.y & 0xffu) push(grp);
     if (COUNT) cnt->nodes++;
     const uint4* n = s.wnodes + 5 * (size_t)node;
     const uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
@@ -657,7 +699,13 @@ GYT_D void grad_emitter(const GradOut& G, const DevScene& s, int li, float3 Cd) 
 // DEFER: the MIS ray's contribution is added by k_finish (k_connect traces
 // the shadow and MIS rays in one launch and leaves it in q.madd), not by the
 // MIS kernel.
-template <bool ADJ, bool DEFER = false>
+//
+// FROZEN: BSDF sampling and the BSDF pdfs (sample pdfs and MIS weights) use
+// the scene's frozen sampling parameters s.sparams, the BSDF values f of the
+// GGX lobes the current parameters. With roulette off, the radiance is then a
+// smooth function of the GGX alpha whose central differences equal the
+// detached-sampling derivative of the adjoint pass.
+template <bool ADJ, bool DEFER = false, bool FROZEN = false>
 GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
                       SamplerTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   float4 h4 = q.hit[i];
@@ -710,6 +758,20 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     Bsdf bsdf;
     bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
     bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+    // the BSDF that samples directions and gives their pdfs (bsdf itself
+    // unless FROZEN)
+    Bsdf fz;
+    if (FROZEN) {
+      fz = bsdf;
+      fz.lobe = load_lobe(s.sparams, s.mtypes, mat);
+    }
+    const Bsdf& sbsdf = FROZEN ? fz : bsdf;
+    // a sample's BSDF value at the current parameters (FROZEN, GGX lobes)
+    auto refit = [&](float3 f, float3 wi_) {
+      if (FROZEN && (bsdf.lobe.type == 3 || bsdf.lobe.type == 4) && !is_zero(f))
+        return bsdf.lobe.eval(bsdf.local(h.wo), bsdf.local(wi_));
+      return f;
+    };
     // the ten dimensions this bounce can use: six for direct lighting (PT.cpp:38
     // arguments in GCC's right-to-left order: v.z v.y v.x u.y u.x uLight), three
     // for the BSDF sample (PT.cpp:47, again z y x) and one for roulette
@@ -765,7 +827,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
           labs = wi;
         }
         if (pdf > 0.f && !is_zero(Li)) {
-          float spdf = bsdf.pdf(h.wo, wi);
+          float spdf = sbsdf.pdf(h.wo, wi);
           float3 f = bsdf.eval(h.wo, wi);
           float cosT = fabsf(dot(h.n, wi));
           if (!is_zero(f)) {
@@ -790,7 +852,8 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
         // BSDF-sampled half of the MIS estimate (Integrator.cpp:66-101)
         float3 wi2;
         float pdf2;
-        float3 f2 = bsdf.sample(h.wo, &wi2, &pdf2, vx, vy, vz);
+        float3 f2 = sbsdf.sample(h.wo, &wi2, &pdf2, vx, vy, vz);
+        if (FROZEN) f2 = refit(f2, wi2);
         float cos2 = fabsf(dot(h.n, wi2));
         if (pdf2 != 0.f && !is_zero(f2)) {
           float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
@@ -818,7 +881,8 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     rng.cursor += 3;
     float3 wi;
     float pdf;
-    float3 f = bsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
+    float3 f = sbsdf.sample(h.wo, &wi, &pdf, rx, ry, rz);
+    if (FROZEN) f = refit(f, wi);
     if (!(is_zero(f) || pdf == 0.f)) {
       float3 est = f * fabsf(dot(h.n, wi)) / pdf;
       delta = bsdf.lobe.delta();
@@ -879,11 +943,12 @@ GYT_D uint32_t coherent_slot(uint32_t i, uint32_t key) {
   return order[threadIdx.x];
 }
 
+template <bool FROZEN>
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm)
     k_shade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q, SamplerTables tab, DebugOut dbg) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t j = coherent_slot(i, i < n ? shade_class(s, q, i) : kClassIdle);
-  if (j != ~0u) shade_path<false, true>(cur, j, s, prm, q, tab, dbg);
+  if (j != ~0u) shade_path<false, true, FROZEN>(cur, j, s, prm, q, tab, dbg);
 }
 
 // MIS-ray result of one queue entry (every MIS kernel). DEFER: the
@@ -1502,8 +1567,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_light_trace(DevScene s, LtCam c, 
        t += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long g = ids ? ids[t] : t;
     float* out = rec ? rec + 6ull * prm.max_depth * t : nullptr;
-    if (out)
-      for (uint32_t k = 0; k < prm.max_depth; ++k) out[6 * k] = -1.f;
+    if (out)  // no vertex: (-1, 0, 0, 0, 0, 0)
+      for (uint32_t k = 0; k < prm.max_depth; ++k)
+        for (int f = 0; f < 6; ++f) out[6 * k + f] = f == 0 ? -1.f : 0.f;
     auto emit = [&](uint32_t k, bool on, int X, int Y, float3 L) {
       L = ((L * c.fx) * c.fy) / c.ftotal;
       if (out) {
@@ -1915,6 +1981,47 @@ __device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, co
   return (L1 * w1 + L2 * w2) / lsel;
 }
 
+// The light point of an equi-angular bounce: AreaLight::SampleOnePoint ->
+// Triangle::Sample (light/AreaLight.h:54-58, shape/Triangle.cpp:141-158) for
+// the light drawn with u = (ux, uy): position, interpolated normal (not
+// normalised), position error; the area pdf is 1 / area.
+struct LightPoint {
+  float3 pos, n, err;
+};
+
+GYT_D LightPoint light_point(const LightTri& l, float ux, float uy) {
+  const float su0 = sqrtf(ux);
+  const float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
+  LightPoint q;
+  q.pos = l.p0 * bb0 + l.p1 * bb1 + l.p2 * bb2;
+  q.n = l.n0 * bb0 + l.n1 * bb1 + l.n2 * bb2;
+  q.err = (vabs(l.p0 * bb0) + vabs(l.p1 * bb1) + vabs(l.p2 * bb2)) * gammaf(6);
+  return q;
+}
+
+// VolPathTracing::ConnectToLight (integrator/VPT.cpp:108-146) from the medium
+// point p to the bounce's light point of light li: the phase function toward
+// the light, the transmittance of the segment (VisibilityTester::Tr), the
+// cosine at the light and the inverse squared distance, over the area pdf.
+// Only the light-sampling term: the reference computes an MIS weight but
+// returns L1 unweighted. Called (not inlined), like vpt_direct.
+template <int W>
+__device__ __noinline__ float3 vpt_connect(const DevScene& s, const VPoint& p, float g, int li, float ux, float uy) {
+  const LightTri l = load_light(s, li);
+  const LightPoint q = light_point(l, ux, uy);
+  const float3 dir = p.pos - q.pos;
+  const float3 wi = -norm(dir);
+  float cos_t = 1.f;
+  if (!is_zero(q.n)) {
+    cos_t = dot(norm(dir), q.n);
+    if (cos_t < 0.f) return mk(0.f, 0.f, 0.f);
+  }
+  const float ph = phase_hg(dot(p.wo, wi), g);
+  const float3 tr = vpt_tr<W>(s, p, q.pos, q.err, l.face);
+  const float pdf = 1.f / l.area;
+  return l.Le * ph * tr * cos_t / dot(dir, dir) / pdf;
+}
+
 // One camera sample per thread (grid-stride over the render's samples, or the
 // listed (x, y, s) of xys); film as gyt_render_device's, L_out/cursor_out for
 // parity tests. Capped at four blocks per SM (64 registers, a few spills) and
@@ -1922,7 +2029,14 @@ __device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, co
 // instruction fetch, not by memory. On the Cornell box in fog (binary BVH):
 // 69 Mpaths/s with a whole path per loop pass, 89 with regeneration, 112 with
 // four blocks per SM in a single wave.
-template <int W>
+//
+// EQUI: VolPathTracing with equi-angular sampling (its constructor's default,
+// integrator/VPT.h:13-15): every bounce draws one light and one point on it
+// (VPT.cpp:22-27); a ray through a medium samples its scattering distance
+// equi-angularly about that point (HomogeneousMedium::EquiAngularSampling,
+// volume/Homogeneous.cpp:38-64), and a medium point gathers light only by the
+// connection to that point (ConnectToLight, VPT.cpp:108-146).
+template <int W, bool EQUI>
 __global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
                                                 unsigned long long n, const uint32_t* __restrict__ xys,
                                                 double* __restrict__ film, float* __restrict__ L_out,
@@ -1980,7 +2094,40 @@ __global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params p
       bool scattered = false;
       float3 mpos = o;
       float g = 0.f;
-      if (medium >= 0) {
+      int eli = 0;  // EQUI: the bounce's light, its selection probability and point sample
+      float elsel = 0.f, eux = 0.f, euy = 0.f;
+      if (EQUI) {
+        // VPT.cpp:23-24: Scene::SampleOneLight, then SampleOnePoint's
+        // Vec2(rand(), rand()) in right-to-left order
+        const float ul = rng.next(tab, prm.sampler);
+        euy = rng.next(tab, prm.sampler);
+        eux = rng.next(tab, prm.sampler);
+        eli = sample_light(s, ul, &elsel);
+        if (medium >= 0) {
+          // HomogeneousMedium::EquiAngularSampling (volume/Homogeneous.cpp:38-64):
+          // t in [0, 3] along the ray with density proportional to the inverse
+          // squared distance to the light point
+          const MediumDev md = load_medium(s, medium);
+          g = md.g;
+          const float u = rng.next(tab, prm.sampler);
+          const float3 lpos = light_point(load_light(s, eli), eux, euy).pos;
+          const float dl = dot(lpos - o, d);
+          const float D = length(o + d * dl - lpos);
+          const float ta = atan2f(0.f - dl, D), tb = atan2f(3.f - dl, D);
+          const float tau = D * tanf((1.f - u) * ta + u * tb);
+          const float tt = dl + tau;
+          scattered = tt < tmax;
+          if (scattered) {
+            const float3 tr = mk(expf(-md.st.x * tt), expf(-md.st.y * tt), expf(-md.st.z * tt));
+            const float pdf = D / ((tb - ta) * (D * D + tau * tau));
+            tp = tp * (tr * md.ss / pdf);
+            mpos = o + d * tt;
+          } else {
+            const float pdf = 1.f - (atan2f(fminf(3.f, tmax) - dl, D) - ta) / (tb - ta);
+            tp = tp * (medium_tr(md, tmax, length(d)) / pdf);
+          }
+        }
+      } else if (medium >= 0) {
         // HomogeneousMedium::Sample (volume/Homogeneous.cpp:12-30)
         const MediumDev md = load_medium(s, medium);
         g = md.g;
@@ -2042,7 +2189,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params p
           }
         }
       }
-      if (gather) {
+      if (EQUI && gather && scattered) {
+        // VPT.cpp:36: the connection to the bounce's light point
+        if (elsel > 0.f) L = L + tp * vpt_connect<W>(s, p, g, eli, eux, euy) / elsel;
+      } else if (gather) {
         // one call site for surface and medium points
         const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
         const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
@@ -2159,6 +2309,27 @@ __global__ void k_intersect(DevScene s, uint64_t n, const float* __restrict__ ra
     b1out[i] = p >= 0 && p < s.n_tris ? b1 : 0.f;
     b2out[i] = p >= 0 && p < s.n_tris ? b2 : 0.f;
   }
+}
+
+// One BxDF per case in its local frame, the lobes the shading kernels use:
+// sample (u), evaluate and pdf toward a second direction (we). vec holds wo,
+// u, we (9 floats per case); out 11 floats: f, wi, pdf of the sample, f and
+// pdf toward we.
+__global__ void k_bsdf_table(uint64_t n, const float* __restrict__ params, const uint32_t* __restrict__ types,
+                             const float* __restrict__ vec, float* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Lobe l = load_lobe(params, types, (uint32_t)i);
+  const float* v = vec + 9 * i;
+  const float3 wo = mk(v[0], v[1], v[2]), we = mk(v[6], v[7], v[8]);
+  float3 wi = mk(0.f, 0.f, 0.f);
+  float pdf = 0.f;
+  const float3 f = l.sample(wo, &wi, &pdf, v[3], v[4], v[5]);
+  const float3 fe = l.eval(wo, we);
+  const float pe = l.pdf(wo, we);
+  float* o = out + 11 * i;
+  o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = wi.x; o[4] = wi.y; o[5] = wi.z; o[6] = pdf;
+  o[7] = fe.x; o[8] = fe.y; o[9] = fe.z; o[10] = pe;
 }
 
 __global__ void k_sobol(const uint32_t* __restrict__ mat, uint64_t n, const uint32_t* dims, const uint64_t* idx,
@@ -2304,6 +2475,7 @@ struct gyt_scene {
   std::vector<float4> ltab;       // host copy of the light records
   std::vector<float> light_area;  // per area light
   std::vector<float> power;       // light powers (area lights, then the environment)
+  float* sparams_buf = nullptr;   // device copy of the frozen sampling parameters (gyt_scene_freeze_sampling)
 };
 
 namespace {
@@ -2507,13 +2679,13 @@ float light_distribution(const std::vector<float>& power, std::vector<float>* cd
 // AreaLight::Power (light/AreaLight.h:45-48)
 float area_light_power(const float* em, float area) { return lum(mk(em[0], em[1], em[2]) * area * kPi); }
 
-int32_t check_params(gyt_context* ctx, const GytRenderParams* p) {
+int32_t check_params(gyt_context* ctx, const GytRenderParams* p, uint32_t extra_flags = 0) {
   if (!p) return fail(ctx, GYT_ERR_INVALID, "params: null");
   if (p->spp == 0) return fail(ctx, GYT_ERR_INVALID, "params: spp must be > 0");
   if (p->max_depth == 0 || p->max_depth > 100)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "params: max_depth must be in [1, 100] (Sobol' has 1024 dimensions)");
   if (p->rr_depth > 255) return fail(ctx, GYT_ERR_INVALID, "params: rr_depth too large");
-  if (p->flags & ~GYT_SAMPLER_HALTON) return fail(ctx, GYT_ERR_INVALID, "params: unknown flags");
+  if (p->flags & ~(GYT_SAMPLER_HALTON | extra_flags)) return fail(ctx, GYT_ERR_INVALID, "params: unknown flags");
   return GYT_OK;
 }
 
@@ -2581,6 +2753,7 @@ int32_t run_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCam
   if (st) return st;
   if (scene->dev.has_env)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "light_tracing: environment lights are not sampled (area lights only)");
+  if (scene->dev.sparams) return fail(ctx, GYT_ERR_UNSUPPORTED, "light_tracing: the scene's BSDF sampling is frozen");
   Cam cam;
   st = make_cam(ctx, camera, params, &cam);  // validates the film (and the sampler's enumeration limits)
   if (st) return st;
@@ -2615,10 +2788,13 @@ int32_t run_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCam
 int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
                    uint64_t n, const uint32_t* xys, double* d_film, float* L_out, uint32_t* cursor_out,
                    GytRenderStats* stats) {
-  int32_t st = check_params(ctx, params);
+  int32_t st = check_params(ctx, params, GYT_VOLUME_EQUI_ANGULAR);
   if (st) return st;
   if (scene->dev.has_env)
     return fail(ctx, GYT_ERR_UNSUPPORTED, "render_volume: environment lights are not supported with media");
+  if ((params->flags & GYT_VOLUME_EQUI_ANGULAR) && scene->dev.n_area == 0)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "render_volume: equi-angular sampling needs an area light");
+  if (scene->dev.sparams) return fail(ctx, GYT_ERR_UNSUPPORTED, "render_volume: the scene's BSDF sampling is frozen");
   Cam cam;
   st = make_cam(ctx, camera, params, &cam);
   if (st) return st;
@@ -2632,10 +2808,17 @@ int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
   const uint32_t grid = (uint32_t)std::min<unsigned long long>((count + kBlock - 1) / kBlock,
                                                                 (unsigned long long)std::max(1, ctx->sms) * 4);
   GYT_CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-  if (scene->dev.wnodes)
-    k_vpt<8><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
-  else
-    k_vpt<2><<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
+  const bool equi = (params->flags & GYT_VOLUME_EQUI_ANGULAR) != 0;
+  auto launch = [&](auto kernel) {
+    kernel<<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
+  };
+  if (scene->dev.wnodes) {
+    if (equi) launch(k_vpt<8, true>);
+    else launch(k_vpt<8, false>);
+  } else {
+    if (equi) launch(k_vpt<2, true>);
+    else launch(k_vpt<2, false>);
+  }
   GYT_CK(ctx, cudaGetLastError());
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
@@ -2708,6 +2891,15 @@ int32_t ensure_adj(gyt_context* ctx) {
   return GYT_OK;
 }
 
+// Wavefront iterations that a render of `total` paths of at most max_depth
+// bounces can take with `pool` paths in flight: a path holds a slot for at
+// most max_depth + 1 iterations and a full pool finishes at least
+// pool / (max_depth + 1) paths per iteration; doubled, with room for the
+// tail. The loops stop with GYT_ERR_WATCHDOG past it.
+unsigned long long wavefront_bound(unsigned long long total, uint32_t max_depth, uint32_t pool) {
+  return 2ull * (total / std::max(1u, pool) + 2) * ((unsigned long long)max_depth + 2) + 64;
+}
+
 // The wavefront loop shared by full renders and explicit path lists.
 int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, const GytRenderParams* p,
                   unsigned long long total, const uint32_t* d_list, double* d_film, DebugOut dbg,
@@ -2753,7 +2945,8 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
       else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(P, active, D, q.hit, q.counts + 2, nullptr);
     }
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[2], s));
-    k_shade<<<grid_for(active), kBlock, 0, s>>>(P, active, D, prm, q, tab, dbg);
+    if (D.sparams) k_shade<true><<<grid_for(active), kBlock, 0, s>>>(P, active, D, prm, q, tab, dbg);
+    else k_shade<false><<<grid_for(active), kBlock, 0, s>>>(P, active, D, prm, q, tab, dbg);
     if (prof) GYT_CK(ctx, cudaEventRecord(ctx->kev[3], s));
     // shadow and MIS rays in one launch (profile slot 3; slot 4 stays empty)
     if (W == 8) {
@@ -2787,7 +2980,8 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
     rays += active;
     active = hcounts[5];
     cur ^= 1;
-    if (++iters > 100000) return fail(ctx, GYT_ERR_WATCHDOG, "render: wavefront iteration cap reached");
+    if (++iters > wavefront_bound(total, p->max_depth, ctx->capacity))
+      return fail(ctx, GYT_ERR_WATCHDOG, "render: wavefront iteration cap reached");
   }
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
@@ -2816,6 +3010,9 @@ int32_t run_paths(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, cons
 int32_t run_adjoint(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, const GytRenderParams* p,
                     unsigned long long total, const uint32_t* d_list, const AdjIn& in, GradOut G,
                     GytRenderStats* stats) {
+  if (scene->dev.sparams)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "adjoint: the scene's BSDF sampling is frozen (the replay samples as "
+                                          "the primal did only without it)");
   int32_t st = ensure_pool(ctx);
   if (st) return st;
   st = ensure_adj(ctx);
@@ -2858,7 +3055,8 @@ int32_t run_adjoint(gyt_context* ctx, const gyt_scene* scene, const Cam& cam, co
     GYT_CK(ctx, cudaStreamSynchronize(s));
     active = ctx->h_counter[5];
     cur ^= 1;
-    if (++iters > 100000) return fail(ctx, GYT_ERR_WATCHDOG, "adjoint: wavefront iteration cap reached");
+    if (++iters > wavefront_bound(total, p->max_depth, ctx->capacity))
+      return fail(ctx, GYT_ERR_WATCHDOG, "adjoint: wavefront iteration cap reached");
   }
   GYT_CK(ctx, cudaEventRecord(ctx->ev1, s));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
@@ -3153,11 +3351,11 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   const int nl = (int)power.size();
   std::vector<float> cdf;
   const float fint = light_distribution(power, &cdf);
-  // acceleration structure: binary (two child boxes per 64-byte node, built
-  // on the device or the host) or 8-wide with quantized child boxes (80-byte
-  // nodes, host), per context setting
+  // acceleration structure: binary (two child boxes per 64-byte node) or
+  // 8-wide with quantized child boxes (80-byte nodes), built on the device
+  // or the host, per context setting
   const bool use_wide = ctx->bvh_width == 8;
-  const bool use_dev = !use_wide && ctx->bvh_builder == GYT_BVH_BUILD_DEVICE && d->n_triangles > 0;
+  const bool use_dev = ctx->bvh_builder == GYT_BVH_BUILD_DEVICE && d->n_triangles > 0;
   auto* sc = new gyt_scene();
   sc->ctx = ctx;
   sc->device = ctx->device;
@@ -3208,13 +3406,25 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     if (e == cudaSuccess && n_area) e = tup(&dLightLeaf, (const int*)nullptr, light_tris.size());
     if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
     GpuBvh g;
+    GpuWideBvh gw;
     std::string berr;
-    const int rc = build_bvh_gpu(ctx->stream, dV, dI, nt, &g, &berr);
+    const int rc = use_wide ? build_wide_bvh_gpu(ctx->stream, dV, dI, nt, &gw, &berr)
+                            : build_bvh_gpu(ctx->stream, dV, dI, nt, &g, &berr);
     if (rc) return bail(rc, "scene_create: " + berr);
-    sc->allocs.push_back(g.nodes);  // the scene owns the nodes
-    tmp.push_back(g.order);
-    sc->bytes += (uint64_t)g.n_slots * 64;
-    if (g.max_depth >= (uint32_t)kBStack) return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+    if (use_wide) {
+      sc->allocs.push_back(gw.nodes);  // the scene owns the nodes
+      tmp.push_back(gw.order);
+      g.order = gw.order;
+      sc->bytes += (uint64_t)gw.n_nodes * 80;
+      if (gw.max_depth >= (uint32_t)kWStack)
+        return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+    } else {
+      sc->allocs.push_back(g.nodes);
+      tmp.push_back(g.order);
+      sc->bytes += (uint64_t)g.n_slots * 64;
+      if (g.max_depth >= (uint32_t)kBStack)
+        return bail(GYT_ERR_UNSUPPORTED, "scene_create: BVH deeper than the traversal stack");
+    }
     float4 *dtris = nullptr, *dn = nullptr;
     e = dalloc(sc->allocs, &dtris, (size_t)nt * 3);
     if (e == cudaSuccess) e = dalloc(sc->allocs, &dn, (size_t)nt * 3);
@@ -3228,13 +3438,13 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       e = cudaMemcpyAsync(light_leaf.data(), dLightLeaf, n_area * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
-    ds.nodes = g.nodes;
-    ds.wnodes = nullptr;
+    ds.nodes = use_wide ? nullptr : g.nodes;
+    ds.wnodes = use_wide ? gw.nodes : nullptr;
     ds.tris = dtris;
     ds.tnrm = dn;
-    sc->n_nodes = g.n_inner;
-    sc->n_slots = g.n_slots;
-    sc->bvh_depth = g.max_depth;
+    sc->n_nodes = use_wide ? gw.n_nodes : g.n_inner;
+    sc->n_slots = use_wide ? 0 : g.n_slots;
+    sc->bvh_depth = use_wide ? gw.max_depth : g.max_depth;
   } else {
     WideBvhHost wide;
     BvhHost bin;
@@ -3445,6 +3655,28 @@ int32_t gyt_scene_set_materials(gyt_scene* s, const float* mat_params, const flo
   return GYT_OK;
 }
 
+int32_t gyt_scene_freeze_sampling(gyt_scene* s, const float* mat_params) {
+  if (!s || !s->ctx) return GYT_ERR_INVALID;
+  gyt_context* ctx = s->ctx;
+  GYT_CK(ctx, cudaSetDevice(s->device));
+  if (!mat_params) {
+    s->dev.sparams = nullptr;
+    return GYT_OK;
+  }
+  const size_t nf = (size_t)s->n_materials * 16;
+  for (size_t k = 0; k < nf; ++k)
+    if (!std::isfinite(mat_params[k])) return fail(ctx, GYT_ERR_INVALID, "freeze_sampling: non-finite parameter");
+  if (!s->sparams_buf) {
+    float* p = nullptr;
+    GYT_CK(ctx, dalloc(s->allocs, &p, nf));
+    s->sparams_buf = p;
+  }
+  GYT_CK(ctx, cudaMemcpyAsync(s->sparams_buf, mat_params, nf * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  s->dev.sparams = s->sparams_buf;
+  return GYT_OK;
+}
+
 int32_t gyt_scene_read_bvh(const gyt_scene* s, float* nodes, uint64_t node_capacity, uint32_t* tri_ids,
                            uint64_t tri_capacity, uint64_t* n_slots) {
   if (!s || !n_slots) return GYT_ERR_INVALID;
@@ -3456,6 +3688,26 @@ int32_t gyt_scene_read_bvh(const gyt_scene* s, float* nodes, uint64_t node_capac
     return fail(ctx, GYT_ERR_INVALID, "read_bvh: output arrays too small");
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   if (s->n_slots) GYT_CK(ctx, cudaMemcpy(nodes, s->dev.nodes, s->n_slots * 64, cudaMemcpyDeviceToHost));
+  if (tri_ids && s->n_tris) {
+    std::vector<float4> t0((size_t)s->n_tris * 3);
+    GYT_CK(ctx, cudaMemcpy(t0.data(), s->dev.tris, t0.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint64_t k = 0; k < s->n_tris; ++k) std::memcpy(&tri_ids[k], &t0[3 * k].w, 4);
+  }
+  return GYT_OK;
+}
+
+int32_t gyt_scene_read_wide_bvh(const gyt_scene* s, uint32_t* words, uint64_t word_capacity, uint32_t* tri_ids,
+                                uint64_t tri_capacity, uint64_t* n_nodes) {
+  if (!s || !n_nodes) return GYT_ERR_INVALID;
+  gyt_context* ctx = s->ctx;
+  if (!s->dev.wnodes && s->n_tris) return fail(ctx, GYT_ERR_UNSUPPORTED, "read_wide_bvh: not an 8-wide BVH");
+  const uint64_t n = s->dev.wnodes ? s->n_nodes : 0;
+  *n_nodes = n;
+  if (!words) return GYT_OK;
+  if (word_capacity < n * 20 || (tri_ids && tri_capacity < s->n_tris))
+    return fail(ctx, GYT_ERR_INVALID, "read_wide_bvh: output arrays too small");
+  GYT_CK(ctx, cudaSetDevice(s->device));
+  if (n) GYT_CK(ctx, cudaMemcpy(words, s->dev.wnodes, n * 80, cudaMemcpyDeviceToHost));
   if (tri_ids && s->n_tris) {
     std::vector<float4> t0((size_t)s->n_tris * 3);
     GYT_CK(ctx, cudaMemcpy(t0.data(), s->dev.tris, t0.size() * sizeof(float4), cudaMemcpyDeviceToHost));
@@ -3930,6 +4182,35 @@ int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint
   return GYT_OK;
 }
 
+int32_t gyt_bsdf_table(gyt_context* ctx, uint64_t n, const uint32_t* types, const float* params, const float* vec,
+                       float* out) {
+  if (!ctx || (n && (!types || !params || !vec || !out))) return fail(ctx, GYT_ERR_INVALID, "bsdf_table: null argument");
+  if (n == 0) return GYT_OK;
+  if (n >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "bsdf_table: more than 2^32 cases");
+  for (uint64_t i = 0; i < n; ++i)
+    if (types[i] > GYT_MAT_DIELECTRIC) return fail(ctx, GYT_ERR_INVALID, "bsdf_table: unknown material kind");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  struct Guard {
+    std::vector<void*>& v;
+    ~Guard() { for (void* p : v) cudaFree(p); }
+  } guard{tmp};
+  uint32_t* dt = nullptr;
+  float *dp = nullptr, *dv = nullptr, *dout = nullptr;
+  GYT_CK(ctx, dalloc(tmp, &dt, n));
+  GYT_CK(ctx, dalloc(tmp, &dp, 16 * n));
+  GYT_CK(ctx, dalloc(tmp, &dv, 9 * n));
+  GYT_CK(ctx, dalloc(tmp, &dout, 11 * n));
+  GYT_CK(ctx, cudaMemcpyAsync(dt, types, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(dp, params, 16 * n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  GYT_CK(ctx, cudaMemcpyAsync(dv, vec, 9 * n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  k_bsdf_table<<<grid_for(n), kBlock, 0, ctx->stream>>>(n, dp, dt, dv, dout);
+  GYT_CK(ctx, cudaGetLastError());
+  GYT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  GYT_CK(ctx, cudaMemcpy(out, dout, 11 * n * 4, cudaMemcpyDeviceToHost));
+  return GYT_OK;
+}
+
 int32_t gyt_halton(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out) {
   if (!ctx || (n && (!dims || !indices || !out))) return fail(ctx, GYT_ERR_INVALID, "halton: null argument");
   if (n == 0) return GYT_OK;
@@ -4148,6 +4429,8 @@ int32_t batch_input(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes
     const int W = sc->dev.wnodes ? 8 : 2;
     if (i == 0) in->W = W;
     else if (W != in->W) return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: scenes of different BVH widths");
+    if (sc->dev.sparams)
+      return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: scene " + std::to_string(i) + " has frozen BSDF sampling");
     int32_t st = check_params(ctx, &params[i]);
     if (st) return st;
     Inst& I = in->insts[i];
@@ -4208,8 +4491,7 @@ int32_t run_batch(gyt_context* ctx, const BatchInput& in, GytRenderStats* stats)
     is.capacity = ctx->capacity;
     // a path holds a slot for at most max_depth half-iterations and a full
     // pool retires at least one slot per half-iteration: generous bound
-    const unsigned long long bound =
-        2ull * (is.total / ctx->capacity + 2) * ((unsigned long long)in.max_depth + 2) + 64;
+    const unsigned long long bound = wavefront_bound(is.total, in.max_depth, ctx->capacity);
     is.max_iter = (uint32_t)std::min<unsigned long long>(bound, 1u << 30);
     *ctx->h_iter = is;
     GYT_CK(ctx, cudaMemcpyAsync(ctx->d_iter, ctx->h_iter, sizeof(IterState), cudaMemcpyHostToDevice, s));
@@ -4488,6 +4770,8 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
     return fail(ctx, GYT_ERR_UNSUPPORTED,
                 "render_device_noalloc: paths_in_flight must be in [1, " + std::to_string(GYT_NOALLOC_MAX_PATHS) +
                     "] (the size of the library's built-in scratch array)");
+  if (scene->dev.sparams)
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: the scene's BSDF sampling is frozen");
   int32_t st = check_params(ctx, params);
   if (st) return st;
   Cam cam;
@@ -4496,6 +4780,12 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
   GYT_CK(ctx, cudaSetDevice(ctx->device));
   unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
   if (total >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: more than 2^32 paths");
+  // every wavefront iteration waits for the GPU once: refuse a pool so small
+  // for the render that the loop could run for minutes
+  const unsigned long long max_iters = wavefront_bound(total, params->max_depth, paths_in_flight);
+  if (max_iters > (1ull << 24))
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "render_device_noalloc: paths_in_flight too small for this render (its "
+                                          "iteration bound exceeds 2^24 wavefront iterations)");
   unsigned char* base = nullptr;
   st = noalloc_scratch(ctx, &base);
   if (st) return st;
@@ -4544,7 +4834,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
     active += n_new;
     if (W == 8) k_extend<8, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
     else k_extend<2, false><<<g_ext, kBlock, 0, s>>>(pool[cur], active, D, q.hit, q.counts + 2, nullptr);
-    k_shade<<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, D, prm, q, tab, DebugOut{});
+    k_shade<false><<<grid_for(active), kBlock, 0, s>>>(pool[cur], active, D, prm, q, tab, DebugOut{});
     if (W == 8) k_connect<8, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
     else k_connect<2, false><<<g_sh, kBlock, 0, s>>>(pool[cur], D, q, DebugOut{}, nullptr);
     k_finish<<<grid_for(active), kBlock, 0, s>>>(pool[cur], pool[cur ^ 1], active, d_film, cam.res_x, q.counts + 5,
@@ -4556,7 +4846,7 @@ extern "C" int32_t gyt_render_device_noalloc(gyt_context* ctx, const gyt_scene* 
     GYT_CK(ctx, cudaStreamSynchronize(s));
     active = live;
     cur ^= 1;
-    if (++iters > 10000000) return fail(ctx, GYT_ERR_WATCHDOG, "render_device_noalloc: iteration cap reached");
+    if (++iters > max_iters) return fail(ctx, GYT_ERR_WATCHDOG, "render_device_noalloc: iteration cap reached");
   }
   return GYT_OK;
 }

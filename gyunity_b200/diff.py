@@ -35,6 +35,17 @@ class DiffRenderer:
         mp, em = scenes.apply_inverse_params(self.desc, p)
         self.scene.set_materials(mp, em, keep_light_sampling=keep_light_sampling)
 
+    def freeze_sampling(self, p: "scenes.InverseParams" = None):
+        """Holds BSDF sampling and pdfs at the parameters p for the following
+        forwards (gyt_scene_freeze_sampling); None ends it. Forwards at
+        parameters stepped about p then differ exactly by the detached-sampling
+        derivative the adjoint computes."""
+        if p is None:
+            self.scene.freeze_sampling(None)
+            return
+        mp, _ = scenes.apply_inverse_params(self.desc, p)
+        self.scene.freeze_sampling(mp)
+
     def forward(self, p: "scenes.InverseParams", keep_light_sampling=False):
         """Renders with parameters p; returns the image (h, w, 3) on the
         device in float64 (colour / weight per pixel of the FP64 film, the
@@ -100,8 +111,17 @@ def loss_and_grad(renderer: DiffRenderer, p: "scenes.InverseParams", target):
     return loss, renderer.backward(grad_img)
 
 
-def loss_at(renderer: DiffRenderer, p: "scenes.InverseParams", target, keep_light_sampling=False):
-    img = renderer.forward(p, keep_light_sampling)
+def loss_at(renderer: DiffRenderer, p: "scenes.InverseParams", target, keep_light_sampling=False,
+            frozen_at: "scenes.InverseParams" = None):
+    """The loss of a forward at p; with frozen_at, BSDF sampling and pdfs are
+    held at those parameters during the forward."""
+    if frozen_at is not None:
+        renderer.freeze_sampling(frozen_at)
+    try:
+        img = renderer.forward(p, keep_light_sampling)
+    finally:
+        if frozen_at is not None:
+            renderer.freeze_sampling(None)
     return float(((img - target).double() ** 2).mean().item())
 
 

@@ -73,12 +73,17 @@ def _enum_tables(path):
     return fwd, inv
 
 
-def generate(reference="/root/reference", force=False):
-    src = os.path.join(reference, "Gyunity", "src", "sampler")
-    if not os.path.isdir(src):
+def generate(reference=None, force=False):
+    """Writes the generated header from the reference checkout at
+    ``reference`` (else $GYUNITY_REFERENCE); without a checkout an existing
+    header is kept."""
+    reference = reference or os.environ.get("GYUNITY_REFERENCE")
+    src = os.path.join(reference, "Gyunity", "src", "sampler") if reference else None
+    if not src or not os.path.isdir(src):
         if os.path.exists(OUT):
             return OUT
-        raise FileNotFoundError("Sobol tables: no generated header and no reference checkout at %s" % reference)
+        raise FileNotFoundError("Sobol tables: no generated header and no reference checkout (pass its location or "
+                                "set GYUNITY_REFERENCE); looked at %r" % reference)
     if os.path.exists(OUT) and not force:
         return OUT
     mats = _sobol_matrices(os.path.join(src, "Sobol.cpp"))
@@ -106,4 +111,4 @@ def generate(reference="/root/reference", force=False):
 
 
 if __name__ == "__main__":
-    print(generate(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", force=True))
+    print(generate(sys.argv[1] if len(sys.argv) > 1 else None, force=True))

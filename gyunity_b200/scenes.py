@@ -62,6 +62,7 @@ class RenderParams:
     max_depth: int = 8
     rr_depth: int = 5   # Russian roulette applies when bounce index i > rr_depth (reference: 5)
     sampler: str = "sobol"  # "sobol" (SobolSampler + SobolEnum) or "halton" (HaltonSampler + HaltonEnum)
+    equi_angular: bool = False  # volumetric renders: VolPathTracing's equalAngular (GYT_VOLUME_EQUI_ANGULAR)
 
 
 @dataclasses.dataclass

@@ -43,7 +43,8 @@ enum {
   GYT_ERR_CUDA = 2,         /* CUDA runtime error (message in gyt_last_error) */
   GYT_ERR_OUT_OF_MEMORY = 3,
   GYT_ERR_UNSUPPORTED = 4,  /* feature or size outside what this build handles */
-  GYT_ERR_WATCHDOG = 5      /* a bounded device loop hit its iteration cap */
+  GYT_ERR_WATCHDOG = 5      /* a bounded loop hit its iteration cap (twice the iterations the work can
+                               need); a film then holds the paths finished so far */
 };
 
 /* Material kinds. Parameters are 16 floats per material:
@@ -145,13 +146,14 @@ int32_t gyt_context_set_profile(gyt_context* ctx, int32_t mode);
  * (binary, two child boxes per 64-byte node; the default) or 8 (quantized
  * child boxes, 80-byte nodes). Both replace BVHAccel (accelerator/BVHAccel.cpp). */
 int32_t gyt_context_set_bvh_width(gyt_context* ctx, int32_t width);
-/* Where later gyt_scene_create calls build a binary (width 2) BVH:
- * GYT_BVH_BUILD_DEVICE (the default) or GYT_BVH_BUILD_HOST. Both make the
- * same tree: 16-bin SAH, at most 8 triangles per leaf, identical splits,
+/* Where later gyt_scene_create calls build the BVH: GYT_BVH_BUILD_DEVICE
+ * (the default) or GYT_BVH_BUILD_HOST. For a binary (width 2) BVH both make
+ * the same tree: 16-bin SAH, at most 8 triangles per leaf, identical splits,
  * leaves and child boxes, each leaf's triangles in ascending id order (only
- * the node numbering differs).
- * The 8-wide BVH is always built on the host. Replaces the BVHAccel
- * constructor's build (accelerator/BVHAccel.cpp:154-200). */
+ * the node numbering differs). For the 8-wide BVH both collapse the binary
+ * tree of at most 3 triangles per leaf into the same quantized nodes, word
+ * for word (breadth-first numbering). Replaces the BVHAccel constructor's
+ * build (accelerator/BVHAccel.cpp:154-200). */
 #define GYT_BVH_BUILD_HOST 0
 #define GYT_BVH_BUILD_DEVICE 1
 int32_t gyt_context_set_bvh_builder(gyt_context* ctx, int32_t builder);
@@ -172,6 +174,12 @@ int32_t gyt_scene_info(const gyt_scene* scene, uint64_t* n_triangles, uint64_t* 
  * 8-wide BVH. Inspection and tests; no counterpart in the reference. */
 int32_t gyt_scene_read_bvh(const gyt_scene* scene, float* nodes, uint64_t node_capacity, uint32_t* tri_ids,
                            uint64_t tri_capacity, uint64_t* n_slots);
+/* The same for an 8-wide BVH: n_nodes nodes of 20 words (5 x uint4, the
+ * layout of the traversal kernels) and the leaf-order triangle ids;
+ * GYT_ERR_UNSUPPORTED for a binary BVH. Inspection and tests; no counterpart
+ * in the reference. */
+int32_t gyt_scene_read_wide_bvh(const gyt_scene* scene, uint32_t* words, uint64_t word_capacity, uint32_t* tri_ids,
+                                uint64_t tri_capacity, uint64_t* n_nodes);
 
 /* Integrator::Render: renders the full image and writes rgb_out (host,
  * res_x*res_y*3 floats, row-major from the top-left pixel) = colour/weight
@@ -209,6 +217,15 @@ int32_t gyt_intersect(gyt_context* ctx, const gyt_scene* scene, uint64_t n, cons
 /* sobol::sample (sampler/Sobol.h:46-61) for n (dimension, index) pairs. */
 int32_t gyt_sobol(gyt_context* ctx, uint64_t n, const uint32_t* dims, const uint64_t* indices, float* out);
 
+/* The BxDF lobes of the shading kernels in their local frame, for n cases
+ * (host arrays): material kind types[i] (GYT_MAT_DIFFUSE..GYT_MAT_DIELECTRIC)
+ * with parameters params[16 i..] (the GytSceneDesc.mat_params layout); vec[9 i..]
+ * = wo, u, we. out[11 i..] = the sample BxDF::Sample(wo, u) gives (f rgb, wi,
+ * pdf), then BxDF::Evaluate(wo, we) (rgb) and BxDF::Pdf(wo, we): the BxDFs of
+ * bsdf/BSDF.h:162-616 on the GPU, for parity tests. */
+int32_t gyt_bsdf_table(gyt_context* ctx, uint64_t n, const uint32_t* types, const float* params, const float* vec,
+                       float* out);
+
 /* SobolEnum::GetIndex (sampler/SobolEnum.h:23-28) for n (s, x, y) triplets. */
 int32_t gyt_sobol_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, uint64_t n,
                              const uint32_t* sxy, uint64_t* out);
@@ -233,14 +250,17 @@ int32_t gyt_render_light_tracing_device(gyt_context* ctx, const gyt_scene* scene
                                         const GytRenderParams* params, double* d_splat, GytRenderStats* stats);
 /* Per-photon records for parity tests: for photons[i], max_depth records of
  * 6 floats (on film 1 / 0, or -1 where the path has no such vertex; pixel X,
- * Y; the splatted RGB), vertex 0 = the light vertex. */
+ * Y; the splatted RGB), vertex 0 = the light vertex; a missing vertex's
+ * record is (-1, 0, 0, 0, 0, 0). */
 int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
                               const GytRenderParams* params, uint64_t n, const uint64_t* photons, float* records);
 
 /* ---- Volumetric path tracing -----------------------------------------------
- * VolPathTracing(spp, maxDepth, sampler, samplerEnum, false)
- * (integrator/VPT.cpp:7-104, the estimator without equi-angular sampling)
- * with the scene's homogeneous media (GytSceneDesc::media, tri_medium):
+ * VolPathTracing(spp, maxDepth, sampler, samplerEnum, equalAngular)
+ * (integrator/VPT.h:12-19, integrator/VPT.cpp:7-171) with the scene's
+ * homogeneous media (GytSceneDesc::media, tri_medium). Without
+ * GYT_VOLUME_EQUI_ANGULAR in params->flags, the estimator of
+ * equalAngular = false:
  * camera rays start in no medium; a ray through a medium samples a
  * scattering distance (HomogeneousMedium::Sample, volume/Homogeneous.cpp);
  * at a medium point light is gathered with the Henyey-Greenstein phase
@@ -252,7 +272,20 @@ int32_t gyt_trace_light_paths(gyt_context* ctx, const gyt_scene* scene, const Gy
  * reference's VolPathTracing needs its BSDF pointer initialised to null to
  * pass through surfaces of no material (it reads it uninitialised). A hit
  * at the very end of a shadow segment (the light's own surface) is settled
- * in FP64, as in the path tracer's occlusion test. */
+ * in FP64, as in the path tracer's occlusion test.
+ * With GYT_VOLUME_EQUI_ANGULAR, the estimator of equalAngular = true (the
+ * reference constructor's default): every bounce draws one area light and
+ * one point on it (AreaLight::SampleOnePoint); a ray in a medium samples its
+ * scattering distance in [0, 3] along the ray with density proportional to
+ * the inverse squared distance to that point
+ * (HomogeneousMedium::EquiAngularSampling, volume/Homogeneous.cpp:38-64),
+ * and a medium point gathers light only through the connection to that
+ * point (ConnectToLight, VPT.cpp:108-146: phase function, transmittance of
+ * the segment, cosine at the light over the squared distance and the area
+ * pdf, no MIS weight); surface points gather as without the flag. Needs an
+ * area light (GYT_ERR_UNSUPPORTED otherwise). The flag is accepted by the
+ * three volumetric entry points only. */
+#define GYT_VOLUME_EQUI_ANGULAR 2u
 int32_t gyt_render_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
                           const GytRenderParams* params, float* rgb_out);
 int32_t gyt_render_volume_device(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera,
@@ -334,6 +367,18 @@ int32_t gyt_halton_enum_index(gyt_context* ctx, uint32_t res_x, uint32_t res_y, 
  * derivative assumes). Material types and geometry are unchanged. */
 #define GYT_KEEP_LIGHT_SAMPLING 1u
 int32_t gyt_scene_set_materials(gyt_scene* scene, const float* mat_params, const float* emission, uint32_t flags);
+/* Freezes BSDF sampling for difference checks: while set, gyt_render,
+ * gyt_render_device, gyt_diff_forward and gyt_trace_paths sample BSDF
+ * directions and evaluate every BSDF pdf (sample pdfs and MIS weights) with
+ * mat_params (n_materials x 16 floats, the GytSceneDesc.mat_params layout),
+ * while the BSDF values of the GGX lobes use the scene's current parameters.
+ * Rendered with roulette off and the scene's parameters stepped about the
+ * frozen ones, central differences of an image loss then equal the
+ * detached-sampling derivative gyt_diff_backward computes (for the GGX alpha
+ * as for the albedo). NULL ends it. The adjoint pass, batched renders, light
+ * tracing, volumetric path tracing and gyt_render_device_noalloc refuse a
+ * frozen scene (GYT_ERR_UNSUPPORTED). No counterpart in the reference. */
+int32_t gyt_scene_freeze_sampling(gyt_scene* scene, const float* mat_params);
 /* Primal render for differentiation: gyt_render_device into d_film plus the
  * radiance of every path (d_path_L: device, res_x*res_y*spp*3 floats,
  * indexed by path id = pixel * spp + sample). */
@@ -406,9 +451,11 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
  * loads the library until the process exits) instead of the context's pools,
  * which are allocated on first use. paths_in_flight (1..GYT_NOALLOC_MAX_PATHS)
  * sets how many paths share it; larger values are rejected with
- * GYT_ERR_UNSUPPORTED. The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls on a device share the array: calls whose GPU work
+ * GYT_ERR_UNSUPPORTED, and so is a pool so small for the render that its
+ * iteration bound passes 2^24 wavefront iterations (each waits for the GPU
+ * once). The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array: calls whose GPU work
  * overlaps (other streams or threads) race on it. The scene, the Sobol' tables
  * of the context and the caller's device film (accumulated, not cleared) are
  * the inputs and output. No counterpart in the reference. */

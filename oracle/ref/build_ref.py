@@ -12,7 +12,10 @@ Recipe (no reference build system is run):
   3. compile the translation units on the PathTracing route with g++ and the
      shim headers in ``oracle/ref/shims`` (fmt, spdlog, tbb are absent
      submodules), plus ``oracle/ref/harness.cpp``;
-  4. link ``oracle/_ref/gyref_harness``.
+  4. link ``oracle/_ref/gyref_harness``;
+  5. when the product library is built, link ``oracle/_ref/gyref_dropin``
+     (oracle/ref/dropin.cpp: the binding of include/gyt_integrator.h run
+     inside the reference's own Renderer).
 
 Patches (numbered P1-P9; each is an exact text replacement):
   P1 common/Core.h:42-43     int64/uint64 as long long so the Sampler override
@@ -42,7 +45,9 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT = os.path.join(ORACLE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+# the reference checkout: $GYUNITY_REFERENCE, else where this build's
+# container mounts it
+DEFAULT_REFERENCE = os.environ.get("GYUNITY_REFERENCE") or "/root/reference"
 
 PATCHES = [
     ("common/Core.h", "using int64 = int64_t;", "using int64 = long long;"),
@@ -127,6 +132,33 @@ def build(reference=DEFAULT_REFERENCE, verbose=True):
         list(ex.map(compile_one, units))
     exe = os.path.join(OUT, "gyref_harness")
     _run(["g++"] + CXXFLAGS + [o for _, o in units] + ["-o", exe])
+    if verbose:
+        print("built", exe)
+    build_dropin(reference, verbose)
+    return exe
+
+
+def build_dropin(reference=DEFAULT_REFERENCE, verbose=True):
+    """``oracle/_ref/gyref_dropin``: oracle/ref/dropin.cpp (the reference's
+    Renderer with the GPU integrators of include/gyt_integrator.h) on the
+    reference objects of build(), linked against the product library
+    (gyunity_b200/libgyunity_b200.so, found at run time next to the
+    repository through an $ORIGIN-relative rpath). Skipped when that library
+    has not been built."""
+    lib_dir = os.path.join(os.path.dirname(ORACLE), "gyunity_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libgyunity_b200.so")):
+        return None
+    src = os.path.join(OUT, "src")
+    obj = os.path.join(OUT, "obj")
+    shims = os.path.join(HERE, "shims")
+    inc = ["-I", src, "-I", shims, "-I", os.path.join(reference, "external"),
+           "-I", os.path.join(os.path.dirname(ORACLE), "include"), "-include", os.path.join(shims, "compat.h")]
+    dobj = os.path.join(obj, "dropin.o")
+    _run(["g++"] + CXXFLAGS + inc + ["-c", os.path.join(HERE, "dropin.cpp"), "-o", dobj])
+    objs = [os.path.join(obj, s.replace("/", "_") + ".o") for s in SOURCES] + [os.path.join(obj, "logger_stub.o")]
+    exe = os.path.join(OUT, "gyref_dropin")
+    _run(["g++"] + CXXFLAGS + objs + [dobj, "-L", lib_dir, "-lgyunity_b200",
+                                      "-Wl,-rpath,$ORIGIN/../../gyunity_b200", "-o", exe])
     if verbose:
         print("built", exe)
     return exe

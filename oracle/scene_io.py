@@ -145,6 +145,26 @@ def ref_paths(tmp, scene_path, x, y, s, sampler=None, integrator=None):
     return np.fromfile(b, np.float32).reshape(-1, 4)
 
 
+def ref_sample(tmp, items, warmup, steps, sampler=None, threads=None):
+    """PathTracing::Li of the reference over many scenes, timed: items is a
+    list of (scene path, (n, 3) uint32 x, y, s samples); each scene is loaded
+    (untimed) and its samples traced warmup + steps times on the host threads.
+    Returns the harness's record: paths_per_step, step_s (seconds of each
+    step summed over the scenes), load_s, threads."""
+    import json
+    lst = os.path.join(tmp, "sample_list.txt")
+    with open(lst, "w") as f:
+        for k, (scene_path, xys) in enumerate(items):
+            trip = os.path.join(tmp, "sample_%d.bin" % k)
+            np.ascontiguousarray(xys, np.uint32).tofile(trip)
+            f.write("%s %s\n" % (scene_path, trip))
+    env = dict(_sampler_env(sampler) or {})
+    if threads:
+        env["GYREF_THREADS"] = str(threads)
+    out = run("sample", lst, int(warmup), int(steps), env=env or None)
+    return json.loads(out.strip().splitlines()[-1])
+
+
 def ref_camera(tmp, scene_path):
     b = os.path.join(tmp, "camera.bin")
     run("camera", scene_path, b)

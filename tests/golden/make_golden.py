@@ -11,6 +11,8 @@ checkout is only needed to regenerate; the tests read the fixtures.
     python tests/golden/make_golden.py obj        # only the OBJ-mesh fixtures
     python tests/golden/make_golden.py lt         # only the light-tracing fixtures
     python tests/golden/make_golden.py vpt        # only the volume fixtures
+    python tests/golden/make_golden.py vpt_eq     # only the equi-angular volume fixtures
+    python tests/golden/make_golden.py zstat      # only the per-pixel moments of the z-test
 """
 import dataclasses
 import os
@@ -270,10 +272,68 @@ def volume_golden(tmp):
     np.savez_compressed(os.path.join(HERE, "image_vpt_fog_64x64_8spp.npz"), film=img)
 
 
+def volume_equi_angular_golden(tmp):
+    """VolPathTracing with equi-angular sampling (its constructor's default,
+    harness integrator "vpt_eq") per path on the fog scenes, and rendered on
+    the Cornell box in fog."""
+    rng = np.random.default_rng(20261203)
+    for name, sd in (("fog", scenes.cornell_fog(res=48, spp=4, max_depth=6)),
+                     ("fog_thick", scenes.cornell_fog(res=48, spp=4, max_depth=6, sigma_a=0.2, sigma_s=1.5, g=-0.4,
+                                                      spheres=False)),
+                     ("fog_ball", scenes.fog_ball_box(res=48, spp=4, max_depth=6))):
+        path = os.path.join(tmp, "vpt_eq_%s.gyts" % name)
+        io.write_scene(path, sd)
+        n = 3000
+        x = rng.integers(0, sd.camera.res_x, n)
+        y = rng.integers(0, sd.camera.res_y, n)
+        s = rng.integers(0, sd.params.spp, n)
+        r = io.ref_paths(tmp, path, x, y, s, sampler=sd.params.sampler, integrator="vpt_eq")
+        np.savez_compressed(os.path.join(HERE, "vpt_eq_paths_%s.npz" % name),
+                            xys=np.stack([x, y, s], 1).astype(np.uint32), L=r[:, :3],
+                            cursor=r[:, 3].astype(np.int32))
+    sd = scenes.cornell_fog(res=64, spp=8, max_depth=6)
+    path = os.path.join(tmp, "vpt_eq_img.gyts")
+    io.write_scene(path, sd)
+    img, _ = io.ref_render(tmp, path, integrator="vpt_eq")
+    np.savez_compressed(os.path.join(HERE, "image_vpt_eq_fog_64x64_8spp.npz"), film=img)
+
+
+ZSTAT_SCENES = {
+    "cornell_256x256_16spp": lambda: scenes.cornell_box(res=256, spp=16),
+    "env_knot_96x54_16spp": lambda: dataclasses.replace(
+        scenes.env_knot_small(), params=dataclasses.replace(scenes.env_knot_small().params, spp=16)),
+    "inverse_128x128_16spp": lambda: scenes.inverse_box(level=5, res=128, spp=16, max_depth=8, rr_depth=8),
+}
+
+
+def zstat_golden(tmp):
+    """Per-pixel mean and variance of the reference's PathTracing::Li over
+    samples 0..spp-1 of every pixel (float32), for the per-pixel z-test of
+    the GPU's converged image."""
+    for name, make in ZSTAT_SCENES.items():
+        sd = make()
+        path = os.path.join(tmp, "z_%s.gyts" % name)
+        io.write_scene(path, sd)
+        W, H, S = sd.camera.res_x, sd.camera.res_y, sd.params.spp
+        pix = np.repeat(np.arange(W * H), S)
+        r = io.ref_paths(tmp, path, pix % W, pix // W, np.tile(np.arange(S), W * H))
+        L = r[:, :3].astype(np.float64).reshape(W * H, S, 3)
+        np.savez_compressed(os.path.join(HERE, "zstat_%s.npz" % name), mean=L.mean(1).astype(np.float32),
+                            var=L.var(1, ddof=1).astype(np.float32), spp=S, res=np.array([W, H]))
+
+
 def main():
+    if sys.argv[1:] == ["zstat"]:
+        zstat_golden(tempfile.mkdtemp())
+        print("z-test moments written to", HERE)
+        return
     if sys.argv[1:] == ["vpt"]:
         volume_golden(tempfile.mkdtemp())
         print("volume golden vectors written to", HERE)
+        return
+    if sys.argv[1:] == ["vpt_eq"]:
+        volume_equi_angular_golden(tempfile.mkdtemp())
+        print("equi-angular volume golden vectors written to", HERE)
         return
     if sys.argv[1:] == ["lt"]:
         light_tracing_golden(tempfile.mkdtemp())
@@ -376,6 +436,8 @@ def main():
     obj_golden(tmp)
     light_tracing_golden(tmp)
     volume_golden(tmp)
+    volume_equi_angular_golden(tmp)
+    zstat_golden(tmp)
     print("golden vectors written to", HERE)
 
 

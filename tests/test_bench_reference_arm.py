@@ -37,10 +37,28 @@ def test_reference_arm_with_halton_sampler():
     assert line["value"] > 0 and line["config"]["sampler"].startswith("Halton")
 
 
-def test_batch_sample_is_every_sixteenth_instance():
+def test_batch_cpu_sample_is_the_batch_mix():
+    """The CPU sample covers every instance with 1/512 of its paths (every
+    16th column and 32nd row, all samples per pixel), so its path mix is the
+    batch's."""
     sys.path.insert(0, ROOT)
+    import numpy as np
     import bench
-    ids = [i for i, _ in bench.batch_sample(64)]
-    assert ids == [0, 16, 32, 48]
+    from gyunity_b200 import scenes
+    for i in (0, 5, 37):
+        sd = scenes.batch_instance(1000 + i)
+        xys = bench.batch_grid_samples(sd, i)
+        W, H, S = sd.camera.res_x, sd.camera.res_y, sd.params.spp
+        assert len(xys) * 512 == W * H * S
+        assert np.all(xys[:, 0] % 16 == i % 16) and np.all(xys[:, 1] % 32 == (i // 16) % 32)
+        assert np.array_equal(np.bincount(xys[:, 2], minlength=S), np.full(S, W * H // 512))
     cfg = bench.batch_config(type("A", (), {"batch_instances": 64, "sampler": "sobol"})(), None)
     assert cfg["instances"] == 64 and cfg["workload"] == "uneven_batch_64_instances"
+
+
+def test_reference_arm_batch_line_small():
+    """The batch reference arm end to end on a 2-instance batch."""
+    line = _run("--batch-instances", "2", "--steps", "2", "--warmup", "1")
+    assert KEYS <= set(line)
+    assert line["value"] > 0 and "every 16th column" in line["cpu_baseline"]["sample"]
+    assert line["config"]["instances"] == 2

@@ -48,7 +48,7 @@ def test_halton_per_path_radiance_matches_fp64_replay(ctx, name):
     sd = _halton({"cornell_nospheres": scenes.cornell_box(spheres=False),
                   "mixed": scenes.mixed_materials_box(level=3, res=64)}[name])
     xys = golden("paths_%s_halton.npz" % name)["xys"]
-    rel, same_cursor, flips = _replay(sd, xys, ctx)
+    rel, same_cursor, flips, _ = _replay(sd, xys, ctx)
     ok = rel < 1e-4  # FP32 path vs FP64 replay of the same path, relative to max(|L|, 1e-3)
     print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean(), "decision flips:", flips)
     assert same_cursor.mean() > 0.995

@@ -39,7 +39,7 @@ def test_loaded_mesh_renders_with_per_path_parity(ctx):
     n = 48 * 48 * 2
     k = np.arange(n)
     xys = np.stack([(k // 2) % 48, (k // 2) // 48, k % 2], 1).astype(np.uint32)
-    rel, same_cursor, flips = _replay(sd, xys, ctx)
+    rel, same_cursor, flips, _ = _replay(sd, xys, ctx)
     print("paths within 1e-4:", (rel < 1e-4).mean(), "same dims:", same_cursor.mean(), "flips:", flips)
     assert same_cursor.mean() > 0.995
     assert (rel < 1e-4).mean() > 0.99

@@ -87,7 +87,15 @@ def _replay(sd, xys, ctx):
     _, _, _, occ_own, mis_own = o.paths(x, y, s, precision=64, force_rr=rr, return_decisions=True)
     rel = np.abs(L.astype(np.float64) - Lo).max(1) / np.maximum(np.abs(Lo).max(1), 1e-3)
     flips = float(((occ_own != occ) | (mis_own != mis)).mean())
-    return rel, cur == co, flips
+    # the same replay in FP32: a path the FP32 replay follows (within 1e-4)
+    # but the FP64 one does not took a branch that rounding decides (an exact
+    # tie between two triangles, a grazing direction, a sample on a branch
+    # threshold); what neither replay follows is unexplained
+    L32, _ = o.paths(x, y, s, precision=32, force_rr=rr, force_occ=occ, force_mis=mis)
+    rel32 = np.abs(L.astype(np.float64) - L32).max(1) / np.maximum(np.abs(L32).max(1), 1e-3)
+    causes = {"rounding_decided": int(((rel >= 1e-4) & (rel32 < 1e-4)).sum()),
+              "unexplained": int(((rel >= 1e-4) & (rel32 >= 1e-4)).sum())}
+    return rel, cur == co, flips, causes
 
 
 @pytest.mark.parametrize("name", ["cornell_nospheres", "cornell", "mixed", "env"])
@@ -95,11 +103,13 @@ def test_per_path_radiance_matches_fp64_replay(ctx, name):
     sd = {"cornell_nospheres": scenes.cornell_box(spheres=False), "cornell": scenes.cornell_box(),
           "mixed": scenes.mixed_materials_box(level=3, res=64), "env": scenes.env_knot_small()}[name]
     xys = golden("paths_%s.npz" % name)["xys"]
-    rel, same_cursor, flips = _replay(sd, xys, ctx)
+    rel, same_cursor, flips, causes = _replay(sd, xys, ctx)
     ok = rel < 1e-4  # tolerance: FP32 path vs FP64 replay of the same path, relative to max(|L|, 1e-3)
-    print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean(), "decision flips vs FP64:", flips)
+    print(name, "paths within 1e-4:", ok.mean(), "same dims:", same_cursor.mean(), "decision flips vs FP64:", flips,
+          "outside 1e-4 of %d: %s" % (len(rel), causes))
     assert same_cursor.mean() > 0.995
     assert ok.mean() > 0.99
+    assert causes["unexplained"] <= 0.005 * len(rel)
     # shadow rays end on the light surface (the reference's RayEps cancels
     # ShadowRayEps), so FP32 occlusion by the light itself is a rounding coin
     # flip; bounded here, replayed above

@@ -55,7 +55,7 @@ def test_volume_image_matches_reference(ctx):
     sc = g.Scene(sd, ctx)
     film = g.Film(64, 64)
     cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
-    g.VolPathTracing(8, 6).Render(sc, cam)
+    g.VolPathTracing(8, 6, equal_angular=False).Render(sc, cam)
     img = film.image.astype(np.float64)
     rel_mean = abs(img.mean() - ref.mean()) / ref.mean()
     rmse = np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2))
@@ -116,5 +116,63 @@ def test_volume_rejects_bad_input(ctx):
     with pytest.raises(g.GytError):
         sc.trace_volume_paths(np.array([[16, 0, 0]], np.uint32))
     # the context stays usable after the errors
+    L, cur = sc.trace_volume_paths(np.array([[3, 4, 0]], np.uint32))
+    assert np.isfinite(L).all() and cur[0] >= 2
+
+
+# ---- equi-angular sampling (VolPathTracing's constructor default) ----------
+
+def _equi(sd):
+    return dataclasses.replace(sd, params=dataclasses.replace(sd.params, equi_angular=True))
+
+
+EQ_CASES = {k: CASES[k] for k in ("fog", "fog_thick", "fog_ball")}
+
+
+@pytest.mark.parametrize("name", list(EQ_CASES))
+def test_equi_angular_paths_match_reference(ctx, name):
+    """Per path against the reference's VolPathTracing with equalAngular =
+    true (tests/golden/vpt_eq_paths_*.npz): the light and point drawn every
+    bounce, the equi-angular distance in the medium, the connection to the
+    light point."""
+    gd = golden("vpt_eq_paths_%s.npz" % name)
+    sd = _equi(EQ_CASES[name]())
+    sc = g.Scene(sd, ctx)
+    L, cur = sc.trace_volume_paths(gd["xys"])
+    ref = gd["L"].astype(np.float64)
+    rel = np.abs(L - ref).max(1) / np.maximum(np.abs(ref).max(1), 1e-3)
+    same = cur == gd["cursor"]
+    print(name, "equi-angular paths within 1e-4: %.4f, same dims: %.4f, mean L %s vs %s" % (
+        (rel < 1e-4).mean(), same.mean(), L.mean(0), ref.mean(0)))
+    assert np.isfinite(L).all()
+    assert same.mean() > 0.995
+    assert (rel < 1e-4).mean() > 0.99
+
+
+def test_equi_angular_image_matches_reference(ctx):
+    gd = golden("image_vpt_eq_fog_64x64_8spp.npz")["film"].reshape(64, 64, 4).astype(np.float64)
+    ref = gd[..., :3] / gd[..., 3:]
+    sd = scenes.cornell_fog(res=64, spp=8, max_depth=6)
+    sc = g.Scene(sd, ctx)
+    film = g.Film(64, 64)
+    cam = g.PinHoleCamera(film, sd.camera.pos, sd.camera.look_at, sd.camera.up, sd.camera.fovy, 1.0)
+    g.VolPathTracing(8, 6).Render(sc, cam)  # equal_angular defaults to True, as the reference's constructor
+    img = film.image.astype(np.float64)
+    rel_mean = abs(img.mean() - ref.mean()) / ref.mean()
+    rmse = np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2))
+    print("equi-angular volume image: relative mean %.2e, relative RMSE %.4f" % (rel_mean, rmse))
+    assert rel_mean < 5e-4 and rmse < 0.01
+
+
+def test_equi_angular_needs_an_area_light_and_is_volume_only(ctx):
+    sd = _equi(scenes.cornell_fog(res=16, spp=1, max_depth=3))
+    sc = g.Scene(sd, ctx)
+    d = torch.zeros(16 * 16 * 4, dtype=torch.float64, device="cuda")
+    # the path tracer does not take the volumetric flag
+    with pytest.raises(g.GytError):
+        ctx.render_device(sc, sd.camera, sd.params, d.data_ptr())
+    dark = dataclasses.replace(sd, tri_emission=np.full_like(sd.tri_emission, -1))
+    with pytest.raises(g.GytError):
+        g.Scene(dark, ctx).trace_volume_paths(np.array([[3, 4, 0]], np.uint32))
     L, cur = sc.trace_volume_paths(np.array([[3, 4, 0]], np.uint32))
     assert np.isfinite(L).all() and cur[0] >= 2

@@ -47,5 +47,36 @@ def test_noalloc_matches_allocating_render_twice():
     film = torch.zeros(4, dtype=torch.float64, device="cuda")
     rc = ctx.render_device_noalloc(scene, sd.camera, sd.params, film.data_ptr(), _capi.NOALLOC_MAX_PATHS + 1)
     assert rc == 4 and b"scratch" in ctx._lib.gyt_last_error(ctx.handle)
+    # a pool far too small for the render (a 1024x1024, 16 spp film one path
+    # at a time) is refused before any work, with its reason
+    big = scenes.mixed_materials_box(level=3, res=1024, spp=16)
+    rc = ctx.render_device_noalloc(scene, big.camera, big.params, film.data_ptr(), 1)
+    assert rc == 4 and b"too small" in ctx._lib.gyt_last_error(ctx.handle)
+    scene.close()
+    ctx.close()
+
+
+def test_noalloc_allocates_no_device_memory_on_a_fresh_context():
+    """On a context that has never rendered (its path pools are not
+    allocated), a render through the entry point leaves the device's free
+    memory unchanged."""
+    import torch
+    import gyunity_b200 as g
+    from gyunity_b200 import scenes
+
+    torch.cuda.init()
+    ctx = g.Context(0)
+    sd = scenes.mixed_materials_box(level=3, res=64, spp=4)
+    scene = g.Scene(sd, ctx)
+    film = torch.zeros(64 * 64 * 4, dtype=torch.float64, device="cuda")
+    ctx.check(ctx.render_device_noalloc(scene, sd.camera, sd.params, film.data_ptr()))  # looks up the array
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    ctx.check(ctx.render_device_noalloc(scene, sd.camera, sd.params, film.data_ptr()))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    # both calls rendered every sample (a sample on a pixel edge also weighs on the neighbour)
+    assert film.view(-1, 4)[:, 3].sum().item() >= 2 * 64 * 64 * 4
     scene.close()
     ctx.close()
