@@ -712,8 +712,8 @@ def measure_volume(a, d, g, torch):
     paths = 512 * 512 * 16
     out = {"workload": "Cornell box in a homogeneous medium with mirror and glass spheres, 512x512, 16 spp, depth 8",
            "value": paths * d.world / (t / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": t,
-           "note": "one kernel launch per render (a camera sample per thread; closest-hit, transmittance and "
-                   "shadow rays traced inline); FP64 film"}
+           "note": "wavefront over a pool of paths in flight: closest hits, a volume shade kernel that queues "
+                   "shadow segments and MIS rays, their transmittance walks, film and compaction; FP64 film"}
     # the same render with equi-angular sampling (VolPathTracing's default)
     sde = dataclasses.replace(sd, params=dataclasses.replace(sd.params, equi_angular=True))
     ms = []

@@ -656,12 +656,14 @@ struct Lobe {
     }
     if (type == 3) {  // MicrofacetReflectionBSDF::Sample (BSDF.h:331-346)
       if (wo.z == 0.f) return zero;
-      float3 wh = g.sample(wo * sgnf(wo.z), u0, u1);
-      if (g.pdf(wo, wh) == 0.f) return zero;
+      const float3 wh = g.sample(wo * sgnf(wo.z), u0, u1);
+      // a non-zero pdf means D(wh) > 0, so wh.z > 0 and the reference's
+      // Faceforward of wh to +z leaves it (and this pdf) unchanged
+      const float gp = g.pdf(wo, wh);
+      if (gp == 0.f) return zero;
       *wi = reflect(wo, wh);
       if (!(wo.z * wi->z > 0.f)) return zero;
-      wh = wh * sgnf(wh.z);
-      *pdf = fabsf(g.pdf(wo, wh) / (4.f * dot(*wi, wh)));
+      *pdf = fabsf(gp / (4.f * dot(*wi, wh)));
       return eval(wo, *wi);
     }
     if (type == 4) {  // RoughDielectricBSDF::Sample (BSDF.h:545-613)

@@ -149,9 +149,12 @@ constexpr int kBlock = 256;  // every kernel that traverses the BVH runs blocks 
 // at word 32 k + l of the binary view (bank l) or at element 32 k + l of the
 // 8-byte view, so a warp's pushes and pops never conflict in the binary view
 // and take the two phases any 8-byte warp access takes in the wide one,
-// whatever depth each lane is at. 64 bytes per lane: 16 KB per block of 256.
-constexpr int kBStackSh = 16;
-constexpr int kWStackSh = 8;
+// whatever depth each lane is at. 32 bytes per lane: 8 KB per block of 256
+// threads. Measured on 16 instances of the uneven batch against stacks in
+// local memory: 8 entries +0.2% (both widths), 16 entries -0.5% (the larger
+// slab takes L1 capacity from the node fetches); the 1.31M-triangle mesh +1%.
+constexpr int kBStackSh = 8;
+constexpr int kWStackSh = 4;
 constexpr int kSlabWarps = kBlock / 32;
 __shared__ uint2 g_trav_slab[kSlabWarps * kWStackSh * 32];
 
@@ -1693,17 +1696,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_light_trace(DevScene s, LtCam c, 
 // (Primitive::Intersect, visual/Primitive.cpp:5-18); a ray leaving a surface
 // takes the outside medium when it leaves along the shading normal, else the
 // inside (Intersection::GetMedium, visual/Intersection.h:80-82).
-// The volume kernel's one traversal, called from its three ray sites (closest
-// hit, transmittance hops, shadow segments) rather than inlined at each: the
-// inlined copies kept the path state and three traversal states live at once
-// (128 registers with spills for the binary BVH, 212 for the 8-wide one);
-// called, 64 against 49 Mpaths/s on the Cornell box in fog (binary BVH).
-template <int W>
-__device__ __noinline__ int vpt_trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1,
-                                       float& b2) {
-  return trace<W, false>(s, o, d, tmax, b1, b2);
-}
-
 struct MediumDev {
   float3 sa, ss, st;
   float g;
@@ -1802,189 +1794,11 @@ GYT_D void vpt_hit(const DevScene& s, int prim, float t, float b1, float b2, flo
   }
 }
 
-// VisibilityTester::Tr (visual/Visibility.cpp:13-30): segments between the
-// point and the light point, through surfaces of no material, each
-// attenuated by its medium; a surface with a material blocks.
-template <int W>
-GYT_D float3 vpt_tr(const DevScene& s, const VPoint& p0, float3 lpos, float3 lerr, float3 labs) {
-  float3 tr = mk(1.f, 1.f, 1.f);
-  float3 pos = p0.pos, perr = p0.perr, abs_n = p0.abs_n, n = p0.n;
-  int m_in = p0.m_in, m_out = p0.m_out;
-#pragma unroll 1
-  for (int hop = 0; hop < 64; ++hop) {
-    // Intersection::SpawnTo (visual/Intersection.h:64-72)
-    const float3 org = offset_origin(pos, perr, abs_n, lpos - pos);
-    const float3 tgt = offset_origin(lpos, lerr, labs, org - lpos);
-    float3 d = tgt - org;
-    const float dis = length(d);
-    d = d / dis;
-    const int medium = dot(d, n) > 0.f ? m_out : m_in;
-    const float3 o = org + d * kRayEps;
-    const float seg = dis - kShadowEps;
-    float tmax = seg, b1 = 0.f, b2 = 0.f;
-    int prim = vpt_trace<W>(s, o, d, tmax, b1, b2);
-    // The segment ends on the light's surface: a hit at its very end is
-    // settled in FP64, as the occlusion test of path tracing settles it.
-    if (prim >= 0 && prim < s.n_tris && tmax >= seg * 0.999998f) {
-      const float4* tv = s.tris + 3 * (size_t)prim;
-      if (!wt_intersect_fp64(wt_setup(o, d), f3(__ldg(tv)), f3(__ldg(tv + 1)), f3(__ldg(tv + 2)), seg)) {
-        prim = -1;
-        tmax = seg;
-      }
-    }
-    if (prim >= 0 && material_type(s, prim) != 5u) return mk(0.f, 0.f, 0.f);
-    if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
-    if (prim < 0) return tr;
-    Hit h;
-    uint32_t mat;
-    int light;
-    vpt_hit(s, prim, tmax, b1, b2, o, d, &h, &mat, &light);
-    surface_media(s, prim, medium, &m_in, &m_out);
-    pos = h.pos;
-    perr = h.perr;
-    abs_n = h.abs_n;
-    n = h.n;
-  }
-  return mk(0.f, 0.f, 0.f);
-}
-
-// Scene::IntersectTr (visual/Scene.cpp:14-26): the first surface with a
-// material along the ray and the transmittance up to it. The segment after a
-// surface of no material starts at its hit position (Triangle::Intersect's
-// barycentric point, no offset) in the inside medium of its interface, as
-// the reference's record of an unqueried hit gives.
-template <int W>
-GYT_D bool vpt_intersect_tr(const DevScene& s, float3 o, float3 d, int medium, int* prim_out, float* t_out,
-                            float* b1_out, float* b2_out, float3* o_out, float3* tr_out) {
-  float3 tr = mk(1.f, 1.f, 1.f);
-#pragma unroll 1
-  for (int hop = 0; hop < 64; ++hop) {
-    float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
-    const int prim = vpt_trace<W>(s, o, d, tmax, b1, b2);
-    if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
-    if (prim < 0) {
-      *tr_out = tr;
-      return false;
-    }
-    if (material_type(s, prim) != 5u || prim >= s.n_tris) {
-      *prim_out = prim;
-      *t_out = tmax;
-      *b1_out = b1;
-      *b2_out = b2;
-      *o_out = o;
-      *tr_out = tr;
-      return true;
-    }
-    float3 p0, p1, p2, n0, n1, n2, face;
-    int m, light;
-    load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, &light);
-    const float3 pos = p0 * (1.f - b1 - b2) + p1 * b1 + p2 * b2;
-    int in, out;
-    surface_media(s, prim, medium, &in, &out);
-    medium = in;
-    o = pos + d * kRayEps;
-  }
-  *tr_out = mk(0.f, 0.f, 0.f);
-  return false;
-}
-
-// Integrator::DirectIllumination with handleMedia (integrator/Integrator.cpp:9-107),
-// called (not inlined) from the medium and the surface branch: one copy of its
-// code, which the instruction cache holds better.
-// for a surface point (bsdf) or a medium point (phase g). u: uLight, u.y, u.x,
-// v.z, v.y, v.x as the caller draws them.
-template <int W>
-__device__ __noinline__ float3 vpt_direct(const DevScene& s, const VPoint& p, const Bsdf* bsdf, float g, float ul, float ux,
-                                          float uy, float vx, float vy, float vz) {
-  if (s.n_lights <= 0) return mk(0.f, 0.f, 0.f);
-  float lsel = 0.f;
-  const int li = sample_light(s, ul, &lsel);
-  if (!(lsel > 0.f) || li >= s.n_area) return mk(0.f, 0.f, 0.f);
-  const LightTri l = load_light(s, li);
-  float3 L1 = mk(0.f, 0.f, 0.f), L2 = mk(0.f, 0.f, 0.f);
-  float w1 = 1.f, w2 = 1.f;
-  {
-    // AreaLight::Sample_Li -> Shape::Sample(ref) -> Triangle::Sample
-    const float su0 = sqrtf(ux);
-    const float bb0 = 1.f - su0, bb1 = uy * su0, bb2 = 1.f - bb0 - bb1;
-    const float3 lpos = l.p0 * bb0 + l.p1 * bb1 + l.p2 * bb2;
-    const float3 ln = l.n0 * bb0 + l.n1 * bb1 + l.n2 * bb2;
-    const float3 lerr = (vabs(l.p0 * bb0) + vabs(l.p1 * bb1) + vabs(l.p2 * bb2)) * gammaf(6);
-    float pdf = 1.f / l.area;
-    float3 w = p.pos - lpos;
-    if (length(w) == 0.f) {
-      pdf = 0.f;
-    } else {
-      w = norm(w);
-      pdf *= dot(p.pos - lpos, p.pos - lpos) / fabsf(dot(ln, -w));
-      if (isinf(pdf)) pdf = 0.f;
-    }
-    const float3 wi = norm(lpos - p.pos);
-    const float3 Li = dot(ln, -wi) > 0.f ? l.Le : mk(0.f, 0.f, 0.f);
-    if (pdf > 0.f && !is_zero(Li)) {
-      float spdf, cos_t = 1.f;
-      float3 f;
-      if (p.surface) {
-        spdf = bsdf->pdf(p.wo, wi);
-        f = bsdf->eval(p.wo, wi);
-        cos_t = fabsf(dot(p.n, wi));
-      } else {
-        const float ph = phase_hg(dot(p.wo, wi), g);
-        f = mk(ph, ph, ph);
-        spdf = ph;
-      }
-      if (!is_zero(f)) {
-        const float3 tr = vpt_tr<W>(s, p, lpos, lerr, l.face);
-        w1 = power_heuristic(pdf, spdf);
-        L1 = Li * tr * f * cos_t / pdf;
-      }
-    }
-  }
-  {
-    float3 wi, f;
-    float pdf, cos_t = 1.f;
-    if (p.surface) {
-      f = bsdf->sample(p.wo, &wi, &pdf, vx, vy, vz);
-      cos_t = fabsf(dot(p.n, wi));
-    } else {
-      const float ph = phase_sample(g, p.wo, vx, vy, &wi);
-      f = mk(ph, ph, ph);
-      pdf = ph;
-    }
-    if (pdf != 0.f && !is_zero(f)) {
-      // Intersection::SpawnRay (visual/Intersection.h:74-78)
-      const float3 o2 = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
-      Hit hh;
-      hh.pos = p.pos;
-      hh.perr = p.perr;
-      hh.abs_n = p.abs_n;
-      hh.n = p.n;
-      const float lpdf = tri_light_pdf(l, hh, o2, wi);
-      if (lpdf == 0.f) {
-        w2 = 0.f;
-      } else {
-        w2 = power_heuristic(pdf, lpdf);
-        int prim = -1;
-        float t = 0.f, b1 = 0.f, b2 = 0.f;
-        float3 ro, tr;
-        if (vpt_intersect_tr<W>(s, o2, wi, p.medium_along(wi), &prim, &t, &b1, &b2, &ro, &tr) && prim < s.n_tris &&
-            __float_as_int(__ldg(&s.tnrm[3 * prim + 1].w)) == li) {
-          Hit lh;
-          uint32_t mat;
-          int light;
-          vpt_hit(s, prim, t, b1, b2, ro, wi, &lh, &mat, &light);
-          if (dot(lh.n, -wi) > 0.f) L2 = l.Le * f * tr * cos_t / pdf;  // AreaLight::Emission(isect, -wi)
-        }
-      }
-    }
-  }
-  return (L1 * w1 + L2 * w2) / lsel;
-}
-
-// The light point of an equi-angular bounce: AreaLight::SampleOnePoint ->
-// Triangle::Sample (light/AreaLight.h:54-58, shape/Triangle.cpp:141-158) for
-// the light drawn with u = (ux, uy): position, interpolated normal (not
-// normalised), position error; the area pdf is 1 / area.
+// A point on light l for the sample numbers u = (ux, uy): Triangle::Sample
+// (shape/Triangle.cpp:141-158) as AreaLight::SampleOnePoint
+// (light/AreaLight.h:54-58) and Shape::Sample(ref) (shape/Shape.cpp:6-19) take
+// it: position, interpolated normal (not normalised), position error; the
+// area pdf is 1 / area.
 struct LightPoint {
   float3 pos, n, err;
 };
@@ -1999,247 +1813,413 @@ GYT_D LightPoint light_point(const LightTri& l, float ux, float uy) {
   return q;
 }
 
-// VolPathTracing::ConnectToLight (integrator/VPT.cpp:108-146) from the medium
-// point p to the bounce's light point of light li: the phase function toward
-// the light, the transmittance of the segment (VisibilityTester::Tr), the
-// cosine at the light and the inverse squared distance, over the area pdf.
-// Only the light-sampling term: the reference computes an MIS weight but
-// returns L1 unweighted. Called (not inlined), like vpt_direct.
-template <int W>
-__device__ __noinline__ float3 vpt_connect(const DevScene& s, const VPoint& p, float g, int li, float ux, float uy) {
-  const LightTri l = load_light(s, li);
-  const LightPoint q = light_point(l, ux, uy);
-  const float3 dir = p.pos - q.pos;
-  const float3 wi = -norm(dir);
-  float cos_t = 1.f;
-  if (!is_zero(q.n)) {
-    cos_t = dot(norm(dir), q.n);
-    if (cos_t < 0.f) return mk(0.f, 0.f, 0.f);
-  }
-  const float ph = phase_hg(dot(p.wo, wi), g);
-  const float3 tr = vpt_tr<W>(s, p, q.pos, q.err, l.face);
-  const float pdf = 1.f / l.area;
-  return l.Le * ph * tr * cos_t / dot(dir, dir) / pdf;
+// ----------------------------------------------- volumetric wavefront ---
+// VolPathTracing as a wavefront over the path pool: the path tracer's
+// k_generate, k_extend and k_finish around three kernels of its own. Per
+// bounce k_vshade samples the medium (distance or equi-angular sampling),
+// gathers direct light by queueing a shadow segment (a transmittance walk to
+// the light point) and an MIS ray (a walk to the first surface with a
+// material), and samples the continuation; k_vshadow and k_vmis walk the
+// queued rays and add what they carry to the path's radiance. Each kernel is
+// small and its warps run one kind of work, where the single persistent
+// kernel spent its time on instruction fetch and on a spilled 1.2 KB frame.
+// Path slot fields beyond the path tracer's: o.w = medium + 1 and d.w = the
+// material-less surfaces crossed, both as integer bits (0 for a new camera
+// path: no medium, none crossed).
+//
+// Shadow segment entry (q.so, q.sd, q.sc, q.madd): (origin, segment length),
+// (direction, medium bits), (contribution without the transmittance, path
+// slot bits), (light bits, ux, uy, -): the light point, recomputed at every
+// hop. MIS ray entry (q.mo, q.md, q.mc): (origin, medium bits), (direction,
+// light bits), (contribution without emission and transmittance, slot bits).
+GYT_D int vmedium(float w) { return (int)__float_as_uint(w) - 1; }
+GYT_D float vmedium_bits(int m) { return __uint_as_float((uint32_t)(m + 1)); }
+
+// The first segment of VisibilityTester::Tr (visual/Visibility.cpp:13-30)
+// from p to the light point (Intersection::SpawnTo, visual/Intersection.h:64-72),
+// queued with its contribution c.
+GYT_D void queue_vshadow(const Queues& q, const VPoint& p, const LightTri& l, const LightPoint& lp, int li, float ux,
+                         float uy, float3 c, uint32_t slot) {
+  const float3 org = offset_origin(p.pos, p.perr, p.abs_n, lp.pos - p.pos);
+  const float3 tgt = offset_origin(lp.pos, lp.err, l.face, org - lp.pos);
+  float3 d = tgt - org;
+  const float dis = length(d);
+  d = d / dis;
+  const int medium = dot(d, p.n) > 0.f ? p.m_out : p.m_in;
+  const float3 o = org + d * kRayEps;
+  const uint32_t j = queue_slot(q.counts);
+  q.so[j] = make_float4(o.x, o.y, o.z, dis - kShadowEps);
+  q.sd[j] = make_float4(d.x, d.y, d.z, vmedium_bits(medium));
+  q.sc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(slot));
+  q.madd[j] = make_float4(__int_as_float(li), ux, uy, 0.f);
 }
 
-// One camera sample per thread (grid-stride over the render's samples, or the
-// listed (x, y, s) of xys); film as gyt_render_device's, L_out/cursor_out for
-// parity tests. Capped at four blocks per SM (64 registers, a few spills) and
-// launched as one persistent wave: the kernel is bound by divergence and
-// instruction fetch, not by memory. On the Cornell box in fog (binary BVH):
-// 69 Mpaths/s with a whole path per loop pass, 89 with regeneration, 112 with
-// four blocks per SM in a single wave.
+// Integrator::DirectIllumination with handleMedia (integrator/Integrator.cpp:9-107)
+// at p, queued: the light half as a shadow segment, the BSDF/phase half as an
+// MIS ray. u: uLight, u.y, u.x, v.z, v.y, v.x as the caller draws them.
+GYT_D void vpt_direct_queue(const DevScene& s, const Queues& q, const VPoint& p, const Bsdf* bsdf, float g, float3 tp,
+                            uint32_t slot, float ul, float ux, float uy, float vx, float vy, float vz) {
+  if (s.n_lights <= 0) return;
+  float lsel = 0.f;
+  const int li = sample_light(s, ul, &lsel);
+  if (!(lsel > 0.f) || li >= s.n_area) return;
+  const LightTri l = load_light(s, li);
+  {
+    // AreaLight::Sample_Li -> Shape::Sample(ref) -> Triangle::Sample
+    const LightPoint lp = light_point(l, ux, uy);
+    float pdf = 1.f / l.area;
+    float3 w = p.pos - lp.pos;
+    if (length(w) == 0.f) {
+      pdf = 0.f;
+    } else {
+      w = norm(w);
+      pdf *= dot(p.pos - lp.pos, p.pos - lp.pos) / fabsf(dot(lp.n, -w));
+      if (isinf(pdf)) pdf = 0.f;
+    }
+    const float3 wi = norm(lp.pos - p.pos);
+    const float3 Li = dot(lp.n, -wi) > 0.f ? l.Le : mk(0.f, 0.f, 0.f);
+    if (pdf > 0.f && !is_zero(Li)) {
+      float spdf, cos_t = 1.f;
+      float3 f;
+      if (p.surface) {
+        spdf = bsdf->pdf(p.wo, wi);
+        f = bsdf->eval(p.wo, wi);
+        cos_t = fabsf(dot(p.n, wi));
+      } else {
+        const float ph = phase_hg(dot(p.wo, wi), g);
+        f = mk(ph, ph, ph);
+        spdf = ph;
+      }
+      if (!is_zero(f)) {
+        const float w1 = power_heuristic(pdf, spdf);
+        queue_vshadow(q, p, l, lp, li, ux, uy, tp * (Li * f * cos_t / pdf * w1 / lsel), slot);
+      }
+    }
+  }
+  float3 wi, f;
+  float pdf, cos_t = 1.f;
+  if (p.surface) {
+    f = bsdf->sample(p.wo, &wi, &pdf, vx, vy, vz);
+    cos_t = fabsf(dot(p.n, wi));
+  } else {
+    const float ph = phase_sample(g, p.wo, vx, vy, &wi);
+    f = mk(ph, ph, ph);
+    pdf = ph;
+  }
+  if (pdf != 0.f && !is_zero(f)) {
+    // Intersection::SpawnRay (visual/Intersection.h:74-78)
+    const float3 o2 = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
+    Hit hh;
+    hh.pos = p.pos;
+    hh.perr = p.perr;
+    hh.abs_n = p.abs_n;
+    hh.n = p.n;
+    const float lpdf = tri_light_pdf(l, hh, o2, wi);
+    if (lpdf != 0.f) {
+      const float w2 = power_heuristic(pdf, lpdf);
+      const float3 c = tp * (f * cos_t / pdf * w2 / lsel);
+      const uint32_t j = queue_slot(q.counts + 1);
+      q.mo[j] = make_float4(o2.x, o2.y, o2.z, vmedium_bits(p.medium_along(wi)));
+      q.md[j] = make_float4(wi.x, wi.y, wi.z, __int_as_float(li));
+      q.mc[j] = make_float4(c.x, c.y, c.z, __uint_as_float(slot));
+    }
+  }
+}
+
+// One bounce of VolPathTracing::Li (integrator/VPT.cpp:13-101) for path slot
+// i, whose closest hit k_extend left in q.hit.
 //
 // EQUI: VolPathTracing with equi-angular sampling (its constructor's default,
 // integrator/VPT.h:13-15): every bounce draws one light and one point on it
 // (VPT.cpp:22-27); a ray through a medium samples its scattering distance
 // equi-angularly about that point (HomogeneousMedium::EquiAngularSampling,
 // volume/Homogeneous.cpp:38-64), and a medium point gathers light only by the
-// connection to that point (ConnectToLight, VPT.cpp:108-146).
+// connection to that point (ConnectToLight, VPT.cpp:108-146), queued as a
+// shadow segment. The light point is recomputed from its two numbers where it
+// is used rather than kept.
 template <int W, bool EQUI>
-__global__ void __launch_bounds__(kBlock, 4) k_vpt(DevScene s, Cam cam, Params prm, SamplerTables tab,
-                                                unsigned long long n, const uint32_t* __restrict__ xys,
-                                                double* __restrict__ film, float* __restrict__ L_out,
-                                                uint32_t* __restrict__ cursor_out) {
-  // Path regeneration: every pass of the loop is one bounce of each lane's
-  // path; a lane whose path ended starts its next sample (grid stride) on the
-  // next pass instead of idling until the warp's longest path is done.
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kBlock) k_vshade(PathBuf cur, uint32_t n, DevScene s, Params prm, Queues q,
+                                                   SamplerTables tab) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 h4 = q.hit[i];
+  const int prim = __float_as_int(h4.w);
+  const float tmax = h4.x;
+  const uint32_t meta = cur.meta[i];
+  uint32_t depth = meta & 255u;
+  bool delta = (meta >> 8) & 1u;
+  Rng rng{cur.sidx[i], (meta >> 9) & 2047u};
+  const float4 o4 = cur.o[i], d4 = cur.d[i];
+  float3 o = f3(o4);
+  const float3 d = f3(d4);
+  int medium = vmedium(o4.w);
+  uint32_t crossings = __float_as_uint(d4.w);
+  float3 tp = f3(cur.tp[i]);
+  float3 nd = d;
   const uint32_t dim_limit = prm.sampler ? kHaltonDims : 1024u;
-  bool alive = false;
-  uint32_t x = 0, y = 0;
-  bool u_zero = false, v_zero = false;
-  Rng rng{0, 0};
-  float3 o = mk(0.f, 0.f, 0.f), d = o, tp = o, L = o;
-  int medium = -1, i = 0, crossings = 0;
-  bool delta = false;
-  for (;;) {
-    if (!alive) {
-      if (t >= n) break;
-      uint32_t sm;
-      if (xys) {
-        x = xys[3 * t];
-        y = xys[3 * t + 1];
-        sm = xys[3 * t + 2];
-      } else {
-        const unsigned long long pixel = t / prm.spp;
-        sm = (uint32_t)(t - pixel * prm.spp);
-        y = (uint32_t)(pixel / cam.res_x);
-        x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
-      }
-      // the camera sample (TiledIntegrator::Render, integrator/TiledIntegrator.cpp:40-47)
-      const bool halton = cam.sampler != 0;
-      const uint64_t idx = halton ? halton_enum_index(cam, sm, x, y) : enum_index(tab, cam.log2_res, sm, x, y);
-      rng = Rng{idx, 0};
-      const float su = rng.next(tab, cam.sampler), sv = rng.next(tab, cam.sampler);
-      const float u = __fsub_rn(__fmul_rn(halton ? cam.h_sx : cam.res_pow2, su), (float)x);
-      const float v = __fsub_rn(__fmul_rn(halton ? cam.h_sy : cam.res_pow2, sv), (float)y);
-      u_zero = u == 0.f;
-      v_zero = v == 0.f;
-      camera_ray(cam, __fadd_rn((float)x, u), __fadd_rn((float)y, v), &o, &d);
-      medium = -1;  // the camera's medium (PinHoleCamera::GenerateRay: none)
-      tp = mk(1.f, 1.f, 1.f);
-      L = mk(0.f, 0.f, 0.f);
-      delta = false;
-      i = 0;
-      crossings = 0;
-      alive = true;
-    }
-    // one bounce of VolPathTracing::Li (integrator/VPT.cpp:13-101)
-    bool end = rng.cursor + 16u > dim_limit;  // the sampler's dimensions are spent
-    if (!end) {
-      float tmax = __int_as_float(0x7f800000), hb1 = 0.f, hb2 = 0.f;
-      const int prim = vpt_trace<W>(s, o, d, tmax, hb1, hb2);
-      bool scattered = false;
-      float3 mpos = o;
-      float g = 0.f;
-      int eli = 0;  // EQUI: the bounce's light, its selection probability and point sample
-      float elsel = 0.f, eux = 0.f, euy = 0.f;
-      if (EQUI) {
-        // VPT.cpp:23-24: Scene::SampleOneLight, then SampleOnePoint's
-        // Vec2(rand(), rand()) in right-to-left order
-        const float ul = rng.next(tab, prm.sampler);
-        euy = rng.next(tab, prm.sampler);
-        eux = rng.next(tab, prm.sampler);
-        eli = sample_light(s, ul, &elsel);
-        if (medium >= 0) {
-          // HomogeneousMedium::EquiAngularSampling (volume/Homogeneous.cpp:38-64):
-          // t in [0, 3] along the ray with density proportional to the inverse
-          // squared distance to the light point
-          const MediumDev md = load_medium(s, medium);
-          g = md.g;
-          const float u = rng.next(tab, prm.sampler);
-          const float3 lpos = light_point(load_light(s, eli), eux, euy).pos;
-          const float dl = dot(lpos - o, d);
-          const float D = length(o + d * dl - lpos);
-          const float ta = atan2f(0.f - dl, D), tb = atan2f(3.f - dl, D);
-          const float tau = D * tanf((1.f - u) * ta + u * tb);
-          const float tt = dl + tau;
-          scattered = tt < tmax;
-          if (scattered) {
-            const float3 tr = mk(expf(-md.st.x * tt), expf(-md.st.y * tt), expf(-md.st.z * tt));
-            const float pdf = D / ((tb - ta) * (D * D + tau * tau));
-            tp = tp * (tr * md.ss / pdf);
-            mpos = o + d * tt;
-          } else {
-            const float pdf = 1.f - (atan2f(fminf(3.f, tmax) - dl, D) - ta) / (tb - ta);
-            tp = tp * (medium_tr(md, tmax, length(d)) / pdf);
-          }
-        }
-      } else if (medium >= 0) {
-        // HomogeneousMedium::Sample (volume/Homogeneous.cpp:12-30)
+  bool end = rng.cursor + 16u > dim_limit;  // the sampler's dimensions are spent
+  if (!end) {
+    bool scattered = false;
+    float3 mpos = o;
+    float g = 0.f;
+    int eli = 0;  // EQUI: the bounce's light, its selection probability and point sample
+    float elsel = 0.f, eux = 0.f, euy = 0.f;
+    if (EQUI) {
+      // VPT.cpp:23-24: Scene::SampleOneLight, then SampleOnePoint's
+      // Vec2(rand(), rand()) in right-to-left order
+      const float ul = rng.next(tab, prm.sampler);
+      euy = rng.next(tab, prm.sampler);
+      eux = rng.next(tab, prm.sampler);
+      eli = sample_light(s, ul, &elsel);
+      if (medium >= 0) {
+        // HomogeneousMedium::EquiAngularSampling (volume/Homogeneous.cpp:38-64)
         const MediumDev md = load_medium(s, medium);
         g = md.g;
-        const float uc = rng.next(tab, prm.sampler), ud = rng.next(tab, prm.sampler);
-        const int ch = min((int)(uc * 3.f), 2);
-        const float sc = ch == 0 ? md.st.x : (ch == 1 ? md.st.y : md.st.z);
-        const float dist = -logf(1.f - ud) / sc;
-        const float dl = length(d);
-        const float tt = fminf(dist / dl, tmax);
+        const float u = rng.next(tab, prm.sampler);
+        const float3 lpos = light_point(load_light(s, eli), eux, euy).pos;
+        const float dl = dot(lpos - o, d);
+        const float D = length(o + d * dl - lpos);
+        const float ta = atan2f(0.f - dl, D), tb = atan2f(3.f - dl, D);
+        const float tau = D * tanf((1.f - u) * ta + u * tb);
+        const float tt = dl + tau;
         scattered = tt < tmax;
-        const float tc = fminf(tt, FLT_MAX);  // Exp(-sigma_t * min(t, MaxReal) * |d|)
-        const float3 tr = mk(expf((-md.st.x * tc) * dl), expf((-md.st.y * tc) * dl), expf((-md.st.z * tc) * dl));
-        const float3 dens = scattered ? md.st * tr : tr;
-        float pdf = ((0.f + dens.x) + dens.y) + dens.z;
-        pdf *= 1.f / 3.f;
-        if (pdf == 0.f) pdf = 1.f;
-        tp = tp * (scattered ? tr * md.ss / pdf : tr / pdf);
-        if (scattered) mpos = o + d * tt;
-      }
-      VPoint p;
-      Bsdf bsdf;
-      bool gather = false, pass = false;
-      if (is_zero(tp)) {
-        end = true;
-      } else if (scattered) {
-        p.pos = mpos;
-        p.perr = p.abs_n = p.n = mk(0.f, 0.f, 0.f);
-        p.wo = -d;
-        p.m_in = p.m_out = medium;
-        p.surface = false;
-        gather = true;
-      } else if (prim < 0) {
-        end = true;  // no environment light with media
-      } else {
-        Hit h;
-        uint32_t mat;
-        int light;
-        vpt_hit(s, prim, tmax, hb1, hb2, o, d, &h, &mat, &light);
-        surface_media(s, prim, medium, &p.m_in, &p.m_out);
-        p.pos = h.pos;
-        p.perr = h.perr;
-        p.abs_n = h.abs_n;
-        p.n = h.n;
-        p.wo = h.wo;
-        p.surface = true;
-        if (__ldg(s.mtypes + mat) == 5u) {
-          // no BSDF: pass through without using a bounce (VPT.cpp:70-75)
-          pass = true;
-          o = offset_origin(h.pos, h.perr, h.abs_n, d) + d * kRayEps;
-          medium = dot(d, h.n) > 0.f ? p.m_out : p.m_in;
-          if (++crossings > 64) end = true;
-        } else {
-          bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
-          bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
-          if ((i == 0 || delta) && light >= 0) {
-            if (dot(h.n, h.wo) > 0.f) L = L + tp * load_light(s, light).Le;
-          } else {
-            gather = true;
-          }
-        }
-      }
-      if (EQUI && gather && scattered) {
-        // VPT.cpp:36: the connection to the bounce's light point
-        if (elsel > 0.f) L = L + tp * vpt_connect<W>(s, p, g, eli, eux, euy) / elsel;
-      } else if (gather) {
-        // one call site for surface and medium points
-        const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
-        const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
-        const float ul = rng.next(tab, prm.sampler);
-        L = L + tp * vpt_direct<W>(s, p, scattered ? nullptr : &bsdf, g, ul, ux, uy, vx, vy, vz);
-      }
-      if (!end && !pass) {
         if (scattered) {
-          const float py = rng.next(tab, prm.sampler), px = rng.next(tab, prm.sampler);
-          float3 wi;
-          phase_sample(g, -d, px, py, &wi);
-          o = mpos + wi * kRayEps;  // MediumIntersection::SpawnRay: no offset
-          d = wi;
-          delta = false;
+          const float3 tr = mk(expf(-md.st.x * tt), expf(-md.st.y * tt), expf(-md.st.z * tt));
+          const float pdf = D / ((tb - ta) * (D * D + tau * tau));
+          tp = tp * (tr * md.ss / pdf);
+          mpos = o + d * tt;
         } else {
-          const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
-          float3 wi;
-          float pdf;
-          const float3 f = bsdf.sample(p.wo, &wi, &pdf, rx, ry, rz);
-          if (is_zero(f) || pdf == 0.f) {
-            end = true;
-          } else {
-            tp = tp * (f * fabsf(dot(p.n, wi)) / pdf);
-            delta = bsdf.lobe.delta();
-            o = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
-            d = wi;
-            medium = dot(wi, p.n) > 0.f ? p.m_out : p.m_in;
-          }
+          const float pdf = 1.f - (atan2f(fminf(3.f, tmax) - dl, D) - ta) / (tb - ta);
+          tp = tp * (medium_tr(md, tmax, length(d)) / pdf);
         }
-        if (!end && ++i >= (int)prm.max_depth) end = true;
+      }
+    } else if (medium >= 0) {
+      // HomogeneousMedium::Sample (volume/Homogeneous.cpp:12-30)
+      const MediumDev md = load_medium(s, medium);
+      g = md.g;
+      const float uc = rng.next(tab, prm.sampler), ud = rng.next(tab, prm.sampler);
+      const int ch = min((int)(uc * 3.f), 2);
+      const float sc = ch == 0 ? md.st.x : (ch == 1 ? md.st.y : md.st.z);
+      const float dist = -logf(1.f - ud) / sc;
+      const float dlen = length(d);
+      const float tt = fminf(dist / dlen, tmax);
+      scattered = tt < tmax;
+      const float tc = fminf(tt, FLT_MAX);  // Exp(-sigma_t * min(t, MaxReal) * |d|)
+      const float3 tr = mk(expf((-md.st.x * tc) * dlen), expf((-md.st.y * tc) * dlen), expf((-md.st.z * tc) * dlen));
+      const float3 dens = scattered ? md.st * tr : tr;
+      float pdf = ((0.f + dens.x) + dens.y) + dens.z;
+      pdf *= 1.f / 3.f;
+      if (pdf == 0.f) pdf = 1.f;
+      tp = tp * (scattered ? tr * md.ss / pdf : tr / pdf);
+      if (scattered) mpos = o + d * tt;
+    }
+    VPoint p;
+    Bsdf bsdf;
+    bool gather = false, pass = false;
+    if (is_zero(tp)) {
+      end = true;
+    } else if (scattered) {
+      p.pos = mpos;
+      p.perr = p.abs_n = p.n = mk(0.f, 0.f, 0.f);
+      p.wo = -d;
+      p.m_in = p.m_out = medium;
+      p.surface = false;
+      gather = true;
+    } else if (prim < 0) {
+      end = true;  // no environment light with media
+    } else {
+      Hit h;
+      uint32_t mat;
+      int light;
+      vpt_hit(s, prim, tmax, h4.y, h4.z, o, d, &h, &mat, &light);
+      surface_media(s, prim, medium, &p.m_in, &p.m_out);
+      p.pos = h.pos;
+      p.perr = h.perr;
+      p.abs_n = h.abs_n;
+      p.n = h.n;
+      p.wo = h.wo;
+      p.surface = true;
+      if (__ldg(s.mtypes + mat) == 5u) {
+        // no BSDF: pass through without using a bounce (VPT.cpp:70-75)
+        pass = true;
+        o = offset_origin(h.pos, h.perr, h.abs_n, d) + d * kRayEps;
+        medium = dot(d, h.n) > 0.f ? p.m_out : p.m_in;
+        if (++crossings > 64) end = true;
+      } else {
+        bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
+        bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
+        if ((depth == 0 || delta) && light >= 0) {
+          if (dot(h.n, h.wo) > 0.f) {
+            const float3 L = f3(cur.L[i]) + tp * load_light(s, light).Le;
+            cur.L[i] = make_float4(L.x, L.y, L.z, 0.f);
+          }
+        } else {
+          gather = true;
+        }
       }
     }
-    if (end) {
-      if (L_out) {
-        L_out[3 * t] = L.x;
-        L_out[3 * t + 1] = L.y;
-        L_out[3 * t + 2] = L.z;
+    if (EQUI && gather && scattered) {
+      // VPT.cpp:36: the connection to the bounce's light point
+      // (ConnectToLight, VPT.cpp:108-146) as a shadow segment
+      if (elsel > 0.f) {
+        const LightTri l = load_light(s, eli);
+        const LightPoint lp = light_point(l, eux, euy);
+        const float3 dir = p.pos - lp.pos;
+        const float3 wi = -norm(dir);
+        float cos_t = 1.f;
+        if (!is_zero(lp.n)) cos_t = dot(norm(dir), lp.n);
+        if (!(cos_t < 0.f)) {
+          const float ph = phase_hg(dot(p.wo, wi), g);
+          const float pdf = 1.f / l.area;
+          queue_vshadow(q, p, l, lp, eli, eux, euy, tp * (l.Le * ph * cos_t / dot(dir, dir) / pdf) / elsel, i);
+        }
       }
-      if (cursor_out) cursor_out[t] = rng.cursor;
-      if (film) {
-        film_add(film, cam.res_x, x, y, L);
-        if (u_zero && x > 0) film_add(film, cam.res_x, x - 1, y, L);
-        if (v_zero && y > 0) film_add(film, cam.res_x, x, y - 1, L);
-        if (u_zero && x > 0 && v_zero && y > 0) film_add(film, cam.res_x, x - 1, y - 1, L);
+    } else if (gather) {
+      // one call site for surface and medium points
+      const float vz = rng.next(tab, prm.sampler), vy = rng.next(tab, prm.sampler), vx = rng.next(tab, prm.sampler);
+      const float uy = rng.next(tab, prm.sampler), ux = rng.next(tab, prm.sampler);
+      const float ul = rng.next(tab, prm.sampler);
+      vpt_direct_queue(s, q, p, scattered ? nullptr : &bsdf, g, tp, i, ul, ux, uy, vx, vy, vz);
+    }
+    if (!end && !pass) {
+      if (scattered) {
+        const float py = rng.next(tab, prm.sampler), px = rng.next(tab, prm.sampler);
+        float3 wi;
+        phase_sample(g, -d, px, py, &wi);
+        o = mpos + wi * kRayEps;  // MediumIntersection::SpawnRay: no offset
+        nd = wi;
+        delta = false;
+      } else {
+        const float rz = rng.next(tab, prm.sampler), ry = rng.next(tab, prm.sampler), rx = rng.next(tab, prm.sampler);
+        float3 wi;
+        float pdf;
+        const float3 f = bsdf.sample(p.wo, &wi, &pdf, rx, ry, rz);
+        if (is_zero(f) || pdf == 0.f) {
+          end = true;
+        } else {
+          tp = tp * (f * fabsf(dot(p.n, wi)) / pdf);
+          delta = bsdf.lobe.delta();
+          o = offset_origin(p.pos, p.perr, p.abs_n, wi) + wi * kRayEps;
+          nd = wi;
+          medium = dot(wi, p.n) > 0.f ? p.m_out : p.m_in;
+        }
       }
-      alive = false;
-      t += stride;
+      if (!end && ++depth >= prm.max_depth) end = true;
+    }
+  }
+  if (!end) {
+    cur.o[i] = make_float4(o.x, o.y, o.z, vmedium_bits(medium));
+    cur.d[i] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(crossings));
+    cur.tp[i] = make_float4(tp.x, tp.y, tp.z, 0.f);
+  }
+  cur.meta[i] = meta_pack(depth, delta, rng.cursor, !end);
+}
+
+// The queued shadow segments: VisibilityTester::Tr (visual/Visibility.cpp:13-30),
+// segment after segment through surfaces of no material (a surface with a
+// material blocks), each attenuated by its medium; an unblocked walk adds its
+// contribution times the transmittance to the path. A hit at the very end of
+// a segment (the light's own surface) is settled in FP64, as the path
+// tracer's occlusion test settles it. Grid-stride over the queue.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_vshadow(PathBuf cur, DevScene s, Queues q) {
+  const uint32_t nq = *(volatile uint32_t*)q.counts;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
+    const float4 a = q.so[j], b = q.sd[j], c4 = q.sc[j], x = q.madd[j];
+    float3 o = f3(a), d = f3(b);
+    float seg = a.w;
+    int medium = vmedium(b.w);
+    const int li = __float_as_int(x.x);
+    float3 tr = mk(1.f, 1.f, 1.f);
+    bool lit = false;
+#pragma unroll 1
+    for (int hop = 0; hop < 64; ++hop) {
+      float tmax = seg, b1 = 0.f, b2 = 0.f;
+      int prim = trace<W, false>(s, o, d, tmax, b1, b2);
+      if (prim >= 0 && prim < s.n_tris && tmax >= seg * 0.999998f) {
+        const float4* tv = s.tris + 3 * (size_t)prim;
+        if (!wt_intersect_fp64(wt_setup(o, d), f3(__ldg(tv)), f3(__ldg(tv + 1)), f3(__ldg(tv + 2)), seg)) {
+          prim = -1;
+          tmax = seg;
+        }
+      }
+      if (prim >= 0 && material_type(s, prim) != 5u) break;  // blocked
+      if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(d));
+      if (prim < 0) {
+        lit = true;
+        break;
+      }
+      Hit h;
+      uint32_t mat;
+      int light;
+      vpt_hit(s, prim, tmax, b1, b2, o, d, &h, &mat, &light);
+      int m_in, m_out;
+      surface_media(s, prim, medium, &m_in, &m_out);
+      // the next segment: SpawnTo from the crossed surface to the light point
+      const LightTri l = load_light(s, li);
+      const LightPoint lp = light_point(l, x.y, x.z);
+      const float3 org = offset_origin(h.pos, h.perr, h.abs_n, lp.pos - h.pos);
+      const float3 tgt = offset_origin(lp.pos, lp.err, l.face, org - lp.pos);
+      d = tgt - org;
+      const float dis = length(d);
+      d = d / dis;
+      medium = dot(d, h.n) > 0.f ? m_out : m_in;
+      o = org + d * kRayEps;
+      seg = dis - kShadowEps;
+    }
+    if (lit) {
+      const uint32_t slot = __float_as_uint(c4.w);
+      const float3 L = f3(cur.L[slot]) + f3(c4) * tr;
+      cur.L[slot] = make_float4(L.x, L.y, L.z, 0.f);
+    }
+  }
+}
+
+// The queued MIS rays: Scene::IntersectTr (visual/Scene.cpp:14-26), the first
+// surface with a material along the ray and the transmittance up to it (a
+// passed surface restarts at its barycentric point in its inside medium); a
+// ray that reaches the sampled light's front adds its contribution times the
+// emission and the transmittance (Integrator.cpp:86-101). Grid-stride.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_vmis(PathBuf cur, DevScene s, Queues q) {
+  const uint32_t nq = *(volatile uint32_t*)(q.counts + 1);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
+    const float4 a = q.mo[j], b = q.md[j], c4 = q.mc[j];
+    float3 o = f3(a);
+    const float3 wi = f3(b);
+    int medium = vmedium(a.w);
+    const int li = __float_as_int(b.w);
+    float3 tr = mk(1.f, 1.f, 1.f);
+#pragma unroll 1
+    for (int hop = 0; hop < 64; ++hop) {
+      float tmax = __int_as_float(0x7f800000), b1 = 0.f, b2 = 0.f;
+      const int prim = trace<W, false>(s, o, wi, tmax, b1, b2);
+      if (medium >= 0) tr = tr * medium_tr(load_medium(s, medium), tmax, length(wi));
+      if (prim < 0) break;
+      if (material_type(s, prim) != 5u || prim >= s.n_tris) {
+        if (prim < s.n_tris && __float_as_int(__ldg(&s.tnrm[3 * prim + 1].w)) == li) {
+          Hit lh;
+          uint32_t mat;
+          int light;
+          vpt_hit(s, prim, tmax, b1, b2, o, wi, &lh, &mat, &light);
+          if (dot(lh.n, -wi) > 0.f) {  // AreaLight::Emission(isect, -wi)
+            const uint32_t slot = __float_as_uint(c4.w);
+            const float4* r = s.ltab + kLightRec * li;
+            const float3 Le = mk(__ldg(r).w, __ldg(r + 1).w, __ldg(r + 2).w);
+            const float3 L = f3(cur.L[slot]) + f3(c4) * Le * tr;
+            cur.L[slot] = make_float4(L.x, L.y, L.z, 0.f);
+          }
+        }
+        break;
+      }
+      float3 p0, p1, p2, n0, n1, n2, face;
+      int m, light;
+      load_leaf_tri(s, prim, &p0, &p1, &p2, &n0, &n1, &n2, &face, &m, &light);
+      const float3 pos = p0 * (1.f - b1 - b2) + p1 * b1 + p2 * b2;
+      int in, out;
+      surface_media(s, prim, medium, &in, &out);
+      medium = in;
+      o = pos + wi * kRayEps;
     }
   }
 }
@@ -2785,6 +2765,9 @@ int32_t run_light_tracing(gyt_context* ctx, const gyt_scene* scene, const GytCam
 
 // VolPathTracing (n == 0: every sample of the render into d_film; else the
 // listed (x, y, s) samples, radiance and dimensions used out).
+int32_t ensure_pool(gyt_context* ctx);
+unsigned long long wavefront_bound(unsigned long long total, uint32_t max_depth, uint32_t pool);
+
 int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
                    uint64_t n, const uint32_t* xys, double* d_film, float* L_out, uint32_t* cursor_out,
                    GytRenderStats* stats) {
@@ -2801,31 +2784,65 @@ int32_t run_volume(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
   const unsigned long long total = (unsigned long long)camera->res_x * camera->res_y * params->spp;
   const unsigned long long count = n ? n : total;
   GYT_CK(ctx, cudaSetDevice(ctx->device));
+  st = ensure_pool(ctx);
+  if (st) return st;
   GYT_CK(ctx, after_legacy_stream(ctx));
   const Params prm = make_params(params);
-  // persistent: the four resident blocks per SM of k_vpt, each lane taking
-  // samples until the grid stride runs past the end
-  const uint32_t grid = (uint32_t)std::min<unsigned long long>((count + kBlock - 1) / kBlock,
-                                                                (unsigned long long)std::max(1, ctx->sms) * 4);
-  GYT_CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  const SamplerTables tab = tables(ctx);
+  const DevScene& D = scene->dev;
+  const int W = D.wnodes ? 8 : 2;
   const bool equi = (params->flags & GYT_VOLUME_EQUI_ANGULAR) != 0;
-  auto launch = [&](auto kernel) {
-    kernel<<<grid, kBlock, 0, ctx->stream>>>(scene->dev, cam, prm, tables(ctx), count, xys, d_film, L_out, cursor_out);
-  };
-  if (scene->dev.wnodes) {
-    if (equi) launch(k_vpt<8, true>);
-    else launch(k_vpt<8, false>);
-  } else {
-    if (equi) launch(k_vpt<2, true>);
-    else launch(k_vpt<2, false>);
+  const int g_ext = ctx->pgrid[pindex(kPExtend, W, false)];
+  const int g_walk = std::max(1, ctx->sms) * 4;  // grid-stride walks over the queues
+  const Queues q = ctx->q;
+  const DebugOut dbg{L_out, cursor_out, nullptr, nullptr, nullptr};
+  cudaStream_t sm = ctx->stream;
+  // a crossing of a material-less surface takes a wavefront iteration without a bounce
+  const unsigned long long max_iters = wavefront_bound(count, params->max_depth + 65, ctx->capacity);
+  unsigned long long generated = 0;
+  uint32_t active = 0, iters = 0, launches = 0;
+  unsigned long long slots = 0;
+  int cur = 0;
+  GYT_CK(ctx, cudaEventRecord(ctx->ev0, sm));
+  while (generated < count || active > 0) {
+    const uint32_t n_new = (uint32_t)std::min<unsigned long long>(ctx->capacity - active, count - generated);
+    GYT_CK(ctx, cudaMemsetAsync(q.counts, 0, 8 * sizeof(uint32_t), sm));
+    const PathBuf P = ctx->pool[cur], N = ctx->pool[cur ^ 1];
+    if (n_new) {
+      k_generate<<<grid_for(n_new), kBlock, 0, sm>>>(P, active, n_new, generated, cam, params->spp, xys, tab);
+      ++launches;
+    }
+    generated += n_new;
+    active += n_new;
+    if (W == 8) {
+      k_extend<8, false><<<g_ext, kBlock, 0, sm>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+      if (equi) k_vshade<8, true><<<grid_for(active), kBlock, 0, sm>>>(P, active, D, prm, q, tab);
+      else k_vshade<8, false><<<grid_for(active), kBlock, 0, sm>>>(P, active, D, prm, q, tab);
+      k_vshadow<8><<<g_walk, kBlock, 0, sm>>>(P, D, q);
+      k_vmis<8><<<g_walk, kBlock, 0, sm>>>(P, D, q);
+    } else {
+      k_extend<2, false><<<g_ext, kBlock, 0, sm>>>(P, active, D, q.hit, q.counts + 2, nullptr);
+      if (equi) k_vshade<2, true><<<grid_for(active), kBlock, 0, sm>>>(P, active, D, prm, q, tab);
+      else k_vshade<2, false><<<grid_for(active), kBlock, 0, sm>>>(P, active, D, prm, q, tab);
+      k_vshadow<2><<<g_walk, kBlock, 0, sm>>>(P, D, q);
+      k_vmis<2><<<g_walk, kBlock, 0, sm>>>(P, D, q);
+    }
+    k_finish<<<grid_for(active), kBlock, 0, sm>>>(P, N, active, d_film, cam.res_x, q.counts + 5, q.madd, dbg);
+    launches += 5;
+    GYT_CK(ctx, cudaGetLastError());
+    GYT_CK(ctx, cudaMemcpyAsync(ctx->h_counter, q.counts, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, sm));
+    GYT_CK(ctx, cudaStreamSynchronize(sm));
+    slots += active;
+    active = ctx->h_counter[5];
+    cur ^= 1;
+    if (++iters > max_iters) return fail(ctx, GYT_ERR_WATCHDOG, "render_volume: wavefront iteration cap reached");
   }
-  GYT_CK(ctx, cudaGetLastError());
-  GYT_CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  GYT_CK(ctx, cudaEventRecord(ctx->ev1, sm));
   GYT_CK(ctx, cudaEventSynchronize(ctx->ev1));
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    *stats = GytRenderStats{count, 0, 1, 1, ms};
+    *stats = GytRenderStats{count, slots, iters, launches, ms};
   }
   return GYT_OK;
 }
@@ -4654,18 +4671,23 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
   }
   const GytBatchConfig saved = ctx->bcfg;
   const uint32_t saved_cap = ctx->capacity;
-  // one timed render (after an untimed one) per candidate
+  // per candidate one untimed render, then the median of three timed ones:
+  // a single timed render of the short sample varies by several per cent,
+  // enough to pick the wrong BVH width
   auto trial = [&](const GytBatchConfig& c, const gyt_scene* const* sc, float* mp) -> int32_t {
     ctx->bcfg = c;
     BatchInput in;
     int32_t st = batch_input(ctx, n, sc, cameras, prm.data(), fp.data(), &in);
     if (st) return st;
     GytRenderStats rs;
-    for (int k = 0; k < 2; ++k) {
+    float ms[3];
+    for (int k = 0; k < 4; ++k) {
       st = run_batch(ctx, in, &rs);
       if (st) return st;
+      if (k) ms[k - 1] = rs.ms;
     }
-    *mp = rs.ms > 0.f ? (float)(rs.paths / (rs.ms * 1e3)) : 0.f;
+    std::sort(ms, ms + 3);
+    *mp = ms[1] > 0.f ? (float)(rs.paths / (ms[1] * 1e3)) : 0.f;
     return GYT_OK;
   };
   GytBatchConfig cur = {saved_cap, 8, 0, 1, (uint32_t)(scenes[0] && scenes[0]->dev.wnodes ? 8 : 2)};
