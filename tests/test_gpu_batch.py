@@ -146,6 +146,26 @@ def test_batch_autotune(bctx, scs):
     _same(got, _per_scene(bctx, scs, DESCS))
 
 
+def test_batch_autotune_tries_both_widths(bctx, scs):
+    """With the same scenes built with the 8-wide BVH (on the device) as the
+    alternative, the autotuner picks a width; the batch renders with the
+    chosen scenes give each instance its per-scene film."""
+    c8 = g.Context(0, bvh_width=8)
+    try:
+        s8 = [g.Scene(sd, c8) for sd in DESCS]
+        cams, prms = [sd.camera for sd in DESCS], [sd.params for sd in DESCS]
+        cfg, mp = bctx.batch_autotune(scs, cams, prms, scenes_alt=s8, sample_spp=1)
+        assert mp > 0 and cfg["bvh_width"] in (2, 8)
+        chosen = s8 if cfg["bvh_width"] == 8 else scs
+        got, _ = _batch(bctx, chosen, DESCS)
+        bctx.set_batch_config()
+        _same(got, _per_scene(bctx, chosen, DESCS))
+        for sc in s8:
+            sc.close()
+    finally:
+        c8.close()
+
+
 def test_batch_more_instances_than_one_group(bctx):
     # more instances than the constant-memory table holds: consecutive groups
     descs = [scenes.cornell_box(res=8, spp=1 + k % 3, max_depth=3, spheres=bool(k % 2)) for k in range(150)]
