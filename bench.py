@@ -537,7 +537,7 @@ def measure_batch(a, d, g, torch):
     paths = sum(sd.n_paths() for sd in descs)
 
     t = time.perf_counter()
-    cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=1)
+    cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=8)
     tune_s = time.perf_counter() - t
     # both integrators render the scenes of the width the autotuner chose
     scs = scs8 if cfg["bvh_width"] == 8 else scs2
@@ -624,8 +624,9 @@ def measure_batch(a, d, g, torch):
                 "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s,
                              "widths_tried": [2, 8],
                              "note": "coordinate search over BVH width (binary and 8-wide scenes, both built on "
-                                     "the device), pool size, grid-stride and traversal blocks per SM on a 1-spp "
-                                     "sample; the per-scene renders use the chosen width too"},
+                                     "the device), pool size, grid-stride and traversal blocks per SM on a sample "
+                                     "of every instance at spp x 8 / 64 (the batch's mix), median of three renders "
+                                     "per candidate; the per-scene renders use the chosen width too"},
                 "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": imgs_bytes, "steps": e2e_steps,
                         "note": "gyt_render_batch with the scenes resident: cameras and parameters in, "

@@ -433,7 +433,9 @@ int32_t gyt_render_batch_device(gyt_context* ctx, uint32_t n, const gyt_scene* c
 int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes, const GytCamera* cameras,
                          const GytRenderParams* params, float* const* rgb_out);
 /* Autotuner: times batched renders of the given instances with at most
- * sample_spp samples per pixel (0 = 1) over pool sizes, grid shapes and, when
+ * sample_spp samples per pixel (0 = 1; each instance's spp scaled by
+ * sample_spp / the batch's largest spp, at least 1, so that the sample keeps
+ * the batch's mix of instances) over pool sizes, grid shapes and, when
  * scenes_alt (the same scenes built with the other BVH width) is given, the
  * BVH width; sets the fastest configuration on the context and returns it in
  * *best with its throughput in *best_mpaths (Mpaths/s; may be NULL). */
