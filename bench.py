@@ -465,7 +465,8 @@ def measure_single(a, d, g, torch):
         ctx.render_device(scene, cam, prm, film.data_ptr())
         cnt = ctx.read_profile()
         ctx.set_profile(0)
-        out = roofline(prof, cnt, stats[-1]["path_slots"], node_bytes=80 if a.bvh_width == 8 else 64)
+        out = roofline(prof, cnt, stats[-1]["path_slots"], paths // a.steps,
+                       node_bytes=80 if a.bvh_width == 8 else 64)
         line = {"metric": METRIC_SINGLE, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh, no dataset)",
@@ -585,11 +586,13 @@ def measure_batch(a, d, g, torch):
     e2e_steps = max(1, min(a.steps, 2))
     imgs_bytes = sum(c.res_x * c.res_y * 3 * 4 for c in cams)
     h2d = len(descs) * (ctypes.sizeof(_c().GytCamera) + ctypes.sizeof(_c().GytRenderParams))
-    ctx.render_batch(scs, cams, prms)
+    # the images land in pinned host buffers that the steps reuse
+    imgs = [torch.empty((c.res_y, c.res_x, 3), dtype=torch.float32, pin_memory=True).numpy() for c in cams]
+    ctx.render_batch(scs, cams, prms, out=imgs)
     d.barrier()
     t = time.perf_counter()
     for _ in range(e2e_steps):
-        ctx.render_batch(scs, cams, prms)
+        ctx.render_batch(scs, cams, prms, out=imgs)
     e2e_s = d.max(time.perf_counter() - t) / e2e_steps
 
     line = None
@@ -606,7 +609,7 @@ def measure_batch(a, d, g, torch):
         per_scene()
         cnt = ctx.read_profile()
         ctx.set_profile(0)
-        out = roofline(prof, cnt, prof["rays"]["extend"], node_bytes=80 if cfg["bvh_width"] == 8 else 64)
+        out = roofline(prof, cnt, prof["rays"]["extend"], paths, node_bytes=80 if cfg["bvh_width"] == 8 else 64)
         out["rays_match_counting_pass"] = prof["rays"] == cnt["rays"]
         value = paths * d.world / (b_ms / 1e3) / 1e6
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
@@ -630,7 +633,8 @@ def measure_batch(a, d, g, torch):
                 "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": imgs_bytes, "steps": e2e_steps,
                         "note": "gyt_render_batch with the scenes resident: cameras and parameters in, "
-                                "every image copied to host memory"},
+                                "films zeroed, every image resolved and copied to pinned host buffers "
+                                "that the steps reuse"},
                 "gpu_launches": launches, "graph_launches": a.steps,
                 "iterations_per_step": stats[-1]["iterations"],
                 "roofline": out, "rays_per_s": rays_per_s(prof, b_ms / d.world),
@@ -849,11 +853,12 @@ def measure_adjoint(a, d, g, torch):
 STATE_READ, STATE_WRITE, HIT, RAY, CONTRIB = 76, 68, 16, 32, 16
 
 
-def kernel_bytes(kernel, prof, cnt, slots, node_bytes):
+def kernel_bytes(kernel, prof, cnt, slots, node_bytes, gen_paths):
     """Algorithmic bytes of all launches of one kernel in a profiled render:
     traversal bytes per ray = BVH nodes x node size + triangle tests x 48 B
     (counts from the counting pass) on top of the ray and hit records; the
-    shade, finish and generate kernels by their path-state records."""
+    shade and finish kernels by the path-state records of the slots they
+    visit, the generate kernel by those of the gen_paths paths it writes."""
     rays = cnt["rays"]
 
     def trav(k):
@@ -868,10 +873,10 @@ def kernel_bytes(kernel, prof, cnt, slots, node_bytes):
         return slots * (STATE_READ + HIT + STATE_WRITE) + (rays["shadow"] + rays["mis"]) * (RAY + CONTRIB)
     if kernel == "finish":
         return slots * (STATE_READ + 4) + slots * (STATE_READ + 8)
-    return slots * STATE_WRITE
+    return gen_paths * STATE_WRITE
 
 
-def roofline(prof, cnt, slots, node_bytes=64):
+def roofline(prof, cnt, slots, gen_paths, node_bytes=64):
     """Bandwidth roofline of the dominant kernel. achieved = algorithmic bytes
     of its launches / their CUDA-event time (kernel_bytes); the same figures
     for every kernel under "kernels", and the ncu issue utilisation and SIMD
@@ -881,7 +886,7 @@ def roofline(prof, cnt, slots, node_bytes=64):
     dom = max(ms, key=ms.get)
     launches = max(1, prof["launches"][dom])
     rays = cnt["rays"]
-    byts = kernel_bytes(dom, prof, cnt, slots, node_bytes)
+    byts = kernel_bytes(dom, prof, cnt, slots, node_bytes, gen_paths)
     achieved = byts / (ms[dom] / 1e3) / 1e9
     traffic, ncu = None, {}
     tf = os.path.join(ROOT, "profiles", "traffic.json")
@@ -898,7 +903,7 @@ def roofline(prof, cnt, slots, node_bytes=64):
     kernels = {}
     for k, t in ms.items():
         n = max(1, prof["launches"][k])
-        b = kernel_bytes(k, prof, cnt, slots, node_bytes)
+        b = kernel_bytes(k, prof, cnt, slots, node_bytes, gen_paths)
         kernels["k_" + k] = {"share": t / sum(ms.values()), "launches": n, "avg_launch_ms": t / n,
                              "algorithmic_bytes_per_launch": b / n,
                              "achieved_gbs": b / (t / 1e3) / 1e9 if t > 0 else None,

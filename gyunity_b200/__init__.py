@@ -165,10 +165,21 @@ class Context:
         self.check(self._lib.gyt_render_batch_device(self.handle, n, sc, cams, prms, films, ctypes.byref(st)))
         return {"paths": st.paths, "iterations": st.iterations, "launches": st.launches, "ms": st.ms}
 
-    def render_batch(self, scenes, cameras, params):
-        """gyt_render_batch: one host image (h, w, 3) per instance."""
+    def render_batch(self, scenes, cameras, params, out=None):
+        """gyt_render_batch: one host image (h, w, 3) per instance, written
+        into ``out`` (C-contiguous float32 arrays of those shapes, e.g. kept
+        from an earlier call or in pinned memory) when given."""
         n, sc, cams, prms = self._batch_arrays(scenes, cameras, params)
-        imgs = [np.empty((c.res_y, c.res_x, 3), np.float32) for c in cameras]
+        if out is None:
+            imgs = [np.empty((c.res_y, c.res_x, 3), np.float32) for c in cameras]
+        else:
+            imgs = list(out)
+            if len(imgs) != n:
+                raise ValueError("render_batch: %d output images for %d instances" % (len(imgs), n))
+            for im, c in zip(imgs, cameras):
+                if (not isinstance(im, np.ndarray) or im.dtype != np.float32 or im.shape != (c.res_y, c.res_x, 3)
+                        or not im.flags.c_contiguous or not im.flags.writeable):
+                    raise ValueError("render_batch: output images must be writeable C-contiguous float32 (h, w, 3)")
         outs = (ctypes.c_void_p * n)(*[im.ctypes.data for im in imgs])
         self.check(self._lib.gyt_render_batch(self.handle, n, sc, cams, prms, outs))
         return imgs

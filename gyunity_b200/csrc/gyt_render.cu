@@ -142,6 +142,14 @@ constexpr int kWStack = 48;  // node groups: one per level of the wide BVH
 constexpr int kBStack = 64;  // binary BVH: one entry per level
 constexpr int kBlock = 256;  // every kernel that traverses the BVH runs blocks of kBlock threads
 
+// The primitive word of a closest-hit record (q.hit .w): -1 for a miss, the
+// leaf-order triangle (< 2^28) or n_tris + sphere index; hits of the
+// closest-hit kernels carry the triangle's shading class + 1 in bits 28-30
+// (0: not recorded, as for spheres).
+constexpr int kClsShift = 28;
+GYT_D int hit_prim(int w) { return w < 0 ? w : (w & ((1 << kClsShift) - 1)); }
+GYT_D uint32_t hit_cls(int w) { return w < 0 ? 0u : (uint32_t)w >> kClsShift; }
+
 // Traversal stacks live in a per-warp slab of shared memory: each lane keeps
 // its top kBStackSh binary entries (4 bytes) or kWStackSh wide node groups
 // (8 bytes) there, deeper entries in a local-memory tail that only deep
@@ -220,8 +228,9 @@ GYT_D RayConst ray_const(float3 o, float3 d) {
 }
 
 // Triangles [first, first + count) in leaf order against the ray. ANY stops
-// at the first hit (returns true).
-template <bool ANY, bool COUNT, class S>
+// at the first hit (returns true). CLS: the hit's shading class + 1 (the
+// .w word of the triangle's second vertex) goes to bits 28-30 of prim.
+template <bool ANY, bool COUNT, bool CLS = false, class S>
 GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count, float& tmax, float& b1,
                      float& b2, int& prim, TraceCount* cnt) {
   if (COUNT) cnt->tris += count;
@@ -230,7 +239,7 @@ GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count
     float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
     float th, u, v;
     if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
-      prim = (int)(first + k);
+      prim = CLS ? (int)((first + k) | (__float_as_uint(t1.w) << kClsShift)) : (int)(first + k);
       if (ANY) return true;
       tmax = th;
       b1 = u;
@@ -261,7 +270,7 @@ struct BinaryTraversal {
   }
 
   // Returns true when the traversal is finished (or, for ANY, on a hit).
-  template <bool ANY, bool COUNT, class S>
+  template <bool ANY, bool COUNT, bool CLS = false, class S>
   GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
 #pragma unroll 1
@@ -297,7 +306,7 @@ struct BinaryTraversal {
       }
     }
     uint32_t code = ~(uint32_t)node;
-    if (test_tris<ANY, COUNT>(s, rc.wr, code >> 3, (code & 7u) + 1u, tmax, b1, b2, prim, cnt)) return true;
+    if (test_tris<ANY, COUNT, CLS>(s, rc.wr, code >> 3, (code & 7u) + 1u, tmax, b1, b2, prim, cnt)) return true;
     if (sp == 0) return true;
     node = pop();
     return false;
@@ -342,14 +351,14 @@ struct WideTraversal {
     sp = 0;
   }
 
-  template <bool ANY, bool COUNT, class S>
+  template <bool ANY, bool COUNT, bool CLS = false, class S>
   GYT_D bool step(const S& s, const RayConst& rc, float3 o, float& tmax, float& b1, float& b2, int& prim,
                   TraceCount* cnt) {
 #pragma unroll 1
     while (tmask) {
       const uint32_t k = __ffs(tmask) - 1;
       tmask &= tmask - 1u;
-      if (test_tris<ANY, COUNT>(s, rc.wr, tri_base + k, 1u, tmax, b1, b2, prim, cnt)) return true;
+      if (test_tris<ANY, COUNT, CLS>(s, rc.wr, tri_base + k, 1u, tmax, b1, b2, prim, cnt)) return true;
     }
     if ((grp.y & 0xffu) == 0u) {
       if (sp == 0) return true;
@@ -438,14 +447,17 @@ GYT_D int trace(const DevScene& s, float3 o, float3 d, float& tmax, float& b1, f
 }
 
 // Persistent traversal with dynamic ray fetching: every lane of a warp keeps
-// a ray; lanes whose ray is finished take new ray indices (one atomicAdd per
-// warp) before the next traversal step, so warps stay full until the queue
-// runs dry. load(i, o, d, tmax) fetches ray i; done(i, prim, tmax, b1, b2)
-// consumes its result.
+// a ray; lanes whose ray is finished take new ray indices before the next
+// traversal step (one atomicAdd per warp), so warps stay full until the
+// queue runs dry. (Reserving 64 indices per atomic and handing them out as
+// lanes go idle was slower on the uneven batch: 365 against 373 Mpaths/s.)
+// load(i, o, d, tmax) fetches ray i; done(i, prim, tmax, b1, b2) consumes
+// its result.
 //
 // BATCH: every ray carries its own geometry (load fills the lane's TraceGeo);
-// otherwise all rays use the scene s.
-template <int W, bool ANY, bool COUNT, bool BATCH = false, class Load, class Done>
+// otherwise all rays use the scene s. CLS: triangle hits carry their shading
+// class (test_tris).
+template <int W, bool ANY, bool COUNT, bool BATCH = false, bool CLS = false, class Load, class Done>
 GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load load, Done done,
                             unsigned long long* counters) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -490,8 +502,8 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
       // already walks down to a leaf)
 #pragma unroll 1
       for (int k = 0; k < (W == 8 ? 4 : 2); ++k) {
-        const bool fin = BATCH ? tv.template step<ANY, COUNT>(lg, rc, o, tmax, b1, b2, prim, &cnt)
-                               : tv.template step<ANY, COUNT>(s, rc, o, tmax, b1, b2, prim, &cnt);
+        const bool fin = BATCH ? tv.template step<ANY, COUNT, CLS>(lg, rc, o, tmax, b1, b2, prim, &cnt)
+                               : tv.template step<ANY, COUNT, CLS>(s, rc, o, tmax, b1, b2, prim, &cnt);
         if (fin) {
           if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
           else trace_spheres<ANY>(s, o, d, tmax, prim);
@@ -625,7 +637,7 @@ template <int W, bool COUNT>
 __global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
     k_extend(PathBuf cur, uint32_t n, DevScene s, float4* __restrict__ hits, uint32_t* __restrict__ fetch,
              unsigned long long* counters) {
-  persistent_trace<W, false, COUNT>(
+  persistent_trace<W, false, COUNT, false, true>(
       s, fetch, n,
       [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo&) {
         o = f3(cur.o[i]);
@@ -716,7 +728,7 @@ template <bool ADJ, bool DEFER = false, bool FROZEN = false, int SAMPLER = -1>
 GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const Params& prm, const Queues& q,
                       SamplerTables tab, const DebugOut& dbg, const AdjBuf& A = AdjBuf{}, const GradOut& G = GradOut{}) {
   float4 h4 = q.hit[i];
-  int prim = __float_as_int(h4.w);
+  int prim = hit_prim(__float_as_int(h4.w));
   uint32_t meta = cur.meta[i];
   uint32_t depth = meta & 255u;
   bool delta = (meta >> 8) & 1u;
@@ -927,6 +939,8 @@ constexpr uint32_t kClassMiss = 5, kClassIdle = 6, kShadeClasses = 7;
 GYT_D uint32_t shade_class(const DevScene& s, const Queues& q, uint32_t i) {
   const int prim = __float_as_int(q.hit[i].w);
   if (prim < 0) return kClassMiss;
+  const uint32_t c = hit_cls(prim);
+  if (c) return c - 1u;
   const uint32_t m = prim < s.n_tris ? (uint32_t)__float_as_int(__ldg(&s.tnrm[3 * prim].w))
                                      : __ldg(s.sphere_mat + (prim - s.n_tris));
   return min(__ldg(s.mtypes + m), 4u);
@@ -1050,6 +1064,34 @@ __global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_connect(P
       COUNT ? counters + 2 : nullptr);
 }
 
+// Stream compaction at block granularity: the position in the next pool of
+// this thread's live path, in thread order within the block, with one atomic
+// per block on the shared counter (a warp-granular atomic puts 16K+ requests
+// per launch on that one address). Every thread of the block calls it.
+GYT_D uint32_t block_compact(bool live, uint32_t* __restrict__ counter) {
+  __shared__ uint32_t warp_base[kBlock / 32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t ball = __ballot_sync(0xffffffffu, live);
+  if (lane == 0) warp_base[w] = __popc(ball);
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t c = lane < kBlock / 32 ? warp_base[lane] : 0u;
+    uint32_t inc = c;
+#pragma unroll
+    for (int o = 1; o < kBlock / 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= (uint32_t)o) inc += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, kBlock / 32 - 1);
+    uint32_t base = 0;
+    if (lane == 0 && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (lane < kBlock / 32) warp_base[lane] = base + inc - c;
+  }
+  __syncthreads();
+  return warp_base[w] + __popc(ball & ((1u << lane) - 1u));
+}
+
 GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) {
   double* p = film + 4ull * ((unsigned long long)y * w + x);
   atomicAdd(p, (double)L.x);
@@ -1063,21 +1105,18 @@ GYT_D void film_add(double* film, uint32_t w, uint32_t x, uint32_t y, float3 L) 
 __global__ void __launch_bounds__(kBlock) k_finish(PathBuf cur, PathBuf nxt, uint32_t n, double* __restrict__ film,
                                                    uint32_t res_x, uint32_t* __restrict__ counter,
                                                    const float4* __restrict__ madd, DebugOut dbg) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t meta = cur.meta[i];
-  float4 L4 = cur.L[i];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x * blockDim.x >= n) return;  // the whole block is idle
+  uint32_t meta = i < n ? cur.meta[i] : 0u;
+  float4 L4 = i < n ? cur.L[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   if (meta & kMisQueued) {  // the MIS contribution of this bounce (k_connect)
     const float4 m = madd[i];
     L4 = make_float4(L4.x + m.x, L4.y + m.y, L4.z + m.z, 0.f);
     meta &= ~kMisQueued;
   }
+  const uint32_t j = block_compact(meta & kAlive, counter);
+  if (i >= n) return;
   if (meta & kAlive) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
-    base = g.shfl(base, 0);
-    uint32_t j = base + g.thread_rank();
     nxt.o[j] = cur.o[i];
     nxt.d[j] = cur.d[i];
     nxt.tp[j] = cur.tp[i];
@@ -1219,13 +1258,10 @@ __global__ void __launch_bounds__(kBlock) k_mis_adj(PathBuf cur, AdjBuf A, DevSc
 __global__ void __launch_bounds__(kBlock) k_finish_adj(PathBuf cur, PathBuf nxt, AdjBuf A, AdjBuf AN, uint32_t n,
                                                        uint32_t* __restrict__ counter) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t meta = cur.meta[i];
+  if (blockIdx.x * blockDim.x >= n) return;  // the whole block is idle
+  const uint32_t meta = i < n ? cur.meta[i] : 0u;
+  const uint32_t j = block_compact(meta & kAlive, counter);
   if (!(meta & kAlive)) return;
-  cg::coalesced_group g = cg::coalesced_threads();
-  uint32_t base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
-  const uint32_t j = g.shfl(base, 0) + g.thread_rank();
   nxt.o[j] = cur.o[i];
   nxt.d[j] = cur.d[i];
   nxt.tp[j] = cur.tp[i];
@@ -1317,7 +1353,7 @@ __global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
     k_extend_batch(PathBuf cur, const IterState* __restrict__ st, float4* __restrict__ hits,
                    uint32_t* __restrict__ fetch) {
   const uint32_t n = st->n;
-  persistent_trace<W, false, false, true>(
+  persistent_trace<W, false, false, true, true>(
       c_insts[0].s, fetch, n,
       [&](uint32_t i, float3& o, float3& d, float& tmax, TraceGeo& g) {
         o = f3(cur.o[i]);
@@ -1393,22 +1429,30 @@ __global__ void __launch_bounds__(kBlock) k_finish_batch(PathBuf cur, PathBuf nx
   // loads after testing the path: 14% faster on the uneven batch); batched
   // renders keep no path ids
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= st->n) return;
-  uint32_t meta = cur.meta[i];
-  float4 L4 = cur.L[i];
-  const uint32_t pix = cur.pix[i], inst = cur.inst[i];
-  const float4 o = cur.o[i], d = cur.d[i], tp = cur.tp[i];
-  const unsigned long long sidx = cur.sidx[i];
+  const uint32_t n = st->n;
+  if (blockIdx.x * blockDim.x >= n) return;  // the whole block is idle
+  const bool in = i < n;
+  uint32_t meta = in ? cur.meta[i] : 0u;
+  float4 L4 = in ? cur.L[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  uint32_t pix = 0, inst = 0;
+  float4 o = L4, d = L4, tp = L4;
+  unsigned long long sidx = 0;
+  if (in) {
+    pix = cur.pix[i];
+    inst = cur.inst[i];
+    o = cur.o[i];
+    d = cur.d[i];
+    tp = cur.tp[i];
+    sidx = cur.sidx[i];
+  }
   if (meta & kMisQueued) {  // the MIS contribution of this bounce (k_connect_batch)
     const float4 m = madd[i];
     L4 = make_float4(L4.x + m.x, L4.y + m.y, L4.z + m.z, 0.f);
     meta &= ~kMisQueued;
   }
+  const uint32_t j = block_compact(meta & kAlive, counter);
+  if (!in) return;
   if (meta & kAlive) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
-    const uint32_t j = g.shfl(base, 0) + g.thread_rank();
     nxt.o[j] = o;
     nxt.d[j] = d;
     nxt.tp[j] = tp;
@@ -1948,7 +1992,7 @@ __global__ void __launch_bounds__(kBlock, EQUI ? 4 : 3) k_vshade(PathBuf cur, ui
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 h4 = q.hit[i];
-  const int prim = __float_as_int(h4.w);
+  const int prim = hit_prim(__float_as_int(h4.w));
   const float tmax = h4.x;
   const uint32_t meta = cur.meta[i];
   uint32_t depth = meta & 255u;
@@ -2366,8 +2410,9 @@ const void* persistent_fn(int kind) {
 // store identical floats. leaf_of[t] = k.
 __global__ void k_leaf_data(uint32_t nt, const uint32_t* __restrict__ order, const float* __restrict__ V,
                             const uint32_t* __restrict__ I, const float* __restrict__ N,
-                            const int2* __restrict__ info, const uint32_t* __restrict__ tmed, float4* __restrict__ tris,
-                            float4* __restrict__ tnrm, int* __restrict__ leaf_of) {
+                            const int2* __restrict__ info, const uint32_t* __restrict__ tmed,
+                            const uint32_t* __restrict__ mtype, float4* __restrict__ tris, float4* __restrict__ tnrm,
+                            int* __restrict__ leaf_of) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   const uint32_t t = order[k];
@@ -2387,8 +2432,10 @@ __global__ void k_leaf_data(uint32_t nt, const uint32_t* __restrict__ order, con
       __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(cr.x, cr.x), __fmul_rn(cr.y, cr.y)), __fmul_rn(cr.z, cr.z)));
   const float3 face = mk(__fdiv_rn(cr.x, len), __fdiv_rn(cr.y, len), __fdiv_rn(cr.z, len));
   const int2 in = info[t];
+  const uint32_t cls = min(mtype[in.x], 4u) + 1u;
   for (int c = 0; c < 3; ++c) {
-    tris[3 * (size_t)k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? __int_as_float((int)t) : 0.f);
+    tris[3 * (size_t)k + c] =
+        make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? __int_as_float((int)t) : (c == 1 ? __uint_as_float(cls) : 0.f));
     const float3 n = N ? mk(N[3 * (size_t)vi[c]], N[3 * (size_t)vi[c] + 1], N[3 * (size_t)vi[c] + 2]) : face;
     const float w = c == 0 ? __int_as_float(in.x) : (c == 1 ? __int_as_float(in.y) : __uint_as_float(tmed ? tmed[t] : 0u));
     tnrm[3 * (size_t)k + c] = make_float4(n.x, n.y, n.z, w);
@@ -3268,7 +3315,9 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
   const bool has_env = d->env && d->env_w && d->env_h;
   if (has_env && ((uint64_t)d->env_w * d->env_h > (1ull << 28) || d->env_w < 1 || d->env_h < 1))
     return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: environment map too large");
-  if ((uint64_t)d->n_triangles >= (1ull << 28)) return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many triangles");
+  // closest-hit records keep the primitive in 28 bits (hit_prim)
+  if ((uint64_t)d->n_triangles + d->n_spheres >= (1ull << 28))
+    return fail(ctx, GYT_ERR_UNSUPPORTED, "scene_create: too many primitives");
   for (uint32_t m = 0; m < d->n_materials; ++m)
     if (d->mat_type[m] > GYT_MAT_NONE) return fail(ctx, GYT_ERR_INVALID, "scene_create: unknown material type");
   if (d->n_media && !d->media) return fail(ctx, GYT_ERR_INVALID, "scene_create: media array missing");
@@ -3426,6 +3475,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     if (e == cudaSuccess) e = tup(&dI, d->indices, (size_t)nt * 3);
     if (e == cudaSuccess && d->normals) e = tup(&dN, d->normals, (size_t)d->n_vertices * 3);
     if (e == cudaSuccess) e = tup(&dInfo, info.data(), info.size());
+    uint32_t* dMtype = nullptr;
+    if (e == cudaSuccess) e = tup(&dMtype, d->mat_type, d->n_materials);
     uint32_t* dTmed = nullptr;
     if (e == cudaSuccess && !tmed.empty()) e = tup(&dTmed, tmed.data(), tmed.size());
     if (e == cudaSuccess) e = tup(&dLeafOf, (const int*)nullptr, nt);
@@ -3457,7 +3508,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
     if (e == cudaSuccess) e = dalloc(sc->allocs, &dn, (size_t)nt * 3);
     if (e != cudaSuccess) return bail(cuda_code(e), std::string("scene_create: ") + cudaGetErrorString(e));
     sc->bytes += (uint64_t)nt * 3 * 2 * sizeof(float4);
-    k_leaf_data<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(nt, g.order, dV, dI, dN, dInfo, dTmed, dtris, dn, dLeafOf);
+    k_leaf_data<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(nt, g.order, dV, dI, dN, dInfo, dTmed, dMtype, dtris, dn,
+                                                               dLeafOf);
     if (n_area)
       k_gather_int<<<(n_area + 255) / 256, 256, 0, ctx->stream>>>((uint32_t)n_area, dLights, dLeafOf, dLightLeaf);
     e = cudaGetLastError();
@@ -3497,7 +3549,8 @@ int32_t gyt_scene_create(gyt_context* ctx, const GytSceneDesc* d, gyt_scene** ou
       float3 p[3] = {vtx(I[0]), vtx(I[1]), vtx(I[2])};
       float3 face = norm(cross(p[1] - p[0], p[2] - p[0]));
       for (int c = 0; c < 3; ++c) {
-        tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : 0.f);
+        const int cls = (int)std::min(d->mat_type[info[t].x], 4u) + 1;
+        tris[3 * k + c] = make_float4(p[c].x, p[c].y, p[c].z, c == 0 ? bits((int)t) : (c == 1 ? bits(cls) : 0.f));
         float3 n = d->normals ? mk(d->normals[3 * I[c]], d->normals[3 * I[c] + 1], d->normals[3 * I[c] + 2]) : face;
         uint32_t mw = tmed.empty() ? 0u : tmed[t];
         float w = c == 0 ? bits(info[t].x) : (c == 1 ? bits(info[t].y) : bits((int)mw));
@@ -3757,12 +3810,9 @@ int32_t gyt_render_device(gyt_context* ctx, const gyt_scene* scene, const GytCam
   return run_paths(ctx, scene, cam, params, total, nullptr, d_film, DebugOut{}, stats);
 }
 
-int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
-                   float* rgb_out) {
-  if (!ctx || !scene || !camera || !rgb_out) return fail(ctx, GYT_ERR_INVALID, "render: null argument");
-  GYT_CK(ctx, cudaSetDevice(ctx->device));
-  size_t npix = (size_t)camera->res_x * camera->res_y;
-  size_t fb = npix * 4 * sizeof(double), rb = npix * 3 * sizeof(float);
+// The context's FP64 film and RGB staging buffers of the host-image renders
+// (grown to the largest request, kept until the context is destroyed).
+int32_t ensure_host_films(gyt_context* ctx, size_t fb, size_t rb) {
   if (fb > ctx->film_bytes) {
     cudaFree(ctx->d_film);
     ctx->d_film = nullptr;
@@ -3777,6 +3827,17 @@ int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* ca
     GYT_CK(ctx, cudaMalloc((void**)&ctx->d_rgb, rb));
     ctx->rgb_bytes = rb;
   }
+  return GYT_OK;
+}
+
+int32_t gyt_render(gyt_context* ctx, const gyt_scene* scene, const GytCamera* camera, const GytRenderParams* params,
+                   float* rgb_out) {
+  if (!ctx || !scene || !camera || !rgb_out) return fail(ctx, GYT_ERR_INVALID, "render: null argument");
+  GYT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t npix = (size_t)camera->res_x * camera->res_y;
+  size_t fb = npix * 4 * sizeof(double), rb = npix * 3 * sizeof(float);
+  int32_t st0 = ensure_host_films(ctx, fb, rb);
+  if (st0) return st0;
   GYT_CK(ctx, cudaMemsetAsync(ctx->d_film, 0, fb, ctx->stream));
   int32_t st = gyt_render_device(ctx, scene, camera, params, ctx->d_film, nullptr);
   if (st) return st;
@@ -4630,27 +4691,22 @@ int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* s
     if (!rgb_out[i]) return fail(ctx, GYT_ERR_INVALID, "batch: null image at " + std::to_string(i));
     off[i + 1] = off[i] + (size_t)cameras[i].res_x * cameras[i].res_y;
   }
-  std::vector<void*> tmp;
-  struct Guard {
-    std::vector<void*>& v;
-    ~Guard() {
-      for (void* p : v) cudaFree(p);
-    }
-  } guard{tmp};
-  double* films = nullptr;
-  float* rgb = nullptr;
-  GYT_CK(ctx, dalloc(tmp, &films, off[n] * 4));
-  GYT_CK(ctx, dalloc(tmp, &rgb, off[n] * 3));
+  if (off[n] >= (1ull << 32)) return fail(ctx, GYT_ERR_UNSUPPORTED, "batch: more than 2^32 pixels");
+  int32_t st = ensure_host_films(ctx, off[n] * 4 * sizeof(double), off[n] * 3 * sizeof(float));
+  if (st) return st;
+  double* films = ctx->d_film;
+  float* rgb = ctx->d_rgb;
   GYT_CK(ctx, cudaMemsetAsync(films, 0, off[n] * 4 * sizeof(double), ctx->stream));
   std::vector<double*> fp(n);
   for (uint32_t i = 0; i < n; ++i) fp[i] = films + 4 * off[i];
-  int32_t st = gyt_render_batch_device(ctx, n, scenes, cameras, params, fp.data(), nullptr);
+  st = gyt_render_batch_device(ctx, n, scenes, cameras, params, fp.data(), nullptr);
   if (st) return st;
+  // the films are contiguous: one resolve for all, then one copy per image
+  if (off[n]) k_resolve<<<grid_for(off[n]), kBlock, 0, ctx->stream>>>(films, rgb, (uint32_t)off[n]);
+  GYT_CK(ctx, cudaGetLastError());
   for (uint32_t i = 0; i < n; ++i) {
     const size_t npix = off[i + 1] - off[i];
     if (!npix) continue;
-    k_resolve<<<grid_for(npix), kBlock, 0, ctx->stream>>>(fp[i], rgb + 3 * off[i], (uint32_t)npix);
-    GYT_CK(ctx, cudaGetLastError());
     GYT_CK(ctx, cudaMemcpyAsync(rgb_out[i], rgb + 3 * off[i], npix * 3 * sizeof(float), cudaMemcpyDeviceToHost,
                                 ctx->stream));
   }

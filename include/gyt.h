@@ -429,7 +429,9 @@ int32_t gyt_render_batch_device(gyt_context* ctx, uint32_t n, const gyt_scene* c
                                 const GytCamera* cameras, const GytRenderParams* params, double* const* d_films,
                                 GytRenderStats* stats);
 /* The same with host images: rgb_out[i] receives res_x*res_y*3 floats as
- * gyt_render writes them. */
+ * gyt_render writes them. Like gyt_render, the context keeps its FP64 film
+ * and RGB staging buffers (grown to the largest call) until it is destroyed;
+ * copies into page-locked rgb_out buffers run at full PCIe rate. */
 int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes, const GytCamera* cameras,
                          const GytRenderParams* params, float* const* rgb_out);
 /* Autotuner: times batched renders of the given instances with at most

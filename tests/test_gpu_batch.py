@@ -110,6 +110,14 @@ def test_batch_host_images(bctx, scs):
                               sd.camera.up, sd.camera.fovy, sd.camera.film_distance)
         ref = g.GpuPathTracing(sd.params.spp, sd.params.max_depth, sd.params.rr_depth).Render(sc, cam).GetImage()
         np.testing.assert_allclose(im, ref, rtol=1e-6, atol=1e-7)
+    # again into caller-owned images (the context's film buffers reused and re-zeroed)
+    out = [np.full((sd.camera.res_y, sd.camera.res_x, 3), -1.0, np.float32) for sd in DESCS]
+    again = bctx.render_batch(scs, [sd.camera for sd in DESCS], [sd.params for sd in DESCS], out=out)
+    for im, o, a in zip(imgs, out, again):
+        assert a is o
+        np.testing.assert_allclose(o, im, rtol=1e-6, atol=1e-7)
+    with pytest.raises(ValueError):
+        bctx.render_batch(scs, [sd.camera for sd in DESCS], [sd.params for sd in DESCS], out=out[:-1])
 
 
 def test_batch_many_small_instances(bctx):
