@@ -627,9 +627,10 @@ def measure_batch(a, d, g, torch):
                 "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s,
                              "widths_tried": [2, 8],
                              "note": "coordinate search over BVH width (binary and 8-wide scenes, both built on "
-                                     "the device), pool size, grid-stride and traversal blocks per SM on a sample "
-                                     "of every instance at spp x 8 / 64 (the batch's mix), median of three renders "
-                                     "per candidate; the per-scene renders use the chosen width too"},
+                                     "the device), grid-stride and traversal blocks per SM on a sample of every "
+                                     "instance at spp x 8 / 64 (the batch's mix), median of three renders per "
+                                     "candidate; pool sizes 2M-32M on a sample at spp x 32 / 64; the per-scene "
+                                     "renders use the chosen width and pool too"},
                 "e2e": {"value": paths * d.world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": imgs_bytes, "steps": e2e_steps,
                         "note": "gyt_render_batch with the scenes resident: cameras and parameters in, "

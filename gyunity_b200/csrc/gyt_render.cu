@@ -4759,20 +4759,21 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
   // per candidate one untimed render, then the median of three timed ones:
   // a single timed render of the short sample varies by several per cent,
   // enough to pick the wrong BVH width
-  auto trial = [&](const GytBatchConfig& c, const gyt_scene* const* sc, float* mp) -> int32_t {
+  auto trial = [&](const GytBatchConfig& c, const gyt_scene* const* sc, float* mp, int timed = 3) -> int32_t {
     ctx->bcfg = c;
     BatchInput in;
     int32_t st = batch_input(ctx, n, sc, cameras, prm.data(), fp.data(), &in);
     if (st) return st;
     GytRenderStats rs;
     float ms[3];
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k <= timed; ++k) {
       st = run_batch(ctx, in, &rs);
       if (st) return st;
       if (k) ms[k - 1] = rs.ms;
     }
-    std::sort(ms, ms + 3);
-    *mp = ms[1] > 0.f ? (float)(rs.paths / (ms[1] * 1e3)) : 0.f;
+    std::sort(ms, ms + timed);
+    const float med = ms[timed / 2];
+    *mp = med > 0.f ? (float)(rs.paths / (med * 1e3)) : 0.f;
     return GYT_OK;
   };
   GytBatchConfig cur = {saved_cap, 8, 0, 1, (uint32_t)(scenes[0] && scenes[0]->dev.wnodes ? 8 : 2)};
@@ -4791,15 +4792,42 @@ int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const*
       cur.bvh_width = scenes_alt[0] && scenes_alt[0]->dev.wnodes ? 8 : 2;
     }
   }
-  for (uint32_t cap : {1u << 20, 1u << 21, 1u << 22}) {
-    if (cap == cur.paths_in_flight) continue;
-    GytBatchConfig c = cur;
-    c.paths_in_flight = cap;
-    float mp = 0.f;
-    st = trial(c, cur_scenes, &mp);
-    if (st == GYT_ERR_OUT_OF_MEMORY) { cudaGetLastError(); continue; }
-    if (st) { ctx->bcfg = saved; return st; }
-    if (mp > cur_mp) { cur_mp = mp; cur = c; }
+  // Pool size. Every half-iteration pays a fixed cost (the persistent
+  // traversal kernels' last rays, launch gaps), so larger pools win on long
+  // renders, while the drain at a render's end grows with the pool: a short
+  // sample undervalues them (on the uneven batch 4M, 8M and 16M paths in
+  // flight gave 376, 395 and 406 Mpaths/s, while the 1/8 sample preferred 4M).
+  // The candidates are therefore timed on a sample four times larger (at most
+  // the whole batch), all of them on the same one, one timed render each
+  // after an untimed one (a render of that size varies by well under 1%).
+  {
+    std::vector<GytRenderParams> big(params, params + n);
+    const uint32_t bspp = std::min<uint32_t>(spp_max, sspp * 4u);
+    uint64_t big_paths = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint64_t scaled = ((uint64_t)big[i].spp * bspp + spp_max / 2) / spp_max;
+      big[i].spp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(scaled, bspp));
+      big_paths += (uint64_t)cameras[i].res_x * cameras[i].res_y * big[i].spp;
+    }
+    std::swap(prm, big);
+    uint32_t best_cap = cur.paths_in_flight;
+    float best_mp = 0.f;
+    for (uint32_t cap : {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25}) {
+      if (cap > (1u << 21) && (uint64_t)cap > 2 * big_paths) break;  // a pool the sample cannot fill
+      GytBatchConfig c = cur;
+      c.paths_in_flight = cap;
+      float mp = 0.f;
+      st = trial(c, cur_scenes, &mp, 1);
+      if (st == GYT_ERR_OUT_OF_MEMORY) { cudaGetLastError(); continue; }
+      if (st) { std::swap(prm, big); ctx->bcfg = saved; return st; }
+      if (mp > best_mp) { best_mp = mp; best_cap = cap; }
+    }
+    std::swap(prm, big);
+    if (best_cap != cur.paths_in_flight) {
+      cur.paths_in_flight = best_cap;
+      st = trial(cur, cur_scenes, &cur_mp);  // the baseline of the next steps, on the base sample
+      if (st) { ctx->bcfg = saved; return st; }
+    }
   }
   for (uint32_t sb : {4u, 16u}) {
     GytBatchConfig c = cur;

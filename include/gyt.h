@@ -437,10 +437,13 @@ int32_t gyt_render_batch(gyt_context* ctx, uint32_t n, const gyt_scene* const* s
 /* Autotuner: times batched renders of the given instances with at most
  * sample_spp samples per pixel (0 = 1; each instance's spp scaled by
  * sample_spp / the batch's largest spp, at least 1, so that the sample keeps
- * the batch's mix of instances) over pool sizes, grid shapes and, when
- * scenes_alt (the same scenes built with the other BVH width) is given, the
- * BVH width; sets the fastest configuration on the context and returns it in
- * *best with its throughput in *best_mpaths (Mpaths/s; may be NULL). */
+ * the batch's mix of instances) over grid shapes and, when scenes_alt (the
+ * same scenes built with the other BVH width) is given, the BVH width; the
+ * pool sizes (2M to 32M paths in flight, those the sample can fill) on a
+ * sample four times larger, since a short sample undervalues large pools.
+ * Sets the fastest configuration on the context and returns it in *best
+ * with its throughput on the base sample in *best_mpaths (Mpaths/s; may be
+ * NULL). */
 int32_t gyt_batch_autotune(gyt_context* ctx, uint32_t n, const gyt_scene* const* scenes,
                            const gyt_scene* const* scenes_alt, const GytCamera* cameras,
                            const GytRenderParams* params, uint32_t sample_spp, GytBatchConfig* best,
