@@ -67,6 +67,8 @@ def parse():
                          "uses the library default (binary, built on the GPU)")
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
     ap.add_argument("--batch-instances", type=int, default=64, help="instances of the uneven batch workload")
+    ap.add_argument("--paths-in-flight", type=int, default=1 << 24,
+                    help="path pool of the single-scene, volume and adjoint contexts (the batch's is autotuned)")
     ap.add_argument("--no-single-scene", action="store_true",
                     help="batch workload: skip the single-scene (procedural mesh) measurement")
     ap.add_argument("--adjoint-iters", type=int, default=200,
@@ -393,7 +395,7 @@ def measure_single(a, d, g, torch):
     """One scene per step through gyt_render_device (--workload mesh, env,
     cornell); returns the JSON line on rank 0."""
     sd = workload(a)
-    ctx = g.Context(d.local, bvh_width=a.bvh_width, bvh_builder=a.bvh_builder)
+    ctx = g.Context(d.local, capacity=a.paths_in_flight, bvh_width=a.bvh_width, bvh_builder=a.bvh_builder)
     t0 = time.perf_counter()
     scene = g.Scene(sd, ctx)
     scene_s = time.perf_counter() - t0
@@ -471,7 +473,7 @@ def measure_single(a, d, g, torch):
                 "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh, no dataset)",
                 "config": config(a, sd, {"parallelism": "independent frames per GPU" if d.world > 1 else "1 GPU",
-                                         "paths_in_flight": 1 << 21,
+                                         "paths_in_flight": a.paths_in_flight,
                                          "bvh": own}),
                 "wall_ms_per_step": wall * 1e3 / a.steps,
                 "iterations_per_step": stats[-1]["iterations"],
@@ -706,7 +708,7 @@ def measure_volume(a, d, g, torch):
     host cores over the first 128 rows."""
     from gyunity_b200 import scenes
     sd = scenes.cornell_fog(res=512, spp=16, max_depth=8)
-    ctx = g.Context(d.local)
+    ctx = g.Context(d.local, capacity=a.paths_in_flight)
     sc = g.Scene(sd, ctx)
     film = torch.zeros(512 * 512 * 4, dtype=torch.float64, device="cuda")
     ms = []
@@ -760,7 +762,7 @@ def measure_adjoint(a, d, g, torch):
     the FD check on 16 parameters (step 1e-3) and the Adam run from the
     perturbed parameters."""
     from gyunity_b200 import diff, scenes
-    ctx = g.Context(d.local)
+    ctx = g.Context(d.local, capacity=a.paths_in_flight)
     hidden = scenes.inverse_params(groups=256, emitters=4, seed=7)
     sd = scenes.inverse_box(hidden, level=5, res=512, spp=32, max_depth=8, rr_depth=8)
     r = diff.DiffRenderer(ctx, sd)
