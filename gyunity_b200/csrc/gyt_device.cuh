@@ -423,9 +423,12 @@ GYT_D void tri_hit(float3 p0, float3 p1, float3 p2, float3 n0, float3 n1, float3
   h->sv = dv;
 }
 
-// OffsetRayOrigin (math/GeometryUtils.h:39-64)
-GYT_D float3 offset_origin(float3 p, float3 perr, float3 n, float3 w) {
-  float d = dot(vabs(n), perr);
+// OffsetRayOrigin (math/GeometryUtils.h:39-64): the offset distance
+// d = |n| . pErr, then the origin moved by d along n (towards w) and rounded
+// one float away. A shading kernel that spawns several rays from one point
+// computes d once (offset_dist) and calls offset_origin_d.
+GYT_D float offset_dist(float3 perr, float3 n) { return dot(vabs(n), perr); }
+GYT_D float3 offset_origin_d(float3 p, float d, float3 n, float3 w) {
   float3 off = n * d;
   if (dot(w, n) < 0.f) off = -off;
   float3 po = p + off;
@@ -433,6 +436,9 @@ GYT_D float3 offset_origin(float3 p, float3 perr, float3 n, float3 w) {
   if (off.y > 0.f) po.y = next_up(po.y); else if (off.y < 0.f) po.y = next_down(po.y);
   if (off.z > 0.f) po.z = next_up(po.z); else if (off.z < 0.f) po.z = next_down(po.z);
   return po;
+}
+GYT_D float3 offset_origin(float3 p, float3 perr, float3 n, float3 w) {
+  return offset_origin_d(p, offset_dist(perr, n), n, w);
 }
 
 // --------------------------------------------------------------- BSDFs ----

@@ -207,15 +207,40 @@ struct RayConst {
   float ix, iy, iz;  // reciprocal direction (tiny components clamped to 2^-80)
 };
 
-// The geometry one ray is traced against: the scene's, or in a batch the
-// ray's own instance's (the traversal reads only these fields).
-struct TraceGeo {
-  const uint4* wnodes;
-  const float4* nodes;
-  const float4* tris;
-  const float4* spheres;
-  int n_tris, n_spheres;
+struct Inst {
+  DevScene s;
+  Cam cam;
+  Params prm;
+  double* film;
+  unsigned long long first;  // first global path index of the instance
 };
+
+// The instance table lives in constant memory: warps almost always hold paths
+// of one instance (the pool is refilled instance after instance), so the
+// per-path reads of scene fields are uniform constant-cache hits and the
+// compiler can keep them out of the way of the kernels' global stores.
+// Larger batches run as consecutive groups of kMaxBatch instances.
+constexpr uint32_t kMaxBatch = 128;
+__constant__ Inst c_insts[kMaxBatch];
+
+// The geometry one ray of a batch is traced against: its instance, whose
+// fields the traversal reads from the instance table when it needs them (a
+// lane keeps one index instead of four pointers and two counts).
+struct TraceGeo {
+  uint32_t inst;
+};
+GYT_D const uint4* geo_wnodes(const DevScene& s) { return s.wnodes; }
+GYT_D const float4* geo_nodes(const DevScene& s) { return s.nodes; }
+GYT_D const float4* geo_tris(const DevScene& s) { return s.tris; }
+GYT_D const float4* geo_spheres(const DevScene& s) { return s.spheres; }
+GYT_D int geo_ntris(const DevScene& s) { return s.n_tris; }
+GYT_D int geo_nspheres(const DevScene& s) { return s.n_spheres; }
+GYT_D const uint4* geo_wnodes(const TraceGeo& g) { return c_insts[g.inst].s.wnodes; }
+GYT_D const float4* geo_nodes(const TraceGeo& g) { return c_insts[g.inst].s.nodes; }
+GYT_D const float4* geo_tris(const TraceGeo& g) { return c_insts[g.inst].s.tris; }
+GYT_D const float4* geo_spheres(const TraceGeo& g) { return c_insts[g.inst].s.spheres; }
+GYT_D int geo_ntris(const TraceGeo& g) { return c_insts[g.inst].s.n_tris; }
+GYT_D int geo_nspheres(const TraceGeo& g) { return c_insts[g.inst].s.n_spheres; }
 
 GYT_D RayConst ray_const(float3 o, float3 d) {
   RayConst c;
@@ -235,7 +260,7 @@ GYT_D bool test_tris(const S& s, const WtRay& wr, uint32_t first, uint32_t count
                      float& b2, int& prim, TraceCount* cnt) {
   if (COUNT) cnt->tris += count;
   for (uint32_t k = 0; k < count; ++k) {
-    const float4* t = s.tris + 3 * (size_t)(first + k);
+    const float4* t = geo_tris(s) + 3 * (size_t)(first + k);
     float4 t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2);
     float th, u, v;
     if (wt_intersect<ANY>(wr, f3(t0), f3(t1), f3(t2), tmax, &th, &u, &v)) {
@@ -276,7 +301,7 @@ struct BinaryTraversal {
 #pragma unroll 1
     while (node >= 0) {
       if (COUNT) cnt->nodes++;
-      const float4* n = s.nodes + 4 * (size_t)node;
+      const float4* n = geo_nodes(s) + 4 * (size_t)node;
       float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
       int4 n3 = __ldg((const int4*)(n + 3));
       const float ox = o.x * rc.ix, oy = o.y * rc.iy, oz = o.z * rc.iz;
@@ -371,7 +396,7 @@ struct WideTraversal {
     grp.y &= ~(1u << p);
     if (grp.y & 0xffu) push(grp);
     if (COUNT) cnt->nodes++;
-    const uint4* n = s.wnodes + 5 * (size_t)node;
+    const uint4* n = geo_wnodes(s) + 5 * (size_t)node;
     const uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
     const float sx = __int_as_float(((int)(int8_t)(w0.w & 0xffu) + 127) << 23);
     const float sy = __int_as_float(((int)(int8_t)((w0.w >> 8) & 0xffu) + 127) << 23);
@@ -415,13 +440,14 @@ struct TraversalOf<8> { using type = WideTraversal; };
 // The analytic spheres after the BVH (linear; the configurations hold few).
 template <bool ANY, class S>
 GYT_D void trace_spheres(const S& s, float3 o, float3 d, float& tmax, int& prim) {
-  for (int k = 0; k < s.n_spheres; ++k) {
+  const int ns = geo_nspheres(s);
+  for (int k = 0; k < ns; ++k) {
     if (ANY && prim >= 0) return;
-    float4 sp4 = __ldg(s.spheres + k);
+    float4 sp4 = __ldg(geo_spheres(s) + k);
     Ray r = sphere_object_ray(o, d, tmax, 0.f);
     float th;
     if (sphere_root(sp4, r, &th)) {
-      prim = s.n_tris + k;
+      prim = geo_ntris(s) + k;
       tmax = th;
     }
   }
@@ -491,7 +517,7 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
           prim = -1;
           rc = ray_const(o, d);
           tv.init(rc);
-          if ((BATCH ? lg.n_tris : s.n_tris) == 0) {
+          if ((BATCH ? geo_ntris(lg) : s.n_tris) == 0) {
             if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
             else trace_spheres<ANY>(s, o, d, tmax, prim);
             done((uint32_t)ri, prim, tmax, b1, b2);
@@ -780,6 +806,8 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
       sphere_hit(__ldg(s.spheres + k), r, h4.x, &h);
       mat = __ldg(s.sphere_mat + k);
     }
+    // the spawned rays' offset distance, once for the three rays of this bounce
+    const float ofs_d = offset_dist(h.perr, h.abs_n);
     Bsdf bsdf;
     bsdf.lobe = load_lobe(s.mparams, s.mtypes, mat);
     bsdf.su = h.su; bsdf.sv = h.sv; bsdf.n = h.n; bsdf.gn = h.geo_n;
@@ -804,6 +832,14 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
     if (SAMPLER == 1 || (SAMPLER < 0 && prm.sampler)) halton10(tab, rng.index, rng.cursor, u10);
     else sobol10(tab.bits, rng.index, rng.cursor, u10);
     const bool emit = (depth == 0 || delta) && light >= 0;
+    // the continuation's four dimensions (arguments again in right-to-left
+    // order) wait in shared memory while direct lighting runs: four registers
+    // fewer live across it in the 64-register build (blocks of kBlock threads)
+    __shared__ float s_cont[4][kBlock];
+    s_cont[0][threadIdx.x] = emit ? u10[0] : u10[6];
+    s_cont[1][threadIdx.x] = emit ? u10[1] : u10[7];
+    s_cont[2][threadIdx.x] = emit ? u10[2] : u10[8];
+    s_cont[3][threadIdx.x] = emit ? u10[3] : u10[9];
     if (emit) {
       LightTri l = load_light(s, light);
       if (dot(h.n, h.wo) > 0.f) {
@@ -857,7 +893,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
           float cosT = fabsf(dot(h.n, wi));
           if (!is_zero(f)) {
             // Intersection::SpawnTo (Intersection.h:64-72)
-            float3 org = offset_origin(h.pos, h.perr, h.abs_n, lpos - h.pos);
+            float3 org = offset_origin_d(h.pos, ofs_d, h.abs_n, lpos - h.pos);
             float3 tgt = offset_origin(lpos, lerr, labs, org - lpos);
             float3 dd = tgt - org;
             float dis = length(dd);
@@ -881,7 +917,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
         if (FROZEN) f2 = refit(f2, wi2);
         float cos2 = fabsf(dot(h.n, wi2));
         if (pdf2 != 0.f && !is_zero(f2)) {
-          float3 o2 = offset_origin(h.pos, h.perr, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
+          float3 o2 = offset_origin_d(h.pos, ofs_d, h.abs_n, wi2) + wi2 * kRayEps;  // SpawnRay
           // the light triangle again from the light table rather than kept live
           // across the BSDF evaluation and sampling
           float lpdf = env_light ? env_pdf_dir(s.env, wi2) : tri_light_pdf(load_light(s, li), h, o2, wi2);
@@ -900,9 +936,9 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
         }
       }
     }
-    // continuation (PT.cpp:45-62); arguments again in right-to-left order
-    float rz = emit ? u10[0] : u10[6], ry = emit ? u10[1] : u10[7], rx = emit ? u10[2] : u10[8];
-    const float urr = emit ? u10[3] : u10[9];
+    // continuation (PT.cpp:45-62)
+    float rz = s_cont[0][threadIdx.x], ry = s_cont[1][threadIdx.x], rx = s_cont[2][threadIdx.x];
+    const float urr = s_cont[3][threadIdx.x];
     rng.cursor += 3;
     float3 wi;
     float pdf;
@@ -922,7 +958,7 @@ GYT_D void shade_path(const PathBuf& cur, uint32_t i, const DevScene& s, const P
       }
       if (survive) {
         tp = tp * est;
-        float3 no = offset_origin(h.pos, h.perr, h.abs_n, wi) + wi * kRayEps;
+        float3 no = offset_origin_d(h.pos, ofs_d, h.abs_n, wi) + wi * kRayEps;
         cur.o[i] = make_float4(no.x, no.y, no.z, 0.f);
         cur.d[i] = make_float4(wi.x, wi.y, wi.z, 0.f);
         cur.tp[i] = make_float4(tp.x, tp.y, tp.z, 0.f);
@@ -1286,21 +1322,7 @@ __global__ void __launch_bounds__(kBlock) k_finish_adj(PathBuf cur, PathBuf nxt,
 // refilled from the concatenation of all instances' paths (instance-major),
 // every path slot carries its instance, and each kernel reads the scene,
 // camera, parameters and film of the instance it works on.
-struct Inst {
-  DevScene s;
-  Cam cam;
-  Params prm;
-  double* film;
-  unsigned long long first;  // first global path index of the instance
-};
 
-// The instance table lives in constant memory: warps almost always hold paths
-// of one instance (the pool is refilled instance after instance), so the
-// per-path reads of scene fields are uniform constant-cache hits and the
-// compiler can keep them out of the way of the kernels' global stores.
-// Larger batches run as consecutive groups of kMaxBatch instances.
-constexpr uint32_t kMaxBatch = 128;
-__constant__ Inst c_insts[kMaxBatch];
 
 // Device-side loop state of a batched render (one half-iteration moves the
 // pool from one buffer to the other).
@@ -1350,9 +1372,7 @@ __global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const It
   }
 }
 
-GYT_D TraceGeo geo_of(const DevScene& s) {
-  return TraceGeo{s.wnodes, s.nodes, s.tris, s.spheres, s.n_tris, s.n_spheres};
-}
+
 
 template <int W>
 __global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
@@ -1365,7 +1385,7 @@ __global__ void __launch_bounds__(kBlock, extend_blocks_per_sm<W>())
         o = f3(cur.o[i]);
         d = f3(cur.d[i]);
         tmax = __int_as_float(0x7f800000);
-        g = geo_of(c_insts[cur.inst[i]].s);
+        g.inst = cur.inst[i];
       },
       [&](uint32_t i, int prim, float tmax, float b1, float b2) {
         hits[i] = make_float4(tmax, b1, b2, __int_as_float(prim));
@@ -1400,7 +1420,7 @@ __global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_connect_b
         o = f3(a);
         d = f3(b);
         tmax = a.w;
-        g = geo_of(c_insts[cur.inst[__float_as_uint(b.w)]].s);
+        g.inst = cur.inst[__float_as_uint(b.w)];
       },
       [&](uint32_t j, int prim, float, float, float) {
         if (prim < 0) {
@@ -1417,7 +1437,7 @@ __global__ void __launch_bounds__(kBlock, shadow_blocks_per_sm<W>()) k_connect_b
         o = f3(q.mo[j]);
         d = f3(q.md[j]);
         tmax = __int_as_float(0x7f800000);
-        g = geo_of(c_insts[cur.inst[__float_as_uint(q.mc[j].w)]].s);
+        g.inst = cur.inst[__float_as_uint(q.mc[j].w)];
       },
       [&](uint32_t j, int prim, float, float b1, float b2) {
         const uint32_t slot = __float_as_uint(q.mc[j].w);
