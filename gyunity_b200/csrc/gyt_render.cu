@@ -537,8 +537,17 @@ GYT_D void persistent_trace(const DevScene& s, uint32_t* next, uint32_t n, Load 
         const bool fin = BATCH ? tv.template step<ANY, COUNT, CLS>(lg, rc, o, tmax, b1, b2, prim, &cnt)
                                : tv.template step<ANY, COUNT, CLS>(s, rc, o, tmax, b1, b2, prim, &cnt);
         if (fin) {
-          if (BATCH) trace_spheres<ANY>(lg, o, d, tmax, prim);
-          else trace_spheres<ANY>(s, o, d, tmax, prim);
+          if ((BATCH ? geo_nspheres(lg) : s.n_spheres) > 0) {
+            // the direction again from the ray's record (load only reads):
+            // the traversal needs the origin and the ray constants, so the
+            // lane does not keep the direction live through it
+            float3 o2, d2;
+            float t2;
+            TraceGeo g2;
+            load((uint32_t)ri, o2, d2, t2, g2);
+            if (BATCH) trace_spheres<ANY>(lg, o, d2, tmax, prim);
+            else trace_spheres<ANY>(s, o, d2, tmax, prim);
+          }
           done((uint32_t)ri, prim, tmax, b1, b2);
           ri = -1;
           break;
