@@ -67,6 +67,8 @@ def parse():
                          "uses the library default (binary, built on the GPU)")
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
     ap.add_argument("--batch-instances", type=int, default=64, help="instances of the uneven batch workload")
+    ap.add_argument("--batch-paths-in-flight", type=int, default=0,
+                    help="batch pool size instead of the autotuner's choice (small cases for ncu captures)")
     ap.add_argument("--paths-in-flight", type=int, default=1 << 24,
                     help="path pool of the single-scene, volume and adjoint contexts (the batch's is autotuned)")
     ap.add_argument("--no-single-scene", action="store_true",
@@ -542,6 +544,10 @@ def measure_batch(a, d, g, torch):
     t = time.perf_counter()
     cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=8)
     tune_s = time.perf_counter() - t
+    if a.batch_paths_in_flight:
+        cfg["paths_in_flight"] = a.batch_paths_in_flight
+        ctx.set_batch_config(cfg["paths_in_flight"], cfg["stride_blocks_per_sm"], cfg["trace_blocks_per_sm"],
+                             cfg["use_graph"])
     # both integrators render the scenes of the width the autotuner chose
     scs = scs8 if cfg["bvh_width"] == 8 else scs2
 
