@@ -631,6 +631,24 @@ GYT_D float tri_light_pdf(const LightTri& l, const Hit& h, float3 o, float3 wi) 
 }
 
 // -------------------------------------------------------------- kernels ---
+// Path p of a film (pixel after pixel, spp samples each): its pixel (x, y)
+// and sample s. Integer divisions, 32-bit while p fits (every film of fewer
+// than 2^32 samples), 64-bit beyond.
+GYT_D void path_coords(unsigned long long p, uint32_t spp, uint32_t res_x, uint32_t* x, uint32_t* y, uint32_t* s) {
+  if (p < (1ull << 32)) {
+    const uint32_t q = (uint32_t)p;
+    const uint32_t pixel = q / spp;
+    *s = q - pixel * spp;
+    *y = pixel / res_x;
+    *x = pixel - *y * res_x;
+  } else {
+    const unsigned long long pixel = p / spp;
+    *s = (uint32_t)(p - pixel * spp);
+    *y = (uint32_t)(pixel / res_x);
+    *x = (uint32_t)(pixel - (unsigned long long)*y * res_x);
+  }
+}
+
 // Camera path of sample s in pixel (x, y) into slot k (TiledIntegrator::Render
 // body, integrator/TiledIntegrator.cpp:37-48).
 GYT_D void gen_path(PathBuf& dst, uint32_t k, uint32_t x, uint32_t y, uint32_t s, const Cam& cam, SamplerTables tab) {
@@ -666,10 +684,7 @@ __global__ void __launch_bounds__(kBlock) k_generate(PathBuf dst, uint32_t base,
     y = __ldg(list + 3 * p + 1);
     s = __ldg(list + 3 * p + 2);
   } else {
-    unsigned long long pixel = p / spp;
-    s = (uint32_t)(p - pixel * spp);
-    y = (uint32_t)(pixel / cam.res_x);
-    x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+    path_coords(p, spp, cam.res_x, &x, &y, &s);
   }
   gen_path(dst, base + j, x, y, s, cam, tab);
   dst.pid[base + j] = (uint32_t)p;
@@ -1222,10 +1237,7 @@ __global__ void __launch_bounds__(kBlock) k_generate_adj(PathBuf dst, AdjBuf A, 
     y = __ldg(list + 3 * p + 1);
     s = __ldg(list + 3 * p + 2);
   } else {
-    const unsigned long long pixel = p / spp;
-    s = (uint32_t)(p - pixel * spp);
-    y = (uint32_t)(pixel / cam.res_x);
-    x = (uint32_t)(pixel - (unsigned long long)y * cam.res_x);
+    path_coords(p, spp, cam.res_x, &x, &y, &s);
   }
   const uint32_t k = base + j;
   gen_path(dst, k, x, y, s, cam, tab);
@@ -1371,11 +1383,8 @@ __global__ void __launch_bounds__(kBlock) k_generate_batch(PathBuf dst, const It
       if (c_insts[mid].first <= g) lo = mid; else hi = mid;
     }
     const Inst& I = c_insts[lo];
-    const unsigned long long p = g - I.first;
-    const unsigned long long pixel = p / I.prm.spp;
-    const uint32_t s = (uint32_t)(p - pixel * I.prm.spp);
-    const uint32_t y = (uint32_t)(pixel / I.cam.res_x);
-    const uint32_t x = (uint32_t)(pixel - (unsigned long long)y * I.cam.res_x);
+    uint32_t x, y, s;
+    path_coords(g - I.first, I.prm.spp, I.cam.res_x, &x, &y, &s);
     const Cam cam = I.cam;
     gen_path(dst, base + j, x, y, s, cam, tab);
     dst.inst[base + j] = lo;
