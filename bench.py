@@ -390,7 +390,7 @@ def run_ours(a):
 
 
 def bvh_label(width, builder):
-    return "8-wide, host-built" if width == 8 else "binary, %s-built" % builder
+    return "%s, %s-built" % ("8-wide" if width == 8 else "binary", builder)
 
 
 def measure_single(a, d, g, torch):
