@@ -67,6 +67,8 @@ def parse():
                          "uses the library default (binary, built on the GPU)")
     ap.add_argument("--bvh-builder", default="device", choices=["device", "host"])
     ap.add_argument("--batch-instances", type=int, default=64, help="instances of the uneven batch workload")
+    ap.add_argument("--batch-width", type=int, default=0, choices=[0, 2, 8],
+                    help="batch BVH width instead of the autotuner's choice between both (0)")
     ap.add_argument("--batch-paths-in-flight", type=int, default=0,
                     help="batch pool size instead of the autotuner's choice (small cases for ncu captures)")
     ap.add_argument("--paths-in-flight", type=int, default=1 << 24,
@@ -542,7 +544,10 @@ def measure_batch(a, d, g, torch):
     paths = sum(sd.n_paths() for sd in descs)
 
     t = time.perf_counter()
-    cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=8)
+    if a.batch_width:
+        cfg, tune_mp = ctx.batch_autotune(scs8 if a.batch_width == 8 else scs2, cams, prms, sample_spp=8)
+    else:
+        cfg, tune_mp = ctx.batch_autotune(scs2, cams, prms, scenes_alt=scs8, sample_spp=8)
     tune_s = time.perf_counter() - t
     if a.batch_paths_in_flight:
         cfg["paths_in_flight"] = a.batch_paths_in_flight
@@ -633,7 +638,7 @@ def measure_batch(a, d, g, torch):
                 "equal_rmse": {"max_rel_film_diff": fdiff,
                                "note": "same paths in both runs; only the order of the FP64 film sums differs"},
                 "autotune": {"config": cfg, "sample_mpaths": tune_mp, "seconds": tune_s,
-                             "widths_tried": [2, 8],
+                             "widths_tried": [a.batch_width] if a.batch_width else [2, 8],
                              "note": "coordinate search over BVH width (binary and 8-wide scenes, both built on "
                                      "the device), grid-stride and traversal blocks per SM on a sample of every "
                                      "instance at spp x 8 / 64 (the batch's mix), median of three renders per "
